@@ -1,0 +1,277 @@
+// ref_driver.cu -- TEST INFRASTRUCTURE. Drives the reference's OWN device
+// kernels (compiled from the reference sources by oracle/Makefile into
+// oracle/_ref/ref_driver) through the single-GPU sequence of the reference's
+// process_stream (algorithms/streamgc/src/streamgc.cu:809-1053) and
+// drain_and_compact (streamgc.cu:1243-1314), on a graph and update streams read
+// from a file, and dumps the device state at every epoch boundary.
+//
+//   --launch det   local_update_kernel<<<1, 32>>>: one warp walks each batch in
+//                  stream order (the deterministic reference run the golden
+//                  fixtures come from)
+//   --launch ref   the reference's own launch shape (streamgc.cu:847-853), timed
+//
+// The partition is built the way allocate_gpu_partition does it for one GPU
+// (streamgc.cu:144-444): identity hash map, max_owned = n + n/4, per-row
+// capacity max(d + d*SLACK/100, 8), base rows pre-populated, histogram rows for
+// degree > threshold, managed priority/snapshot/overflow counters.
+//
+// Input file (little endian): u32 n, u64 nnz, u32 hist_thr, u32 epoch_size,
+// u32 batch, u32 slack_pct, u64 n_init, u64 n_bench, u32 row_ptr[n+1],
+// u32 col[nnz], u32 degree[n], EdgeUpdate init[n_init], EdgeUpdate bench[n_bench].
+// Output: a sequence of records {char tag[16], u64 bytes, payload}.
+#include "streamgc.cuh"
+#include "color_select.cuh"
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+PartitionEntry* partition_map = nullptr;
+uint32_t partition_map_size = 0;
+
+__global__ void local_update_kernel(EdgeUpdate* updates, uint32_t num_updates, GPUPartition* partition, uint32_t histogram_threshold);
+__global__ void epoch_snapshot_kernel(GPUPartition* partition, uint32_t num_vertices_global);
+__global__ void compact_csr_kernel(GPUPartition* partition);
+__global__ void drain_overflow_local_kernel(GPUPartition* partition, uint32_t overflow_count, uint32_t* num_failed);
+__global__ void rebuild_bitmaps_kernel(GPUPartition* partition);
+
+static FILE* g_out = nullptr;
+
+static void rec(const char* tag, const void* p, uint64_t bytes) {
+    char t[16] = {0};
+    strncpy(t, tag, 15);
+    fwrite(t, 1, 16, g_out);
+    fwrite(&bytes, 8, 1, g_out);
+    if (bytes) fwrite(p, 1, bytes, g_out);
+}
+
+template <class T>
+static std::vector<T> d2h(const T* d, size_t count) {
+    std::vector<T> h(count);
+    if (count) CUDA_CHECK(cudaMemcpy(h.data(), d, count * sizeof(T), cudaMemcpyDeviceToHost));
+    return h;
+}
+
+struct Built {
+    GPUPartition h;
+    GPUPartition* d;
+    uint32_t total;
+};
+
+static Built build(uint32_t n, const std::vector<uint32_t>& rp, const std::vector<uint32_t>& col,
+                   const std::vector<uint32_t>& deg, uint32_t thr, uint32_t slack) {
+    GPUPartition h;
+    memset(&h, 0, sizeof(h));
+    const uint32_t max_owned = n + n / 4;
+    uint32_t map_size = 1;
+    while (map_size < n * 2) map_size <<= 1;
+    h.num_owned = n;
+    h.max_owned = max_owned;
+    h.max_ghost = 0;
+    h.index_map_size = map_size;
+    h.ghost_map_size = 4;
+    CUDA_CHECK(cudaMalloc(&h.owned, max_owned * sizeof(VertexState)));
+    CUDA_CHECK(cudaMemset(h.owned, 0, max_owned * sizeof(VertexState)));
+    CUDA_CHECK(cudaMalloc(&h.owned_to_global, max_owned * 4));
+    CUDA_CHECK(cudaMalloc(&h.ghost, 16));
+    CUDA_CHECK(cudaMemset(h.ghost, 0, 16));
+    CUDA_CHECK(cudaMalloc(&h.global_to_owned, map_size * 8));
+    CUDA_CHECK(cudaMalloc(&h.global_to_ghost, 4 * 8));
+    CUDA_CHECK(cudaMemset(h.global_to_ghost, 0xFF, 4 * 8));
+    CUDA_CHECK(cudaMalloc(&h.neighbor_bitmap, max_owned * 8));
+    CUDA_CHECK(cudaMemset(h.neighbor_bitmap, 0, max_owned * 8));
+    CUDA_CHECK(cudaMalloc(&h.high_degree_map, max_owned * 4));
+    std::vector<uint32_t> hd(max_owned, HASH_EMPTY);
+    uint32_t nhd = 0;
+    for (uint32_t i = 0; i < n; i++)
+        if (deg[i] > thr) hd[i] = nhd++;
+    h.num_high_degree = nhd;
+    CUDA_CHECK(cudaMemcpy(h.high_degree_map, hd.data(), max_owned * 4, cudaMemcpyHostToDevice));
+    if (nhd) {
+        CUDA_CHECK(cudaMalloc(&h.freq_histogram, (size_t)nhd * MAX_HISTOGRAM_COLORS * 4));
+        CUDA_CHECK(cudaMemset(h.freq_histogram, 0, (size_t)nhd * MAX_HISTOGRAM_COLORS * 4));
+    }
+    CUDA_CHECK(cudaMallocManaged(&h.init_priority, (size_t)n * 8));
+    for (uint32_t v = 0; v < n; v++) h.init_priority[v] = compute_priority(deg[v], v);
+    CUDA_CHECK(cudaMallocManaged(&h.epoch_snapshot, (size_t)n * 2));
+    memset(h.epoch_snapshot, 0, (size_t)n * 2);
+    std::vector<uint32_t> lrp(max_owned + 1, 0);
+    for (uint32_t i = 0; i < n; i++) {
+        const uint32_t cnt = rp[i + 1] - rp[i];
+        const uint32_t cap = std::max(cnt + (cnt * slack) / 100, (uint32_t)8);
+        lrp[i + 1] = lrp[i] + cap;
+    }
+    const uint32_t total = lrp[n];
+    std::vector<uint32_t> lcol(total, CSR_INVALID);
+    for (uint32_t i = 0; i < n; i++)
+        for (uint32_t j = rp[i]; j < rp[i + 1]; j++) lcol[lrp[i] + (j - rp[i])] = col[j];
+    CUDA_CHECK(cudaMalloc(&h.row_ptr, (max_owned + 1) * 4));
+    CUDA_CHECK(cudaMemset(h.row_ptr, 0, (max_owned + 1) * 4));
+    CUDA_CHECK(cudaMemcpy(h.row_ptr, lrp.data(), (n + 1) * 4, cudaMemcpyHostToDevice));
+    CUDA_CHECK(cudaMalloc(&h.col_idx, (size_t)total * 4 + 16));
+    CUDA_CHECK(cudaMemcpy(h.col_idx, lcol.data(), (size_t)total * 4, cudaMemcpyHostToDevice));
+    CUDA_CHECK(cudaMalloc(&h.ghost_row_ptr, (max_owned + 1) * 4));
+    CUDA_CHECK(cudaMemset(h.ghost_row_ptr, 0, (max_owned + 1) * 4));
+    CUDA_CHECK(cudaMalloc(&h.ghost_col_idx, 16));
+    CUDA_CHECK(cudaMemset(h.ghost_col_idx, 0xFF, 16));
+    CUDA_CHECK(cudaMalloc(&h.overflow_local, OVERFLOW_CAPACITY * sizeof(OverflowEdge)));
+    CUDA_CHECK(cudaMallocManaged(&h.overflow_local_count, 4));
+    CUDA_CHECK(cudaMallocManaged(&h.overflow_ghost_count, 4));
+    *h.overflow_local_count = 0;
+    *h.overflow_ghost_count = 0;
+    std::vector<uint32_t> o2g(n), hash(map_size * 2, HASH_EMPTY);
+    for (uint32_t i = 0; i < n; i++) {
+        o2g[i] = i;
+        hash_insert_host(hash.data(), map_size, i, i);
+    }
+    CUDA_CHECK(cudaMemcpy(h.owned_to_global, o2g.data(), n * 4, cudaMemcpyHostToDevice));
+    CUDA_CHECK(cudaMemcpy(h.global_to_owned, hash.data(), map_size * 8, cudaMemcpyHostToDevice));
+    Built b;
+    b.h = h;
+    b.total = total;
+    CUDA_CHECK(cudaMalloc(&b.d, sizeof(GPUPartition)));
+    CUDA_CHECK(cudaMemcpy(b.d, &h, sizeof(GPUPartition), cudaMemcpyHostToDevice));
+    return b;
+}
+
+static void dump(const Built& b, uint32_t n, const char* tag) {
+    char t[64];
+    auto st = d2h(reinterpret_cast<const uint32_t*>(b.h.owned), n);
+    auto bm = d2h(b.h.neighbor_bitmap, n);
+    auto col = d2h(b.h.col_idx, b.total);
+    std::vector<uint16_t> snap(b.h.epoch_snapshot, b.h.epoch_snapshot + n);
+    auto hist = d2h(b.h.freq_histogram, (size_t)b.h.num_high_degree * MAX_HISTOGRAM_COLORS);
+    const uint32_t ovf = *b.h.overflow_local_count;
+    snprintf(t, sizeof(t), "%s", tag);
+    rec(t, nullptr, 0);
+    rec("states", st.data(), st.size() * 4);
+    rec("bitmaps", bm.data(), bm.size() * 8);
+    rec("col", col.data(), col.size() * 4);
+    rec("snapshot", snap.data(), snap.size() * 2);
+    rec("hist", hist.data(), hist.size() * 4);
+    rec("ovf_count", &ovf, 4);
+}
+
+int main(int argc, char** argv) {
+    const char* in = nullptr;
+    const char* out = nullptr;
+    bool det = true;
+    for (int i = 1; i < argc; i++) {
+        if (!strcmp(argv[i], "--in") && i + 1 < argc) in = argv[++i];
+        else if (!strcmp(argv[i], "--out") && i + 1 < argc) out = argv[++i];
+        else if (!strcmp(argv[i], "--launch") && i + 1 < argc) det = strcmp(argv[++i], "ref") != 0;
+    }
+    if (!in || !out) {
+        fprintf(stderr, "usage: %s --in <case.bin> --out <dump.bin> [--launch det|ref]\n", argv[0]);
+        return 2;
+    }
+    FILE* f = fopen(in, "rb");
+    if (!f) { fprintf(stderr, "cannot open %s\n", in); return 2; }
+    uint32_t n, thr, E, batch, slack;
+    uint64_t nnz, ni, nb;
+    bool ok = fread(&n, 4, 1, f) == 1 && fread(&nnz, 8, 1, f) == 1 && fread(&thr, 4, 1, f) == 1 &&
+              fread(&E, 4, 1, f) == 1 && fread(&batch, 4, 1, f) == 1 && fread(&slack, 4, 1, f) == 1 &&
+              fread(&ni, 8, 1, f) == 1 && fread(&nb, 8, 1, f) == 1;
+    std::vector<uint32_t> rp(n + 1), col(nnz), deg(n);
+    std::vector<EdgeUpdate> init(ni), bench(nb);
+    ok = ok && fread(rp.data(), 4, n + 1, f) == n + 1 && fread(col.data(), 4, nnz, f) == nnz &&
+         fread(deg.data(), 4, n, f) == n && fread(init.data(), 16, ni, f) == ni && fread(bench.data(), 16, nb, f) == nb;
+    fclose(f);
+    if (!ok) { fprintf(stderr, "short input\n"); return 2; }
+    g_out = fopen(out, "wb");
+    CUDA_CHECK(cudaSetDevice(0));
+    Built b = build(n, rp, col, deg, thr, slack);
+    EdgeUpdate* d_up;
+    CUDA_CHECK(cudaMalloc(&d_up, (size_t)batch * sizeof(EdgeUpdate)));
+    int epoch_no = 0;
+    // Deterministic runs drain entry by entry in buffer order: the reference
+    // kernel is launched once per entry on a partition copy whose overflow
+    // pointer is advanced to that entry (its thread 0 then drains it).
+    GPUPartition* d_one = nullptr;
+    CUDA_CHECK(cudaMalloc(&d_one, sizeof(GPUPartition)));
+    auto drain = [&](uint32_t c) {
+        if (!det) {
+            drain_overflow_local_kernel<<<(c + 255) / 256, 256>>>(b.d, c, nullptr);
+            return;
+        }
+        for (uint32_t k = 0; k < c; k++) {
+            GPUPartition one = b.h;
+            one.overflow_local = b.h.overflow_local + k;
+            CUDA_CHECK(cudaMemcpy(d_one, &one, sizeof(GPUPartition), cudaMemcpyHostToDevice));
+            drain_overflow_local_kernel<<<1, 1>>>(d_one, 1, nullptr);
+            CUDA_CHECK(cudaDeviceSynchronize());
+        }
+    };
+    auto epoch = [&]() {
+        const int blk = (n + 255) / 256;
+        epoch_snapshot_kernel<<<blk, 256>>>(b.d, n);
+        compact_csr_kernel<<<blk, 256>>>(b.d);
+        CUDA_CHECK(cudaDeviceSynchronize());
+        const uint32_t lo = *b.h.overflow_local_count;
+        if (lo > 0) {
+            *b.h.overflow_local_count = 0;
+            drain(std::min(lo, OVERFLOW_CAPACITY));
+        }
+        CUDA_CHECK(cudaDeviceSynchronize());
+        rebuild_bitmaps_kernel<<<blk, 256>>>(b.d);
+        CUDA_CHECK(cudaDeviceSynchronize());
+    };
+    auto process = [&](const std::vector<EdgeUpdate>& ups, const char* phase) -> double {
+        uint64_t processed = 0, since = 0;
+        auto t0 = std::chrono::high_resolution_clock::now();
+        while (processed < ups.size()) {
+            const uint32_t c = (uint32_t)std::min<uint64_t>(batch, ups.size() - processed);
+            CUDA_CHECK(cudaMemcpy(d_up, ups.data() + processed, (size_t)c * 16, cudaMemcpyHostToDevice));
+            if (det) {
+                local_update_kernel<<<1, 32>>>(d_up, c, b.d, thr);
+            } else {
+                const int threads = std::min<int>(c * 32, 256);
+                const int blocks = std::max<int>((c * 32 + threads - 1) / threads, 1);
+                local_update_kernel<<<blocks, threads>>>(d_up, c, b.d, thr);
+            }
+            CUDA_CHECK(cudaDeviceSynchronize());
+            processed += c;
+            since += c;
+            if (since >= E) {
+                epoch();
+                since = 0;
+                if (det) {
+                    char t[32];
+                    snprintf(t, sizeof(t), "%s_e%d", phase, epoch_no);
+                    dump(b, n, t);
+                }
+                epoch_no++;
+            }
+        }
+        return std::chrono::duration<double, std::milli>(std::chrono::high_resolution_clock::now() - t0).count();
+    };
+    auto drain_and_compact = [&](const char* tag) {
+        const int blk = (n + 255) / 256;
+        compact_csr_kernel<<<blk, 256>>>(b.d);
+        CUDA_CHECK(cudaDeviceSynchronize());
+        const uint32_t lo = *b.h.overflow_local_count;
+        if (lo > 0) {
+            *b.h.overflow_local_count = 0;
+            drain(std::min(lo, OVERFLOW_CAPACITY));
+        }
+        CUDA_CHECK(cudaDeviceSynchronize());
+        rebuild_bitmaps_kernel<<<blk, 256>>>(b.d);
+        CUDA_CHECK(cudaDeviceSynchronize());
+        dump(b, n, tag);
+    };
+    const double init_ms = process(init, "init");
+    drain_and_compact("init_dc");
+    const double bench_ms = process(bench, "bench");
+    drain_and_compact("bench_dc");
+    double mups = bench_ms > 0 ? nb / bench_ms / 1000.0 : 0.0;
+    rec("timing", nullptr, 0);
+    double tm[3] = {init_ms, bench_ms, mups};
+    rec("ms", tm, sizeof(tm));
+    fclose(g_out);
+    printf("ref_driver: n=%u init %.2f ms, bench %.2f ms (%.3f M updates/s), launch=%s, epochs=%d\n", n, init_ms,
+           bench_ms, mups, det ? "det" : "ref", epoch_no);
+    return 0;
+}

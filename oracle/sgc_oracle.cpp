@@ -1,0 +1,883 @@
+// sgc_oracle.cpp -- CPU ORACLE for the StreamGC single-GPU coloring path.
+//
+// TEST INFRASTRUCTURE ONLY. This file is the checker: tests/, the smoke entry
+// point and the bench's cpu_baseline leg may load it; the product library never
+// does. It restates, in plain sequential C++17 (+OpenMP where the step is
+// order-independent), what the reference computes on one GPU:
+//
+//   update rules       algorithms/streamgc/src/kernels/local_update.cu:12-147
+//   recolor            algorithms/streamgc/src/kernels/recolor.cu:49-163
+//   color selection    algorithms/streamgc/include/color_select.cuh:10-115
+//   bitmap/histogram   algorithms/streamgc/include/color_select.cuh:120-251
+//   epoch maintenance  algorithms/streamgc/src/kernels/epoch_maintenance.cu:5-128,
+//                      driver algorithms/streamgc/src/streamgc.cu:949-1036
+//   drain_and_compact  algorithms/streamgc/src/streamgc.cu:1243-1314
+//   Tier-1 repair      algorithms/streamgc/src/kernels/conflict_repair.cu:10-114,
+//                      loop algorithms/streamgc/src/streamgc.cu:1317-1393
+//   Tier-2 repair      algorithms/streamgc/src/streamgc.cu:1057-1240
+//   slack CSR build    algorithms/streamgc/src/streamgc.cu:350-433
+//   validator          algorithms/streamgc/src/streamgc.cu:448-556
+//   static greedy      algorithms/streamgc/src/streamgc.cu:559-592
+//   stream generators  algorithms/streamgc/src/host/stream_gen.cpp:30-177
+//   graph loader       algorithms/streamgc/src/host/graph_loader.cpp:29-169
+//
+// Deterministic choices where the reference GPU code is racy (documented):
+//  * updates are applied strictly in stream order (the reference run with
+//    local_update_kernel launched as a single warp);
+//  * overflow drain re-inserts entries in buffer order;
+//  * Tier-1 is a Jacobi sweep: every vertex decides on the colors as they were
+//    at the start of the sweep (the reference thread-per-vertex kernel reads a
+//    racy mix; its bitmaps are rebuilt before the sweep, which Jacobi keeps).
+//
+// Algorithmic byte counters count every array element each step touches
+// (read + write for read-modify-write), at element granularity.
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <random>
+#include <string>
+#include <unordered_set>
+#include <utility>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/streamgc_types.h"
+
+namespace {
+
+constexpr uint32_t INV = SGC_CSR_INVALID;
+constexpr uint32_t EMPTY = SGC_HASH_EMPTY;
+constexpr uint32_t OVF_CAP = SGC_OVERFLOW_CAPACITY;
+
+struct Bytes {
+    uint64_t update = 0;   // local update path
+    uint64_t epoch = 0;    // snapshot + compact + drain + rebuild
+    uint64_t tier1 = 0;    // tier-1 sweeps (rebuild + detect)
+    uint64_t tier2 = 0;
+};
+
+struct Oracle {
+    uint32_t n = 0;
+    uint32_t hist_thr = 64;
+    uint32_t maxc = 1024;          // MAX_HISTOGRAM_COLORS
+    std::vector<uint64_t> rp;      // logical row starts, rp[n] = total slots
+    std::vector<uint32_t> col;     // slack CSR slots
+    std::vector<uint32_t> st;      // packed (color | version << 16)
+    std::vector<uint64_t> bm;      // neighbor bitmaps
+    std::vector<uint32_t> hdmap;   // vertex -> histogram row or EMPTY
+    std::vector<uint32_t> hist;    // num_hd * maxc
+    uint32_t num_hd = 0;
+    std::vector<uint32_t> deg;     // frozen init degree (priority = deg<<32 | id)
+    std::vector<uint8_t> edited;   // row changed since creation; else its base run is sorted, hole-free
+    std::vector<uint32_t> base_len;
+    std::vector<uint16_t> snap;    // published snapshot
+    std::vector<OverflowEdge> ovf; // OVF_CAP entries
+    uint32_t ovf_count = 0;        // may exceed OVF_CAP (reference counts every overflow)
+    uint64_t ovf_lost = 0;         // entries dropped because pos >= OVF_CAP
+    uint64_t drain_failed = 0;
+    uint64_t recolors = 0;
+    uint64_t updates_applied = 0;
+    uint64_t skipped_updates = 0;
+    Bytes bytes;
+    std::string err;
+
+    // -------- state helpers (vertex_state.cuh:17-27, priority.cuh:8-10) --------
+    inline uint16_t color(uint32_t x) const { return (uint16_t)(st[x] & 0xFFFFu); }
+    inline uint16_t ver(uint32_t x) const { return (uint16_t)(st[x] >> 16); }
+    inline uint64_t prio(uint32_t x) const { return ((uint64_t)deg[x] << 32) | x; }
+    inline uint32_t* hrow(uint32_t x) {
+        uint32_t h = hdmap[x];
+        return h == EMPTY ? nullptr : &hist[(uint64_t)h * maxc];
+    }
+
+    // -------- color selection (color_select.cuh:10-115) --------
+    // `cols` is the color source for the >64 fallback scan: live state in the
+    // update path, the start-of-sweep copy in the Jacobi Tier-1 sweep.
+    uint16_t fac_bitmap(uint32_t x, const std::vector<uint32_t>& cols, uint64_t& b) const {
+        uint64_t bmv = bm[x];
+        b += 8;
+        if (~bmv != 0) return (uint16_t)(__builtin_ctzll(~bmv) + 1);
+        bool used[256];
+        std::memset(used, 0, sizeof(used));
+        for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+            uint32_t ng = col[j];
+            b += 4;
+            if (ng == INV) continue;
+            if (ng >= n) continue;                 // not an owned vertex: hash miss
+            uint16_t c = (uint16_t)(cols[ng] & 0xFFFFu);
+            b += 4;
+            if (c > 0 && c < 256) used[c] = true;
+        }
+        for (uint16_t c = 1; c < 256; c++)
+            if (!used[c]) return c;
+        return 256;
+    }
+    uint16_t fac_hist(uint32_t x, uint64_t& b) const {
+        const uint32_t* h = &hist[(uint64_t)hdmap[x] * maxc];
+        for (uint32_t c = 0; c < maxc; c++) {
+            b += 4;
+            if (h[c] == 0) return (uint16_t)(c + 1);
+        }
+        uint32_t mn = h[0], mc = 0;
+        for (uint32_t c = 1; c < maxc; c++) {
+            b += 4;
+            if (h[c] < mn) { mn = h[c]; mc = c; }
+        }
+        return (uint16_t)(mc + 1);
+    }
+    uint16_t fac(uint32_t x, const std::vector<uint32_t>& cols, uint64_t& b) const {
+        b += 4;  // high_degree_map read
+        if (hdmap[x] != EMPTY) return fac_hist(x, b);
+        return fac_bitmap(x, cols, b);
+    }
+
+    // -------- incremental bitmap/histogram maintenance (color_select.cuh:120-209) --------
+    void nbr_color_change(uint32_t x, uint16_t oldc, uint16_t newc, uint64_t& b) {
+        if (oldc == newc) return;
+        if (oldc == 0 && newc == 0) return;
+        if (newc != 0 && newc <= 64) { bm[x] |= 1ull << (newc - 1); b += 16; }
+        b += 4;
+        uint32_t* h = hrow(x);
+        if (h) {
+            if (oldc != 0 && oldc <= maxc) { h[oldc - 1] -= 1u; b += 8; }
+            if (newc != 0 && newc <= maxc) { h[newc - 1] += 1u; b += 8; }
+        }
+    }
+    void new_nbr(uint32_t x, uint16_t c, uint64_t& b) {
+        if (c == 0) return;
+        if (c <= 64) { bm[x] |= 1ull << (c - 1); b += 16; }
+        b += 4;
+        uint32_t* h = hrow(x);
+        if (h && c <= maxc) { h[c - 1] += 1u; b += 8; }
+    }
+    void removed_nbr(uint32_t x, uint16_t c, uint64_t& b) {
+        if (c == 0) return;
+        b += 4;
+        uint32_t* h = hrow(x);
+        if (h && c <= maxc) { h[c - 1] -= 1u; b += 8; }
+    }
+
+    // Binary search of an unedited row's sorted base run; ~0 when absent.
+    // Gives the slot the reference's linear scan stops at: the run holds no INV
+    // and no duplicate, and only INV follows it.
+    uint64_t pristine_find(uint32_t x, uint32_t nbr, uint64_t& b) const {
+        uint64_t lo = rp[x], hi = rp[x] + base_len[x];
+        while (lo < hi) {
+            const uint64_t m = lo + (hi - lo) / 2;
+            b += 4;
+            if (col[m] < nbr) lo = m + 1;
+            else hi = m;
+        }
+        if (lo < rp[x] + base_len[x] && col[lo] == nbr) return lo;
+        return ~0ull;
+    }
+
+    // -------- slack CSR row edits (local_update.cu:12-56) --------
+    void add_slot(uint32_t x, uint32_t nbr, uint64_t& b) {
+        uint64_t from = rp[x];
+        if (!edited[x]) {
+            if (pristine_find(x, nbr, b) != ~0ull) return;
+            from = rp[x] + base_len[x];
+        }
+        for (uint64_t j = from; j < rp[x + 1]; j++) {
+            uint32_t s = col[j];
+            b += 4;
+            if (s == INV) { col[j] = nbr; b += 4; edited[x] = 1; return; }
+            if (s == nbr) return;
+        }
+        uint32_t pos = ovf_count++;
+        if (pos < OVF_CAP) { ovf[pos].local_vertex_idx = x; ovf[pos].neighbor_global = nbr; b += 8; }
+        else ovf_lost++;
+    }
+    void remove_slot(uint32_t x, uint32_t nbr, uint64_t& b) {
+        if (!edited[x]) {
+            const uint64_t p = pristine_find(x, nbr, b);
+            if (p != ~0ull) { col[p] = INV; b += 4; edited[x] = 1; }
+            return;
+        }
+        for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+            b += 4;
+            if (col[j] == nbr) { col[j] = INV; b += 4; return; }
+        }
+    }
+
+    // -------- recolor (recolor.cu:49-163) --------
+    void recolor(uint32_t x, uint64_t& b) {
+        uint16_t oldc = color(x);
+        uint16_t newc = fac(x, st, b);
+        b += 4;
+        if (newc == oldc) return;
+        uint16_t nv = (uint16_t)(ver(x) + 1);
+        st[x] = sgc_pack_state(newc, nv);
+        b += 4;
+        recolors++;
+        // update_incremental_state: every live row entry, duplicates included.
+        for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+            uint32_t ng = col[j];
+            b += 4;
+            if (ng == INV || ng >= n) continue;
+            nbr_color_change(ng, oldc, newc, b);
+        }
+    }
+    void try_reduce(uint32_t x, uint16_t freed, uint64_t& b) {
+        uint16_t cur = color(x);
+        b += 4;
+        if (cur == 0) return;
+        if (freed >= cur) return;
+        uint16_t best = fac(x, st, b);
+        if (best < cur) recolor(x, b);
+    }
+
+    // -------- one update (local_update.cu:61-147), stream order --------
+    void apply_one(const EdgeUpdate& e) {
+        uint64_t& b = bytes.update;
+        b += 16;
+        uint32_t u = e.u, v = e.v;
+        if (u >= n || v >= n) { skipped_updates++; return; }  // hash miss -> continue
+        updates_applied++;
+        if (e.type == SGC_UPDATE_ADD) {
+            add_slot(u, v, b);
+            add_slot(v, u, b);
+            b += 4;
+            if (color(u) == 0) {
+                uint16_t c = fac(u, st, b);
+                st[u] = sgc_pack_state(c, 1);
+                b += 4;
+            }
+            b += 4;
+            if (color(v) == 0) {
+                new_nbr(v, color(u), b);
+                uint16_t c = fac(v, st, b);
+                st[v] = sgc_pack_state(c, 1);
+                b += 4;
+            }
+            new_nbr(u, color(v), b);
+            new_nbr(v, color(u), b);
+            if (color(u) == color(v) && color(u) != 0) {
+                b += 16;
+                uint32_t loser = (prio(u) < prio(v)) ? u : v;
+                recolor(loser, b);
+            }
+        } else if (e.type == SGC_UPDATE_DEL) {
+            uint16_t fu = color(v);
+            uint16_t fv = color(u);
+            b += 8;
+            remove_slot(u, v, b);
+            remove_slot(v, u, b);
+            removed_nbr(u, fu, b);
+            removed_nbr(v, fv, b);
+            try_reduce(u, fu, b);
+            try_reduce(v, fv, b);
+        }
+    }
+
+    // -------- epoch steps (epoch_maintenance.cu:5-128) --------
+    void snapshot() {
+        for (uint32_t x = 0; x < n; x++) snap[x] = color(x);
+        bytes.epoch += (uint64_t)n * 6;
+    }
+    void compact_all() {
+        uint64_t b = 0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : b)
+        for (int64_t xi = 0; xi < (int64_t)n; xi++) {
+            uint32_t x = (uint32_t)xi;
+            uint64_t w = rp[x];
+            for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                b += 4;
+                if (col[j] != INV) {
+                    if (w != j) { col[w] = col[j]; b += 4; }
+                    w++;
+                }
+            }
+            for (uint64_t j = w; j < rp[x + 1]; j++) { col[j] = INV; b += 4; }
+        }
+        bytes.epoch += b;
+    }
+    // drain_overflow_local_kernel, entries in buffer order; returns failures.
+    uint64_t drain(uint32_t cnt) {
+        uint64_t failed = 0;
+        for (uint32_t i = 0; i < cnt; i++) {
+            uint32_t x = ovf[i].local_vertex_idx, nb = ovf[i].neighbor_global;
+            bool done = false;
+            for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                bytes.epoch += 4;
+                uint32_t s = col[j];
+                if (s == INV) { col[j] = nb; done = true; edited[x] = 1; break; }
+                if (s == nb) { done = true; break; }
+            }
+            if (!done) failed++;
+        }
+        drain_failed += failed;
+        return failed;
+    }
+    uint64_t rebuild_one(uint32_t x, const std::vector<uint32_t>& cols, uint64_t& b) {
+        uint64_t m = 0;
+        for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+            uint32_t ng = col[j];
+            b += 4;
+            if (ng == INV || ng >= n) continue;
+            uint16_t c = (uint16_t)(cols[ng] & 0xFFFFu);
+            b += 4;
+            if (c != 0 && c <= 64) m |= 1ull << (c - 1);
+        }
+        return m;
+    }
+    void rebuild_all(uint64_t& bsum) {
+        uint64_t b = 0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : b)
+        for (int64_t xi = 0; xi < (int64_t)n; xi++) {
+            uint32_t x = (uint32_t)xi;
+            b += 4;
+            if (hdmap[x] != EMPTY) continue;
+            bm[x] = rebuild_one(x, st, b);
+            b += 8;
+        }
+        bsum += b;
+    }
+    // Reads the overflow count, resets it, drains (streamgc.cu:967-995).
+    uint64_t drain_pending() {
+        uint32_t cnt = ovf_count;
+        if (cnt == 0) return 0;
+        ovf_count = 0;
+        return drain(std::min(cnt, OVF_CAP));
+    }
+    // Reference epoch: snapshot, compact, drain, rebuild (streamgc.cu:949-1012).
+    void epoch() {
+        snapshot();
+        compact_all();
+        drain_pending();
+        rebuild_all(bytes.epoch);
+    }
+    // drain_and_compact (streamgc.cu:1243-1314).
+    uint64_t drain_and_compact() {
+        compact_all();
+        uint64_t f = drain_pending();
+        rebuild_all(bytes.epoch);
+        return f;
+    }
+
+    // -------- Tier-1 (conflict_repair.cu:10-114), Jacobi sweep --------
+    uint32_t tier1_sweep() {
+        std::vector<uint32_t> old = st;  // colors every decision reads
+        uint32_t count = 0;
+        uint64_t b = 0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : count, b)
+        for (int64_t xi = 0; xi < (int64_t)n; xi++) {
+            uint32_t x = (uint32_t)xi;
+            uint16_t my = (uint16_t)(old[x] & 0xFFFFu);
+            uint16_t myver = (uint16_t)(old[x] >> 16);
+            b += 4 + 16;
+            bool has = false;
+            for (uint64_t j = rp[x]; j < rp[x + 1] && !has; j++) {
+                b += 4;
+                if (col[j] != INV) has = true;
+            }
+            if (my == 0) {
+                if (has) {
+                    uint16_t c = fac(x, old, b);
+                    st[x] = sgc_pack_state(c, (uint16_t)(myver + 1));
+                    b += 4;
+                    count++;
+                }
+                continue;
+            }
+            uint64_t myp = prio(x);
+            b += 4;
+            bool need = false;
+            for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                uint32_t ng = col[j];
+                b += 4;
+                if (ng == INV || ng >= n) continue;
+                uint16_t nc = (uint16_t)(old[ng] & 0xFFFFu);
+                b += 4;
+                if (nc == my && nc != 0) {
+                    b += 4;
+                    if (myp < prio(ng)) { need = true; break; }
+                }
+            }
+            if (need) {
+                count++;
+                if (my <= 64) { bm[x] |= 1ull << (my - 1); b += 16; }
+                uint16_t c = fac(x, old, b);
+                st[x] = sgc_pack_state(c, (uint16_t)(myver + 1));
+                b += 4;
+            }
+        }
+        bytes.tier1 += b;
+        return count;
+    }
+    // run_conflict_repair loop (streamgc.cu:1317-1393). Returns iterations run;
+    // *last_count = conflicts counted by the last sweep.
+    int tier1(uint32_t* history, int hist_cap, uint32_t* last_count) {
+        uint32_t prev = UINT32_MAX;
+        int plateau = 0;
+        uint32_t cnt = 0;
+        for (int it = 0; it < 20; it++) {
+            rebuild_all(bytes.tier1);
+            cnt = tier1_sweep();
+            if (history && it < hist_cap) history[it] = cnt;
+            if (cnt == 0) { if (last_count) *last_count = 0; return it + 1; }
+            if (cnt == prev) {
+                plateau++;
+                if (plateau >= 3) { if (last_count) *last_count = cnt; return it + 1; }
+            } else {
+                plateau = 0;
+            }
+            prev = cnt;
+        }
+        if (last_count) *last_count = cnt;
+        return 20;
+    }
+
+    // -------- Tier-2 (streamgc.cu:1057-1240) --------
+    uint32_t tier2() {
+        std::vector<std::vector<uint32_t>> adj(n);
+        {
+            std::vector<uint32_t> d(n, 0);
+            for (uint32_t x = 0; x < n; x++)
+                for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                    uint32_t y = col[j];
+                    if (y != INV && y < n && y != x) { d[x]++; d[y]++; }
+                }
+            for (uint32_t x = 0; x < n; x++) if (d[x]) adj[x].reserve(d[x]);
+            for (uint32_t x = 0; x < n; x++)
+                for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                    uint32_t y = col[j];
+                    bytes.tier2 += 4;
+                    if (y == INV || y >= n || y == x) continue;
+                    adj[x].push_back(y);
+                    adj[y].push_back(x);
+                }
+        }
+        auto greedy = [&](uint32_t v) -> bool {
+            bool used[1024];
+            std::memset(used, 0, sizeof(used));
+            for (uint32_t w : adj[v]) {
+                uint16_t nc = color(w);
+                bytes.tier2 += 4;
+                if (nc != 0 && nc < 1024) used[nc] = true;
+            }
+            for (uint16_t c = 1; c < 1024; c++) {
+                if (!used[c]) {
+                    if (color(v) != c) {
+                        st[v] = sgc_pack_state(c, (uint16_t)(ver(v) + 1));
+                        bytes.tier2 += 4;
+                        return true;
+                    }
+                    return false;
+                }
+            }
+            return false;
+        };
+        uint32_t total = 0;
+        for (uint32_t u = 0; u < n; u++) {
+            if (color(u) != 0 || adj[u].empty()) continue;
+            if (greedy(u)) total++;
+        }
+        for (int pass = 0; pass < 30; pass++) {
+            std::vector<uint32_t> fix;
+            for (uint32_t u = 0; u < n; u++)
+                for (uint32_t v : adj[u]) {
+                    if (v <= u) continue;
+                    if (color(u) == color(v) && color(u) != 0) fix.push_back(v);
+                }
+            if (fix.empty()) break;
+            std::sort(fix.begin(), fix.end());
+            fix.erase(std::unique(fix.begin(), fix.end()), fix.end());
+            uint32_t fixed = 0;
+            for (uint32_t v : fix) if (greedy(v)) fixed++;
+            total += fixed;
+            if (fixed == 0) break;
+        }
+        return total;
+    }
+};
+
+// ---------------- stream generators (stream_gen.cpp) ----------------
+struct PairHash {
+    size_t operator()(const std::pair<uint32_t, uint32_t>& p) const {
+        return std::hash<uint64_t>()((uint64_t)p.first << 32 | p.second);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+// ---------------- lifecycle ----------------
+
+// Builds the single-GPU slack CSR exactly as allocate_gpu_partition
+// (streamgc.cu:350-433): cap = max(d + d*slack/100, 8), base edges first in
+// loader order, the rest INVALID. High-degree rows: degree > threshold
+// (streamgc.cu:225-250), histogram row index in vertex order.
+void* og_create(uint32_t n, const uint64_t* row_ptr, const uint32_t* col_idx, const uint32_t* degree,
+                uint32_t hist_thr, uint32_t slack_pct, uint32_t max_hist_colors) {
+    Oracle* g = new Oracle();
+    g->n = n;
+    g->hist_thr = hist_thr;
+    g->maxc = max_hist_colors ? max_hist_colors : SGC_MAX_HISTOGRAM_COLORS_DEFAULT;
+    g->rp.assign((size_t)n + 1, 0);
+    for (uint32_t x = 0; x < n; x++) {
+        uint32_t cnt = (uint32_t)(row_ptr[x + 1] - row_ptr[x]);
+        uint32_t extra = (uint32_t)(((uint64_t)cnt * slack_pct) / 100);
+        uint32_t cap = std::max<uint32_t>(cnt + extra, 8u);
+        g->rp[x + 1] = g->rp[x] + cap;
+    }
+    g->col.assign(g->rp[n], INV);
+    for (uint32_t x = 0; x < n; x++) {
+        uint64_t p = g->rp[x];
+        for (uint64_t j = row_ptr[x]; j < row_ptr[x + 1]; j++) g->col[p++] = col_idx[j];
+    }
+    g->st.assign(n, 0);
+    g->bm.assign(n, 0);
+    g->edited.assign(n, 0);
+    g->base_len.resize(n);
+    for (uint32_t x = 0; x < n; x++) {
+        g->base_len[x] = (uint32_t)(row_ptr[x + 1] - row_ptr[x]);
+        for (uint64_t j = row_ptr[x] + 1; j < row_ptr[x + 1]; j++)
+            if (col_idx[j - 1] >= col_idx[j]) { g->edited[x] = 1; break; }  // not strictly ascending: scan it
+    }
+    g->deg.assign(degree, degree + n);
+    g->hdmap.assign(n, EMPTY);
+    for (uint32_t x = 0; x < n; x++)
+        if (degree[x] > hist_thr) g->hdmap[x] = g->num_hd++;
+    g->hist.assign((size_t)g->num_hd * g->maxc, 0);
+    g->snap.assign(n, 0);
+    g->ovf.resize(OVF_CAP);
+    return g;
+}
+
+void og_destroy(void* h) { delete (Oracle*)h; }
+
+uint32_t og_num_vertices(void* h) { return ((Oracle*)h)->n; }
+uint64_t og_total_slots(void* h) { return ((Oracle*)h)->rp.back(); }
+uint32_t og_num_high_degree(void* h) { return ((Oracle*)h)->num_hd; }
+uint32_t og_max_hist_colors(void* h) { return ((Oracle*)h)->maxc; }
+
+// ---------------- updates and epochs ----------------
+
+void og_apply(void* h, const EdgeUpdate* ups, uint64_t n) {
+    Oracle* g = (Oracle*)h;
+    for (uint64_t i = 0; i < n; i++) g->apply_one(ups[i]);
+}
+void og_epoch(void* h) { ((Oracle*)h)->epoch(); }
+uint64_t og_drain_and_compact(void* h) { return ((Oracle*)h)->drain_and_compact(); }
+void og_snapshot(void* h) { ((Oracle*)h)->snapshot(); }
+void og_compact(void* h) { ((Oracle*)h)->compact_all(); }
+uint64_t og_drain_pending(void* h) { return ((Oracle*)h)->drain_pending(); }
+void og_rebuild_bitmaps(void* h) { Oracle* g = (Oracle*)h; g->rebuild_all(g->bytes.epoch); }
+uint32_t og_tier1_sweep(void* h) { return ((Oracle*)h)->tier1_sweep(); }
+int og_tier1(void* h, uint32_t* history, int hist_cap, uint32_t* last_count) {
+    return ((Oracle*)h)->tier1(history, hist_cap, last_count);
+}
+uint32_t og_tier2(void* h) { return ((Oracle*)h)->tier2(); }
+
+// process_stream for one GPU (streamgc.cu:809-1053) in stream order: host
+// batches of `batch` updates, epoch when updates_since_epoch >= epoch_size,
+// checked after each batch. Returns the number of epoch boundaries.
+uint32_t og_process_stream(void* h, const EdgeUpdate* ups, uint64_t n, uint32_t epoch_size, uint32_t batch) {
+    Oracle* g = (Oracle*)h;
+    uint64_t processed = 0, since = 0;
+    uint32_t epochs = 0;
+    if (batch == 0) batch = SGC_HOST_BATCH_SIZE;
+    while (processed < n) {
+        uint64_t b = std::min<uint64_t>(batch, n - processed);
+        for (uint64_t i = 0; i < b; i++) g->apply_one(ups[processed + i]);
+        processed += b;
+        since += b;
+        if (since >= epoch_size) { g->epoch(); since = 0; epochs++; }
+    }
+    return epochs;
+}
+
+// Phase end exactly as main() does after each stream (streamgc.cu:1405-1408):
+// drain_and_compact, Tier-1 loop, Tier-2. Returns tier-2 fixes; tier-1
+// iterations and last count through the out pointers.
+uint32_t og_phase_end(void* h, int* t1_iters, uint32_t* t1_last) {
+    Oracle* g = (Oracle*)h;
+    g->drain_and_compact();
+    uint32_t last = 0;
+    int it = g->tier1(nullptr, 0, &last);
+    if (t1_iters) *t1_iters = it;
+    if (t1_last) *t1_last = last;
+    return g->tier2();
+}
+
+// Epoch with repair-before-publish (the concurrent mode's epoch): compact,
+// drain, Tier-1 loop, Tier-2, then snapshot. Stream batches of min(E, batch).
+uint32_t og_process_stream_repaired(void* h, const EdgeUpdate* ups, uint64_t n, uint32_t epoch_size,
+                                    uint32_t batch) {
+    Oracle* g = (Oracle*)h;
+    if (batch == 0) batch = SGC_HOST_BATCH_SIZE;
+    uint64_t step = std::min<uint64_t>(batch, epoch_size ? epoch_size : batch);
+    uint64_t processed = 0, since = 0;
+    uint32_t epochs = 0;
+    while (processed < n) {
+        uint64_t b = std::min<uint64_t>(step, n - processed);
+        for (uint64_t i = 0; i < b; i++) g->apply_one(ups[processed + i]);
+        processed += b;
+        since += b;
+        if (since >= epoch_size) {
+            g->compact_all();
+            g->drain_pending();
+            g->tier1(nullptr, 0, nullptr);
+            g->tier2();
+            g->snapshot();
+            since = 0;
+            epochs++;
+        }
+    }
+    return epochs;
+}
+
+// ---------------- state access ----------------
+void og_get_states(void* h, uint32_t* out) { Oracle* g = (Oracle*)h; std::memcpy(out, g->st.data(), g->n * 4ull); }
+void og_set_states(void* h, const uint32_t* in) { Oracle* g = (Oracle*)h; std::memcpy(g->st.data(), in, g->n * 4ull); }
+void og_get_bitmaps(void* h, uint64_t* out) { Oracle* g = (Oracle*)h; std::memcpy(out, g->bm.data(), g->n * 8ull); }
+void og_get_hdmap(void* h, uint32_t* out) { Oracle* g = (Oracle*)h; std::memcpy(out, g->hdmap.data(), g->n * 4ull); }
+void og_get_hist(void* h, uint32_t* out) {
+    Oracle* g = (Oracle*)h;
+    std::memcpy(out, g->hist.data(), g->hist.size() * 4ull);
+}
+void og_get_row_ptr(void* h, uint64_t* out) { Oracle* g = (Oracle*)h; std::memcpy(out, g->rp.data(), (g->n + 1ull) * 8); }
+void og_get_col(void* h, uint32_t* out) { Oracle* g = (Oracle*)h; std::memcpy(out, g->col.data(), g->col.size() * 4ull); }
+void og_get_snapshot(void* h, uint16_t* out) { Oracle* g = (Oracle*)h; std::memcpy(out, g->snap.data(), g->n * 2ull); }
+uint32_t og_overflow_count(void* h) { return ((Oracle*)h)->ovf_count; }
+void og_get_overflow(void* h, uint32_t* out_pairs, uint32_t cnt) {
+    Oracle* g = (Oracle*)h;
+    for (uint32_t i = 0; i < cnt && i < OVF_CAP; i++) {
+        out_pairs[2 * i] = g->ovf[i].local_vertex_idx;
+        out_pairs[2 * i + 1] = g->ovf[i].neighbor_global;
+    }
+}
+// counters: [updates_applied, skipped, recolors, ovf_lost, drain_failed,
+//            bytes.update, bytes.epoch, bytes.tier1, bytes.tier2]
+void og_counters(void* h, uint64_t* out) {
+    Oracle* g = (Oracle*)h;
+    out[0] = g->updates_applied; out[1] = g->skipped_updates; out[2] = g->recolors;
+    out[3] = g->ovf_lost; out[4] = g->drain_failed;
+    out[5] = g->bytes.update; out[6] = g->bytes.epoch; out[7] = g->bytes.tier1; out[8] = g->bytes.tier2;
+}
+void og_reset_bytes(void* h) { ((Oracle*)h)->bytes = Bytes(); }
+
+// ---------------- color selection probe (known-answer tests) ----------------
+// Sets vertex x's bitmap / histogram row and returns FindAvailableColor(x).
+uint16_t og_fac(void* h, uint32_t x) {
+    Oracle* g = (Oracle*)h;
+    uint64_t b = 0;
+    return g->fac(x, g->st, b);
+}
+void og_set_bitmap(void* h, uint32_t x, uint64_t v) { ((Oracle*)h)->bm[x] = v; }
+void og_set_hist_row(void* h, uint32_t x, const uint32_t* vals, uint32_t cnt) {
+    Oracle* g = (Oracle*)h;
+    uint32_t* r = g->hrow(x);
+    if (!r) return;
+    for (uint32_t i = 0; i < cnt && i < g->maxc; i++) r[i] = vals[i];
+}
+
+// ---------------- validator (streamgc.cu:448-556) ----------------
+// out: [violations, uncolored_with_edges, distinct_edges, max_color, entries_out_of_range]
+void og_validate(void* h, uint64_t* out) {
+    Oracle* g = (Oracle*)h;
+    std::unordered_set<uint64_t> es;
+    std::vector<uint32_t> eff(g->n, 0);
+    uint64_t oor = 0;
+    for (uint32_t x = 0; x < g->n; x++)
+        for (uint64_t j = g->rp[x]; j < g->rp[x + 1]; j++) {
+            uint32_t y = g->col[j];
+            if (y == INV) continue;
+            if (y >= g->n) { oor++; continue; }
+            eff[x]++;
+            uint32_t lo = std::min(x, y), hi = std::max(x, y);
+            es.insert(((uint64_t)lo << 32) | hi);
+        }
+    uint64_t viol = 0;
+    for (uint64_t e : es) {
+        uint32_t a = (uint32_t)(e >> 32), b = (uint32_t)e;
+        if (g->color(a) == g->color(b) && g->color(a) != 0) viol++;
+    }
+    uint64_t unc = 0;
+    uint16_t mx = 0;
+    for (uint32_t x = 0; x < g->n; x++) {
+        if (g->color(x) == 0 && eff[x] > 0) unc++;
+        mx = std::max(mx, g->color(x));
+    }
+    out[0] = viol; out[1] = unc; out[2] = es.size(); out[3] = mx; out[4] = oor;
+}
+
+// Same checks for an arbitrary color vector against a base CSR (u64 offsets).
+void og_validate_colors(uint32_t n, const uint64_t* rp, const uint32_t* col, const uint16_t* colors, uint64_t* out) {
+    uint64_t viol = 0, unc = 0;
+    uint16_t mx = 0;
+    for (uint32_t x = 0; x < n; x++) {
+        bool hasn = false;
+        for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+            uint32_t y = col[j];
+            if (y == INV || y >= n) continue;
+            hasn = true;
+            if (x <= y && colors[x] == colors[y] && colors[x] != 0) viol++;
+        }
+        if (colors[x] == 0 && hasn) unc++;
+        mx = std::max(mx, colors[x]);
+    }
+    out[0] = viol; out[1] = unc; out[2] = mx;
+}
+
+// ---------------- static greedy (streamgc.cu:559-592) ----------------
+uint16_t og_static_greedy(uint32_t n, const uint64_t* rp, const uint32_t* col) {
+    std::vector<uint16_t> c(n, 0);
+    std::vector<bool> used((size_t)n + 1, false);
+    for (uint32_t v = 0; v < n; v++) {
+        for (uint64_t j = rp[v]; j < rp[v + 1]; j++) if (c[col[j]]) used[c[col[j]]] = true;
+        uint16_t k = 1;
+        while (used[k]) k++;
+        c[v] = k;
+        for (uint64_t j = rp[v]; j < rp[v + 1]; j++) if (c[col[j]]) used[c[col[j]]] = false;
+    }
+    uint16_t mx = 0;
+    for (uint32_t v = 0; v < n; v++) mx = std::max(mx, c[v]);
+    return mx;
+}
+
+// ---------------- stream generators (stream_gen.cpp:30-177) ----------------
+// Init stream: u<v edges in CSR order, std::sort by (min deg desc, max deg desc).
+// out must hold nnz/2 pairs; returns count.
+uint64_t og_gen_init_stream(uint32_t n, const uint64_t* rp, const uint32_t* col, const uint32_t* degree,
+                            uint32_t* out_pairs) {
+    std::vector<std::pair<uint32_t, uint32_t>> edges;
+    for (uint32_t u = 0; u < n; u++)
+        for (uint64_t j = rp[u]; j < rp[u + 1]; j++)
+            if (u < col[j]) edges.push_back({u, col[j]});
+    std::sort(edges.begin(), edges.end(), [&degree](const auto& a, const auto& b) {
+        uint32_t mina = std::min(degree[a.first], degree[a.second]);
+        uint32_t minb = std::min(degree[b.first], degree[b.second]);
+        if (mina != minb) return mina > minb;
+        uint32_t maxa = std::max(degree[a.first], degree[a.second]);
+        uint32_t maxb = std::max(degree[b.first], degree[b.second]);
+        return maxa > maxb;
+    });
+    for (size_t i = 0; i < edges.size(); i++) { out_pairs[2 * i] = edges[i].first; out_pairs[2 * i + 1] = edges[i].second; }
+    return edges.size();
+}
+
+// Churn bench stream (stream_gen.cpp:65-177) through libstdc++'s
+// mt19937_64 / uniform_int_distribution. out_pairs: 2*stream_size, out_types: stream_size.
+void og_gen_bench_stream(uint32_t n, const uint64_t* rp, const uint32_t* col, uint64_t stream_size,
+                         uint32_t insert_pct, uint64_t seed, uint32_t* out_pairs, uint8_t* out_types) {
+    std::mt19937_64 rng(seed);
+    std::unordered_set<std::pair<uint32_t, uint32_t>, PairHash> live;
+    std::vector<std::pair<uint32_t, uint32_t>> live_vec;
+    for (uint32_t u = 0; u < n; u++)
+        for (uint64_t j = rp[u]; j < rp[u + 1]; j++)
+            if (u < col[j]) { live.insert({u, col[j]}); live_vec.push_back({u, col[j]}); }
+    std::vector<std::pair<uint32_t, uint32_t>> pool;
+    std::uniform_int_distribution<uint32_t> pct(0, 99);
+    uint64_t k = 0;
+    for (uint64_t i = 0; i < stream_size; i++) {
+        bool ins = pct(rng) < insert_pct;
+        if (ins) {
+            if (!pool.empty()) {
+                std::uniform_int_distribution<size_t> pd(0, pool.size() - 1);
+                size_t idx = pd(rng);
+                auto e = pool[idx];
+                pool[idx] = pool.back();
+                pool.pop_back();
+                live.insert(e);
+                live_vec.push_back(e);
+                out_pairs[2 * k] = e.first; out_pairs[2 * k + 1] = e.second; out_types[k] = 0; k++;
+            } else {
+                std::uniform_int_distribution<uint32_t> vd(0, n - 1);
+                uint32_t u = vd(rng), v = vd(rng);
+                if (u == v) v = (v + 1) % n;
+                uint32_t a = std::min(u, v), b = std::max(u, v);
+                if (live.find({a, b}) == live.end()) {
+                    live.insert({a, b});
+                    live_vec.push_back({a, b});
+                    out_pairs[2 * k] = a; out_pairs[2 * k + 1] = b; out_types[k] = 0; k++;
+                } else {
+                    i--;
+                    continue;
+                }
+            }
+        } else {
+            if (live_vec.empty()) { i--; continue; }
+            std::uniform_int_distribution<size_t> ed(0, live_vec.size() - 1);
+            size_t idx = ed(rng);
+            auto e = live_vec[idx];
+            live.erase(e);
+            live_vec[idx] = live_vec.back();
+            live_vec.pop_back();
+            pool.push_back(e);
+            out_pairs[2 * k] = e.first; out_pairs[2 * k + 1] = e.second; out_types[k] = 1; k++;
+        }
+    }
+}
+
+// ---------------- graph loader (graph_loader.cpp:29-169) ----------------
+// Two-call protocol: og_load_mtx returns a handle; og_loaded_* copy out.
+struct Loaded {
+    uint32_t n = 0;
+    std::vector<uint64_t> rp;
+    std::vector<uint32_t> col, deg;
+};
+void* og_load_mtx(const char* path) {
+    FILE* f = fopen(path, "r");
+    if (!f) return nullptr;
+    char line[4096];
+    bool pattern = false;
+    if (fgets(line, sizeof(line), f) && strstr(line, "pattern")) pattern = true;
+    while (fgets(line, sizeof(line), f)) if (line[0] != '%') break;
+    unsigned rows = 0, cols = 0;
+    unsigned long long nnz = 0;
+    if (sscanf(line, "%u %u %llu", &rows, &cols, &nnz) != 3) { fclose(f); return nullptr; }
+    uint32_t n = rows > cols ? rows : cols;
+    std::vector<std::pair<uint32_t, uint32_t>> raw;
+    raw.reserve(nnz);
+    for (uint64_t i = 0; i < nnz; i++) {
+        uint32_t u = 0, v = 0;
+        if (fscanf(f, "%u %u", &u, &v) != 2) break;
+        if (!pattern) { int c; while ((c = fgetc(f)) != '\n' && c != EOF) {} }
+        u--; v--;
+        if (u == v) continue;
+        if (u > v) std::swap(u, v);
+        raw.push_back({u, v});
+    }
+    fclose(f);
+    std::sort(raw.begin(), raw.end());
+    raw.erase(std::unique(raw.begin(), raw.end()), raw.end());
+    Loaded* L = new Loaded();
+    L->n = n;
+    L->deg.assign(n, 0);
+    for (auto& e : raw) { L->deg[e.first]++; L->deg[e.second]++; }
+    L->rp.assign((size_t)n + 1, 0);
+    for (uint32_t v = 0; v < n; v++) L->rp[v + 1] = L->rp[v] + L->deg[v];
+    L->col.assign(raw.size() * 2, 0);
+    std::vector<uint64_t> off(L->rp.begin(), L->rp.end() - 1);
+    for (auto& e : raw) { L->col[off[e.first]++] = e.second; L->col[off[e.second]++] = e.first; }
+    for (uint32_t v = 0; v < n; v++) std::sort(L->col.begin() + L->rp[v], L->col.begin() + L->rp[v + 1]);
+    return L;
+}
+uint32_t og_loaded_n(void* h) { return ((Loaded*)h)->n; }
+uint64_t og_loaded_nnz(void* h) { return ((Loaded*)h)->col.size(); }
+void og_loaded_copy(void* h, uint64_t* rp, uint32_t* col, uint32_t* deg) {
+    Loaded* L = (Loaded*)h;
+    std::memcpy(rp, L->rp.data(), L->rp.size() * 8);
+    std::memcpy(col, L->col.data(), L->col.size() * 4);
+    std::memcpy(deg, L->deg.data(), L->deg.size() * 4);
+}
+void og_loaded_free(void* h) { delete (Loaded*)h; }
+
+int og_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"

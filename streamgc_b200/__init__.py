@@ -1,0 +1,424 @@
+"""streamgc_b200 -- B200-native streaming graph coloring (single GPU).
+
+Python binding of libstreamgc_b200.so (C ABI in include/streamgc_b200.h). The
+library owns every computation; this module only moves numpy arrays across
+the ABI. There is no fallback: without the built library (streamgc_b200/lib/)
+every call raises.
+
+The reference program (algorithms/streamgc/src/streamgc.cu main) maps onto:
+    Graph.load_mtx / rmat / chung_lu / delaunay     graph input
+    Graph.init_stream / churn_stream / kcore_stream the update streams
+    StreamGC(graph, ...)                            allocate_gpu_partition
+    StreamGC.apply / epoch / publish / repair       process_stream pieces
+    StreamGC.process_stream                         process_stream
+    StreamGC.validate                               check_coloring_valid
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libstreamgc_b200.so")
+
+MODE_DETERMINISTIC = 0
+MODE_CONCURRENT = 1
+ADD, DEL = 0, 1
+
+EDGE_UPDATE = np.dtype([("u", "<u4"), ("v", "<u4"), ("type", "u1"), ("_pad", "u1", (7,))], align=True)
+assert EDGE_UPDATE.itemsize == 16
+
+DL = dict(states=0, colors=1, bitmaps=2, hist=3, row_ptr=4, col=5, snapshot=6, highwater=7, hdmap=8, overflow=9)
+
+
+class StreamGCError(RuntimeError):
+    pass
+
+
+class _Config(C.Structure):
+    _fields_ = [("num_gpus", C.c_uint32), ("num_vertices", C.c_uint32), ("num_edges", C.c_uint64),
+                ("stream_buffer_size", C.c_uint32), ("epoch_size", C.c_uint32),
+                ("priority_refresh_interval", C.c_uint32), ("histogram_threshold", C.c_uint32),
+                ("rebalance_threshold", C.c_float)]
+
+
+class _Options(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("slack_pct", C.c_uint32), ("max_hist_colors", C.c_uint32),
+                ("max_batch", C.c_uint32), ("device", C.c_int32), ("flags", C.c_uint32)]
+
+
+class RepairReport(C.Structure):
+    _fields_ = [("tier1_iterations", C.c_uint32), ("tier1_last_count", C.c_uint32), ("tier2_ran", C.c_uint32),
+                ("tier2_fixed", C.c_uint32), ("tier2_gave_up", C.c_uint32), ("drained", C.c_uint32),
+                ("drain_failed", C.c_uint64), ("proper", C.c_uint32), ("_pad", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("_")}
+
+
+class Stats(C.Structure):
+    _fields_ = [("updates_submitted", C.c_uint64), ("updates_skipped", C.c_uint64), ("epochs", C.c_uint64),
+                ("overflow_pending", C.c_uint64), ("overflow_lost", C.c_uint64), ("drain_failed", C.c_uint64),
+                ("tier1_sweeps", C.c_uint64), ("tier2_runs", C.c_uint64), ("tier2_fixed", C.c_uint64),
+                ("device_error", C.c_uint32), ("num_vertices", C.c_uint32), ("num_high_degree", C.c_uint32),
+                ("max_hist_colors", C.c_uint32), ("total_slots", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("sweep_ms", C.c_double), ("sweep_count", C.c_uint64), ("sweep_bytes", C.c_uint64),
+                ("live_entries", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Validation(C.Structure):
+    _fields_ = [("violations", C.c_uint64), ("uncolored_with_edges", C.c_uint64), ("edges", C.c_uint64),
+                ("max_color", C.c_uint64), ("out_of_range", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class _CSR(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("nnz", C.c_uint64), ("row_ptr", C.POINTER(C.c_uint64)),
+                ("col_idx", C.POINTER(C.c_uint32)), ("degree", C.POINTER(C.c_uint32))]
+
+
+_u8p, _u16p, _u32p, _u64p, _vp = (C.POINTER(C.c_uint8), C.POINTER(C.c_uint16), C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_uint64), C.c_void_p)
+_lib = None
+
+# every exported entry point of include/streamgc_b200.h and csrc/sgc_host.h
+SIGNATURES = {
+    "sgc_default_options": (C.c_int, [C.POINTER(_Options)]),
+    "sgc_create": (C.c_int, [C.POINTER(_Config), _u32p, _u32p, _u32p, C.POINTER(_vp)]),
+    "sgc_create_ex": (C.c_int, [C.POINTER(_Config), C.POINTER(_Options), _u64p, _u32p, _u32p, C.POINTER(_vp)]),
+    "sgc_destroy": (C.c_int, [_vp]),
+    "sgc_apply": (C.c_int, [_vp, _vp, C.c_uint32, C.c_int]),
+    "sgc_epoch": (C.c_int, [_vp]),
+    "sgc_drain_and_compact": (C.c_int, [_vp, C.POINTER(RepairReport)]),
+    "sgc_repair": (C.c_int, [_vp, C.POINTER(RepairReport)]),
+    "sgc_publish": (C.c_int, [_vp, C.POINTER(RepairReport)]),
+    "sgc_process_stream": (C.c_int, [_vp, _vp, C.c_uint64, C.c_int, _u32p]),
+    "sgc_query": (C.c_int, [_vp, _u32p, _u16p, C.c_uint32]),
+    "sgc_download": (C.c_int, [_vp, C.c_int, _vp, C.c_uint64]),
+    "sgc_upload": (C.c_int, [_vp, C.c_int, _vp, C.c_uint64]),
+    "sgc_find_color": (C.c_int, [_vp, C.c_uint32, _u16p]),
+    "sgc_validate": (C.c_int, [_vp, C.POINTER(Validation)]),
+    "sgc_get_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
+    "sgc_synchronize": (C.c_int, [_vp]),
+    "sgc_cuda_stream": (_vp, [_vp]),
+    "sgc_last_error": (C.c_char_p, []),
+    "sgc_version": (C.c_char_p, []),
+    "sgc_load_mtx": (C.c_int, [C.c_char_p, C.POINTER(_CSR)]),
+    "sgc_csr_from_edges": (C.c_int, [C.c_uint32, _u32p, C.c_uint64, C.POINTER(_CSR)]),
+    "sgc_csr_free": (None, [C.POINTER(_CSR)]),
+    "sgc_write_mtx": (C.c_int, [C.c_char_p, C.POINTER(_CSR)]),
+    "sgc_gen_init_stream": (C.c_uint64, [C.POINTER(_CSR), _u32p]),
+    "sgc_gen_churn_stream": (C.c_int, [C.POINTER(_CSR), C.c_uint64, C.c_uint32, C.c_uint64, _u32p, _u8p]),
+    "sgc_gen_kcore_stream": (C.c_int, [C.POINTER(_CSR), C.c_uint64, C.c_double, C.c_uint64, _u32p, _u8p, _u32p,
+                                       _u32p]),
+    "sgc_core_numbers": (C.c_int, [C.POINTER(_CSR), _u32p]),
+    "sgc_gen_rmat": (C.c_int, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                               C.POINTER(_CSR)]),
+    "sgc_gen_chung_lu": (C.c_int, [C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64, C.POINTER(_CSR)]),
+    "sgc_static_greedy": (C.c_uint32, [C.POINTER(_CSR)]),
+    "sgc_write_coloring": (C.c_int, [C.c_char_p, _u16p, C.c_uint32]),
+}
+
+
+def lib():
+    """Loads libstreamgc_b200.so; raises when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise StreamGCError(f"{LIB_PATH} is missing: run __graft_entry__.build() (make -C streamgc_b200/csrc)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc, what):
+    if rc != 0:
+        msg = lib().sgc_last_error().decode(errors="replace")
+        raise StreamGCError(f"{what} failed ({rc}): {msg}")
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def updates_from(pairs, types=None):
+    """(k,2) uint32 pairs + uint8 types (0=ADD, 1=DEL; default ADD) -> EdgeUpdate records."""
+    pairs = np.asarray(pairs, dtype=np.uint32).reshape(-1, 2)
+    ups = np.zeros(len(pairs), dtype=EDGE_UPDATE)
+    ups["u"] = pairs[:, 0]
+    ups["v"] = pairs[:, 1]
+    if types is not None:
+        ups["type"] = np.asarray(types, dtype=np.uint8)
+    return ups
+
+
+class Graph:
+    """Host CSR (64-bit row offsets, ascending rows, symmetric, no self loops)."""
+
+    def __init__(self, row_ptr, col_idx, degree=None):
+        self.row_ptr = np.ascontiguousarray(row_ptr, dtype=np.uint64)
+        self.col_idx = np.ascontiguousarray(col_idx, dtype=np.uint32)
+        self.n = len(self.row_ptr) - 1
+        self.degree = (np.ascontiguousarray(degree, dtype=np.uint32) if degree is not None
+                       else np.diff(self.row_ptr).astype(np.uint32))
+
+    @property
+    def nnz(self):
+        return int(self.row_ptr[-1])
+
+    def _c(self):
+        c = _CSR()
+        c.n = self.n
+        c.nnz = self.nnz
+        c.row_ptr = _p(self.row_ptr, _u64p)
+        c.col_idx = _p(self.col_idx, _u32p)
+        c.degree = _p(self.degree, _u32p)
+        return c
+
+    @staticmethod
+    def _take(c):
+        g = Graph(np.ctypeslib.as_array(c.row_ptr, (c.n + 1,)).copy(),
+                  np.ctypeslib.as_array(c.col_idx, (max(c.nnz, 1),))[: c.nnz].copy(),
+                  np.ctypeslib.as_array(c.degree, (max(c.n, 1),))[: c.n].copy())
+        lib().sgc_csr_free(C.byref(c))
+        return g
+
+    @staticmethod
+    def load_mtx(path):
+        c = _CSR()
+        _check(lib().sgc_load_mtx(path.encode(), C.byref(c)), f"load_mtx({path})")
+        return Graph._take(c)
+
+    @staticmethod
+    def from_edges(n, pairs):
+        pairs = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1, 2)
+        c = _CSR()
+        _check(lib().sgc_csr_from_edges(n, _p(pairs, _u32p), len(pairs), C.byref(c)), "csr_from_edges")
+        return Graph._take(c)
+
+    @staticmethod
+    def rmat(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=42):
+        cs = _CSR()
+        _check(lib().sgc_gen_rmat(scale, edge_factor, a, b, c, seed, C.byref(cs)), "gen_rmat")
+        return Graph._take(cs)
+
+    @staticmethod
+    def chung_lu(n, exponent=2.1, avg_degree=17.0, max_degree=100000.0, seed=42):
+        cs = _CSR()
+        _check(lib().sgc_gen_chung_lu(n, exponent, avg_degree, max_degree, seed, C.byref(cs)), "gen_chung_lu")
+        return Graph._take(cs)
+
+    @staticmethod
+    def delaunay(n, seed=42):
+        """Delaunay triangulation of n uniform points in the unit square (scipy/Qhull)."""
+        from scipy.spatial import Delaunay
+        pts = np.random.default_rng(seed).random((n, 2))
+        tri = Delaunay(pts).simplices.astype(np.uint32)
+        e = np.concatenate([tri[:, [0, 1]], tri[:, [1, 2]], tri[:, [0, 2]]])
+        return Graph.from_edges(n, e)
+
+    def write_mtx(self, path):
+        c = self._c()
+        _check(lib().sgc_write_mtx(path.encode(), C.byref(c)), "write_mtx")
+
+    def init_stream(self):
+        out = np.zeros(max(self.nnz, 2), dtype=np.uint32)
+        c = self._c()
+        k = lib().sgc_gen_init_stream(C.byref(c), _p(out, _u32p))
+        return updates_from(out[: 2 * k].reshape(-1, 2))
+
+    def churn_stream(self, size, insert_pct=50, seed=42):
+        pairs = np.zeros(2 * size, dtype=np.uint32)
+        types = np.zeros(size, dtype=np.uint8)
+        c = self._c()
+        _check(lib().sgc_gen_churn_stream(C.byref(c), size, insert_pct, seed, _p(pairs, _u32p), _p(types, _u8p)),
+               "gen_churn_stream")
+        return updates_from(pairs.reshape(-1, 2), types)
+
+    def kcore_stream(self, size, percentile=90.0, seed=42):
+        pairs = np.zeros(2 * size, dtype=np.uint32)
+        types = np.zeros(size, dtype=np.uint8)
+        k = np.zeros(1, dtype=np.uint32)
+        cs = np.zeros(1, dtype=np.uint32)
+        c = self._c()
+        _check(lib().sgc_gen_kcore_stream(C.byref(c), size, percentile, seed, _p(pairs, _u32p), _p(types, _u8p),
+                                          _p(k, _u32p), _p(cs, _u32p)), "gen_kcore_stream")
+        return updates_from(pairs.reshape(-1, 2), types), int(k[0]), int(cs[0])
+
+    def core_numbers(self):
+        out = np.zeros(self.n, dtype=np.uint32)
+        c = self._c()
+        _check(lib().sgc_core_numbers(C.byref(c), _p(out, _u32p)), "core_numbers")
+        return out
+
+    def static_greedy(self):
+        c = self._c()
+        return int(lib().sgc_static_greedy(C.byref(c)))
+
+
+def write_coloring(path, colors):
+    colors = np.ascontiguousarray(colors, dtype=np.uint16)
+    _check(lib().sgc_write_coloring(path.encode(), _p(colors, _u16p), len(colors)), "write_coloring")
+
+
+class StreamGC:
+    """One graph resident on one GPU (a handle of the C ABI)."""
+
+    def __init__(self, graph: Graph, epoch_size=32768, histogram_threshold=64, slack_pct=300,
+                 max_hist_colors=1024, max_batch=32768, device=0, profile=False):
+        L = lib()
+        cfg = _Config(1, graph.n, graph.nnz, 1 << 20, epoch_size, 100, histogram_threshold, 0.2)
+        opt = _Options()
+        L.sgc_default_options(C.byref(opt))
+        opt.slack_pct, opt.max_hist_colors, opt.max_batch, opt.device = slack_pct, max_hist_colors, max_batch, device
+        opt.flags = 1 if profile else 0
+        self.h = _vp()
+        self.graph = graph
+        self.n = graph.n
+        self.max_batch = max_batch
+        self.epoch_size = epoch_size
+        _check(L.sgc_create_ex(C.byref(cfg), C.byref(opt), _p(graph.row_ptr, _u64p), _p(graph.col_idx, _u32p),
+                               _p(graph.degree, _u32p), C.byref(self.h)), "sgc_create_ex")
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sgc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- stepping ----
+    def apply(self, ups, mode=MODE_DETERMINISTIC):
+        """Host EdgeUpdate array (numpy) or a device pointer (int) with an explicit count via apply_ptr."""
+        ups = np.ascontiguousarray(ups, dtype=EDGE_UPDATE)
+        for s in range(0, len(ups), self.max_batch):
+            part = ups[s: s + self.max_batch]
+            _check(lib().sgc_apply(self.h, part.ctypes.data, len(part), mode), "sgc_apply")
+
+    def apply_ptr(self, ptr, n, mode=MODE_CONCURRENT):
+        """Updates already in device (or pinned host) memory at address `ptr`."""
+        _check(lib().sgc_apply(self.h, C.c_void_p(ptr), n, mode), "sgc_apply")
+
+    def epoch(self):
+        _check(lib().sgc_epoch(self.h), "sgc_epoch")
+
+    def drain_and_compact(self):
+        r = RepairReport()
+        _check(lib().sgc_drain_and_compact(self.h, C.byref(r)), "sgc_drain_and_compact")
+        return r.as_dict()
+
+    def repair(self):
+        r = RepairReport()
+        _check(lib().sgc_repair(self.h, C.byref(r)), "sgc_repair")
+        return r.as_dict()
+
+    def publish(self):
+        r = RepairReport()
+        _check(lib().sgc_publish(self.h, C.byref(r)), "sgc_publish")
+        return r.as_dict()
+
+    def process_stream(self, ups, mode=MODE_DETERMINISTIC):
+        ups = np.ascontiguousarray(ups, dtype=EDGE_UPDATE)
+        ne = np.zeros(1, dtype=np.uint32)
+        _check(lib().sgc_process_stream(self.h, ups.ctypes.data, len(ups), mode, _p(ne, _u32p)),
+               "sgc_process_stream")
+        return int(ne[0])
+
+    def synchronize(self):
+        _check(lib().sgc_synchronize(self.h), "sgc_synchronize")
+
+    def cuda_stream(self):
+        return lib().sgc_cuda_stream(self.h)
+
+    # ---- reads ----
+    def query(self, vertices):
+        v = np.ascontiguousarray(vertices, dtype=np.uint32)
+        out = np.zeros(len(v), dtype=np.uint16)
+        _check(lib().sgc_query(self.h, _p(v, _u32p), _p(out, _u16p), len(v)), "sgc_query")
+        return out
+
+    def stats(self):
+        s = Stats()
+        rc = lib().sgc_get_stats(self.h, C.byref(s))
+        d = s.as_dict()
+        if rc not in (0, -4):
+            _check(rc, "sgc_get_stats")
+        return d
+
+    def _dl(self, what, dtype, count):
+        out = np.zeros(count, dtype=dtype)
+        _check(lib().sgc_download(self.h, DL[what], out.ctypes.data, out.nbytes), f"download {what}")
+        return out
+
+    def states(self):
+        return self._dl("states", np.uint32, self.n)
+
+    def colors(self):
+        return self._dl("colors", np.uint16, self.n)
+
+    def bitmaps(self):
+        return self._dl("bitmaps", np.uint64, self.n)
+
+    def hist(self):
+        s = self.stats()
+        return self._dl("hist", np.uint32, s["num_high_degree"] * s["max_hist_colors"])
+
+    def row_ptr(self):
+        return self._dl("row_ptr", np.uint64, self.n + 1)
+
+    def col(self):
+        return self._dl("col", np.uint32, self.stats()["total_slots"])
+
+    def snapshot(self):
+        return self._dl("snapshot", np.uint16, self.n)
+
+    def highwater(self):
+        return self._dl("highwater", np.uint32, self.n)
+
+    def hdmap(self):
+        return self._dl("hdmap", np.uint32, self.n)
+
+    def overflow(self):
+        pend = self.stats()["overflow_pending"]
+        return self._dl("overflow", np.uint32, 2 * min(pend, 262144)).reshape(-1, 2)
+
+    def upload(self, what, arr):
+        arr = np.ascontiguousarray(arr)
+        _check(lib().sgc_upload(self.h, DL[what], arr.ctypes.data, arr.nbytes), f"upload {what}")
+
+    def find_color(self, x):
+        c = np.zeros(1, dtype=np.uint16)
+        _check(lib().sgc_find_color(self.h, x, _p(c, _u16p)), "sgc_find_color")
+        return int(c[0])
+
+    def validate(self):
+        v = Validation()
+        _check(lib().sgc_validate(self.h, C.byref(v)), "sgc_validate")
+        return v.as_dict()
+
+
+def version():
+    return lib().sgc_version().decode()

@@ -1,0 +1,743 @@
+// sgc_api.cu -- the C ABI (include/streamgc_b200.h): one handle per graph,
+// owning its device state and one CUDA stream. The host side is a thin
+// sequencer; every step on the graph runs as a kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/streamgc_b200.h"
+#include "sgc_kernels.cuh"
+
+using namespace sgc;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                      \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return fail(SGC_ECUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// Control block on the device: counters every kernel family writes.
+struct Ctl {
+    uint32_t ovf_count;
+    uint32_t err;
+    uint32_t drain_n;
+    uint32_t dirty_count;
+    uint32_t item_count;
+    uint32_t pend_count;
+    uint32_t fac_count;
+    uint32_t ticket;
+    unsigned long long ovf_lost;
+    unsigned long long nskip;
+    unsigned long long drain_failed;
+    unsigned long long symsum;
+    unsigned long long live;
+    unsigned long long pad[3];
+};
+
+}  // namespace
+
+struct sgc_handle {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    sgc_options opt{};
+    StreamGCConfig cfg{};
+    uint32_t n = 0, num_hd = 0, maxc = 1024;
+    uint64_t total_slots = 0;
+    uint64_t device_bytes = 0;
+    Dev g{};
+    // owned device buffers
+    std::vector<void*> allocs;
+    Ctl* ctl = nullptr;
+    uint16_t* snap[2] = {nullptr, nullptr};
+    int front = 0;
+    EdgeUpdate* d_batch = nullptr;
+    EdgeUpdate* h_stage = nullptr;  // pinned staging for pageable inputs
+    cudaEvent_t stage_free = nullptr;
+    EdgeOrder eo{};
+    uint32_t seq = 0;
+    SweepBufs sb{};
+    uint32_t* dirty_list = nullptr;
+    Tier2Bufs t2{};
+    uint32_t* h_small = nullptr;    // pinned readback scratch
+    int last_mode = SGC_MODE_DETERMINISTIC;
+    // host counters
+    uint64_t updates = 0, epochs = 0, tier1_sweeps = 0, tier2_runs = 0, tier2_fixed = 0;
+    // profiling
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
+    double sweep_ms = 0;
+    uint64_t sweep_count = 0, sweep_bytes = 0, live_entries = 0;
+};
+
+namespace {
+
+template <class T>
+int dalloc(sgc_handle* h, T** p, size_t count, int fill = -1) {
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SGC_ENOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    }
+    h->allocs.push_back(q);
+    h->device_bytes += bytes;
+    if (fill >= 0) CK(cudaMemsetAsync(q, fill, bytes, h->stream));
+    *p = (T*)q;
+    return SGC_OK;
+}
+
+#define TRY(x)                   \
+    do {                         \
+        int r_ = (x);            \
+        if (r_ != SGC_OK) return r_; \
+    } while (0)
+
+// Scatters the base CSR into the slack layout: warp per row.
+__global__ void scatter_base_kernel(uint32_t n, const uint64_t* __restrict__ brp, const uint32_t* __restrict__ bcol,
+                                    const uint64_t* __restrict__ rp, uint32_t* __restrict__ col) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t x = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; x < n; x += warps) {
+        const uint64_t s = brp[x], e = brp[x + 1], d = rp[x];
+        for (uint64_t j = s + (threadIdx.x & 31); j < e; j += 32) col[d + (j - s)] = bcol[j];
+    }
+}
+
+__global__ void find_color_kernel(Dev g, uint32_t x, uint16_t* out) {
+    const uint16_t c = warp_fac(g, x, g.st);
+    if (lane_id() == 0) *out = c;
+}
+
+int check_cuda(const char* where) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(SGC_ECUDA, "%s: %s", where, cudaGetErrorString(e));
+    return SGC_OK;
+}
+
+cudaEvent_t take_event(sgc_handle* h) {
+    if (!h->ev_pool.empty()) {
+        cudaEvent_t e = h->ev_pool.back();
+        h->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Gathers the elapsed time of recorded sweep event pairs (stream must be idle).
+void collect_events(sgc_handle* h) {
+    for (auto& pr : h->ev_pending) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) {
+            h->sweep_ms += ms;
+            h->sweep_count++;
+        }
+        h->ev_pool.push_back(pr.first);
+        h->ev_pool.push_back(pr.second);
+    }
+    h->ev_pending.clear();
+}
+
+int sync(sgc_handle* h) {
+    CK(cudaStreamSynchronize(h->stream));
+    collect_events(h);
+    return SGC_OK;
+}
+
+// ---- epoch building blocks ----
+
+int compact_dirty(sgc_handle* h) {
+    CK(cudaMemsetAsync(&h->ctl->dirty_count, 0, 4, h->stream));
+    launch_dirty_list(h->g, h->dirty_list, &h->ctl->dirty_count, h->stream);
+    launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, h->stream);
+    return check_cuda("compact");
+}
+
+int drain(sgc_handle* h, bool ordered, unsigned long long* failed_counter) {
+    launch_take_overflow(h->g, &h->ctl->drain_n, h->stream);
+    launch_drain(h->g, &h->ctl->drain_n, ordered, failed_counter, h->stream);
+    return check_cuda("drain");
+}
+
+// Sweep with optional event timing around the edge passes.
+int sweep(sgc_handle* h, SweepMode mode) {
+    const bool prof = (h->opt.flags & SGC_OPT_PROFILE) != 0 && mode == SWEEP_TIER1;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (prof) {
+        a = take_event(h);
+        b = take_event(h);
+        cudaEventRecord(a, h->stream);
+    }
+    launch_sweep(h->g, h->sb, mode, h->num_sms, h->stream);
+    if (prof) {
+        cudaEventRecord(b, h->stream);
+        h->ev_pending.push_back({a, b});
+    }
+    return check_cuda("sweep");
+}
+
+int build_items(sgc_handle* h) {
+    launch_build_items(h->g, h->sb, h->stream);
+    return check_cuda("build_items");
+}
+
+void publish_snapshot(sgc_handle* h) {
+    const int back = 1 - h->front;
+    launch_snapshot(h->g, h->snap[back], h->stream);
+    h->front = back;
+}
+
+// Tier-1 loop of run_conflict_repair (streamgc.cu:1317-1393); rows compact and
+// items built. Tier-2 runs unless convergence on a mirror-complete CSR proves
+// it a no-op.
+int repair_loop(sgc_handle* h, sgc_repair_report* rep) {
+    uint32_t prev = 0xFFFFFFFFu, cnt = 0;
+    int plateau = 0, it = 0;
+    CK(cudaMemsetAsync(&h->ctl->symsum, 0, 16, h->stream));
+    for (it = 0; it < 20; it++) {
+        TRY(sweep(h, SWEEP_TIER1));
+        h->tier1_sweeps++;
+        CK(cudaMemcpyAsync(h->h_small, &h->ctl->pend_count, 4, cudaMemcpyDeviceToHost, h->stream));
+        if (it == 0) CK(cudaMemcpyAsync(h->h_small + 2, &h->ctl->symsum, 16, cudaMemcpyDeviceToHost, h->stream));
+        TRY(sync(h));
+        cnt = h->h_small[0];
+        if (it == 0) h->live_entries = *(unsigned long long*)(h->h_small + 4);
+        if (cnt == 0) break;
+        if (cnt == prev) {
+            if (++plateau >= 3) break;
+        } else {
+            plateau = 0;
+        }
+        prev = cnt;
+    }
+    const unsigned long long sym = *(unsigned long long*)(h->h_small + 2);
+    const uint32_t iters = it < 20 ? it + 1 : 20;
+    if (h->opt.flags & SGC_OPT_PROFILE) h->sweep_bytes += (uint64_t)iters * (8ull * h->live_entries + 28ull * h->n);
+    sgc_repair_report r{};
+    r.tier1_iterations = iters;
+    r.tier1_last_count = cnt;
+    bool proper = (cnt == 0 && sym == 0);
+    if (!proper) {
+        bool gave_up = false;
+        const uint32_t fixed = run_tier2(h->g, h->t2, h->stream, h->h_small, &gave_up);
+        TRY(check_cuda("tier2"));
+        r.tier2_ran = 1;
+        r.tier2_fixed = fixed;
+        r.tier2_gave_up = gave_up ? 1 : 0;
+        h->tier2_runs++;
+        h->tier2_fixed += fixed;
+        proper = !gave_up;
+    }
+    r.proper = proper ? 1 : 0;
+    if (rep) {
+        r.drained = rep->drained;
+        r.drain_failed = rep->drain_failed;
+        *rep = r;
+    }
+    return SGC_OK;
+}
+
+int read_drain(sgc_handle* h, sgc_repair_report* rep, unsigned long long before_failed) {
+    CK(cudaMemcpyAsync(h->h_small, &h->ctl->drain_n, 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_small + 2, &h->ctl->drain_failed, 8, cudaMemcpyDeviceToHost, h->stream));
+    TRY(sync(h));
+    if (rep) {
+        rep->drained = h->h_small[0];
+        rep->drain_failed = *(unsigned long long*)(h->h_small + 2) - before_failed;
+    }
+    return SGC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sgc_default_options(sgc_options* o) {
+    if (!o) return fail(SGC_EINVAL, "null options");
+    std::memset(o, 0, sizeof(*o));
+    o->struct_size = sizeof(sgc_options);
+    o->slack_pct = SGC_CSR_EXTRA_SLACK_PCT_DEFAULT;
+    o->max_hist_colors = SGC_MAX_HISTOGRAM_COLORS_DEFAULT;
+    o->max_batch = SGC_HOST_BATCH_SIZE;
+    o->device = 0;
+    o->flags = 0;
+    return SGC_OK;
+}
+
+int sgc_destroy(sgc_handle* h) {
+    if (!h) return SGC_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : h->allocs) cudaFree(p);
+    if (h->h_stage) cudaFreeHost(h->h_stage);
+    if (h->h_small) cudaFreeHost(h->h_small);
+    if (h->stage_free) cudaEventDestroy(h->stage_free);
+    for (auto& pr : h->ev_pending) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    for (auto e : h->ev_pool) cudaEventDestroy(e);
+    if (h->t2.rev_keys) cudaFree(h->t2.rev_keys);
+    if (h->t2.rev_keys2) cudaFree(h->t2.rev_keys2);
+    if (h->t2.cub_tmp) cudaFree(h->t2.cub_tmp);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return SGC_OK;
+}
+
+int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const uint64_t* row_ptr,
+                  const uint32_t* col_idx, const uint32_t* degree, sgc_handle** out) {
+    if (!cfg || !row_ptr || !degree || !out) return fail(SGC_EINVAL, "null argument");
+    *out = nullptr;
+    sgc_options opt;
+    sgc_default_options(&opt);
+    if (opt_in) {
+        if (opt_in->struct_size != sizeof(sgc_options)) return fail(SGC_EINVAL, "sgc_options.struct_size mismatch");
+        opt = *opt_in;
+    }
+    if (cfg->num_gpus > 1) return fail(SGC_ENOTSUP, "num_gpus=%u: this library runs the single-GPU path", cfg->num_gpus);
+    if (opt.max_hist_colors == 0 || opt.max_hist_colors % 4 || opt.max_hist_colors > 65535)
+        return fail(SGC_EINVAL, "max_hist_colors must be a positive multiple of 4");
+    if (opt.max_batch == 0) return fail(SGC_EINVAL, "max_batch must be positive");
+    const uint32_t n = cfg->num_vertices;
+    if (n == 0) return fail(SGC_EINVAL, "num_vertices is 0");
+    if (row_ptr[0] != 0) return fail(SGC_EINVAL, "row_ptr[0] must be 0");
+    const uint64_t nnz = row_ptr[n];
+    if (nnz && !col_idx) return fail(SGC_EINVAL, "col_idx is null");
+    // host-side layout: capacity max(d + d*slack/100, 8) (streamgc.cu:373-378)
+    std::vector<uint64_t> rp((size_t)n + 1, 0);
+    std::vector<uint32_t> hdmap(n, EMPTY);
+    std::vector<uint32_t> hw(n, 0);
+    uint32_t num_hd = 0;
+    for (uint32_t x = 0; x < n; x++) {
+        if (row_ptr[x + 1] < row_ptr[x]) return fail(SGC_EINVAL, "row_ptr not monotone at %u", x);
+        const uint64_t cnt64 = row_ptr[x + 1] - row_ptr[x];
+        if (cnt64 > 0x3FFFFFFFull) return fail(SGC_EINVAL, "row %u too long", x);
+        const uint32_t cnt = (uint32_t)cnt64;
+        const uint32_t extra = (uint32_t)(((uint64_t)cnt * opt.slack_pct) / 100);
+        const uint32_t cap = std::max<uint32_t>(cnt + extra, 8u);
+        rp[x + 1] = rp[x] + cap;
+        hw[x] = cnt;
+        if (degree[x] > cfg->histogram_threshold) hdmap[x] = num_hd++;
+    }
+    for (uint64_t j = 0; j < nnz; j++)
+        if (col_idx[j] == INV) return fail(SGC_EINVAL, "col_idx holds the INVALID sentinel at %llu", (unsigned long long)j);
+    // rows whose base entries are not strictly ascending start "edited": the
+    // binary-search fast path only serves sorted, duplicate-free rows
+    std::vector<uint32_t> edited((n + 31) / 32 + 1, 0);
+    for (uint32_t x = 0; x < n; x++)
+        for (uint64_t j = row_ptr[x] + 1; j < row_ptr[x + 1]; j++)
+            if (col_idx[j - 1] >= col_idx[j]) { edited[x >> 5] |= 1u << (x & 31); break; }
+
+    sgc_handle* h = new sgc_handle();
+    h->opt = opt;
+    h->cfg = *cfg;
+    h->device = opt.device;
+    h->n = n;
+    h->num_hd = num_hd;
+    h->maxc = opt.max_hist_colors;
+    h->total_slots = rp[n];
+    auto bail = [&](int code) { sgc_destroy(h); return code; };
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return bail(fail(SGC_ECUDA, "cudaSetDevice(%d) failed", h->device)); }
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(fail(SGC_ECUDA, "stream create failed"));
+
+    int r = SGC_OK;
+#define A(...) do { r = dalloc(h, __VA_ARGS__); if (r) return bail(r); } while (0)
+    Dev& g = h->g;
+    g.n = n;
+    g.maxc = h->maxc;
+    uint64_t* d_rp; A(&d_rp, (size_t)n + 1);
+    const uint64_t padded = ((h->total_slots + 3) & ~3ull) + 8;  // 16-byte loads stay inside
+    uint32_t* d_col; A(&d_col, padded, 0xFF);
+    A(&g.st, n, 0);
+    A(&g.bm, n, 0);
+    uint32_t* d_hdmap; A(&d_hdmap, n);
+    A(&g.hist, (size_t)num_hd * h->maxc, 0);
+    uint32_t* d_deg; A(&d_deg, n);
+    A(&g.hw, n);
+    A(&g.dirty, (n + 31) / 32 + 1, 0);
+    A(&g.edited, (n + 31) / 32 + 1, 0);
+    A(&g.ovf, OVF_CAP);
+    A(&h->ctl, 1, 0);
+    A(&h->snap[0], n, 0);
+    A(&h->snap[1], n, 0);
+    g.rp = d_rp;
+    g.col = d_col;
+    g.hdmap = d_hdmap;
+    g.deg = d_deg;
+    g.ovf_count = &h->ctl->ovf_count;
+    g.ovf_lost = &h->ctl->ovf_lost;
+    g.nskip = &h->ctl->nskip;
+    g.err = &h->ctl->err;
+    if (cudaMemcpyAsync(d_rp, rp.data(), rp.size() * 8, cudaMemcpyHostToDevice, h->stream) ||
+        cudaMemcpyAsync(d_hdmap, hdmap.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) ||
+        cudaMemcpyAsync(d_deg, degree, (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) ||
+        cudaMemcpyAsync(g.hw, hw.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) ||
+        cudaMemcpyAsync(g.edited, edited.data(), edited.size() * 4, cudaMemcpyHostToDevice, h->stream))
+        return bail(fail(SGC_ECUDA, "upload failed"));
+    // base entries: staged through a temporary device copy of the base CSR
+    if (nnz) {
+        uint64_t* d_brp = nullptr;
+        uint32_t* d_bcol = nullptr;
+        if (cudaMalloc(&d_brp, ((size_t)n + 1) * 8) || cudaMalloc(&d_bcol, nnz * 4)) {
+            cudaFree(d_brp);
+            cudaGetLastError();
+            return bail(fail(SGC_ENOMEM, "base CSR staging allocation failed"));
+        }
+        cudaMemcpyAsync(d_brp, row_ptr, ((size_t)n + 1) * 8, cudaMemcpyHostToDevice, h->stream);
+        cudaMemcpyAsync(d_bcol, col_idx, nnz * 4, cudaMemcpyHostToDevice, h->stream);
+        scatter_base_kernel<<<h->num_sms * 8, 256, 0, h->stream>>>(n, d_brp, d_bcol, d_rp, d_col);
+        cudaStreamSynchronize(h->stream);
+        cudaFree(d_brp);
+        cudaFree(d_bcol);
+        if ((r = check_cuda("scatter_base"))) return bail(r);
+    }
+    // update staging + same-edge ordering
+    const uint32_t mb = opt.max_batch;
+    A(&h->d_batch, mb);
+    if (cudaHostAlloc(&h->h_stage, (size_t)mb * sizeof(EdgeUpdate), cudaHostAllocDefault) != cudaSuccess)
+        return bail(fail(SGC_ENOMEM, "pinned staging allocation failed"));
+    if (cudaHostAlloc(&h->h_small, 256, cudaHostAllocDefault) != cudaSuccess)
+        return bail(fail(SGC_ENOMEM, "pinned scratch allocation failed"));
+    cudaEventCreateWithFlags(&h->stage_free, cudaEventDisableTiming);
+    uint32_t tsize = 1;
+    while (tsize < 2 * mb) tsize <<= 1;
+    EdgeOrder& eo = h->eo;
+    A(&eo.tkey, tsize, 0xFF);
+    A(&eo.thead, tsize, 0xFF);
+    A(&eo.tslot, mb);
+    A(&eo.tnext, mb);
+    A(&eo.tprev, mb);
+    A(&eo.done, mb, 0);
+    eo.ticket = &h->ctl->ticket;
+    eo.tmask = tsize - 1;
+    // sweep buffers
+    SweepBufs& sb = h->sb;
+    const uint64_t icap = h->total_slots / SWEEP_CH + (uint64_t)n + 1;
+    if (icap > 0xFFFFFFF0ull) return bail(fail(SGC_ENOTSUP, "sweep item list beyond 2^32 entries"));
+    sb.item_cap = (uint32_t)icap;
+    A(&sb.items, icap);
+    sb.item_count = &h->ctl->item_count;
+    A(&sb.acc_bm, n, 0);
+    A(&sb.acc_fl, n, 0);
+    A(&sb.pend_v, n);
+    A(&sb.pend_w, n);
+    sb.pend_count = &h->ctl->pend_count;
+    A(&sb.fac_v, n);
+    sb.fac_count = &h->ctl->fac_count;
+    sb.symsum = &h->ctl->symsum;
+    sb.live = &h->ctl->live;
+    A(&h->dirty_list, n);
+    // tier-2 buffers
+    Tier2Bufs& t2 = h->t2;
+    A(&t2.inU, n);
+    A(&t2.inF, n);
+    A(&t2.inL, n);
+    A(&t2.done, n);
+    A(&t2.list, n);
+    A(&t2.list2, n);
+    A(&t2.count, 16, 0);
+    A(&t2.rev_start, n);
+    A(&t2.rev_end, n);
+    A(&t2.pend_v, n);
+    A(&t2.pend_w, n);
+    t2.rev_cap = 1u << 20;
+    if (cudaMalloc(&t2.rev_keys, (size_t)t2.rev_cap * 8) || cudaMalloc(&t2.rev_keys2, (size_t)t2.rev_cap * 8))
+        return bail(fail(SGC_ENOMEM, "tier-2 reverse buffer allocation failed"));
+    t2.cub_tmp_bytes = tier2_cub_bytes(n, t2.rev_cap);
+    if (cudaMalloc(&t2.cub_tmp, t2.cub_tmp_bytes)) return bail(fail(SGC_ENOMEM, "tier-2 scratch allocation failed"));
+#undef A
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(fail(SGC_ECUDA, "create sync failed"));
+    if ((r = check_cuda("create"))) return bail(r);
+    *out = h;
+    return SGC_OK;
+}
+
+int sgc_create(const StreamGCConfig* cfg, const uint32_t* row_ptr, const uint32_t* col_idx, const uint32_t* degree,
+               sgc_handle** out) {
+    if (!cfg || !row_ptr) return fail(SGC_EINVAL, "null argument");
+    std::vector<uint64_t> rp((size_t)cfg->num_vertices + 1);
+    for (size_t i = 0; i < rp.size(); i++) rp[i] = row_ptr[i];
+    return sgc_create_ex(cfg, nullptr, rp.data(), col_idx, degree, out);
+}
+
+int sgc_apply(sgc_handle* h, const EdgeUpdate* ups, uint32_t n, int mode) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    if (n == 0) return SGC_OK;
+    if (!ups) return fail(SGC_EINVAL, "null updates");
+    if (n > h->opt.max_batch) return fail(SGC_EINVAL, "batch %u exceeds max_batch %u", n, h->opt.max_batch);
+    if (mode != SGC_MODE_DETERMINISTIC && mode != SGC_MODE_CONCURRENT) return fail(SGC_EINVAL, "bad mode %d", mode);
+    CK(cudaSetDevice(h->device));
+    const EdgeUpdate* src = ups;
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, ups) != cudaSuccess) cudaGetLastError();
+    if (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) {
+        src = ups;  // caller keeps it alive until the stream passes this point
+    } else if (attr.type == cudaMemoryTypeHost) {
+        CK(cudaMemcpyAsync(h->d_batch, ups, (size_t)n * sizeof(EdgeUpdate), cudaMemcpyHostToDevice, h->stream));
+        src = h->d_batch;
+    } else {
+        CK(cudaEventSynchronize(h->stage_free));
+        std::memcpy(h->h_stage, ups, (size_t)n * sizeof(EdgeUpdate));
+        CK(cudaMemcpyAsync(h->d_batch, h->h_stage, (size_t)n * sizeof(EdgeUpdate), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaEventRecord(h->stage_free, h->stream));
+        src = h->d_batch;
+    }
+    if (mode == SGC_MODE_DETERMINISTIC) {
+        launch_det_apply(h->g, src, n, h->stream);
+    } else {
+        h->seq++;
+        if (h->seq == 0) {  // wrapped: clear the done marks before reuse
+            CK(cudaMemsetAsync(h->eo.done, 0, (size_t)h->opt.max_batch * 4, h->stream));
+            h->seq = 1;
+        }
+        launch_conc_apply(h->g, src, n, h->eo, h->seq, h->num_sms, h->stream);
+    }
+    h->last_mode = mode;
+    h->updates += n;
+    return check_cuda("apply");
+}
+
+int sgc_epoch(sgc_handle* h) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    CK(cudaSetDevice(h->device));
+    publish_snapshot(h);
+    TRY(compact_dirty(h));
+    TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, nullptr));
+    TRY(build_items(h));
+    TRY(sweep(h, SWEEP_REBUILD));
+    h->epochs++;
+    return SGC_OK;
+}
+
+int sgc_drain_and_compact(sgc_handle* h, sgc_repair_report* rep) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpyAsync(h->h_small + 8, &h->ctl->drain_failed, 8, cudaMemcpyDeviceToHost, h->stream));
+    TRY(sync(h));
+    const unsigned long long before = *(unsigned long long*)(h->h_small + 8);
+    TRY(compact_dirty(h));
+    TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, &h->ctl->drain_failed));
+    TRY(build_items(h));
+    TRY(sweep(h, SWEEP_REBUILD));
+    return read_drain(h, rep, before);
+}
+
+int sgc_repair(sgc_handle* h, sgc_repair_report* rep) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    CK(cudaSetDevice(h->device));
+    sgc_repair_report r{};
+    CK(cudaMemcpyAsync(h->h_small + 8, &h->ctl->drain_failed, 8, cudaMemcpyDeviceToHost, h->stream));
+    TRY(sync(h));
+    const unsigned long long before = *(unsigned long long*)(h->h_small + 8);
+    TRY(compact_dirty(h));
+    TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, &h->ctl->drain_failed));
+    TRY(build_items(h));
+    // drain_and_compact's rebuild is subsumed: the first Tier-1 sweep rebuilds every bitmap first.
+    TRY(read_drain(h, &r, before));
+    TRY(repair_loop(h, &r));
+    if (rep) *rep = r;
+    return SGC_OK;
+}
+
+int sgc_publish(sgc_handle* h, sgc_repair_report* rep) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    CK(cudaSetDevice(h->device));
+    sgc_repair_report r{};
+    TRY(compact_dirty(h));
+    TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, &h->ctl->drain_failed));
+    TRY(build_items(h));
+    TRY(repair_loop(h, &r));
+    publish_snapshot(h);
+    h->epochs++;
+    if (rep) *rep = r;
+    return check_cuda("publish");
+}
+
+int sgc_process_stream(sgc_handle* h, const EdgeUpdate* ups, uint64_t n, int mode, uint32_t* epochs) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    const uint32_t E = h->cfg.epoch_size;
+    uint64_t batch = mode == SGC_MODE_DETERMINISTIC ? SGC_HOST_BATCH_SIZE
+                                                     : std::min<uint64_t>(E ? E : SGC_HOST_BATCH_SIZE, h->opt.max_batch);
+    batch = std::min<uint64_t>(batch, h->opt.max_batch);
+    uint64_t processed = 0, since = 0;
+    uint32_t ne = 0;
+    while (processed < n) {
+        const uint32_t b = (uint32_t)std::min<uint64_t>(batch, n - processed);
+        TRY(sgc_apply(h, ups + processed, b, mode));
+        processed += b;
+        since += b;
+        if (since >= E) {
+            if (mode == SGC_MODE_DETERMINISTIC) TRY(sgc_epoch(h));
+            else TRY(sgc_publish(h, nullptr));
+            since = 0;
+            ne++;
+        }
+    }
+    if (epochs) *epochs = ne;
+    return SGC_OK;
+}
+
+int sgc_query(sgc_handle* h, const uint32_t* v, uint16_t* out, uint32_t k) {
+    if (!h || (k && (!v || !out))) return fail(SGC_EINVAL, "null argument");
+    if (!k) return SGC_OK;
+    CK(cudaSetDevice(h->device));
+    uint32_t* dv = nullptr;
+    uint16_t* dout = nullptr;
+    CK(cudaMallocAsync(&dv, (size_t)k * 4, h->stream));
+    CK(cudaMallocAsync(&dout, (size_t)k * 2, h->stream));
+    CK(cudaMemcpyAsync(dv, v, (size_t)k * 4, cudaMemcpyHostToDevice, h->stream));
+    launch_query(h->snap[h->front], h->n, dv, dout, k, h->stream);
+    CK(cudaMemcpyAsync(out, dout, (size_t)k * 2, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaFreeAsync(dv, h->stream));
+    CK(cudaFreeAsync(dout, h->stream));
+    return sync(h);
+}
+
+int sgc_download(sgc_handle* h, int what, void* dst, uint64_t bytes) {
+    if (!h || !dst) return fail(SGC_EINVAL, "null argument");
+    CK(cudaSetDevice(h->device));
+    const void* src = nullptr;
+    uint64_t need = 0;
+    uint16_t* tmp = nullptr;
+    switch (what) {
+        case SGC_DL_STATES: src = h->g.st; need = h->n * 4ull; break;
+        case SGC_DL_BITMAPS: src = h->g.bm; need = h->n * 8ull; break;
+        case SGC_DL_HIST: src = h->g.hist; need = (uint64_t)h->num_hd * h->maxc * 4; break;
+        case SGC_DL_ROW_PTR: src = h->g.rp; need = (h->n + 1ull) * 8; break;
+        case SGC_DL_COL: src = h->g.col; need = h->total_slots * 4; break;
+        case SGC_DL_SNAPSHOT: src = h->snap[h->front]; need = h->n * 2ull; break;
+        case SGC_DL_HIGHWATER: src = h->g.hw; need = h->n * 4ull; break;
+        case SGC_DL_HDMAP: src = h->g.hdmap; need = h->n * 4ull; break;
+        case SGC_DL_COLORS: {
+            CK(cudaMallocAsync(&tmp, h->n * 2ull, h->stream));
+            launch_colors(h->g, tmp, h->stream);
+            src = tmp;
+            need = h->n * 2ull;
+            break;
+        }
+        case SGC_DL_OVERFLOW: {
+            CK(cudaMemcpyAsync(h->h_small, &h->ctl->ovf_count, 4, cudaMemcpyDeviceToHost, h->stream));
+            TRY(sync(h));
+            const uint32_t c = std::min<uint32_t>(h->h_small[0], OVF_CAP);
+            src = h->g.ovf;
+            need = c * 8ull;
+            break;
+        }
+        default: return fail(SGC_EINVAL, "bad download target %d", what);
+    }
+    if (bytes < need) {
+        if (tmp) cudaFreeAsync(tmp, h->stream);
+        return fail(SGC_EINVAL, "download target %d needs %llu bytes", what, (unsigned long long)need);
+    }
+    if (need) CK(cudaMemcpyAsync(dst, src, need, cudaMemcpyDeviceToHost, h->stream));
+    if (tmp) CK(cudaFreeAsync(tmp, h->stream));
+    return sync(h);
+}
+
+int sgc_upload(sgc_handle* h, int what, const void* src, uint64_t bytes) {
+    if (!h || !src) return fail(SGC_EINVAL, "null argument");
+    CK(cudaSetDevice(h->device));
+    void* dst = nullptr;
+    uint64_t need = 0;
+    switch (what) {
+        case SGC_DL_STATES: dst = h->g.st; need = h->n * 4ull; break;
+        case SGC_DL_BITMAPS: dst = h->g.bm; need = h->n * 8ull; break;
+        case SGC_DL_HIST: dst = h->g.hist; need = (uint64_t)h->num_hd * h->maxc * 4; break;
+        default: return fail(SGC_EINVAL, "upload target %d not writable", what);
+    }
+    if (bytes != need) return fail(SGC_EINVAL, "upload target %d needs exactly %llu bytes", what, (unsigned long long)need);
+    CK(cudaMemcpyAsync(dst, src, need, cudaMemcpyHostToDevice, h->stream));
+    return sync(h);
+}
+
+int sgc_find_color(sgc_handle* h, uint32_t x, uint16_t* color) {
+    if (!h || !color) return fail(SGC_EINVAL, "null argument");
+    if (x >= h->n) return fail(SGC_EINVAL, "vertex %u out of range", x);
+    CK(cudaSetDevice(h->device));
+    uint16_t* d = nullptr;
+    CK(cudaMallocAsync(&d, 2, h->stream));
+    find_color_kernel<<<1, 32, 0, h->stream>>>(h->g, x, d);
+    CK(cudaMemcpyAsync(color, d, 2, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaFreeAsync(d, h->stream));
+    return sync(h);
+}
+
+int sgc_validate(sgc_handle* h, sgc_validation* out) {
+    if (!h || !out) return fail(SGC_EINVAL, "null argument");
+    CK(cudaSetDevice(h->device));
+    uint64_t v[5] = {0, 0, 0, 0, 0};
+    const int r = run_validate(h->g, h->stream, v);
+    if (r < 0) return fail(SGC_ECUDA, "validator failed (%d)", r);
+    out->violations = v[0];
+    out->uncolored_with_edges = v[1];
+    out->edges = v[2];
+    out->max_color = v[3];
+    out->out_of_range = v[4];
+    return SGC_OK;
+}
+
+int sgc_get_stats(sgc_handle* h, sgc_stats* o) {
+    if (!h || !o) return fail(SGC_EINVAL, "null argument");
+    CK(cudaSetDevice(h->device));
+    Ctl c;
+    CK(cudaMemcpyAsync(&c, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+    TRY(sync(h));
+    std::memset(o, 0, sizeof(*o));
+    o->updates_submitted = h->updates;
+    o->updates_skipped = c.nskip;
+    o->epochs = h->epochs;
+    o->overflow_pending = c.ovf_count;
+    o->overflow_lost = c.ovf_lost;
+    o->drain_failed = c.drain_failed;
+    o->tier1_sweeps = h->tier1_sweeps;
+    o->tier2_runs = h->tier2_runs;
+    o->tier2_fixed = h->tier2_fixed;
+    o->device_error = c.err;
+    o->num_vertices = h->n;
+    o->num_high_degree = h->num_hd;
+    o->max_hist_colors = h->maxc;
+    o->total_slots = h->total_slots;
+    o->device_bytes = h->device_bytes;
+    o->sweep_ms = h->sweep_ms;
+    o->sweep_count = h->sweep_count;
+    o->sweep_bytes = h->sweep_bytes;
+    o->live_entries = h->live_entries;
+    return c.err ? fail(SGC_EDEVICE, "device error word 0x%x", c.err) : SGC_OK;
+}
+
+int sgc_synchronize(sgc_handle* h) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    CK(cudaSetDevice(h->device));
+    return sync(h);
+}
+
+void* sgc_cuda_stream(sgc_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+const char* sgc_last_error(void) { return g_err.c_str(); }
+
+const char* sgc_version(void) { return "streamgc_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

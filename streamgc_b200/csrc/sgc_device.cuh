@@ -1,0 +1,448 @@
+// sgc_device.cuh -- warp-cooperative device primitives of the streaming
+// coloring path (sm_100a).
+//
+// Semantics follow the reference's single-GPU path operation for operation:
+//   row insert / delete          algorithms/streamgc/src/kernels/local_update.cu:12-56
+//   FindAvailableColor           algorithms/streamgc/include/color_select.cuh:10-115
+//   neighbor bitmap / histogram  algorithms/streamgc/include/color_select.cuh:120-209
+//   recolor / color reduction    algorithms/streamgc/src/kernels/recolor.cu:49-163
+//   ADD / DEL sequence           algorithms/streamgc/src/kernels/local_update.cu:61-147
+// What changes is how each step maps onto the hardware: a whole warp scans a
+// row with 16-byte loads (128 slots per warp-load, 2 in flight per lane) and a
+// ballot picks the first candidate slot; color selection over a 1024-bin
+// histogram row is a warp-wide load + ballot + min-reduction; the neighbor
+// walk after a recolor spreads its bitmap/histogram atomics over 32 lanes.
+// The per-vertex (color, version) word only changes through atomicCAS, so the
+// same code is exact when one warp applies updates in stream order and safe
+// when many warps apply a batch concurrently.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/streamgc_types.h"
+
+namespace sgc {
+
+constexpr uint32_t INV = SGC_CSR_INVALID;
+constexpr uint32_t EMPTY = SGC_HASH_EMPTY;
+constexpr uint32_t FULL = 0xFFFFFFFFu;
+constexpr uint32_t OVF_CAP = SGC_OVERFLOW_CAPACITY;
+
+// Error bits written to the handle's device error word.
+enum : uint32_t {
+    ERR_WAIT_TIMEOUT = 1u << 0,   // a same-edge predecessor wait ran out
+    ERR_BAD_UPDATE = 1u << 1,     // update endpoint outside [0, n)
+    ERR_LIST_OVERFLOW = 1u << 2,  // a work list exceeded its capacity
+};
+
+// Device view of one graph's state (handle layout). Row x owns logical slots
+// [rp[x], rp[x+1]); hw[x] bounds the slots ever written since the row was last
+// compacted (every slot at or past rp[x]+hw[x] holds INV), so after compaction
+// the row's live entries are exactly [rp[x], rp[x]+hw[x]).
+struct Dev {
+    uint32_t n;
+    uint32_t maxc;                 // histogram colors per row (multiple of 4)
+    const uint64_t* rp;            // n+1 row starts (64-bit: slabs beyond 2^32 slots)
+    uint32_t* col;                 // slots, padded so 16-byte loads never leave the allocation
+    uint32_t* st;                  // packed (color | version << 16)
+    uint64_t* bm;                  // neighbor color bitmaps
+    const uint32_t* hdmap;         // vertex -> histogram row, EMPTY for bitmap mode
+    uint32_t* hist;                // num_hd * maxc counters
+    const uint32_t* deg;           // frozen initial degree: priority = (deg << 32) | id
+    uint32_t* hw;                  // per-row high-water mark (slots, relative to rp[x])
+    uint32_t* dirty;               // bitmask of rows edited since their last compaction
+    uint32_t* edited;              // bitmask of rows edited since creation (clear = pristine:
+                                   // base entries sorted ascending in [rp, rp+hw), INV after)
+    OverflowEdge* ovf;             // OVF_CAP entries
+    uint32_t* ovf_count;           // counts every overflow, stored or not
+    unsigned long long* ovf_lost;  // overflows beyond OVF_CAP (edge dropped, as the reference does)
+    unsigned long long* nskip;     // updates skipped: an endpoint outside [0, n) (hash miss)
+    uint32_t* err;
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint16_t color_of(uint32_t w) { return (uint16_t)(w & 0xFFFFu); }
+__device__ __forceinline__ uint16_t version_of(uint32_t w) { return (uint16_t)(w >> 16); }
+__device__ __forceinline__ uint32_t pack(uint16_t c, uint16_t v) { return ((uint32_t)v << 16) | c; }
+
+// priority(a) < priority(b) for priority = (deg << 32) | id (priority.cuh:8-23)
+__device__ __forceinline__ bool prio_less(uint32_t da, uint32_t a, uint32_t db, uint32_t b) {
+    return (da < db) || (da == db && a < b);
+}
+
+// Coherent (L1-bypassing) loads for words other warps may be changing.
+__device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
+__device__ __forceinline__ uint64_t ld_cg(const uint64_t* p) { return __ldcg((const unsigned long long*)p); }
+__device__ __forceinline__ uint4 ld_cg4(const uint32_t* p) { return __ldcg(reinterpret_cast<const uint4*>(p)); }
+
+__device__ __forceinline__ uint32_t pick4(const uint4& q, int k) {
+    return k == 0 ? q.x : (k == 1 ? q.y : (k == 2 ? q.z : q.w));
+}
+
+// Bit k of the result is set when slot i+k lies in [s, e) and pred(slot).
+template <class P>
+__device__ __forceinline__ uint32_t mask4(const uint4& q, uint64_t i, uint64_t s, uint64_t e, P pred) {
+    uint32_t m = 0;
+    m |= (i + 0 >= s && i + 0 < e && pred(q.x)) ? 1u : 0u;
+    m |= (i + 1 >= s && i + 1 < e && pred(q.y)) ? 2u : 0u;
+    m |= (i + 2 >= s && i + 2 < e && pred(q.z)) ? 4u : 0u;
+    m |= (i + 3 >= s && i + 3 < e && pred(q.w)) ? 8u : 0u;
+    return m;
+}
+
+// Warp-collective: first slot index p in [s, e) whose value satisfies pred,
+// scanning in slot order exactly like the reference's serial loop. Loads are
+// 16-byte aligned (col must be 16-byte aligned and padded past the last row
+// to a multiple of 4 slots). Returns false when no slot matches.
+template <class P>
+__device__ __forceinline__ bool warp_find(const uint32_t* col, uint64_t s, uint64_t e, P pred,
+                                          uint64_t& pos, uint32_t& val) {
+    const uint32_t lane = lane_id();
+    for (uint64_t c = s & ~3ull; c < e; c += 256) {
+        const uint64_t i0 = c + 4ull * lane, i1 = i0 + 128;
+        uint4 a = make_uint4(INV, INV, INV, INV), b = a;
+        if (i0 < e) a = ld_cg4(col + i0);
+        if (i1 < e) b = ld_cg4(col + i1);
+        const uint32_t ma = mask4(a, i0, s, e, pred);
+        const uint32_t mb = mask4(b, i1, s, e, pred);
+        const uint32_t ba = __ballot_sync(FULL, ma != 0);
+        if (ba) {
+            const int src = __ffs(ba) - 1;
+            const int k = __ffs(ma) - 1;
+            const uint32_t v = ma ? pick4(a, k) : 0u;
+            const int ks = __shfl_sync(FULL, k, src);
+            val = __shfl_sync(FULL, v, src);
+            pos = c + 4ull * src + ks;
+            return true;
+        }
+        const uint32_t bb = __ballot_sync(FULL, mb != 0);
+        if (bb) {
+            const int src = __ffs(bb) - 1;
+            const int k = __ffs(mb) - 1;
+            const uint32_t v = mb ? pick4(b, k) : 0u;
+            const int ks = __shfl_sync(FULL, k, src);
+            val = __shfl_sync(FULL, v, src);
+            pos = c + 128 + 4ull * src + ks;
+            return true;
+        }
+    }
+    return false;
+}
+
+// Warp-collective visit of every slot in [s, e): f(slot_index, value) runs on
+// the lane that loaded the slot (each slot once).
+template <class F>
+__device__ __forceinline__ void warp_for_each(const uint32_t* col, uint64_t s, uint64_t e, F f) {
+    const uint32_t lane = lane_id();
+    for (uint64_t c = s & ~3ull; c < e; c += 128) {
+        const uint64_t i = c + 4ull * lane;
+        if (i < e) {
+            const uint4 q = ld_cg4(col + i);
+            if (i + 0 >= s) f(i + 0, q.x);
+            if (i + 1 >= s && i + 1 < e) f(i + 1, q.y);
+            if (i + 2 >= s && i + 2 < e) f(i + 2, q.z);
+            if (i + 3 >= s && i + 3 < e) f(i + 3, q.w);
+        }
+    }
+}
+
+__device__ __forceinline__ void mark_dirty(const Dev& g, uint32_t x) {
+    atomicOr(g.dirty + (x >> 5), 1u << (x & 31));
+    if (!(ld_cg(g.edited + (x >> 5)) & (1u << (x & 31)))) atomicOr(g.edited + (x >> 5), 1u << (x & 31));
+}
+__device__ __forceinline__ bool pristine(const Dev& g, uint32_t x) {
+    return !(ld_cg(g.edited + (x >> 5)) & (1u << (x & 31)));
+}
+
+// Warp-collective 32-ary search for `key` in the ascending run col[s, e):
+// each round probes 32 evenly spaced slots and keeps the bucket holding the
+// last probe <= key. Returns the slot index, or ~0 when key is absent.
+__device__ __forceinline__ uint64_t warp_bsearch(const uint32_t* col, uint64_t s, uint64_t e, uint32_t key) {
+    const uint32_t lane = lane_id();
+    uint64_t lo = s, hi = e;
+    while (hi - lo > 32) {
+        const uint64_t step = (hi - lo) / 32;
+        const uint32_t v = ld_cg(col + lo + lane * step);
+        const uint32_t b = __ballot_sync(FULL, v <= key);
+        if (!b) return ~0ull;
+        const uint32_t L = 31 - __clz(b);
+        const uint64_t nlo = lo + L * step;
+        hi = (L == 31) ? hi : nlo + step;
+        lo = nlo;
+    }
+    const uint64_t i = lo + lane;
+    const bool hit = i < hi && ld_cg(col + i) == key;
+    const uint32_t b = __ballot_sync(FULL, hit);
+    return b ? lo + (__ffs(b) - 1) : ~0ull;
+}
+
+// ---------------- slack-CSR row edits (local_update.cu:12-56) ----------------
+
+enum { ADD_INSERTED = 0, ADD_PRESENT = 1, ADD_OVERFLOW = 2 };
+
+// add_local_neighbor: claim the first INV slot unless `nbr` shows up first;
+// a full row appends to the overflow buffer (counter always advances, entry
+// stored only below capacity).
+__device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t nbr, bool exact) {
+    const uint64_t s = g.rp[x], e = g.rp[x + 1];
+    uint64_t from = s;
+    if (pristine(g, x)) {
+        // Sorted base entries, no holes: the scan would stop at nbr if present,
+        // else at the first INV right after the base run.
+        const uint64_t len = ld_cg(g.hw + x);
+        if (warp_bsearch(g.col, s, s + len, nbr) != ~0ull) return ADD_PRESENT;
+        if (exact) from = s + len;  // one warp in stream order: the row cannot change under us
+    }
+    for (;;) {
+        uint64_t p = 0;
+        uint32_t v = 0;
+        const bool hit = warp_find(g.col, from, e, [nbr](uint32_t t) { return t == INV || t == nbr; }, p, v);
+        if (!hit) {
+            if (lane_id() == 0) {
+                const uint32_t pos = atomicAdd(g.ovf_count, 1u);
+                if (pos < OVF_CAP) {
+                    g.ovf[pos].local_vertex_idx = x;
+                    g.ovf[pos].neighbor_global = nbr;
+                } else {
+                    atomicAdd(g.ovf_lost, 1ull);
+                }
+            }
+            __syncwarp();
+            return ADD_OVERFLOW;
+        }
+        if (v == nbr) return ADD_PRESENT;
+        uint32_t old = 0;
+        if (lane_id() == 0) {
+            old = atomicCAS(g.col + p, INV, nbr);
+            if (old == INV) {
+                atomicMax(g.hw + x, (uint32_t)(p - s + 1));
+                mark_dirty(g, x);
+            }
+        }
+        old = __shfl_sync(FULL, old, 0);
+        if (old == INV) return ADD_INSERTED;
+        if (old == nbr) return ADD_PRESENT;
+        from = p + 1;  // lost the slot to a concurrent insert: keep scanning after it
+    }
+}
+
+// remove_local_neighbor: first slot equal to nbr becomes INV (lazy delete).
+__device__ __forceinline__ void warp_remove_slot(const Dev& g, uint32_t x, uint32_t nbr, bool exact) {
+    const uint64_t s = g.rp[x];
+    const uint64_t e = s + ld_cg(g.hw + x);
+    uint64_t from = s;
+    if (pristine(g, x)) {
+        const uint64_t p = warp_bsearch(g.col, s, e, nbr);
+        if (p != ~0ull) {
+            uint32_t old = 0;
+            if (lane_id() == 0) {
+                old = atomicCAS(g.col + p, nbr, INV);
+                if (old == nbr) mark_dirty(g, x);
+            }
+            old = __shfl_sync(FULL, old, 0);
+            if (old == nbr) return;
+        } else if (exact) {
+            return;  // absent from the sorted run and nothing after it
+        }
+    }
+    for (;;) {
+        uint64_t p = 0;
+        uint32_t v = 0;
+        if (!warp_find(g.col, from, e, [nbr](uint32_t t) { return t == nbr; }, p, v)) return;
+        uint32_t old = 0;
+        if (lane_id() == 0) {
+            old = atomicCAS(g.col + p, nbr, INV);
+            if (old == nbr) mark_dirty(g, x);
+        }
+        old = __shfl_sync(FULL, old, 0);
+        if (old == nbr) return;
+        from = p + 1;
+    }
+}
+
+// ---------------- color selection (color_select.cuh:10-115) ----------------
+
+// Histogram mode: first zero counter -> its color; else the first minimum.
+// Whole row (maxc counters) is loaded warp-wide, 16 bytes per lane per step.
+__device__ __forceinline__ uint16_t warp_fac_hist(const uint32_t* h, uint32_t maxc) {
+    const uint32_t lane = lane_id();
+    uint32_t best_v = FULL, best_i = FULL;  // lane-local first minimum
+    for (uint32_t base = 0; base < maxc; base += 128) {
+        const uint32_t i = base + 4 * lane;
+        uint4 q = make_uint4(FULL, FULL, FULL, FULL);
+        const bool ok = i < maxc;
+        if (ok) q = ld_cg4(h + i);
+        uint32_t zm = 0;
+        if (ok) zm = (q.x == 0 ? 1u : 0u) | (q.y == 0 ? 2u : 0u) | (q.z == 0 ? 4u : 0u) | (q.w == 0 ? 8u : 0u);
+        const uint32_t bz = __ballot_sync(FULL, zm != 0);
+        if (bz) {
+            const int src = __ffs(bz) - 1;
+            const int k = __shfl_sync(FULL, __ffs(zm) - 1, src);
+            return (uint16_t)(base + 4 * src + k + 1);
+        }
+        if (ok) {
+            if (q.x < best_v) { best_v = q.x; best_i = i; }
+            if (q.y < best_v) { best_v = q.y; best_i = i + 1; }
+            if (q.z < best_v) { best_v = q.z; best_i = i + 2; }
+            if (q.w < best_v) { best_v = q.w; best_i = i + 3; }
+        }
+    }
+    // First minimum over the whole row: smallest value, ties to the smallest index.
+    for (int off = 16; off > 0; off >>= 1) {
+        const uint32_t ov = __shfl_xor_sync(FULL, best_v, off);
+        const uint32_t oi = __shfl_xor_sync(FULL, best_i, off);
+        if (ov < best_v || (ov == best_v && oi < best_i)) { best_v = ov; best_i = oi; }
+    }
+    return (uint16_t)(best_i + 1);
+}
+
+// Bitmap mode fallback when all 64 bits are set: first color in 1..255 no live
+// neighbor holds (reading neighbor colors from `cols`), else 256.
+__device__ __forceinline__ uint16_t warp_fac_scan(const Dev& g, uint32_t x, const uint32_t* cols) {
+    const uint64_t s = g.rp[x], e = s + ld_cg(g.hw + x);
+    uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    warp_for_each(g.col, s, e, [&](uint64_t, uint32_t ng) {
+        if (ng == INV || ng >= g.n) return;
+        const uint16_t c = color_of(ld_cg(cols + ng));
+        if (c > 0 && c < 256) {
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if ((c >> 5) == k) w[k] |= 1u << (c & 31);
+        }
+    });
+#pragma unroll
+    for (int k = 0; k < 8; k++) w[k] = __reduce_or_sync(FULL, w[k]);
+    w[0] |= 1u;  // color 0 is never a candidate
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+        if (~w[k]) return (uint16_t)(k * 32 + __ffs(~w[k]) - 1);
+    return 256;
+}
+
+// FindAvailableColor: histogram row when the vertex has one, else bitmap.
+__device__ __forceinline__ uint16_t warp_fac(const Dev& g, uint32_t x, const uint32_t* cols) {
+    const uint32_t hd = __ldg(g.hdmap + x);
+    if (hd != EMPTY) return warp_fac_hist(g.hist + (uint64_t)hd * g.maxc, g.maxc);
+    const uint64_t bmv = ld_cg(g.bm + x);
+    if (~bmv) return (uint16_t)__ffsll((long long)~bmv);
+    return warp_fac_scan(g, x, cols);
+}
+
+// ---------------- incremental bitmap / histogram (color_select.cuh:120-209) ----------------
+
+__device__ __forceinline__ void nbr_color_change(const Dev& g, uint32_t x, uint16_t oldc, uint16_t newc) {
+    if (oldc == newc) return;
+    if (newc != 0 && newc <= 64) atomicOr((unsigned long long*)(g.bm + x), 1ull << (newc - 1));
+    const uint32_t hd = __ldg(g.hdmap + x);
+    if (hd != EMPTY) {
+        uint32_t* h = g.hist + (uint64_t)hd * g.maxc;
+        if (oldc != 0 && oldc <= g.maxc) atomicSub(h + oldc - 1, 1u);
+        if (newc != 0 && newc <= g.maxc) atomicAdd(h + newc - 1, 1u);
+    }
+}
+__device__ __forceinline__ void new_nbr(const Dev& g, uint32_t x, uint16_t c) {
+    if (c == 0) return;
+    if (c <= 64) atomicOr((unsigned long long*)(g.bm + x), 1ull << (c - 1));
+    const uint32_t hd = __ldg(g.hdmap + x);
+    if (hd != EMPTY && c <= g.maxc) atomicAdd(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
+}
+__device__ __forceinline__ void removed_nbr(const Dev& g, uint32_t x, uint16_t c) {
+    if (c == 0) return;
+    const uint32_t hd = __ldg(g.hdmap + x);
+    if (hd != EMPTY && c <= g.maxc) atomicSub(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
+}
+
+// ---------------- recolor (recolor.cu:87-163) ----------------
+
+__device__ __forceinline__ uint32_t warp_load_state(const Dev& g, uint32_t x) {
+    uint32_t w = 0;
+    if (lane_id() == 0) w = ld_cg(g.st + x);
+    return __shfl_sync(FULL, w, 0);
+}
+
+// recolor_vertex: new = FAC(x); if different, CAS (new, version+1) in, retrying
+// on a fresh word; the winner propagates old -> new to every live row entry.
+__device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x) {
+    uint32_t cur = warp_load_state(g, x);
+    uint16_t newc = warp_fac(g, x, g.st);
+    if (newc == color_of(cur)) return;
+    for (;;) {
+        const uint32_t want = pack(newc, (uint16_t)(version_of(cur) + 1));
+        uint32_t got = 0;
+        if (lane_id() == 0) got = atomicCAS(g.st + x, cur, want);
+        got = __shfl_sync(FULL, got, 0);
+        if (got == cur) break;
+        cur = got;
+        newc = warp_fac(g, x, g.st);
+        if (newc == color_of(cur)) return;
+    }
+    const uint16_t oldc = color_of(cur);
+    const uint64_t s = g.rp[x], e = s + ld_cg(g.hw + x);
+    warp_for_each(g.col, s, e, [&](uint64_t, uint32_t ng) {
+        if (ng == INV || ng >= g.n) return;
+        nbr_color_change(g, ng, oldc, newc);
+    });
+    __syncwarp();
+}
+
+// try_color_reduction: after a delete freed `freed`, move to a lower color if one is open.
+__device__ __forceinline__ void warp_try_reduce(const Dev& g, uint32_t x, uint16_t freed) {
+    const uint16_t cur = color_of(warp_load_state(g, x));
+    if (cur == 0) return;
+    if (freed >= cur) return;
+    const uint16_t best = warp_fac(g, x, g.st);
+    if (best < cur) warp_recolor(g, x);
+}
+
+// Colors x with FAC when it is still uncolored; version becomes 1
+// (local_update.cu:90-101). Returns the color x holds afterwards.
+__device__ __forceinline__ void warp_color_if_uncolored(const Dev& g, uint32_t x) {
+    const uint32_t cur = warp_load_state(g, x);
+    if (color_of(cur) != 0) return;
+    const uint16_t c = warp_fac(g, x, g.st);
+    if (lane_id() == 0) atomicCAS(g.st + x, cur, pack(c, 1));
+    __syncwarp();
+}
+
+// ---------------- one update (local_update.cu:61-147) ----------------
+
+// `exact`: the caller is the only warp touching the graph (stream order), so a
+// pristine row's binary-search answer is final; concurrent callers fall back
+// to the linear scan whenever the search does not find the key.
+__device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v, uint8_t type, bool exact) {
+    if (type == SGC_UPDATE_ADD) {
+        warp_add_slot(g, u, v, exact);
+        warp_add_slot(g, v, u, exact);
+        warp_color_if_uncolored(g, u);
+        if (color_of(warp_load_state(g, v)) == 0) {
+            if (lane_id() == 0) new_nbr(g, v, color_of(ld_cg(g.st + u)));
+            __syncwarp();
+            warp_color_if_uncolored(g, v);
+        }
+        if (lane_id() == 0) {
+            new_nbr(g, u, color_of(ld_cg(g.st + v)));
+            new_nbr(g, v, color_of(ld_cg(g.st + u)));
+        }
+        __syncwarp();
+        const uint16_t cu = color_of(warp_load_state(g, u));
+        const uint16_t cv = color_of(warp_load_state(g, v));
+        if (cu == cv && cu != 0) {
+            const uint32_t loser = prio_less(__ldg(g.deg + u), u, __ldg(g.deg + v), v) ? u : v;
+            warp_recolor(g, loser);
+        }
+    } else if (type == SGC_UPDATE_DEL) {
+        const uint16_t fu = color_of(warp_load_state(g, v));
+        const uint16_t fv = color_of(warp_load_state(g, u));
+        warp_remove_slot(g, u, v, exact);
+        warp_remove_slot(g, v, u, exact);
+        if (lane_id() == 0) {
+            removed_nbr(g, u, fu);
+            removed_nbr(g, v, fv);
+        }
+        __syncwarp();
+        warp_try_reduce(g, u, fu);
+        warp_try_reduce(g, v, fv);
+    }
+}
+
+}  // namespace sgc

@@ -1,0 +1,549 @@
+// sgc_kernels.cu -- kernels of the handle API (sm_100a).
+//
+//   det_apply_kernel      one warp applies a batch in stream order: the
+//                         reference's local_update_kernel run as a single warp
+//                         (local_update.cu:61-147), bit-exact.
+//   conc_*                a batch applied by one warp per update. A hash pre-pass
+//                         links each update to the previous update of the same
+//                         edge in the batch, and the persistent apply kernel hands
+//                         out updates in stream order and waits (bounded) for
+//                         that predecessor, so every edge sees its own updates in
+//                         stream order and the edge set after a batch equals the
+//                         sequential one; updates of different edges overlap.
+//   dirty list + compact  stable per-row compaction (epoch_maintenance.cu:20-61)
+//                         of only the rows edited since their last compaction
+//                         (every other row is already compact, so compacting it
+//                         is the identity); reads each row up to its high-water.
+//   take_overflow/drain   streamgc.cu:967-995 + epoch_maintenance.cu:66-87.
+//   sweep                 degree-balanced pass over every live adjacency entry:
+//                         rebuild_bitmaps (epoch_maintenance.cu:113-128) and the
+//                         Tier-1 decision (conflict_repair.cu:10-114) fused, as a
+//                         Jacobi sweep (every decision reads start-of-sweep
+//                         colors; new words are committed after the sweep).
+#include <cuda_runtime.h>
+#include <cuda/atomic>
+
+#include "sgc_kernels.cuh"
+
+namespace sgc {
+
+// ---------------------------------------------------------------------------
+// warp helpers
+// ---------------------------------------------------------------------------
+
+// One atomicAdd per warp; returns this lane's slot when pred, else NONE32.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* count, bool pred) {
+    const uint32_t m = __ballot_sync(FULL, pred);
+    if (!m) return NONE32;
+    const uint32_t lane = lane_id();
+    const int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+    base = __shfl_sync(FULL, base, leader);
+    return pred ? base + __popc(m & ((1u << lane) - 1)) : NONE32;
+}
+
+// Exclusive warp prefix sum.
+__device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t& total) {
+    const uint32_t lane = lane_id();
+    uint32_t x = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, x, off);
+        if (lane >= (uint32_t)off) x += y;
+    }
+    total = __shfl_sync(FULL, x, 31);
+    return x - v;
+}
+
+// ---------------------------------------------------------------------------
+// update kernels
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(32) det_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n) {
+    for (uint32_t i = 0; i < n; i++) {
+        const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
+        const uint32_t u = r.x, v = r.y;
+        const uint8_t type = (uint8_t)(r.z & 0xFFu);
+        if (u >= g.n || v >= g.n) {
+            if (lane_id() == 0) atomicAdd(g.nskip, 1ull);
+            continue;  // get_owned_index miss: the reference skips the update
+        }
+        warp_apply(g, u, v, type, true);
+    }
+}
+
+__device__ __forceinline__ unsigned long long edge_key(uint32_t u, uint32_t v) {
+    const uint32_t a = u < v ? u : v, b = u < v ? v : u;
+    return ((unsigned long long)a << 32) | b;
+}
+__device__ __forceinline__ uint32_t key_hash(unsigned long long k) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return (uint32_t)k;
+}
+
+__global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n, EdgeOrder eo) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *eo.ticket = 0;
+    if (i >= n) return;
+    const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
+    const uint32_t u = r.x, v = r.y;
+    const uint8_t type = (uint8_t)(r.z & 0xFFu);
+    if ((type != SGC_UPDATE_ADD && type != SGC_UPDATE_DEL) || u >= g.n || v >= g.n) {
+        eo.tslot[i] = NONE32;
+        return;
+    }
+    const unsigned long long key = edge_key(u, v);
+    uint32_t h = key_hash(key) & eo.tmask;
+    for (uint32_t probe = 0; probe <= eo.tmask; probe++) {
+        const unsigned long long k = atomicCAS(eo.tkey + h, EMPTY64, key);
+        if (k == EMPTY64 || k == key) break;
+        h = (h + 1) & eo.tmask;
+    }
+    eo.tslot[i] = h;
+    eo.tnext[i] = atomicExch(eo.thead + h, i);
+}
+
+__global__ void conc_prep_prev(uint32_t n, EdgeOrder eo) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t h = eo.tslot[i];
+    uint32_t best = NONE32;
+    if (h != NONE32) {
+        for (uint32_t j = eo.thead[h]; j != NONE32; j = eo.tnext[j])
+            if (j < i && (best == NONE32 || j > best)) best = j;
+    }
+    eo.tprev[i] = best;
+}
+
+// Bounded wait for the same-edge predecessor: ~2^22 polls with a sleep, then
+// the error word records a timeout and the update proceeds.
+__device__ __forceinline__ void wait_done(const EdgeOrder& eo, const Dev& g, uint32_t p, uint32_t seq) {
+    if (lane_id() == 0) {
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> d(eo.done[p]);
+        uint32_t polls = 0;
+        while (d.load(cuda::memory_order_acquire) != seq) {
+            if (++polls > (1u << 22)) {
+                atomicOr(g.err, ERR_WAIT_TIMEOUT);
+                break;
+            }
+            __nanosleep(64);
+        }
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(256) conc_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n,
+                                                         EdgeOrder eo, uint32_t seq) {
+    for (;;) {
+        uint32_t i = 0;
+        if (lane_id() == 0) i = atomicAdd(eo.ticket, 1u);
+        i = __shfl_sync(FULL, i, 0);
+        if (i >= n) break;
+        const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
+        const uint32_t u = r.x, v = r.y;
+        const uint8_t type = (uint8_t)(r.z & 0xFFu);
+        const uint32_t h = eo.tslot[i];
+        if (h == NONE32) {
+            if ((u >= g.n || v >= g.n) && lane_id() == 0) atomicAdd(g.nskip, 1ull);
+        } else {
+            const uint32_t p = eo.tprev[i];
+            if (p != NONE32) wait_done(eo, g, p, seq);
+            warp_apply(g, u, v, type, false);
+        }
+        if (lane_id() == 0) {
+            if (h != NONE32) {  // no kernel reads the table during apply: reset it for the next batch
+                eo.tkey[h] = EMPTY64;
+                eo.thead[h] = NONE32;
+            }
+            __threadfence();
+            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> d(eo.done[i]);
+            d.store(seq, cuda::memory_order_release);
+        }
+        __syncwarp();
+    }
+}
+
+void launch_det_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, cudaStream_t s) {
+    if (n) det_apply_kernel<<<1, 32, 0, s>>>(g, ups, n);
+}
+
+void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const EdgeOrder& eo, uint32_t seq,
+                       int num_sms, cudaStream_t s) {
+    if (!n) return;
+    const uint32_t blk = (n + 255) / 256;
+    conc_prep_insert<<<blk, 256, 0, s>>>(g, ups, n, eo);
+    conc_prep_prev<<<blk, 256, 0, s>>>(n, eo);
+    static int occ = 0;
+    if (!occ) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, conc_apply_kernel, 256, 0);
+        if (occ < 1) occ = 1;
+    }
+    uint32_t grid = (uint32_t)(num_sms * occ);
+    const uint32_t need = (n + 7) / 8;  // 8 warps per block
+    if (grid > need) grid = need;
+    conc_apply_kernel<<<grid, 256, 0, s>>>(g, ups, n, eo, seq);
+}
+
+// ---------------------------------------------------------------------------
+// compaction of edited rows
+// ---------------------------------------------------------------------------
+
+__global__ void dirty_list_kernel(Dev g, uint32_t* list, uint32_t* count) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nw = (g.n + 31) / 32;
+    uint32_t bits = 0;
+    if (w < nw) {
+        bits = g.dirty[w];
+        if (bits) g.dirty[w] = 0;
+    }
+    uint32_t total = 0;
+    const uint32_t off = warp_excl_scan(__popc(bits), total);
+    uint32_t base = 0;
+    if (lane_id() == 0 && total) base = atomicAdd(count, total);
+    base = __shfl_sync(FULL, base, 0);
+    uint32_t k = base + off;
+    while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        list[k++] = w * 32 + b;
+    }
+}
+
+void launch_dirty_list(const Dev& g, uint32_t* list, uint32_t* count, cudaStream_t s) {
+    const uint32_t nw = (g.n + 31) / 32;
+    dirty_list_kernel<<<(nw + 255) / 256, 256, 0, s>>>(g, list, count);
+}
+
+// Warp per edited row: stable in-place compaction of [rp, rp + hw), INV tail,
+// hw = live count.
+__global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __restrict__ list,
+                                                      const uint32_t* __restrict__ count) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = lane_id();
+    const uint32_t cnt = *count;
+    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
+        const uint32_t x = list[k];
+        const uint64_t s = g.rp[x];
+        const uint64_t e = s + g.hw[x];
+        uint64_t w = s;
+        for (uint64_t c = s & ~3ull; c < e; c += 128) {
+            const uint64_t i = c + 4ull * lane;
+            uint4 q = make_uint4(INV, INV, INV, INV);
+            if (i < e) q = ld_cg4(g.col + i);
+            uint32_t vals[4] = {q.x, q.y, q.z, q.w};
+            uint32_t m = 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (i + j >= s && i + j < e && vals[j] != INV) m |= 1u << j;
+            uint32_t total = 0;
+            const uint32_t pre = warp_excl_scan(__popc(m), total);
+            __syncwarp();
+            uint64_t dst = w + pre;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (m & (1u << j)) {
+                    if (dst != i + j) g.col[dst] = vals[j];
+                    dst++;
+                }
+            w += total;
+            __syncwarp();
+        }
+        for (uint64_t j = w + lane; j < e; j += 32) g.col[j] = INV;
+        if (lane == 0) g.hw[x] = (uint32_t)(w - s);
+        __syncwarp();
+    }
+}
+
+void launch_compact(const Dev& g, const uint32_t* list, const uint32_t* count, uint32_t max_rows, cudaStream_t s) {
+    if (!max_rows) return;
+    uint32_t blocks = (max_rows + 7) / 8;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    compact_kernel<<<blocks, 256, 0, s>>>(g, list, count);
+}
+
+// ---------------------------------------------------------------------------
+// overflow drain (streamgc.cu:967-995, epoch_maintenance.cu:66-87)
+// ---------------------------------------------------------------------------
+
+__global__ void take_overflow_kernel(Dev g, uint32_t* drain_n) {
+    const uint32_t c = *g.ovf_count;
+    if (c) *g.ovf_count = 0;
+    *drain_n = c < OVF_CAP ? c : OVF_CAP;
+}
+void launch_take_overflow(const Dev& g, uint32_t* drain_n, cudaStream_t s) {
+    take_overflow_kernel<<<1, 1, 0, s>>>(g, drain_n);
+}
+
+// Re-insert without re-appending: first INV or equal slot; none -> failure.
+__device__ __forceinline__ bool warp_drain_insert(const Dev& g, uint32_t x, uint32_t nbr) {
+    const uint64_t s = g.rp[x], e = g.rp[x + 1];
+    uint64_t from = s;
+    for (;;) {
+        uint64_t p = 0;
+        uint32_t v = 0;
+        if (!warp_find(g.col, from, e, [nbr](uint32_t t) { return t == INV || t == nbr; }, p, v)) return false;
+        if (v == nbr) return true;
+        uint32_t old = 0;
+        if (lane_id() == 0) {
+            old = atomicCAS(g.col + p, INV, nbr);
+            if (old == INV) {
+                atomicMax(g.hw + x, (uint32_t)(p - s + 1));
+                mark_dirty(g, x);
+            }
+        }
+        old = __shfl_sync(FULL, old, 0);
+        if (old == INV || old == nbr) return true;
+        from = p + 1;
+    }
+}
+
+__global__ void drain_kernel(Dev g, const uint32_t* __restrict__ drain_n, int ordered, unsigned long long* failed) {
+    const uint32_t cnt = *drain_n;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t step = ordered ? 1 : warps;
+    if (ordered && w0 != 0) return;
+    for (uint32_t k = w0; k < cnt; k += step) {
+        const OverflowEdge oe = g.ovf[k];
+        const bool ok = warp_drain_insert(g, oe.local_vertex_idx, oe.neighbor_global);
+        if (!ok && lane_id() == 0 && failed) atomicAdd(failed, 1ull);
+    }
+}
+void launch_drain(const Dev& g, const uint32_t* drain_n, bool ordered, unsigned long long* failed, cudaStream_t s) {
+    if (ordered) drain_kernel<<<1, 32, 0, s>>>(g, drain_n, 1, failed);
+    else drain_kernel<<<148 * 4, 256, 0, s>>>(g, drain_n, 0, failed);
+}
+
+// ---------------------------------------------------------------------------
+// snapshot / query / colors
+// ---------------------------------------------------------------------------
+
+__global__ void snapshot_kernel(Dev g, uint16_t* snap) {
+    for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < g.n; x += gridDim.x * blockDim.x)
+        snap[x] = color_of(g.st[x]);
+}
+void launch_snapshot(const Dev& g, uint16_t* snap, cudaStream_t s) {
+    snapshot_kernel<<<(g.n + 255) / 256 < 148 * 16 ? (g.n + 255) / 256 : 148 * 16, 256, 0, s>>>(g, snap);
+}
+void launch_colors(const Dev& g, uint16_t* out, cudaStream_t s) { launch_snapshot(g, out, s); }
+
+__global__ void query_kernel(const uint16_t* __restrict__ snap, uint32_t n, const uint32_t* __restrict__ v,
+                             uint16_t* __restrict__ out, uint32_t k) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < k) {
+        const uint32_t x = v[i];
+        out[i] = x < n ? snap[x] : 0;
+    }
+}
+void launch_query(const uint16_t* snap, uint32_t n, const uint32_t* v, uint16_t* out, uint32_t k, cudaStream_t s) {
+    if (k) query_kernel<<<(k + 255) / 256, 256, 0, s>>>(snap, n, v, out, k);
+}
+
+// ---------------------------------------------------------------------------
+// degree-balanced sweep: rebuild + Tier-1 decision (Jacobi)
+// ---------------------------------------------------------------------------
+
+__global__ void build_items_kernel(Dev g, SweepBufs b) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t k = 0;
+    if (x < g.n) {
+        const uint32_t len = g.hw[x];
+        if (len > SWEEP_TINY) k = (len + SWEEP_CH - 1) / SWEEP_CH;
+    }
+    uint32_t total = 0;
+    const uint32_t off = warp_excl_scan(k, total);
+    uint32_t base = 0;
+    if (lane_id() == 0 && total) base = atomicAdd(b.item_count, total);
+    base = __shfl_sync(FULL, base, 0);
+    if (base + off + k > b.item_cap) {
+        if (k) atomicOr(g.err, ERR_LIST_OVERFLOW);
+        return;
+    }
+    for (uint32_t j = 0; j < k; j++) b.items[base + off + j] = (unsigned long long)x | ((unsigned long long)j << 32);
+}
+void launch_build_items(const Dev& g, const SweepBufs& b, cudaStream_t s) {
+    cudaMemsetAsync(b.item_count, 0, sizeof(uint32_t), s);
+    build_items_kernel<<<(g.n + 255) / 256, 256, 0, s>>>(g, b);
+}
+
+// Ordered-pair hash for the symmetry checksum: the sum over all entries x->y
+// of H(x,y) - H(y,x) is 0 when every entry has its mirror (and otherwise is 0
+// only with probability ~2^-64).
+__device__ __forceinline__ unsigned long long pair_hash(uint32_t x, uint32_t y) {
+    unsigned long long z = ((unsigned long long)x << 32 | y) + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ unsigned long long sym_term(uint32_t x, uint32_t y) {
+    return pair_hash(x, y) - pair_hash(y, x);
+}
+
+// Warp per item: up to SWEEP_CH live entries of one row. Nothing in the graph
+// changes during a sweep, so loads take the read-only path.
+__global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = lane_id();
+    const uint32_t cnt = *b.item_count;
+    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
+        const unsigned long long it = b.items[k];
+        const uint32_t x = (uint32_t)it;
+        const uint32_t j = (uint32_t)(it >> 32);
+        const uint64_t rs = g.rp[x];
+        const uint64_t s = rs + (uint64_t)j * SWEEP_CH;
+        const uint64_t re = rs + g.hw[x];
+        const uint64_t e = s + SWEEP_CH < re ? s + SWEEP_CH : re;
+        const uint16_t myc = color_of(__ldg(g.st + x));
+        const uint32_t mydeg = __ldg(g.deg + x);
+        unsigned long long bits = 0, sym = 0;
+        bool conf = false;
+        for (uint64_t c = s & ~3ull; c < e; c += 128) {
+            const uint64_t i = c + 4ull * lane;
+            if (i < e) {
+                const uint4 q = __ldg(reinterpret_cast<const uint4*>(g.col + i));
+                const uint32_t vals[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int t = 0; t < 4; t++) {
+                    const uint32_t ng = vals[t];
+                    if (i + t < s || i + t >= e || ng >= g.n) continue;
+                    if (ng != x) sym += sym_term(x, ng);
+                    const uint16_t nc = color_of(__ldg(g.st + ng));
+                    if (nc != 0 && nc <= 64) bits |= 1ull << (nc - 1);
+                    if (nc == myc && nc != 0 && !conf && prio_less(mydeg, x, __ldg(g.deg + ng), ng)) conf = true;
+                }
+            }
+        }
+        const uint32_t lo = __reduce_or_sync(FULL, (uint32_t)bits);
+        const uint32_t hi = __reduce_or_sync(FULL, (uint32_t)(bits >> 32));
+        const bool anyc = __any_sync(FULL, conf);
+        for (int off = 16; off > 0; off >>= 1) sym += __shfl_xor_sync(FULL, sym, off);
+        if (lane == 0) {
+            const unsigned long long m = ((unsigned long long)hi << 32) | lo;
+            if (m) atomicOr(b.acc_bm + x, m);
+            if (anyc) atomicOr(b.acc_fl + x, 1u);
+            if (sym) atomicAdd(b.symsum, sym);
+        }
+    }
+}
+
+// Thread per vertex: short rows are swept here directly; long rows read the
+// accumulators. REBUILD writes bitmaps; TIER1 also decides the recolors.
+__global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b, int mode) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    bool fac_needed = false;
+    uint32_t pend_word = 0;
+    bool pend = false;
+    unsigned long long sym = 0, live = 0;
+    if (x < g.n) {
+        const uint32_t len = g.hw[x];
+        const uint32_t hd = __ldg(g.hdmap + x);
+        const uint32_t w = __ldg(g.st + x);
+        const uint16_t myc = color_of(w);
+        unsigned long long bits = 0;
+        bool conf = false;
+        live = len;
+        if (len <= SWEEP_TINY) {
+            const uint64_t s = g.rp[x];
+            const uint32_t mydeg = __ldg(g.deg + x);
+            for (uint32_t t = 0; t < len; t++) {
+                const uint32_t ng = __ldg(g.col + s + t);
+                if (ng >= g.n) continue;
+                if (ng != x) sym += sym_term(x, ng);
+                const uint16_t nc = color_of(__ldg(g.st + ng));
+                if (nc != 0 && nc <= 64) bits |= 1ull << (nc - 1);
+                if (nc == myc && nc != 0 && !conf && prio_less(mydeg, x, __ldg(g.deg + ng), ng)) conf = true;
+            }
+        } else {
+            bits = b.acc_bm[x];
+            conf = b.acc_fl[x] != 0;
+            if (bits) b.acc_bm[x] = 0;
+            if (conf) b.acc_fl[x] = 0;
+        }
+        if (mode == SWEEP_REBUILD) {
+            if (hd == EMPTY) g.bm[x] = bits;
+        } else {
+            bool decide = false;
+            if (myc == 0) {
+                decide = len > 0;  // has_neighbors: any non-INV slot
+            } else if (conf) {
+                decide = true;
+                if (myc <= 64) bits |= 1ull << (myc - 1);
+            }
+            if (hd == EMPTY) {
+                g.bm[x] = bits;
+                if (decide) {
+                    if (~bits) {
+                        pend = true;
+                        pend_word = pack((uint16_t)__ffsll((long long)~bits), (uint16_t)(version_of(w) + 1));
+                    } else {
+                        fac_needed = true;
+                    }
+                }
+            } else if (decide) {
+                if (myc != 0 && myc <= 64) g.bm[x] |= 1ull << (myc - 1);  // own bit on the (unused) bitmap
+                fac_needed = true;
+            }
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        sym += __shfl_xor_sync(FULL, sym, off);
+        live += __shfl_xor_sync(FULL, live, off);
+    }
+    if (lane_id() == 0) {
+        if (sym) atomicAdd(b.symsum, sym);
+        if (live) atomicAdd(b.live, live);
+    }
+    if (mode == SWEEP_TIER1) {
+        const uint32_t pi = warp_append(b.pend_count, pend);
+        if (pend) {
+            b.pend_v[pi] = x;
+            b.pend_w[pi] = pend_word;
+        }
+        const uint32_t fi = warp_append(b.fac_count, fac_needed);
+        if (fac_needed) b.fac_v[fi] = x;
+    }
+}
+
+// Warp per vertex whose new color needs the histogram row or the >64 scan;
+// colors read are the start-of-sweep ones (nothing is committed yet).
+__global__ void __launch_bounds__(256) sweep_fac_kernel(Dev g, SweepBufs b) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t cnt = *b.fac_count;
+    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
+        const uint32_t x = b.fac_v[k];
+        const uint32_t w = ld_cg(g.st + x);
+        const uint16_t c = warp_fac(g, x, g.st);
+        if (lane_id() == 0) {
+            const uint32_t pi = atomicAdd(b.pend_count, 1u);
+            b.pend_v[pi] = x;
+            b.pend_w[pi] = pack(c, (uint16_t)(version_of(w) + 1));
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void sweep_commit_kernel(Dev g, SweepBufs b) {
+    const uint32_t cnt = *b.pend_count;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
+        g.st[b.pend_v[k]] = b.pend_w[k];
+}
+
+void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s) {
+    if (mode == SWEEP_TIER1) {
+        cudaMemsetAsync(b.pend_count, 0, sizeof(uint32_t), s);
+        cudaMemsetAsync(b.fac_count, 0, sizeof(uint32_t), s);
+    }
+    sweep_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b);
+    sweep_finalize_kernel<<<(g.n + 255) / 256, 256, 0, s>>>(g, b, (int)mode);
+    if (mode == SWEEP_TIER1) {
+        sweep_fac_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
+        sweep_commit_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
+    }
+}
+
+}  // namespace sgc

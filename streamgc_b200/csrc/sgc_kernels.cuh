@@ -1,0 +1,87 @@
+// sgc_kernels.cuh -- kernel declarations and launch helpers of the handle API.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sgc_device.cuh"
+
+namespace sgc {
+
+constexpr uint32_t SWEEP_CH = 512;    // slots per warp work item in a sweep
+constexpr uint32_t SWEEP_TINY = 16;   // rows this short are swept by one thread
+constexpr uint32_t NONE32 = 0xFFFFFFFFu;
+constexpr unsigned long long EMPTY64 = 0xFFFFFFFFFFFFFFFFull;
+
+// Per-sweep work state: warp items for rows longer than SWEEP_TINY, per-vertex
+// accumulators, the Jacobi pending list and the FAC work list.
+struct SweepBufs {
+    unsigned long long* items;   // x | chunk << 32
+    uint32_t* item_count;
+    uint32_t item_cap;
+    unsigned long long* acc_bm;  // OR of neighbor colors 1..64, per vertex
+    uint32_t* acc_fl;            // bit0: a same-colored neighbor has higher priority
+    uint32_t* pend_v;            // Jacobi commit list
+    uint32_t* pend_w;
+    uint32_t* pend_count;
+    uint32_t* fac_v;             // vertices whose new color needs a warp (histogram or >64 scan)
+    uint32_t* fac_count;
+    unsigned long long* symsum;  // sum over entries x->y (y != x, y < n) of H(x,y) - H(y,x)
+    unsigned long long* live;    // live entries seen by the sweep
+};
+
+// Same-edge ordering for a concurrently applied batch.
+struct EdgeOrder {
+    unsigned long long* tkey;  // open-addressed edge keys
+    uint32_t* thead;           // per key: last update index pushed
+    uint32_t* tslot;           // per update: its key slot (NONE32 = not an edge op)
+    uint32_t* tnext;           // per update: next in the key's push list
+    uint32_t* tprev;           // per update: previous update of the same edge (stream order)
+    uint32_t* done;            // per update: batch sequence number once applied
+    uint32_t* ticket;          // work ticket of the persistent apply kernel
+    uint32_t tmask;            // table size - 1
+};
+
+enum SweepMode : int { SWEEP_REBUILD = 0, SWEEP_TIER1 = 1 };
+
+// ---- launchers (sgc_kernels.cu) ----
+void launch_det_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, cudaStream_t s);
+void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const EdgeOrder& eo, uint32_t seq,
+                       int num_sms, cudaStream_t s);
+void launch_dirty_list(const Dev& g, uint32_t* list, uint32_t* count, cudaStream_t s);
+void launch_compact(const Dev& g, const uint32_t* list, const uint32_t* count, uint32_t max_rows, cudaStream_t s);
+void launch_take_overflow(const Dev& g, uint32_t* drain_n, cudaStream_t s);
+void launch_drain(const Dev& g, const uint32_t* drain_n, bool ordered, unsigned long long* failed, cudaStream_t s);
+void launch_snapshot(const Dev& g, uint16_t* snap, cudaStream_t s);
+void launch_build_items(const Dev& g, const SweepBufs& b, cudaStream_t s);
+void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s);
+void launch_query(const uint16_t* snap, uint32_t n, const uint32_t* v, uint16_t* out, uint32_t k, cudaStream_t s);
+void launch_colors(const Dev& g, uint16_t* out, cudaStream_t s);
+
+// Tier-2 (sgc_tier2.cu)
+struct Tier2Bufs {
+    uint8_t* inU;
+    uint8_t* inF;
+    uint8_t* inL;
+    uint8_t* done;
+    uint32_t* list;        // current ordered list
+    uint32_t* list2;
+    uint32_t* count;       // [0] list count, [1] list2 count, [2] fixed, [3] rev count, [4] selected
+    unsigned long long* rev_keys;   // (y << 32) | x for entries x -> y with inL[y]
+    unsigned long long* rev_keys2;
+    uint32_t rev_cap;
+    uint32_t* rev_start;   // per list position: first index into sorted rev keys
+    uint32_t* rev_end;
+    void* cub_tmp;
+    size_t cub_tmp_bytes;
+    uint32_t* pend_v;
+    uint32_t* pend_w;
+};
+// Runs the reference's Tier-2 (streamgc.cu:1057-1240) exactly; returns fixes.
+// Rows must be compact (after compaction + drain).
+uint32_t run_tier2(const Dev& g, Tier2Bufs& b, cudaStream_t s, uint32_t* host_scratch, bool* gave_up);
+size_t tier2_cub_bytes(uint32_t n, uint32_t rev_cap);
+
+// Validator (sgc_tier2.cu): [violations, uncolored_with_edges, distinct_edges, max_color, out_of_range]
+int run_validate(const Dev& g, cudaStream_t s, uint64_t* out);
+
+}  // namespace sgc

@@ -1,0 +1,156 @@
+"""CUDA path: known-answer tests on the device, API edge cases, the stream_gc
+program and the reference's own integration test linked against the drop-in."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import streamgc_b200 as S
+from oracle import oracle as O
+from tests.golden import make_golden as MG
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def tiny(hd=False):
+    g = S.Graph(np.array([0, 0, 0], dtype=np.uint64), np.zeros(0, dtype=np.uint32),
+                np.array([65 if hd else 0, 0], dtype=np.uint32))
+    return S.StreamGC(g, histogram_threshold=64)
+
+
+@pytest.mark.parametrize("bitmap,expect", [(0, 1), (0x1, 2), (0b10111, 4), (0b11, 3), ((1 << 64) - 1, 1)])
+def test_device_bitmap_kats(bitmap, expect):
+    with tiny() as h:
+        h.upload("bitmaps", np.array([bitmap, 0], dtype=np.uint64))
+        assert h.find_color(0) == expect
+
+
+@pytest.mark.parametrize("counts,expect", [([], 1), ([3, 2, 1, 5, 4], 6), ([2, 1, 0, 3], 3)])
+def test_device_histogram_kats(counts, expect):
+    with tiny(hd=True) as h:
+        row = np.zeros(1024, dtype=np.uint32)
+        row[:len(counts)] = counts
+        h.upload("hist", row)
+        assert h.find_color(0) == expect
+
+
+def test_device_histogram_first_minimum_and_wrap():
+    with tiny(hd=True) as h:
+        row = np.full(1024, 7, dtype=np.uint32)
+        row[10] = row[500] = 3
+        row[0] = 0xFFFFFFFF
+        h.upload("hist", row)
+        assert h.find_color(0) == 11
+
+
+@pytest.mark.parametrize("cu,cv,du,dv", [(1, 2, 10, 5), (3, 3, 10, 5), (5, 5, 10, 10), (0, 0, 10, 5)])
+def test_device_loser_rule_matches_oracle(cu, cv, du, dv):
+    rp = np.array([0, 0, 0], dtype=np.uint64)
+    deg = np.array([du, dv], dtype=np.uint32)
+    g = O.Oracle(rp, np.zeros(0, dtype=np.uint32), deg)
+    g.set_states(np.array([cu, cv], dtype=np.uint32))
+    ups = S.updates_from([[0, 1]])
+    g.apply(ups)
+    with S.StreamGC(S.Graph(rp, np.zeros(0, dtype=np.uint32), deg)) as h:
+        h.upload("states", np.array([cu, cv], dtype=np.uint32))
+        h.apply(ups)
+        assert np.array_equal(h.states(), g.states())
+
+
+def test_edge_cases_match_oracle():
+    """Self loops, out-of-range endpoints (skipped), query-type records, DEL of
+    absent edges, ADD of present edges, empty batches."""
+    c = MG.build_case("overflow512")
+    n = len(c["deg"])
+    ups = S.updates_from([[3, 3], [0, n + 5], [n, 1], [1, 2], [1, 2], [7, 300], [7, 300], [9, 9], [4, 5]],
+                         [0, 0, 1, 1, 0, 1, 0, 1, 2])
+    g = O.Oracle(c["rp"], c["col"], c["deg"])
+    g.apply(ups)
+    with S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"])) as h:
+        h.apply(ups[:0])
+        h.apply(ups)
+        assert np.array_equal(h.states(), g.states())
+        assert np.array_equal(h.col(), g.col())
+        assert np.array_equal(h.bitmaps(), g.bitmaps())
+        assert h.stats()["updates_skipped"] == g.counters()["skipped"] == 2
+        h.epoch()
+        g.epoch()
+        assert np.array_equal(h.col(), g.col())
+
+
+def test_concurrent_duplicate_edges_keep_stream_order():
+    """ADD/DEL/ADD/DEL ... of one edge inside one concurrent batch ends like the stream says."""
+    c = MG.build_case("delaunay2k")
+    seq = []
+    for r in range(40):
+        seq += [[5, 9], [5, 9]]
+    types = [0, 1] * 40 + [0]
+    seq += [[5, 9]]
+    ups = S.updates_from(seq, types)
+    with S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"])) as h:
+        h.apply(ups, S.MODE_CONCURRENT)
+        h.drain_and_compact()
+        rp, col = h.row_ptr(), h.col()
+        assert (col[rp[5]:rp[6]] == 9).sum() == 1 and (col[rp[9]:rp[10]] == 5).sum() == 1
+        assert h.stats()["device_error"] == 0
+
+
+def test_query_reads_published_snapshot():
+    c = MG.build_case("delaunay2k")
+    with S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"]), epoch_size=2048) as h:
+        h.process_stream(c["init"], S.MODE_CONCURRENT)
+        h.publish()
+        snap = h.snapshot()
+        v = np.array([0, 5, 2047, 10 ** 6], dtype=np.uint32)
+        assert h.query(v).tolist() == [snap[0], snap[5], snap[2047], 0]
+
+
+def test_bad_arguments_raise():
+    c = MG.build_case("overflow512")
+    with S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"]), max_batch=64) as h:
+        with pytest.raises(S.StreamGCError):
+            S.lib()  # noqa: B018
+            S._check(S.lib().sgc_apply(h.h, c["bench"].ctypes.data, 65, 0), "apply")
+        with pytest.raises(S.StreamGCError):
+            S._check(S.lib().sgc_apply(h.h, c["bench"].ctypes.data, 4, 7), "apply")
+        with pytest.raises(S.StreamGCError):
+            h.find_color(10 ** 6)
+
+
+def test_stream_gc_program(tmp_path):
+    g = S.Graph.delaunay(3000, seed=3)
+    mtx = str(tmp_path / "del3k.mtx")
+    g.write_mtx(mtx)
+    out = tmp_path / "out"
+    exe = os.path.join(ROOT, "streamgc_b200", "lib", "stream_gc")
+    r = subprocess.run([exe, "--graph", mtx, "--stream", "20000", "--insert-pct", "50", "--epoch-size", "4096",
+                        "--seed", "42", "--output-dir", str(out), "--validate"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Coloring valid: 0 violations" in r.stdout
+    base = out / "streamgc_1gpu_stream20000_50pct.coloring"
+    colors = np.fromfile(str(base), dtype="<u2")
+    assert len(colors) == 3000
+    import json
+    meta = json.loads((out / "streamgc_1gpu_stream20000_50pct.coloring.meta").read_text())
+    assert list(meta)[:8] == ["algorithm", "graph", "num_vertices", "num_edges", "num_colors_used",
+                              "static_greedy_colors", "color_ratio", "init_time_ms"]
+    assert meta["num_colors_used"] == int(colors.max()) and meta["graph"] == "del3k"
+    assert meta["static_greedy_colors"] == g.static_greedy()
+    # deterministic mode: the coloring equals the oracle's after the same phases
+    o = O.Oracle(g.row_ptr, g.col_idx, g.degree)
+    o.process_stream(g.init_stream(), 4096)
+    o.phase_end()
+    o.process_stream(g.churn_stream(20000, 50, 42), 4096)
+    o.phase_end()
+    assert np.array_equal(colors, o.colors())
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "test_single_gpu_dropin")),
+                    reason="drop-in link check binary not built (no reference tree at build time)")
+def test_reference_integration_test_runs_on_dropin_kernels():
+    exe = os.path.join(ROOT, "oracle", "_ref", "test_single_gpu_dropin")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "4 passed, 0 failed" in r.stdout

@@ -1,0 +1,152 @@
+"""CUDA path vs the oracle (and the reference's own kernels via the golden
+epoch hashes): bit-exact for every integer array at every epoch boundary."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import streamgc_b200 as S
+from oracle import oracle as O
+from tests import _util
+from tests.golden import make_golden as MG
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", list(MG.CASES))
+def test_deterministic_mode_matches_oracle_every_epoch(name):
+    c = MG.build_case(name)
+    ora = list(_util.oracle_epochs(c))
+    gpu = list(_util.gpu_epochs(c, S.MODE_DETERMINISTIC))
+    assert [t for t, _ in ora] == [t for t, _ in gpu]
+    for (tag, a), (_, b) in zip(ora, gpu):
+        for k in _util.ARRAY_NAMES:
+            if not np.array_equal(a[k], b[k]):
+                bad = np.nonzero(a[k] != b[k])[0][:8]
+                pytest.fail(f"{name} {tag} {k}: first differing indices {bad.tolist()} "
+                            f"oracle={a[k][bad].tolist()} gpu={b[k][bad].tolist()}")
+
+
+@pytest.mark.skipif(not os.path.exists(MG.GOLDEN_JSON), reason="golden epoch fixtures not generated yet")
+@pytest.mark.parametrize("name", list(MG.CASES))
+def test_deterministic_mode_matches_reference_kernels(name):
+    gold = json.load(open(MG.GOLDEN_JSON))[name]
+    c = MG.build_case(name)
+    n = 0
+    for tag, arrays in _util.gpu_epochs(c, S.MODE_DETERMINISTIC):
+        for k in _util.ARRAY_NAMES:
+            assert _util.sha(arrays[k]) == gold["epochs"][tag][k], f"{name} {tag} {k}"
+        n += 1
+    assert n == len(gold["epochs"])
+
+
+def _both(name):
+    c = MG.build_case(name)
+    g = O.Oracle(c["rp"], c["col"], c["deg"], hist_threshold=c["thr"], slack_pct=c["slack"])
+    h = S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"]), epoch_size=c["E"], histogram_threshold=c["thr"],
+                   slack_pct=c["slack"], max_batch=c["batch"])
+    return c, g, h
+
+
+@pytest.mark.parametrize("name", list(MG.CASES))
+def test_phase_end_repair_matches_oracle(name):
+    """Reference epochs during each phase, then drain_and_compact + Tier-1
+    (Jacobi) + Tier-2 at phase end: bit-exact states, bitmaps and CSR."""
+    c, g, h = _both(name)
+    try:
+        for ups in (c["init"], c["bench"]):
+            g.process_stream(ups, c["E"], c["batch"])
+            since = 0
+            for s in range(0, len(ups), c["batch"]):
+                part = ups[s:s + c["batch"]]
+                h.apply(part)
+                since += len(part)
+                if since >= c["E"]:
+                    h.epoch()
+                    since = 0
+            it, last, fixed = g.phase_end()
+            rep = h.repair()
+            assert (rep["tier1_iterations"], rep["tier1_last_count"]) == (it, last)
+            assert rep["tier2_fixed"] == fixed
+            assert np.array_equal(h.states(), g.states())
+            assert np.array_equal(h.bitmaps(), g.bitmaps())
+            assert np.array_equal(h.col(), g.col())
+            v, w = h.validate(), g.validate()
+            assert v == w, (v, w)
+            assert v["violations"] == 0
+    finally:
+        h.close()
+        g.close()
+
+
+def test_tier2_exact_on_forced_conflicts():
+    """Conflicts planted in the state: Tier-1 alone vs the oracle, then Tier-2."""
+    c = MG.build_case("rmat11")
+    g = O.Oracle(c["rp"], c["col"], c["deg"], hist_threshold=c["thr"])
+    h = S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"]), histogram_threshold=c["thr"])
+    try:
+        rng = np.random.default_rng(5)
+        st = (rng.integers(0, 4, size=len(c["deg"]))).astype(np.uint32)  # colors 0..3: many conflicts
+        g.set_states(st)
+        h.upload("states", st)
+        it, last, fixed = g.phase_end()
+        rep = h.repair()
+        assert (rep["tier1_iterations"], rep["tier1_last_count"], rep["tier2_fixed"]) == (it, last, fixed)
+        assert np.array_equal(h.states(), g.states())
+        assert h.validate()["violations"] == g.validate()["violations"]
+    finally:
+        h.close()
+        g.close()
+
+
+@pytest.mark.parametrize("name", ["delaunay2k", "rmat11", "overflow512"])
+def test_concurrent_mode_publishes_proper_snapshots(name):
+    """Concurrent batches: every published snapshot is proper on the live CSR,
+    the edge multiset per row equals the sequential one, colors within slack."""
+    c, g, h = _both(name)
+    try:
+        g.process_stream_repaired(c["init"], c["E"], c["batch"])
+        for ups in (c["init"], c["bench"]):
+            for s in range(0, len(ups), c["batch"]):
+                h.apply(ups[s:s + c["batch"]], S.MODE_CONCURRENT)
+                rep = h.publish()
+                assert rep["proper"] == 1
+                snap = h.snapshot()
+                v = O.validate_colors(h.row_ptr(), h.col(), snap)
+                assert v["violations"] == 0 and v["uncolored_with_edges"] == 0
+        g.process_stream_repaired(c["bench"], c["E"], c["batch"])
+        g.drain_and_compact()
+        h.drain_and_compact()
+        oracle_colors = int(g.colors().max())
+        # same live edge multiset per row as the sequential oracle, unless a full
+        # row made an insert wait in the overflow buffer and then drop (which edge
+        # loses the last slot depends on the order the inserts arrive in)
+        st, oc = h.stats(), g.counters()
+        exact = st["drain_failed"] == 0 and st["overflow_lost"] == 0 and oc["drain_failed"] == 0 \
+            and oc["overflow_lost"] == 0
+        gr, gc = h.row_ptr(), h.col()
+        orp, ocol = g.row_ptr(), g.col()
+        for x in range(len(c["deg"]) if exact else 0):
+            a = np.sort(gc[gr[x]:gr[x + 1]])
+            b = np.sort(ocol[orp[x]:orp[x + 1]])
+            assert np.array_equal(a, b), f"row {x}"
+        assert int(h.colors().max()) <= oracle_colors + 4
+        assert h.stats()["device_error"] == 0
+    finally:
+        h.close()
+        g.close()
+
+
+def test_validator_matches_oracle_on_improper_state():
+    c = MG.build_case("overflow512")
+    g = O.Oracle(c["rp"], c["col"], c["deg"])
+    h = S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"]))
+    try:
+        st = np.random.default_rng(1).integers(0, 3, size=len(c["deg"])).astype(np.uint32)
+        g.set_states(st)
+        h.upload("states", st)
+        assert h.validate() == g.validate()
+    finally:
+        h.close()
+        g.close()
