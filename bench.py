@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Throughput of the streaming graph-coloring path on B200.
+
+Workload (default, `--workload skewed`): R-MAT graph with 2^20 vertices and
+edge factor 48 (a,b,c,d = .57,.19,.19,.05; symmetrised, de-duplicated, self
+loops dropped; ~44.4M undirected edges), colored by its degree-sorted init
+stream, then a dense stream of 2,000,000 updates over the k-core at the 90th
+percentile of core numbers (two inserts of non-adjacent core pairs per delete
+of a live core edge), epoch E = 32,768, histogram threshold 64, alpha = 4.
+`--workload small`: Delaunay triangulation of 131,072 uniform points (seed 42)
+with the reference's 50/50 churn stream of 1,000,000 updates.
+
+One step = one epoch: E updates applied concurrently (one warp per update)
+followed by the repaired publish (compaction of edited rows, overflow drain,
+fused rebuild + Tier-1 sweeps, Tier-2 when needed, double-buffered snapshot).
+`value` times steps on the device with CUDA events on the library's stream,
+inputs resident in HBM, L2 flushed (256 MiB write) before every timed step;
+`e2e` times the same steps through the C ABI from pinned host memory with the
+host->device copy of each batch and the read-back of the step's counters
+inside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "updates/sec on 1 B200 (plain vs batched/served); p50/p99 update-to-visible ms"
+E = 32768
+HIST_THR = 64
+
+
+def log(*a):
+    print("[bench]", *a, file=sys.stderr, flush=True)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def build_workload(kind, stream_len):
+    import streamgc_b200 as S
+    t = time.time()
+    if kind == "skewed":
+        g = S.Graph.rmat(20, 48, 0.57, 0.19, 0.19, seed=42)
+        bench, k, csize = g.kcore_stream(stream_len, 90.0, 42)
+        desc = dict(workload="rmat20_ef48_kcore90_dense", graph="R-MAT scale 20, edge factor 48, (.57,.19,.19,.05), seed 42",
+                    vertices=g.n, undirected_edges=g.nnz // 2, stream=f"k-core dense, {stream_len} updates, 2 inserts per delete, seed 42",
+                    core_k=k, core_vertices=csize)
+    else:
+        g = S.Graph.delaunay(131072, seed=42)
+        bench = g.churn_stream(stream_len, 50, 42)
+        desc = dict(workload="delaunay17_churn", graph="Delaunay of 131072 uniform points, seed 42", vertices=g.n,
+                    undirected_edges=g.nnz // 2, stream=f"churn 50% insert, {stream_len} updates, seed 42")
+    init = g.init_stream()
+    desc.update(epoch_size=E, histogram_threshold=HIST_THR, alpha=4)
+    log(f"workload {desc['workload']}: n={g.n} m={g.nnz // 2} init={len(init)} stream={len(bench)} "
+        f"({time.time() - t:.1f}s)")
+    return g, init, bench, desc
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                out, _ = self.p.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def read_traffic():
+    """dram bytes per launch of the sweep kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)).get("sweep_dram_bytes_per_sweep")
+        except Exception:
+            return None
+    return None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_ours(a):
+    import torch
+    import streamgc_b200 as S
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    nbatch = a.warmup + 2 * a.steps + a.cpu_batches
+    stream_len = max(2_000_000 if a.workload == "skewed" else 1_000_000, nbatch * E)
+    g, init, bench, desc = build_workload(a.workload, stream_len)
+
+    t = time.time()
+    h = S.StreamGC(g, epoch_size=E, histogram_threshold=HIST_THR, slack_pct=300, max_batch=1 << 20,
+                   device=local, profile=True)
+    for s in range(0, len(init), 1 << 20):
+        h.apply(init[s:s + (1 << 20)], S.MODE_CONCURRENT)
+    rep = h.publish()
+    h.synchronize()
+    log(f"init colored on GPU in {time.time() - t:.1f}s: {rep}")
+    if not rep["proper"]:
+        raise SystemExit("init coloring not proper")
+
+    dev_stream = torch.from_numpy(bench.view(np.uint8)).to(f"cuda:{local}")
+    dptr = dev_stream.data_ptr()
+    ext = torch.cuda.ExternalStream(h.cuda_stream(), device=f"cuda:{local}")
+    flush = torch.empty(64 << 20, dtype=torch.int32, device=f"cuda:{local}")  # 256 MiB > 126 MB L2
+    pinned = torch.from_numpy(bench.view(np.uint8)).pin_memory()
+    hptr = pinned.data_ptr()
+
+    def step(ptr, b, timed_events=None):
+        h.apply_ptr(ptr + b * E * 16, E, S.MODE_CONCURRENT)
+        return h.publish()
+
+    b = 0
+    for _ in range(a.warmup):
+        step(dptr, b)
+        b += 1
+    h.synchronize()
+    st0 = h.stats()
+    evs = []
+    reps = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(a.steps):
+            with torch.cuda.stream(ext):
+                flush.add_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            reps.append(step(dptr, b))
+            e1.record(ext)
+            evs.append((e0, e1))
+            b += 1
+        ext.synchronize()
+        torch.cuda.synchronize()
+        step_ms = [x.elapsed_time(y) for x, y in evs]
+        st1 = h.stats()
+        # e2e: same steps through the C ABI from pinned host memory, wall clock
+        h.synchronize()
+        d0 = h.stats()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            step(hptr, b)
+            h.stats()  # the step's result read back to the host
+            b += 1
+        h.synchronize()
+        e2e_s = time.perf_counter() - t0
+        d1 = h.stats()
+    total_ms = sum(step_ms)
+    if dist:
+        tt = torch.tensor([total_ms, e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms, e2e_s = float(tt[0]), float(tt[1])
+    val = h.validate()
+    cpu = None
+    if rank == 0 and world == 1 and a.cpu_batches > 0:
+        cpu = cpu_baseline(g, h, bench, b, a.cpu_batches, a.cpu_seconds)
+    if rank == 0:
+        updates = world * a.steps * E
+        peak, peak_kind = load_peaks()
+        sweep_ms = st1["sweep_ms"] - st0["sweep_ms"]
+        sweep_bytes = st1["sweep_bytes"] - st0["sweep_bytes"]
+        sweeps = st1["sweep_count"] - st0["sweep_count"]
+        achieved = (sweep_bytes / (sweep_ms / 1e3) / 1e9) if sweep_ms > 0 else 0.0
+        traffic = read_traffic()
+        lat = sorted(step_ms)
+        p50 = lat[len(lat) // 2]
+        p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
+        conf = dict(desc)
+        conf.update(mode="concurrent (warp per update) + repaired publish per epoch",
+                    l2="flushed before every timed step (256 MiB write)", parallelism=f"replicas x{world}",
+                    valid_after_run=val["violations"] == 0 and val["uncolored_with_edges"] == 0,
+                    colors_used=int(val["max_color"]), static_greedy_colors=None,
+                    tier1_sweeps_per_step=round(sweeps / max(1, a.steps), 2),
+                    tier2_runs_in_timed=sum(r["tier2_ran"] for r in reps),
+                    all_published_proper=all(r["proper"] for r in reps))
+        out = {
+            "metric": METRIC, "value": updates / (total_ms / 1e3), "unit": "updates/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": conf,
+            "latency_ms": {"update_to_visible_p50": p50, "update_to_visible_p99": p99},
+            "roofline": {"bound": "hbm", "kernel": "tier-1 sweep (sweep_items + finalize + fac + commit)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)" if peak_kind == "measured"
+                         else "fallback", "traffic": traffic,
+                         "algorithmic_bytes_per_sweep": sweep_bytes / max(1, sweeps),
+                         "sweep_ms_avg": sweep_ms / max(1, sweeps), "sweeps_timed": sweeps},
+            "e2e": {"value": world * a.steps * E / e2e_s, "unit": "updates/s",
+                    "h2d_bytes_per_step": (d1["h2d_bytes"] - d0["h2d_bytes"]) // a.steps,
+                    "d2h_bytes_per_step": (d1["d2h_bytes"] - d0["d2h_bytes"]) // a.steps},
+            "gpu_launches": st1["kernel_launches"] - st0["kernel_launches"],
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out), flush=True)
+    h.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(g, h, bench, first_batch, nb, budget_s):
+    """The oracle (CPU restatement, OpenMP where order-independent) timed on the
+    same state and the next batches of the same stream."""
+    from oracle import oracle as O
+    o = O.Oracle(g.row_ptr, g.col_idx, g.degree, hist_threshold=HIST_THR)
+    o.load_state(h.col(), h.states(), h.bitmaps(), h.hist())
+    done = 0
+    t0 = time.perf_counter()
+    for k in range(nb):
+        lo = (first_batch + k) * E
+        if lo + E > len(bench):
+            break
+        o.process_stream_repaired(bench[lo:lo + E], E, E)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    if not done:
+        return None
+    return {"value": done * E / dt, "unit": "updates/s", "cores": int(O.lib().og_num_threads()), "kind": "port",
+            "sample": f"{done} epochs of {E} updates following the GPU-timed ones, same state, "
+                      f"updates in stream order + repaired epoch ({dt:.1f}s)"}
+
+
+def run_reference(a):
+    """The reference path's CPU restatement (oracle port): it has no CPU
+    implementation of its own, so the oracle stands for it."""
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    stream_len = max(2_000_000 if a.workload == "skewed" else 1_000_000, (a.warmup + a.steps) * E)
+    g, init, bench, desc = build_workload(a.workload, stream_len)
+    t = time.time()
+    o = O.Oracle(g.row_ptr, g.col_idx, g.degree, hist_threshold=HIST_THR)
+    o.process_stream_repaired(init, len(init), len(init))
+    log(f"oracle init {time.time() - t:.1f}s")
+    for k in range(a.warmup):
+        o.process_stream_repaired(bench[k * E:(k + 1) * E], E, E)
+    times = []
+    for k in range(a.warmup, a.warmup + a.steps):
+        t0 = time.perf_counter()
+        o.process_stream_repaired(bench[k * E:(k + 1) * E], E, E)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    v = a.steps * E / total
+    cores = int(O.lib().og_num_threads())
+    conf = dict(desc)
+    conf.update(mode="CPU oracle: updates in stream order + repaired epoch", parallelism="1 process")
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "updates/s", "n_gpus": world,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total / a.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": conf,
+           "cpu_baseline": {"value": v, "unit": "updates/s", "cores": cores, "kind": "port",
+                            "sample": f"{a.steps} epochs of {E} updates after {a.warmup} warm-up epochs"},
+           "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=24)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="skewed", choices=["skewed", "small"])
+    ap.add_argument("--cpu-batches", type=int, default=8, help="epochs timed on the CPU baseline (0: skip)")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    a = ap.parse_args()
+    if a.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

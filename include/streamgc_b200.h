@@ -80,6 +80,9 @@ typedef struct sgc_stats {
     uint64_t sweep_count;        /* SGC_OPT_PROFILE: sweeps timed */
     uint64_t sweep_bytes;        /* algorithmic bytes of the timed sweeps: 8 per live entry + 28 per vertex */
     uint64_t live_entries;       /* live adjacency entries at the last sweep */
+    uint64_t kernel_launches;    /* kernels launched by this handle */
+    uint64_t h2d_bytes;          /* update bytes copied host -> device by sgc_apply */
+    uint64_t d2h_bytes;          /* bytes the library read back (repair counters, stats) */
 } sgc_stats;
 
 typedef struct sgc_validation {

@@ -67,6 +67,7 @@ def lib():
             "og_process_stream": (C.c_uint32, [_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32]),
             "og_process_stream_repaired": (C.c_uint32, [_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32]),
             "og_phase_end": (C.c_uint32, [_vp, C.POINTER(C.c_int), _u32p]),
+            "og_load_state": (None, [_vp, _u32p, _u32p, _u64p, _u32p]),
             "og_get_states": (None, [_vp, _u32p]),
             "og_set_states": (None, [_vp, _u32p]),
             "og_get_bitmaps": (None, [_vp, _u64p]),
@@ -172,6 +173,13 @@ class Oracle:
         a = np.zeros(self.n, dtype=np.uint32)
         self.L.og_get_states(self.h, _p(a, _u32p))
         return a
+
+    def load_state(self, col, states, bitmaps, hist):
+        col = np.ascontiguousarray(col, dtype=np.uint32)
+        states = np.ascontiguousarray(states, dtype=np.uint32)
+        bitmaps = np.ascontiguousarray(bitmaps, dtype=np.uint64)
+        hist = np.ascontiguousarray(hist, dtype=np.uint32)
+        self.L.og_load_state(self.h, _p(col, _u32p), _p(states, _u32p), _p(bitmaps, _u64p), _p(hist, _u32p))
 
     def set_states(self, a):
         a = np.ascontiguousarray(a, dtype=np.uint32)

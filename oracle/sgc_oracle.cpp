@@ -635,6 +635,23 @@ uint32_t og_process_stream_repaired(void* h, const EdgeUpdate* ups, uint64_t n, 
     return epochs;
 }
 
+// Overwrites slots, states, bitmaps and histograms with a state taken from
+// elsewhere (same row layout). A row whose slots differ from the current ones
+// is marked edited. Used to time the CPU path from the same starting state.
+void og_load_state(void* h, const uint32_t* col, const uint32_t* states, const uint64_t* bitmaps,
+                   const uint32_t* hist) {
+    Oracle* g = (Oracle*)h;
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t xi = 0; xi < (int64_t)g->n; xi++) {
+        const uint32_t x = (uint32_t)xi;
+        if (std::memcmp(&g->col[g->rp[x]], col + g->rp[x], (g->rp[x + 1] - g->rp[x]) * 4)) g->edited[x] = 1;
+    }
+    std::memcpy(g->col.data(), col, g->col.size() * 4);
+    std::memcpy(g->st.data(), states, g->n * 4ull);
+    std::memcpy(g->bm.data(), bitmaps, g->n * 8ull);
+    std::memcpy(g->hist.data(), hist, g->hist.size() * 4ull);
+}
+
 // ---------------- state access ----------------
 void og_get_states(void* h, uint32_t* out) { Oracle* g = (Oracle*)h; std::memcpy(out, g->st.data(), g->n * 4ull); }
 void og_set_states(void* h, const uint32_t* in) { Oracle* g = (Oracle*)h; std::memcpy(g->st.data(), in, g->n * 4ull); }

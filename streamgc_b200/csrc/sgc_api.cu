@@ -90,6 +90,8 @@ struct sgc_handle {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
     double sweep_ms = 0;
     uint64_t sweep_count = 0, sweep_bytes = 0, live_entries = 0;
+    uint64_t launches = 0;          // kernels this handle launched
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;  // bytes the library moved across PCIe / C2C
 };
 
 namespace {
@@ -174,12 +176,14 @@ int compact_dirty(sgc_handle* h) {
     CK(cudaMemsetAsync(&h->ctl->dirty_count, 0, 4, h->stream));
     launch_dirty_list(h->g, h->dirty_list, &h->ctl->dirty_count, h->stream);
     launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, h->stream);
+    h->launches += 2;
     return check_cuda("compact");
 }
 
 int drain(sgc_handle* h, bool ordered, unsigned long long* failed_counter) {
     launch_take_overflow(h->g, &h->ctl->drain_n, h->stream);
     launch_drain(h->g, &h->ctl->drain_n, ordered, failed_counter, h->stream);
+    h->launches += 2;
     return check_cuda("drain");
 }
 
@@ -193,6 +197,7 @@ int sweep(sgc_handle* h, SweepMode mode) {
         cudaEventRecord(a, h->stream);
     }
     launch_sweep(h->g, h->sb, mode, h->num_sms, h->stream);
+    h->launches += mode == SWEEP_TIER1 ? 4 : 2;
     if (prof) {
         cudaEventRecord(b, h->stream);
         h->ev_pending.push_back({a, b});
@@ -202,12 +207,14 @@ int sweep(sgc_handle* h, SweepMode mode) {
 
 int build_items(sgc_handle* h) {
     launch_build_items(h->g, h->sb, h->stream);
+    h->launches += 1;
     return check_cuda("build_items");
 }
 
 void publish_snapshot(sgc_handle* h) {
     const int back = 1 - h->front;
     launch_snapshot(h->g, h->snap[back], h->stream);
+    h->launches += 1;
     h->front = back;
 }
 
@@ -223,6 +230,7 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep) {
         h->tier1_sweeps++;
         CK(cudaMemcpyAsync(h->h_small, &h->ctl->pend_count, 4, cudaMemcpyDeviceToHost, h->stream));
         if (it == 0) CK(cudaMemcpyAsync(h->h_small + 2, &h->ctl->symsum, 16, cudaMemcpyDeviceToHost, h->stream));
+        h->d2h_bytes += it == 0 ? 20 : 4;
         TRY(sync(h));
         cnt = h->h_small[0];
         if (it == 0) h->live_entries = *(unsigned long long*)(h->h_small + 4);
@@ -243,7 +251,7 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep) {
     bool proper = (cnt == 0 && sym == 0);
     if (!proper) {
         bool gave_up = false;
-        const uint32_t fixed = run_tier2(h->g, h->t2, h->stream, h->h_small, &gave_up);
+        const uint32_t fixed = run_tier2(h->g, h->t2, h->stream, h->h_small, &gave_up, &h->launches);
         TRY(check_cuda("tier2"));
         r.tier2_ran = 1;
         r.tier2_fixed = fixed;
@@ -264,6 +272,7 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep) {
 int read_drain(sgc_handle* h, sgc_repair_report* rep, unsigned long long before_failed) {
     CK(cudaMemcpyAsync(h->h_small, &h->ctl->drain_n, 4, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(h->h_small + 2, &h->ctl->drain_failed, 8, cudaMemcpyDeviceToHost, h->stream));
+    h->d2h_bytes += 12;
     TRY(sync(h));
     if (rep) {
         rep->drained = h->h_small[0];
@@ -497,16 +506,19 @@ int sgc_apply(sgc_handle* h, const EdgeUpdate* ups, uint32_t n, int mode) {
         src = ups;  // caller keeps it alive until the stream passes this point
     } else if (attr.type == cudaMemoryTypeHost) {
         CK(cudaMemcpyAsync(h->d_batch, ups, (size_t)n * sizeof(EdgeUpdate), cudaMemcpyHostToDevice, h->stream));
+        h->h2d_bytes += (uint64_t)n * sizeof(EdgeUpdate);
         src = h->d_batch;
     } else {
         CK(cudaEventSynchronize(h->stage_free));
         std::memcpy(h->h_stage, ups, (size_t)n * sizeof(EdgeUpdate));
         CK(cudaMemcpyAsync(h->d_batch, h->h_stage, (size_t)n * sizeof(EdgeUpdate), cudaMemcpyHostToDevice, h->stream));
         CK(cudaEventRecord(h->stage_free, h->stream));
+        h->h2d_bytes += (uint64_t)n * sizeof(EdgeUpdate);
         src = h->d_batch;
     }
     if (mode == SGC_MODE_DETERMINISTIC) {
         launch_det_apply(h->g, src, n, h->stream);
+        h->launches += 1;
     } else {
         h->seq++;
         if (h->seq == 0) {  // wrapped: clear the done marks before reuse
@@ -514,6 +526,7 @@ int sgc_apply(sgc_handle* h, const EdgeUpdate* ups, uint32_t n, int mode) {
             h->seq = 1;
         }
         launch_conc_apply(h->g, src, n, h->eo, h->seq, h->num_sms, h->stream);
+        h->launches += 3;
     }
     h->last_mode = mode;
     h->updates += n;
@@ -704,6 +717,7 @@ int sgc_get_stats(sgc_handle* h, sgc_stats* o) {
     CK(cudaSetDevice(h->device));
     Ctl c;
     CK(cudaMemcpyAsync(&c, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+    h->d2h_bytes += sizeof(Ctl);
     TRY(sync(h));
     std::memset(o, 0, sizeof(*o));
     o->updates_submitted = h->updates;
@@ -725,6 +739,9 @@ int sgc_get_stats(sgc_handle* h, sgc_stats* o) {
     o->sweep_count = h->sweep_count;
     o->sweep_bytes = h->sweep_bytes;
     o->live_entries = h->live_entries;
+    o->kernel_launches = h->launches;
+    o->h2d_bytes = h->h2d_bytes;
+    o->d2h_bytes = h->d2h_bytes;
     return c.err ? fail(SGC_EDEVICE, "device error word 0x%x", c.err) : SGC_OK;
 }
 

@@ -12,18 +12,64 @@
 #include <utility>
 #include <vector>
 
+#include <omp.h>
+#include <parallel/algorithm>
+
 namespace {
 
 constexpr uint32_t INV = SGC_CSR_INVALID;
 
 inline uint64_t key_of(uint32_t a, uint32_t b) { return ((uint64_t)a << 32) | b; }
 
-// Flat set of u64 keys (edge membership); iteration order is never used.
+// Open-addressing set of u64 edge keys (a << 32 | b, a < b, so ~0 and ~0-1 are
+// never keys: they mark empty and deleted slots). Membership only.
 struct KeySet {
-    std::unordered_set<uint64_t> s;
-    bool has(uint64_t k) const { return s.find(k) != s.end(); }
-    void add(uint64_t k) { s.insert(k); }
-    void del(uint64_t k) { s.erase(k); }
+    static constexpr uint64_t EMPTY = ~0ull, DEAD = ~0ull - 1;
+    std::vector<uint64_t> t;
+    uint64_t mask = 0, used = 0;
+    explicit KeySet(uint64_t expect = 1024) {
+        uint64_t cap = 1024;
+        while (cap < 2 * expect + 16) cap <<= 1;
+        t.assign(cap, EMPTY);
+        mask = cap - 1;
+    }
+    static uint64_t mix(uint64_t k) {
+        k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ull; return k ^ (k >> 33);
+    }
+    bool has(uint64_t k) const {
+        for (uint64_t i = mix(k) & mask;; i = (i + 1) & mask) {
+            if (t[i] == k) return true;
+            if (t[i] == EMPTY) return false;
+        }
+    }
+    void grow() {
+        std::vector<uint64_t> old;
+        old.swap(t);
+        t.assign(old.size() * 2, EMPTY);
+        mask = t.size() - 1;
+        used = 0;
+        for (uint64_t k : old)
+            if (k != EMPTY && k != DEAD) add(k);
+    }
+    void add(uint64_t k) {
+        if (2 * (used + 1) > t.size()) grow();
+        uint64_t dead = EMPTY;
+        for (uint64_t i = mix(k) & mask;; i = (i + 1) & mask) {
+            if (t[i] == k) return;
+            if (t[i] == DEAD && dead == EMPTY) dead = i;
+            if (t[i] == EMPTY) {
+                if (dead != EMPTY) t[dead] = k;
+                else { t[i] = k; used++; }
+                return;
+            }
+        }
+    }
+    void del(uint64_t k) {
+        for (uint64_t i = mix(k) & mask;; i = (i + 1) & mask) {
+            if (t[i] == k) { t[i] = DEAD; return; }
+            if (t[i] == EMPTY) return;
+        }
+    }
 };
 
 // Symmetric CSR from normalised (min, max) keys, sorted and unique.
@@ -41,19 +87,19 @@ int csr_from_sorted_keys(uint32_t n, const std::vector<uint64_t>& keys, sgc_csr*
     }
     for (uint32_t v = 0; v < n; v++) out->row_ptr[v + 1] = out->row_ptr[v] + out->degree[v];
     std::vector<uint64_t> fill(out->row_ptr, out->row_ptr + n);
-    // keys ascending by (a, b): row a receives b in ascending order; row b
-    // receives a in ascending order too (a visits in ascending order).
+    // Keys ascend by (a, b), so row x first receives every a < x (keys (a, x),
+    // in ascending a) and then every b > x (keys (x, b), ascending b): each
+    // row comes out sorted without a per-row sort.
     for (uint64_t k : keys) {
         const uint32_t a = (uint32_t)(k >> 32), b = (uint32_t)k;
         out->col_idx[fill[a]++] = b;
         out->col_idx[fill[b]++] = a;
     }
-    for (uint32_t v = 0; v < n; v++) std::sort(out->col_idx + out->row_ptr[v], out->col_idx + out->row_ptr[v + 1]);
     return 0;
 }
 
 int csr_from_pairs(uint32_t n, std::vector<uint64_t>& keys, sgc_csr* out) {
-    std::sort(keys.begin(), keys.end());
+    __gnu_parallel::sort(keys.begin(), keys.end());
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
     return csr_from_sorted_keys(n, keys, out);
 }
@@ -137,21 +183,29 @@ int sgc_write_mtx(const char* path, const sgc_csr* g) {
 }
 
 uint64_t sgc_gen_init_stream(const sgc_csr* g, uint32_t* out) {
-    std::vector<std::pair<uint32_t, uint32_t>> e;
+    // Order of generate_init_stream: by (min degree desc, max degree desc) with
+    // std::sort. Each edge carries key = ~min << 32 | ~max, so `key <` gives
+    // exactly the reference comparator's answer for every pair and std::sort
+    // takes the same path (same output, ties included) without re-reading degrees.
+    struct E {
+        uint64_t key;
+        uint32_t u, v;
+    };
+    std::vector<E> e;
     e.reserve(g->nnz / 2);
-    for (uint32_t u = 0; u < g->n; u++)
-        for (uint64_t j = g->row_ptr[u]; j < g->row_ptr[u + 1]; j++)
-            if (u < g->col_idx[j]) e.emplace_back(u, g->col_idx[j]);
     const uint32_t* d = g->degree;
-    // hubs first: larger min-degree, then larger max-degree (ties: introsort order)
-    std::sort(e.begin(), e.end(), [d](const std::pair<uint32_t, uint32_t>& p, const std::pair<uint32_t, uint32_t>& q) {
-        const uint32_t lp = std::min(d[p.first], d[p.second]), lq = std::min(d[q.first], d[q.second]);
-        if (lp != lq) return lp > lq;
-        return std::max(d[p.first], d[p.second]) > std::max(d[q.first], d[q.second]);
-    });
+    for (uint32_t u = 0; u < g->n; u++)
+        for (uint64_t j = g->row_ptr[u]; j < g->row_ptr[u + 1]; j++) {
+            const uint32_t v = g->col_idx[j];
+            if (u < v) {
+                const uint32_t lo = std::min(d[u], d[v]), hi = std::max(d[u], d[v]);
+                e.push_back({((uint64_t)(~lo) << 32) | (uint32_t)(~hi), u, v});
+            }
+        }
+    std::sort(e.begin(), e.end(), [](const E& p, const E& q) { return p.key < q.key; });
     for (size_t i = 0; i < e.size(); i++) {
-        out[2 * i] = e[i].first;
-        out[2 * i + 1] = e[i].second;
+        out[2 * i] = e[i].u;
+        out[2 * i + 1] = e[i].v;
     }
     return e.size();
 }
@@ -160,7 +214,7 @@ int sgc_gen_churn_stream(const sgc_csr* g, uint64_t size, uint32_t insert_pct, u
                          uint8_t* types) {
     if (!g || g->n == 0) return -1;
     std::mt19937_64 rng(seed);
-    KeySet live;
+    KeySet live(g->nnz / 2 + size);
     std::vector<uint64_t> live_vec;  // (a << 32 | b), a < b, in the order the reference keeps
     live_vec.reserve(g->nnz / 2 + size);
     for (uint32_t u = 0; u < g->n; u++)
@@ -268,7 +322,9 @@ int sgc_gen_kcore_stream(const sgc_csr* g, uint64_t size, double pct, uint64_t s
     if (core_k) *core_k = k;
     if (core_size) *core_size = (uint32_t)C.size();
     if (C.size() < 2) return -2;
-    KeySet live;
+    uint64_t core_entries = 0;
+    for (uint32_t u : C) core_entries += g->row_ptr[u + 1] - g->row_ptr[u];
+    KeySet live(core_entries / 2 + size);
     std::vector<uint64_t> live_vec;
     for (uint32_t u : C)
         for (uint64_t j = g->row_ptr[u]; j < g->row_ptr[u + 1]; j++) {
@@ -315,27 +371,45 @@ int sgc_gen_rmat(uint32_t scale, uint32_t ef, double a, double b, double c, uint
     if (scale == 0 || scale > 31 || a < 0 || b < 0 || c < 0 || a + b + c > 1.0) return -1;
     const uint32_t n = 1u << scale;
     const uint64_t m = (uint64_t)ef * n;
-    std::vector<uint64_t> keys;
-    keys.reserve(m);
-    std::mt19937_64 rng(seed);
+    // Draws come in chunks of 2^20; chunk c uses mt19937_64(seed + c * golden)
+    // so the graph does not depend on the thread count.
+    const uint64_t CH = 1ull << 20;
+    const uint64_t nch = (m + CH - 1) / CH;
+    std::vector<std::vector<uint64_t>> parts(nch);
     const double ab = a + b, abc = a + b + c;
-    for (uint64_t i = 0; i < m; i++) {
-        uint32_t u = 0, v = 0;
-        for (uint32_t lvl = 0; lvl < scale; lvl++) {
-            const double r = (double)(rng() >> 11) * (1.0 / 9007199254740992.0);
-            const uint32_t bit = 1u << (scale - 1 - lvl);
-            if (r < a) {
-            } else if (r < ab) {
-                v |= bit;
-            } else if (r < abc) {
-                u |= bit;
-            } else {
-                u |= bit;
-                v |= bit;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t ci = 0; ci < (int64_t)nch; ci++) {
+        std::mt19937_64 rng(seed + (uint64_t)ci * 0x9E3779B97F4A7C15ull);
+        const uint64_t lo = (uint64_t)ci * CH, hi = std::min(m, lo + CH);
+        auto& out_keys = parts[ci];
+        out_keys.reserve(hi - lo);
+        for (uint64_t i = lo; i < hi; i++) {
+            uint32_t u = 0, v = 0;
+            for (uint32_t lvl = 0; lvl < scale; lvl++) {
+                const double r = (double)(rng() >> 11) * (1.0 / 9007199254740992.0);
+                const uint32_t bit = 1u << (scale - 1 - lvl);
+                if (r < a) {
+                } else if (r < ab) {
+                    v |= bit;
+                } else if (r < abc) {
+                    u |= bit;
+                } else {
+                    u |= bit;
+                    v |= bit;
+                }
             }
+            if (u != v) out_keys.push_back(key_of(std::min(u, v), std::max(u, v)));
         }
-        if (u == v) continue;
-        keys.push_back(key_of(std::min(u, v), std::max(u, v)));
+    }
+    std::vector<uint64_t> keys;
+    {
+        uint64_t tot = 0;
+        for (auto& p : parts) tot += p.size();
+        keys.reserve(tot);
+        for (auto& p : parts) {
+            keys.insert(keys.end(), p.begin(), p.end());
+            std::vector<uint64_t>().swap(p);
+        }
     }
     return csr_from_pairs(n, keys, out);
 }

@@ -78,7 +78,8 @@ struct Tier2Bufs {
 };
 // Runs the reference's Tier-2 (streamgc.cu:1057-1240) exactly; returns fixes.
 // Rows must be compact (after compaction + drain).
-uint32_t run_tier2(const Dev& g, Tier2Bufs& b, cudaStream_t s, uint32_t* host_scratch, bool* gave_up);
+uint32_t run_tier2(const Dev& g, Tier2Bufs& b, cudaStream_t s, uint32_t* host_scratch, bool* gave_up,
+                   uint64_t* launches);
 size_t tier2_cub_bytes(uint32_t n, uint32_t rev_cap);
 
 // Validator (sgc_tier2.cu): [violations, uncolored_with_edges, distinct_edges, max_color, out_of_range]

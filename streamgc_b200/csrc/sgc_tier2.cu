@@ -26,6 +26,8 @@
 
 namespace sgc {
 
+size_t tier2_cub_bytes(uint32_t n, uint32_t rev_cap);
+
 namespace {
 
 __device__ __forceinline__ uint64_t row_s(const Dev& g, uint32_t x) { return g.rp[x]; }
@@ -167,17 +169,35 @@ uint32_t grid_for(uint32_t items, uint32_t per_block) {
 }
 
 // Sequential ascending greedy over the ordered list in b.list (count in b.count[4]).
-uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, uint32_t* hs) {
+uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, uint32_t* hs, uint64_t* nl) {
     const uint32_t n = g.n;
     uint32_t* cnt = b.count;  // [0] rem count, [1] next count, [2] fixed, [3] rev count, [4] list count, [5] proc count
     cudaMemsetAsync(b.inL, 0, n, s);
     cudaMemsetAsync(b.done, 0, n, s);
     set_flags_kernel<<<grid_for(m, 256), 256, 0, s>>>(b.list, cnt + 4, b.inL, 1);
-    cudaMemsetAsync(cnt + 3, 0, sizeof(uint32_t), s);
-    rev_collect_kernel<<<148 * 8, 256, 0, s>>>(g, b.inL, b.rev_keys, cnt + 3, b.rev_cap);
-    cudaMemcpyAsync(hs, cnt + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    cudaStreamSynchronize(s);
-    uint32_t nrev = hs[0] < b.rev_cap ? hs[0] : b.rev_cap;
+    uint32_t nrev = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        cudaMemsetAsync(cnt + 3, 0, sizeof(uint32_t), s);
+        rev_collect_kernel<<<148 * 8, 256, 0, s>>>(g, b.inL, b.rev_keys, cnt + 3, b.rev_cap);
+        cudaMemcpyAsync(hs, cnt + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        nrev = hs[0];
+        if (nrev <= b.rev_cap || attempt == 1) break;
+        // more reverse entries than room: grow the buffers (and sort scratch) and collect again
+        cudaFree(b.rev_keys);
+        cudaFree(b.rev_keys2);
+        cudaFree(b.cub_tmp);
+        b.rev_cap = nrev + nrev / 4;
+        b.cub_tmp_bytes = tier2_cub_bytes(g.n, b.rev_cap);
+        if (cudaMalloc(&b.rev_keys, (size_t)b.rev_cap * 8) || cudaMalloc(&b.rev_keys2, (size_t)b.rev_cap * 8) ||
+            cudaMalloc(&b.cub_tmp, b.cub_tmp_bytes)) {
+            cudaGetLastError();
+            b.rev_cap = 0;
+            return 0;
+        }
+        *nl += 1;
+    }
+    if (nrev > b.rev_cap) nrev = b.rev_cap;
     if (nrev) {
         size_t tb = b.cub_tmp_bytes;
         cub::DeviceRadixSort::SortKeys(b.cub_tmp, tb, b.rev_keys, b.rev_keys2, (int)nrev, 0, 64, s);
@@ -186,6 +206,7 @@ uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, 
     uint32_t nrev_h = nrev;
     cudaMemcpyAsync(cnt + 3, &nrev_h, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
     rev_bounds_kernel<<<grid_for(m, 256), 256, 0, s>>>(b.list, cnt + 4, b.rev_keys, cnt + 3, b.rev_start, b.rev_end);
+    *nl += 5;
     // remaining positions 0..m-1
     uint32_t* rem = b.pend_v;
     uint32_t* nxt = b.pend_w;
@@ -201,6 +222,7 @@ uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, 
                                                              b.inL, b.done, b.rev_keys, b.rev_start, b.rev_end,
                                                              cnt + 2);
         set_flags_kernel<<<grid_for(left, 256), 256, 0, s>>>(proc, cnt + 5, b.done, 1);
+        *nl += 2;
         cudaMemcpyAsync(cnt + 0, cnt + 1, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(hs, cnt + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
         cudaStreamSynchronize(s);
@@ -235,7 +257,7 @@ size_t tier2_cub_bytes(uint32_t n, uint32_t rev_cap) {
     return a > c ? a : c;
 }
 
-uint32_t run_tier2(const Dev& g, Tier2Bufs& b, cudaStream_t s, uint32_t* hs, bool* gave_up) {
+uint32_t run_tier2(const Dev& g, Tier2Bufs& b, cudaStream_t s, uint32_t* hs, bool* gave_up, uint64_t* launches) {
     const uint32_t n = g.n;
     uint32_t total = 0;
     if (gave_up) *gave_up = false;
@@ -243,19 +265,22 @@ uint32_t run_tier2(const Dev& g, Tier2Bufs& b, cudaStream_t s, uint32_t* hs, boo
     cudaMemsetAsync(b.inU, 0, n, s);
     mark_uncolored_kernel<<<148 * 8, 256, 0, s>>>(g, b.inU);
     uint32_t m = select_flagged(n, b, b.inU, s, hs);
-    if (m) total += ordered_greedy(g, b, m, s, hs);
+    uint64_t nl = 2;
+    if (m) total += ordered_greedy(g, b, m, s, hs, &nl);
     // step 2: up to 30 detect / fix passes
     bool clean = false;
     for (int pass = 0; pass < 30; pass++) {
         cudaMemsetAsync(b.inF, 0, n, s);
         mark_conflict_kernel<<<148 * 8, 256, 0, s>>>(g, b.inF);
         m = select_flagged(n, b, b.inF, s, hs);
+        nl += 2;
         if (!m) { clean = true; break; }
-        const uint32_t fixed = ordered_greedy(g, b, m, s, hs);
+        const uint32_t fixed = ordered_greedy(g, b, m, s, hs, &nl);
         total += fixed;
         if (!fixed) break;
     }
     if (gave_up) *gave_up = !clean;
+    if (launches) *launches += nl;
     return total;
 }
 
