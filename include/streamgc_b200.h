@@ -147,6 +147,23 @@ int sgc_process_stream(sgc_handle* h, const EdgeUpdate* updates, uint64_t n, int
 /* Point queries against the last published snapshot (host arrays). */
 int sgc_query(sgc_handle* h, const uint32_t* vertices, uint16_t* colors, uint32_t n);
 
+/* Point queries exactly like sgc_query, for callers that must not allocate
+ * device memory: sgc_query takes scratch from the CUDA allocator on each call,
+ * which a serving thread whose tenants already fill their HBM budget, or a
+ * latency-bound path that must not enter the allocator, cannot afford. This
+ * variant calls no cudaMalloc, cudaFree or allocating routine; it stages the
+ * vertex ids and colors in a fixed scratch array compiled into the library
+ * (384 KiB, held by every GPU that loads the library until the process exits).
+ * At most SGC_QUERY_NOALLOC_MAX vertices per call; larger n is rejected with
+ * SGC_EINVAL. The first call on a device looks up the scratch's device address
+ * (once per device); make that first call before any CUDA stream capture. All
+ * handles on a device share the one scratch, so calls whose GPU work overlaps
+ * (different threads or streams) race on it; serialize them. Each call leaves
+ * its data in the scratch; the next call overwrites what it uses.
+ * No counterpart in the reference (it has no device query path). */
+#define SGC_QUERY_NOALLOC_MAX 65536u
+int sgc_query_noalloc(sgc_handle* h, const uint32_t* vertices, uint16_t* colors, uint32_t n);
+
 int sgc_download(sgc_handle* h, int what, void* dst, uint64_t bytes);
 int sgc_upload(sgc_handle* h, int what, const void* src, uint64_t bytes);   /* STATES, BITMAPS, HIST */
 /* FindAvailableColor(x) (color_select.cuh:93-115) on the current device state. */

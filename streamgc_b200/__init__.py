@@ -103,6 +103,7 @@ SIGNATURES = {
     "sgc_publish": (C.c_int, [_vp, C.POINTER(RepairReport)]),
     "sgc_process_stream": (C.c_int, [_vp, _vp, C.c_uint64, C.c_int, _u32p]),
     "sgc_query": (C.c_int, [_vp, _u32p, _u16p, C.c_uint32]),
+    "sgc_query_noalloc": (C.c_int, [_vp, _u32p, _u16p, C.c_uint32]),
     "sgc_download": (C.c_int, [_vp, C.c_int, _vp, C.c_uint64]),
     "sgc_upload": (C.c_int, [_vp, C.c_int, _vp, C.c_uint64]),
     "sgc_find_color": (C.c_int, [_vp, C.c_uint32, _u16p]),
@@ -359,6 +360,14 @@ class StreamGC:
         v = np.ascontiguousarray(vertices, dtype=np.uint32)
         out = np.zeros(len(v), dtype=np.uint16)
         _check(lib().sgc_query(self.h, _p(v, _u32p), _p(out, _u16p), len(v)), "sgc_query")
+        return out
+
+    def query_noalloc(self, vertices):
+        """Like query(), without any device allocation (fixed scratch, at most
+        65536 vertices per call; calls overlapping on the GPU race)."""
+        v = np.ascontiguousarray(vertices, dtype=np.uint32)
+        out = np.zeros(len(v), dtype=np.uint16)
+        _check(lib().sgc_query_noalloc(self.h, _p(v, _u32p), _p(out, _u16p), len(v)), "sgc_query_noalloc")
         return out
 
     def stats(self):

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -626,6 +627,62 @@ int sgc_query(sgc_handle* h, const uint32_t* v, uint16_t* out, uint32_t k) {
     CK(cudaMemcpyAsync(out, dout, (size_t)k * 2, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaFreeAsync(dv, h->stream));
     CK(cudaFreeAsync(dout, h->stream));
+    return sync(h);
+}
+
+}  // extern "C"
+
+// ---- point queries that allocate nothing ----
+// sgc_query takes its device scratch from the stream-ordered allocator on every
+// call. A serving thread that answers queries while its tenants already fill
+// their HBM budget, or one that must not enter the allocator on a latency-bound
+// path, cannot do that; it queries through this fixed scratch compiled into the
+// library instead: one static array per GPU that loads the library, held until
+// the process exits. Vertex ids occupy words [0, MAX); the uint16 colors are
+// packed after them.
+namespace {
+constexpr uint32_t QUERY_NOALLOC_MAX = SGC_QUERY_NOALLOC_MAX;
+static __device__ __align__(256) uint32_t g_query_scratch[QUERY_NOALLOC_MAX + QUERY_NOALLOC_MAX / 2];
+constexpr int MAX_DEVICES = 256;
+std::mutex g_query_scratch_mu;
+uint32_t* g_query_scratch_addr[MAX_DEVICES] = {};  // device address of the array, per device ordinal
+
+// Device address of the scratch on the current device (set-up once per device,
+// with that device current). In host code the array's name is only a host-side
+// stand-in, so kernels get this address, never &g_query_scratch.
+int query_scratch(int device, uint32_t** out) {
+    if (device < 0 || device >= MAX_DEVICES) return fail(SGC_EINVAL, "device ordinal %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_query_scratch_mu);
+    if (!g_query_scratch_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_query_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(SGC_ECUDA, "cudaGetSymbolAddress(query scratch) on device %d: %s", device,
+                        cudaGetErrorString(e));
+        g_query_scratch_addr[device] = static_cast<uint32_t*>(p);
+    }
+    *out = g_query_scratch_addr[device];
+    return SGC_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int sgc_query_noalloc(sgc_handle* h, const uint32_t* v, uint16_t* out, uint32_t k) {
+    if (!h || (k && (!v || !out))) return fail(SGC_EINVAL, "null argument");
+    if (k > QUERY_NOALLOC_MAX)
+        return fail(SGC_EINVAL, "sgc_query_noalloc: %u queries exceed its fixed scratch of %u; split the call", k,
+                    QUERY_NOALLOC_MAX);
+    if (!k) return SGC_OK;
+    CK(cudaSetDevice(h->device));
+    uint32_t* base = nullptr;
+    TRY(query_scratch(h->device, &base));
+    uint32_t* dv = base;
+    uint16_t* dout = reinterpret_cast<uint16_t*>(base + QUERY_NOALLOC_MAX);
+    CK(cudaMemcpyAsync(dv, v, (size_t)k * 4, cudaMemcpyHostToDevice, h->stream));
+    launch_query(h->snap[h->front], h->n, dv, dout, k, h->stream);
+    h->launches += 1;
+    CK(cudaMemcpyAsync(out, dout, (size_t)k * 2, cudaMemcpyDeviceToHost, h->stream));
     return sync(h);
 }
 
