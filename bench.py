@@ -160,7 +160,7 @@ def run_ours(a):
 
     t = time.time()
     h = S.StreamGC(g, epoch_size=E, histogram_threshold=HIST_THR, slack_pct=300, max_batch=1 << 20,
-                   device=local, profile=True)
+                   device=local, profile=True, exact_select=True)
     for s in range(0, len(init), 1 << 20):
         h.apply(init[s:s + (1 << 20)], S.MODE_CONCURRENT)
     rep = h.publish()
@@ -191,6 +191,8 @@ def run_ours(a):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    if a.profile_window:
+        torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
     with ClockSampler(local) as clk:
         for _ in range(a.steps):
             with torch.cuda.stream(ext):
@@ -204,6 +206,8 @@ def run_ours(a):
             b += 1
         ext.synchronize()
         torch.cuda.synchronize()
+        if a.profile_window:
+            torch.cuda.profiler.stop()
         step_ms = [x.elapsed_time(y) for x, y in evs]
         st1 = h.stats()
         # e2e: same steps through the C ABI from pinned host memory, wall clock
@@ -238,7 +242,7 @@ def run_ours(a):
         p50 = lat[len(lat) // 2]
         p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
         conf = dict(desc)
-        conf.update(mode="concurrent (warp per update) + repaired publish per epoch",
+        conf.update(mode="concurrent (warp per update) + repaired publish per epoch, exact color selection",
                     l2="flushed before every timed step (256 MiB write)", parallelism=f"replicas x{world}",
                     valid_after_run=val["violations"] == 0 and val["uncolored_with_edges"] == 0,
                     colors_used=int(val["max_color"]), static_greedy_colors=None,
@@ -338,6 +342,8 @@ def main():
     ap.add_argument("--workload", default="skewed", choices=["skewed", "small"])
     ap.add_argument("--cpu-batches", type=int, default=8, help="epochs timed on the CPU baseline (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--profile-window", action="store_true",
+                    help="bracket the device-timed steps with cudaProfilerStart/Stop (for ncu)")
     a = ap.parse_args()
     if a.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

@@ -37,6 +37,12 @@ typedef struct sgc_handle sgc_handle;
 
 /* sgc_options.flags */
 #define SGC_OPT_PROFILE  1u       /* time sweeps with CUDA events (sgc_stats.sweep_*) */
+/* Exact color selection above the histogram threshold: the first color no live
+ * neighbor holds, from a bitset the warp builds in shared memory while it scans
+ * the row, instead of the reference's global per-vertex histograms (which are
+ * never rebuilt and drift, color_select.cuh:120-209). No histogram rows are
+ * allocated. Bit-exact parity with the reference needs this flag off. */
+#define SGC_OPT_EXACT_SELECT 2u
 
 typedef struct sgc_options {
     uint32_t struct_size;      /* sizeof(sgc_options) */
@@ -73,7 +79,7 @@ typedef struct sgc_stats {
     uint32_t device_error;       /* bit 0: wait timeout, bit 1: bad update, bit 2: list overflow */
     uint32_t num_vertices;
     uint32_t num_high_degree;
-    uint32_t max_hist_colors;
+    uint32_t max_hist_colors;    /* histogram bins per row kept on the device (0 with SGC_OPT_EXACT_SELECT) */
     uint64_t total_slots;        /* slack CSR slots */
     uint64_t device_bytes;       /* device memory held by the handle */
     double   sweep_ms;           /* SGC_OPT_PROFILE: summed device time of sweep edge passes */

@@ -279,13 +279,13 @@ class StreamGC:
     """One graph resident on one GPU (a handle of the C ABI)."""
 
     def __init__(self, graph: Graph, epoch_size=32768, histogram_threshold=64, slack_pct=300,
-                 max_hist_colors=1024, max_batch=32768, device=0, profile=False):
+                 max_hist_colors=1024, max_batch=32768, device=0, profile=False, exact_select=False):
         L = lib()
         cfg = _Config(1, graph.n, graph.nnz, 1 << 20, epoch_size, 100, histogram_threshold, 0.2)
         opt = _Options()
         L.sgc_default_options(C.byref(opt))
         opt.slack_pct, opt.max_hist_colors, opt.max_batch, opt.device = slack_pct, max_hist_colors, max_batch, device
-        opt.flags = 1 if profile else 0
+        opt.flags = (1 if profile else 0) | (2 if exact_select else 0)
         self.h = _vp()
         self.graph = graph
         self.n = graph.n
@@ -394,7 +394,8 @@ class StreamGC:
 
     def hist(self):
         s = self.stats()
-        return self._dl("hist", np.uint32, s["num_high_degree"] * s["max_hist_colors"])
+        rows = s["num_high_degree"] if s["max_hist_colors"] else 0
+        return self._dl("hist", np.uint32, rows * s["max_hist_colors"])
 
     def row_ptr(self):
         return self._dl("row_ptr", np.uint64, self.n + 1)

@@ -65,7 +65,7 @@ struct sgc_handle {
     cudaStream_t stream = nullptr;
     sgc_options opt{};
     StreamGCConfig cfg{};
-    uint32_t n = 0, num_hd = 0, maxc = 1024;
+    uint32_t n = 0, num_hd = 0, maxc = 1024, hist_rows = 0;
     uint64_t total_slots = 0;
     uint64_t device_bytes = 0;
     Dev g{};
@@ -378,13 +378,16 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     Dev& g = h->g;
     g.n = n;
     g.maxc = h->maxc;
+    g.exact = (opt.flags & SGC_OPT_EXACT_SELECT) ? 1u : 0u;
+    const uint32_t hist_rows = g.exact ? 0u : num_hd;  // exact selection keeps no histogram rows
     uint64_t* d_rp; A(&d_rp, (size_t)n + 1);
     const uint64_t padded = ((h->total_slots + 3) & ~3ull) + 8;  // 16-byte loads stay inside
     uint32_t* d_col; A(&d_col, padded, 0xFF);
     A(&g.st, n, 0);
     A(&g.bm, n, 0);
     uint32_t* d_hdmap; A(&d_hdmap, n);
-    A(&g.hist, (size_t)num_hd * h->maxc, 0);
+    A(&g.hist, (size_t)hist_rows * h->maxc, 0);
+    h->hist_rows = hist_rows;
     uint32_t* d_deg; A(&d_deg, n);
     A(&g.hw, n);
     A(&g.dirty, (n + 31) / 32 + 1, 0);
@@ -695,7 +698,7 @@ int sgc_download(sgc_handle* h, int what, void* dst, uint64_t bytes) {
     switch (what) {
         case SGC_DL_STATES: src = h->g.st; need = h->n * 4ull; break;
         case SGC_DL_BITMAPS: src = h->g.bm; need = h->n * 8ull; break;
-        case SGC_DL_HIST: src = h->g.hist; need = (uint64_t)h->num_hd * h->maxc * 4; break;
+        case SGC_DL_HIST: src = h->g.hist; need = (uint64_t)h->hist_rows * h->maxc * 4; break;
         case SGC_DL_ROW_PTR: src = h->g.rp; need = (h->n + 1ull) * 8; break;
         case SGC_DL_COL: src = h->g.col; need = h->total_slots * 4; break;
         case SGC_DL_SNAPSHOT: src = h->snap[h->front]; need = h->n * 2ull; break;
@@ -735,7 +738,7 @@ int sgc_upload(sgc_handle* h, int what, const void* src, uint64_t bytes) {
     switch (what) {
         case SGC_DL_STATES: dst = h->g.st; need = h->n * 4ull; break;
         case SGC_DL_BITMAPS: dst = h->g.bm; need = h->n * 8ull; break;
-        case SGC_DL_HIST: dst = h->g.hist; need = (uint64_t)h->num_hd * h->maxc * 4; break;
+        case SGC_DL_HIST: dst = h->g.hist; need = (uint64_t)h->hist_rows * h->maxc * 4; break;
         default: return fail(SGC_EINVAL, "upload target %d not writable", what);
     }
     if (bytes != need) return fail(SGC_EINVAL, "upload target %d needs exactly %llu bytes", what, (unsigned long long)need);
@@ -789,7 +792,7 @@ int sgc_get_stats(sgc_handle* h, sgc_stats* o) {
     o->device_error = c.err;
     o->num_vertices = h->n;
     o->num_high_degree = h->num_hd;
-    o->max_hist_colors = h->maxc;
+    o->max_hist_colors = h->hist_rows ? h->maxc : 0;
     o->total_slots = h->total_slots;
     o->device_bytes = h->device_bytes;
     o->sweep_ms = h->sweep_ms;

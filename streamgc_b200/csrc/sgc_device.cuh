@@ -42,6 +42,8 @@ enum : uint32_t {
 struct Dev {
     uint32_t n;
     uint32_t maxc;                 // histogram colors per row (multiple of 4)
+    uint32_t exact;                // 1: colors above the threshold are chosen from the live
+                                   // neighbors (no global histogram rows are kept)
     const uint64_t* rp;            // n+1 row starts (64-bit: slabs beyond 2^32 slots)
     uint32_t* col;                 // slots, padded so 16-byte loads never leave the allocation
     uint32_t* st;                  // packed (color | version << 16)
@@ -319,10 +321,50 @@ __device__ __forceinline__ uint16_t warp_fac_scan(const Dev& g, uint32_t x, cons
     return 256;
 }
 
+// Exact selection above the threshold: the first color no live neighbor holds.
+// Colors 1..64 collect in a 64-bit lane mask, higher ones (up to 2047) in a
+// 2048-bit set the warp fills in shared memory while it scans the row (the
+// calling kernels run at most 8 warps per block).
+__device__ __forceinline__ uint16_t warp_fac_exact(const Dev& g, uint32_t x, const uint32_t* cols) {
+    __shared__ uint32_t s_used[8][64];
+    uint32_t* used = s_used[(threadIdx.x >> 5) & 7];
+    const uint32_t lane = lane_id();
+    used[lane] = 0;
+    used[lane + 32] = 0;
+    __syncwarp();
+    unsigned long long low = 0;
+    const uint64_t s = g.rp[x], e = s + ld_cg(g.hw + x);
+    warp_for_each(g.col, s, e, [&](uint64_t, uint32_t ng) {
+        if (ng == INV || ng >= g.n) return;
+        const uint16_t c = color_of(ld_cg(cols + ng));
+        if (c == 0) return;
+        if (c <= 64) low |= 1ull << (c - 1);
+        else if (c < 2048) atomicOr(&used[c >> 5], 1u << (c & 31));
+    });
+    const uint32_t lo = __reduce_or_sync(FULL, (uint32_t)low), hi = __reduce_or_sync(FULL, (uint32_t)(low >> 32));
+    const unsigned long long m = ((unsigned long long)hi << 32) | lo;
+    __syncwarp();
+    if (~m) return (uint16_t)__ffsll((long long)~m);
+    uint32_t w0 = ~used[lane], w1 = ~used[lane + 32];
+    if (lane < 2) w0 = 0;  // words 0-1 hold colors 0..64: settled by the lane masks
+    if (lane == 2) w0 &= ~1u;  // color 64 sits in bit 0 of word 2 and is taken (mask was full)
+    const uint32_t b0 = __ballot_sync(FULL, w0 != 0);
+    if (b0) {
+        const int src = __ffs(b0) - 1;
+        return (uint16_t)(src * 32 + __shfl_sync(FULL, __ffs(w0) - 1, src));
+    }
+    const uint32_t b1 = __ballot_sync(FULL, w1 != 0);
+    if (b1) {
+        const int src = __ffs(b1) - 1;
+        return (uint16_t)(1024 + src * 32 + __shfl_sync(FULL, __ffs(w1) - 1, src));
+    }
+    return 2048;
+}
+
 // FindAvailableColor: histogram row when the vertex has one, else bitmap.
 __device__ __forceinline__ uint16_t warp_fac(const Dev& g, uint32_t x, const uint32_t* cols) {
     const uint32_t hd = __ldg(g.hdmap + x);
-    if (hd != EMPTY) return warp_fac_hist(g.hist + (uint64_t)hd * g.maxc, g.maxc);
+    if (hd != EMPTY) return g.exact ? warp_fac_exact(g, x, cols) : warp_fac_hist(g.hist + (uint64_t)hd * g.maxc, g.maxc);
     const uint64_t bmv = ld_cg(g.bm + x);
     if (~bmv) return (uint16_t)__ffsll((long long)~bmv);
     return warp_fac_scan(g, x, cols);
@@ -334,7 +376,7 @@ __device__ __forceinline__ void nbr_color_change(const Dev& g, uint32_t x, uint1
     if (oldc == newc) return;
     if (newc != 0 && newc <= 64) atomicOr((unsigned long long*)(g.bm + x), 1ull << (newc - 1));
     const uint32_t hd = __ldg(g.hdmap + x);
-    if (hd != EMPTY) {
+    if (hd != EMPTY && !g.exact) {
         uint32_t* h = g.hist + (uint64_t)hd * g.maxc;
         if (oldc != 0 && oldc <= g.maxc) atomicSub(h + oldc - 1, 1u);
         if (newc != 0 && newc <= g.maxc) atomicAdd(h + newc - 1, 1u);
@@ -344,12 +386,12 @@ __device__ __forceinline__ void new_nbr(const Dev& g, uint32_t x, uint16_t c) {
     if (c == 0) return;
     if (c <= 64) atomicOr((unsigned long long*)(g.bm + x), 1ull << (c - 1));
     const uint32_t hd = __ldg(g.hdmap + x);
-    if (hd != EMPTY && c <= g.maxc) atomicAdd(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
+    if (hd != EMPTY && !g.exact && c <= g.maxc) atomicAdd(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
 }
 __device__ __forceinline__ void removed_nbr(const Dev& g, uint32_t x, uint16_t c) {
     if (c == 0) return;
     const uint32_t hd = __ldg(g.hdmap + x);
-    if (hd != EMPTY && c <= g.maxc) atomicSub(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
+    if (hd != EMPTY && !g.exact && c <= g.maxc) atomicSub(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
 }
 
 // ---------------- recolor (recolor.cu:87-163) ----------------
@@ -362,9 +404,12 @@ __device__ __forceinline__ uint32_t warp_load_state(const Dev& g, uint32_t x) {
 
 // recolor_vertex: new = FAC(x); if different, CAS (new, version+1) in, retrying
 // on a fresh word; the winner propagates old -> new to every live row entry.
-__device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x) {
+// `chosen` (nonzero) is FAC(x) already computed on the current state by the
+// caller; in stream order nothing changes in between, so it equals the call
+// the reference makes here.
+__device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x, uint16_t chosen = 0) {
     uint32_t cur = warp_load_state(g, x);
-    uint16_t newc = warp_fac(g, x, g.st);
+    uint16_t newc = chosen ? chosen : warp_fac(g, x, g.st);
     if (newc == color_of(cur)) return;
     for (;;) {
         const uint32_t want = pack(newc, (uint16_t)(version_of(cur) + 1));
@@ -391,7 +436,7 @@ __device__ __forceinline__ void warp_try_reduce(const Dev& g, uint32_t x, uint16
     if (cur == 0) return;
     if (freed >= cur) return;
     const uint16_t best = warp_fac(g, x, g.st);
-    if (best < cur) warp_recolor(g, x);
+    if (best < cur) warp_recolor(g, x, best);
 }
 
 // Colors x with FAC when it is still uncolored; version becomes 1

@@ -100,11 +100,21 @@ def test_tier2_exact_on_forced_conflicts():
         g.close()
 
 
+COLOR_SLACK = 4  # concurrent mode may use at most this many colors above the sequential reference
+
+
+@pytest.mark.parametrize("exact", [True, False])
 @pytest.mark.parametrize("name", ["delaunay2k", "rmat11", "overflow512"])
-def test_concurrent_mode_publishes_proper_snapshots(name):
+def test_concurrent_mode_publishes_proper_snapshots(name, exact):
     """Concurrent batches: every published snapshot is proper on the live CSR,
-    the edge multiset per row equals the sequential one, colors within slack."""
-    c, g, h = _both(name)
+    the edge multiset per row equals the sequential one, and -- with exact
+    color selection, the concurrent configuration -- colors stay within the
+    sequential reference's count + COLOR_SLACK. (With the reference's drifting
+    histograms the count depends on the interleaving, so only properness holds.)"""
+    c = MG.build_case(name)
+    g = O.Oracle(c["rp"], c["col"], c["deg"], hist_threshold=c["thr"], slack_pct=c["slack"])
+    h = S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"]), epoch_size=c["E"], histogram_threshold=c["thr"],
+                   slack_pct=c["slack"], max_batch=c["batch"], exact_select=exact)
     try:
         g.process_stream_repaired(c["init"], c["E"], c["batch"])
         for ups in (c["init"], c["bench"]):
@@ -131,7 +141,8 @@ def test_concurrent_mode_publishes_proper_snapshots(name):
             a = np.sort(gc[gr[x]:gr[x + 1]])
             b = np.sort(ocol[orp[x]:orp[x + 1]])
             assert np.array_equal(a, b), f"row {x}"
-        assert int(h.colors().max()) <= oracle_colors + 4
+        if exact:
+            assert int(h.colors().max()) <= oracle_colors + COLOR_SLACK
         assert h.stats()["device_error"] == 0
     finally:
         h.close()
