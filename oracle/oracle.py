@@ -48,7 +48,7 @@ def lib():
             build()
         L = C.CDLL(LIB_PATH)
         sig = {
-            "og_create": (_vp, [C.c_uint32, _u64p, _u32p, _u32p, C.c_uint32, C.c_uint32, C.c_uint32]),
+            "og_create": (_vp, [C.c_uint32, _u64p, _u32p, _u32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]),
             "og_destroy": (None, [_vp]),
             "og_num_vertices": (C.c_uint32, [_vp]),
             "og_total_slots": (C.c_uint64, [_vp]),
@@ -118,14 +118,17 @@ def updates_from(pairs, types=None):
 class Oracle:
     """Single-GPU StreamGC state restated on the CPU (sequential, stream order)."""
 
-    def __init__(self, row_ptr, col, degree, hist_threshold=64, slack_pct=300, max_hist_colors=1024):
+    def __init__(self, row_ptr, col, degree, hist_threshold=64, slack_pct=300, max_hist_colors=1024,
+                 exact=False):
+        """exact: exact color selection above the threshold and the independent-set
+        Tier-1 (the concurrent configuration's rules); default: the reference's."""
         self.L = lib()
         rp = np.ascontiguousarray(row_ptr, dtype=np.uint64)
         col = np.ascontiguousarray(col, dtype=np.uint32)
         deg = np.ascontiguousarray(degree, dtype=np.uint32)
         self.n = len(rp) - 1
         self.h = self.L.og_create(self.n, _p(rp, _u64p), _p(col, _u32p), _p(deg, _u32p),
-                                  hist_threshold, slack_pct, max_hist_colors)
+                                  hist_threshold, slack_pct, max_hist_colors, 1 if exact else 0)
 
     def close(self):
         if self.h:

@@ -65,6 +65,7 @@ struct Oracle {
     uint32_t n = 0;
     uint32_t hist_thr = 64;
     uint32_t maxc = 1024;          // MAX_HISTOGRAM_COLORS
+    bool exact = false;            // exact selection above the threshold + independent-set Tier-1
     std::vector<uint64_t> rp;      // logical row starts, rp[n] = total slots
     std::vector<uint32_t> col;     // slack CSR slots
     std::vector<uint32_t> st;      // packed (color | version << 16)
@@ -92,7 +93,7 @@ struct Oracle {
     inline uint64_t prio(uint32_t x) const { return ((uint64_t)deg[x] << 32) | x; }
     inline uint32_t* hrow(uint32_t x) {
         uint32_t h = hdmap[x];
-        return h == EMPTY ? nullptr : &hist[(uint64_t)h * maxc];
+        return (h == EMPTY || exact) ? nullptr : &hist[(uint64_t)h * maxc];
     }
 
     // -------- color selection (color_select.cuh:10-115) --------
@@ -130,9 +131,24 @@ struct Oracle {
         }
         return (uint16_t)(mc + 1);
     }
+    // Exact selection: the first color (1..2047) no live neighbor holds, else 2048.
+    uint16_t fac_exact(uint32_t x, const std::vector<uint32_t>& cols, uint64_t& b) const {
+        std::vector<uint8_t> used(2048, 0);
+        for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+            uint32_t ng = col[j];
+            b += 4;
+            if (ng == INV || ng >= n) continue;
+            uint16_t c = (uint16_t)(cols[ng] & 0xFFFFu);
+            b += 4;
+            if (c > 0 && c < 2048) used[c] = 1;
+        }
+        for (uint16_t c = 1; c < 2048; c++)
+            if (!used[c]) return c;
+        return 2048;
+    }
     uint16_t fac(uint32_t x, const std::vector<uint32_t>& cols, uint64_t& b) const {
         b += 4;  // high_degree_map read
-        if (hdmap[x] != EMPTY) return fac_hist(x, b);
+        if (hdmap[x] != EMPTY) return exact ? fac_exact(x, cols, b) : fac_hist(x, b);
         return fac_bitmap(x, cols, b);
     }
 
@@ -207,9 +223,9 @@ struct Oracle {
     }
 
     // -------- recolor (recolor.cu:49-163) --------
-    void recolor(uint32_t x, uint64_t& b) {
+    void recolor(uint32_t x, uint64_t& b, uint16_t chosen = 0) {
         uint16_t oldc = color(x);
-        uint16_t newc = fac(x, st, b);
+        uint16_t newc = chosen ? chosen : fac(x, st, b);
         b += 4;
         if (newc == oldc) return;
         uint16_t nv = (uint16_t)(ver(x) + 1);
@@ -230,7 +246,7 @@ struct Oracle {
         if (cur == 0) return;
         if (freed >= cur) return;
         uint16_t best = fac(x, st, b);
-        if (best < cur) recolor(x, b);
+        if (best < cur) recolor(x, b, best);
     }
 
     // -------- one update (local_update.cu:61-147), stream order --------
@@ -411,9 +427,69 @@ struct Oracle {
         bytes.tier1 += b;
         return count;
     }
+    // Independent-set sweep (exact selection): flag every vertex the reference
+    // rule would recolor, then recolor only those with no flagged neighbor of
+    // higher priority, each to the first color its neighbors leave free
+    // (start-of-sweep colors). Returns the number flagged.
+    uint32_t tier1_indep_sweep() {
+        std::vector<uint32_t> old = st;
+        std::vector<uint8_t> need(n, 0);
+        uint32_t count = 0;
+        uint64_t b = 0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : count, b)
+        for (int64_t xi = 0; xi < (int64_t)n; xi++) {
+            uint32_t x = (uint32_t)xi;
+            uint16_t my = (uint16_t)(old[x] & 0xFFFFu);
+            bool has = false, conf = false;
+            for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                uint32_t ng = col[j];
+                b += 4;
+                if (ng == INV) continue;
+                has = true;
+                if (my == 0 || ng >= n) continue;
+                b += 4;
+                if ((uint16_t)(old[ng] & 0xFFFFu) == my && prio(x) < prio(ng)) conf = true;
+            }
+            bool d = (my == 0) ? has : conf;
+            if (d) {
+                need[x] = 1;
+                count++;
+                if (my != 0 && my <= 64) { bm[x] |= 1ull << (my - 1); b += 16; }
+            }
+        }
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : b)
+        for (int64_t xi = 0; xi < (int64_t)n; xi++) {
+            uint32_t x = (uint32_t)xi;
+            if (!need[x]) continue;
+            bool blocked = false;
+            for (uint64_t j = rp[x]; j < rp[x + 1] && !blocked; j++) {
+                uint32_t y = col[j];
+                b += 4;
+                if (y == INV || y >= n || y == x) continue;
+                if (need[y] && prio(x) < prio(y)) blocked = true;
+            }
+            if (blocked) continue;
+            uint16_t c = fac(x, old, b);
+            st[x] = sgc_pack_state(c, (uint16_t)((old[x] >> 16) + 1));
+        }
+        bytes.tier1 += b;
+        return count;
+    }
+
     // run_conflict_repair loop (streamgc.cu:1317-1393). Returns iterations run;
     // *last_count = conflicts counted by the last sweep.
     int tier1(uint32_t* history, int hist_cap, uint32_t* last_count) {
+        if (exact) {  // independent-set rule: counts only fall; up to 64 sweeps
+            uint32_t cnt = 0;
+            for (int it = 0; it < 64; it++) {
+                rebuild_all(bytes.tier1);
+                cnt = tier1_indep_sweep();
+                if (history && it < hist_cap) history[it] = cnt;
+                if (cnt == 0) { if (last_count) *last_count = 0; return it + 1; }
+            }
+            if (last_count) *last_count = cnt;
+            return 64;
+        }
         uint32_t prev = UINT32_MAX;
         int plateau = 0;
         uint32_t cnt = 0;
@@ -516,8 +592,9 @@ extern "C" {
 // loader order, the rest INVALID. High-degree rows: degree > threshold
 // (streamgc.cu:225-250), histogram row index in vertex order.
 void* og_create(uint32_t n, const uint64_t* row_ptr, const uint32_t* col_idx, const uint32_t* degree,
-                uint32_t hist_thr, uint32_t slack_pct, uint32_t max_hist_colors) {
+                uint32_t hist_thr, uint32_t slack_pct, uint32_t max_hist_colors, uint32_t flags) {
     Oracle* g = new Oracle();
+    g->exact = (flags & 1u) != 0;
     g->n = n;
     g->hist_thr = hist_thr;
     g->maxc = max_hist_colors ? max_hist_colors : SGC_MAX_HISTOGRAM_COLORS_DEFAULT;
@@ -546,7 +623,7 @@ void* og_create(uint32_t n, const uint64_t* row_ptr, const uint32_t* col_idx, co
     g->hdmap.assign(n, EMPTY);
     for (uint32_t x = 0; x < n; x++)
         if (degree[x] > hist_thr) g->hdmap[x] = g->num_hd++;
-    g->hist.assign((size_t)g->num_hd * g->maxc, 0);
+    g->hist.assign(g->exact ? 0 : (size_t)g->num_hd * g->maxc, 0);
     g->snap.assign(n, 0);
     g->ovf.resize(OVF_CAP);
     return g;
@@ -556,7 +633,7 @@ void og_destroy(void* h) { delete (Oracle*)h; }
 
 uint32_t og_num_vertices(void* h) { return ((Oracle*)h)->n; }
 uint64_t og_total_slots(void* h) { return ((Oracle*)h)->rp.back(); }
-uint32_t og_num_high_degree(void* h) { return ((Oracle*)h)->num_hd; }
+uint32_t og_num_high_degree(void* h) { return ((Oracle*)h)->exact ? 0 : ((Oracle*)h)->num_hd; }
 uint32_t og_max_hist_colors(void* h) { return ((Oracle*)h)->maxc; }
 
 // ---------------- updates and epochs ----------------

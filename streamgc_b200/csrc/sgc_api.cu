@@ -189,16 +189,16 @@ int drain(sgc_handle* h, bool ordered, unsigned long long* failed_counter) {
 }
 
 // Sweep with optional event timing around the edge passes.
-int sweep(sgc_handle* h, SweepMode mode) {
-    const bool prof = (h->opt.flags & SGC_OPT_PROFILE) != 0 && mode == SWEEP_TIER1;
+int sweep(sgc_handle* h, SweepMode mode, bool list = false) {
+    const bool prof = (h->opt.flags & SGC_OPT_PROFILE) != 0 && mode != SWEEP_REBUILD;
     cudaEvent_t a = nullptr, b = nullptr;
     if (prof) {
         a = take_event(h);
         b = take_event(h);
         cudaEventRecord(a, h->stream);
     }
-    launch_sweep(h->g, h->sb, mode, h->num_sms, h->stream);
-    h->launches += mode == SWEEP_TIER1 ? 4 : 2;
+    launch_sweep(h->g, h->sb, mode, list, h->num_sms, h->stream);
+    h->launches += mode == SWEEP_REBUILD ? 2 : 4;
     if (prof) {
         cudaEventRecord(b, h->stream);
         h->ev_pending.push_back({a, b});
@@ -206,8 +206,8 @@ int sweep(sgc_handle* h, SweepMode mode) {
     return check_cuda("sweep");
 }
 
-int build_items(sgc_handle* h) {
-    launch_build_items(h->g, h->sb, h->stream);
+int build_items(sgc_handle* h, bool list = false) {
+    launch_build_items(h->g, h->sb, list, h->stream);
     h->launches += 1;
     return check_cuda("build_items");
 }
@@ -223,29 +223,55 @@ void publish_snapshot(sgc_handle* h) {
 // items built. Tier-2 runs unless convergence on a mirror-complete CSR proves
 // it a no-op.
 int repair_loop(sgc_handle* h, sgc_repair_report* rep) {
+    // Reference rule (deterministic parity): at most 20 sweeps, stop at 0 or after
+    // 3 equal counts (streamgc.cu:1317-1393). Independent-set rule (exact color
+    // selection): each sweep resolves at least the highest-priority conflict and
+    // creates none, so the count only falls; up to 64 sweeps.
+    const bool indep = h->g.exact != 0;
+    const SweepMode mode = indep ? SWEEP_INDEP : SWEEP_TIER1;
+    const int max_sweeps = indep ? 64 : 20;
+    uint32_t* count_ptr = indep ? h->sb.need_count : &h->ctl->pend_count;
     uint32_t prev = 0xFFFFFFFFu, cnt = 0;
     int plateau = 0, it = 0;
     CK(cudaMemsetAsync(&h->ctl->symsum, 0, 16, h->stream));
-    for (it = 0; it < 20; it++) {
-        TRY(sweep(h, SWEEP_TIER1));
+    CK(cudaMemsetAsync(h->sb.swept, 0, 16, h->stream));
+    for (it = 0; it < max_sweeps; it++) {
+        // Sweep 0 visits every vertex. Later Jacobi sweeps visit only the
+        // vertices recolored by the previous sweep and their neighbors (plus,
+        // under the independent-set rule, every vertex still conflicted):
+        // every other vertex sees the colors it saw then, so its rebuilt bitmap
+        // and its decision cannot change (the result equals a full sweep).
+        if (it > 0) {
+            launch_next_worklist(h->g, h->sb, h->num_sms, h->stream);
+            TRY(build_items(h, true));
+            h->launches += 2;
+        }
+        TRY(sweep(h, mode, it > 0));
         h->tier1_sweeps++;
-        CK(cudaMemcpyAsync(h->h_small, &h->ctl->pend_count, 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(h->h_small, count_ptr, 4, cudaMemcpyDeviceToHost, h->stream));
         if (it == 0) CK(cudaMemcpyAsync(h->h_small + 2, &h->ctl->symsum, 16, cudaMemcpyDeviceToHost, h->stream));
         h->d2h_bytes += it == 0 ? 20 : 4;
         TRY(sync(h));
         cnt = h->h_small[0];
         if (it == 0) h->live_entries = *(unsigned long long*)(h->h_small + 4);
         if (cnt == 0) break;
-        if (cnt == prev) {
-            if (++plateau >= 3) break;
-        } else {
-            plateau = 0;
+        if (!indep) {
+            if (cnt == prev) {
+                if (++plateau >= 3) break;
+            } else {
+                plateau = 0;
+            }
         }
         prev = cnt;
     }
     const unsigned long long sym = *(unsigned long long*)(h->h_small + 2);
-    const uint32_t iters = it < 20 ? it + 1 : 20;
-    if (h->opt.flags & SGC_OPT_PROFILE) h->sweep_bytes += (uint64_t)iters * (8ull * h->live_entries + 28ull * h->n);
+    const uint32_t iters = it < max_sweeps ? it + 1 : max_sweeps;
+    if (h->opt.flags & SGC_OPT_PROFILE) {
+        unsigned long long sw[2];
+        CK(cudaMemcpyAsync(sw, h->sb.swept, 16, cudaMemcpyDeviceToHost, h->stream));
+        TRY(sync(h));
+        h->sweep_bytes += 8ull * sw[0] + 28ull * sw[1];
+    }
     sgc_repair_report r{};
     r.tier1_iterations = iters;
     r.tier1_last_count = cnt;
@@ -390,6 +416,8 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     h->hist_rows = hist_rows;
     uint32_t* d_deg; A(&d_deg, n);
     A(&g.hw, n);
+    if (g.exact) A(&g.holes, n, 0);  // lazy compaction goes with the concurrent configuration
+    else g.holes = nullptr;
     A(&g.dirty, (n + 31) / 32 + 1, 0);
     A(&g.edited, (n + 31) / 32 + 1, 0);
     A(&g.ovf, OVF_CAP);
@@ -462,6 +490,13 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     sb.fac_count = &h->ctl->fac_count;
     sb.symsum = &h->ctl->symsum;
     sb.live = &h->ctl->live;
+    A(&sb.wmark, (n + 31) / 32 + 1, 0);
+    A(&sb.wl, n);
+    A(&sb.wl_count, 4, 0);
+    A(&sb.swept, 2, 0);
+    A(&sb.needf, n, 0);
+    A(&sb.need_v, n);
+    A(&sb.need_count, 4, 0);
     A(&h->dirty_list, n);
     // tier-2 buffers
     Tier2Bufs& t2 = h->t2;

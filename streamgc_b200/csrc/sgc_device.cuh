@@ -52,6 +52,7 @@ struct Dev {
     uint32_t* hist;                // num_hd * maxc counters
     const uint32_t* deg;           // frozen initial degree: priority = (deg << 32) | id
     uint32_t* hw;                  // per-row high-water mark (slots, relative to rp[x])
+    uint32_t* holes;               // lazy compaction (exact mode): INV slots inside [rp, rp+hw); else null
     uint32_t* dirty;               // bitmask of rows edited since their last compaction
     uint32_t* edited;              // bitmask of rows edited since creation (clear = pristine:
                                    // base entries sorted ascending in [rp, rp+hw), INV after)
@@ -217,7 +218,8 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
         if (lane_id() == 0) {
             old = atomicCAS(g.col + p, INV, nbr);
             if (old == INV) {
-                atomicMax(g.hw + x, (uint32_t)(p - s + 1));
+                const uint32_t prev_hw = atomicMax(g.hw + x, (uint32_t)(p - s + 1));
+                if (g.holes && (uint32_t)(p - s) < prev_hw) atomicSub(g.holes + x, 1u);  // filled a hole
                 mark_dirty(g, x);
             }
         }
@@ -239,7 +241,10 @@ __device__ __forceinline__ void warp_remove_slot(const Dev& g, uint32_t x, uint3
             uint32_t old = 0;
             if (lane_id() == 0) {
                 old = atomicCAS(g.col + p, nbr, INV);
-                if (old == nbr) mark_dirty(g, x);
+                if (old == nbr) {
+                    mark_dirty(g, x);
+                    if (g.holes) atomicAdd(g.holes + x, 1u);
+                }
             }
             old = __shfl_sync(FULL, old, 0);
             if (old == nbr) return;
@@ -254,7 +259,10 @@ __device__ __forceinline__ void warp_remove_slot(const Dev& g, uint32_t x, uint3
         uint32_t old = 0;
         if (lane_id() == 0) {
             old = atomicCAS(g.col + p, nbr, INV);
-            if (old == nbr) mark_dirty(g, x);
+            if (old == nbr) {
+                mark_dirty(g, x);
+                if (g.holes) atomicAdd(g.holes + x, 1u);
+            }
         }
         old = __shfl_sync(FULL, old, 0);
         if (old == nbr) return;

@@ -229,7 +229,11 @@ __global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __r
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
         const uint32_t x = list[k];
         const uint64_t s = g.rp[x];
-        const uint64_t e = s + g.hw[x];
+        const uint32_t hwx = g.hw[x];
+        // Lazy mode: a row whose holes fill at most a quarter of its extent stays
+        // as it is (every reader skips INV slots); it is compacted later.
+        if (g.holes && 4u * g.holes[x] <= hwx) continue;
+        const uint64_t e = s + hwx;
         uint64_t w = s;
         for (uint64_t c = s & ~3ull; c < e; c += 128) {
             const uint64_t i = c + 4ull * lane;
@@ -254,7 +258,10 @@ __global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __r
             __syncwarp();
         }
         for (uint64_t j = w + lane; j < e; j += 32) g.col[j] = INV;
-        if (lane == 0) g.hw[x] = (uint32_t)(w - s);
+        if (lane == 0) {
+            g.hw[x] = (uint32_t)(w - s);
+            if (g.holes) g.holes[x] = 0;
+        }
         __syncwarp();
     }
 }
@@ -292,7 +299,8 @@ __device__ __forceinline__ bool warp_drain_insert(const Dev& g, uint32_t x, uint
         if (lane_id() == 0) {
             old = atomicCAS(g.col + p, INV, nbr);
             if (old == INV) {
-                atomicMax(g.hw + x, (uint32_t)(p - s + 1));
+                const uint32_t prev_hw = atomicMax(g.hw + x, (uint32_t)(p - s + 1));
+                if (g.holes && (uint32_t)(p - s) < prev_hw) atomicSub(g.holes + x, 1u);
                 mark_dirty(g, x);
             }
         }
@@ -348,27 +356,34 @@ void launch_query(const uint16_t* snap, uint32_t n, const uint32_t* v, uint16_t*
 // degree-balanced sweep: rebuild + Tier-1 decision (Jacobi)
 // ---------------------------------------------------------------------------
 
-__global__ void build_items_kernel(Dev g, SweepBufs b) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t k = 0;
-    if (x < g.n) {
-        const uint32_t len = g.hw[x];
-        if (len > SWEEP_TINY) k = (len + SWEEP_CH - 1) / SWEEP_CH;
+__global__ void build_items_kernel(Dev g, SweepBufs b, int list) {
+    const uint32_t lim = list ? *b.wl_count : g.n;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < lim; base += stride) {  // warp-uniform trip count
+        const uint32_t t = base + threadIdx.x;
+        uint32_t k = 0, x = 0;
+        if (t < lim) {
+            x = list ? b.wl[t] : t;
+            const uint32_t len = g.hw[x];
+            if (len > SWEEP_TINY) k = (len + SWEEP_CH - 1) / SWEEP_CH;
+        }
+        uint32_t total = 0;
+        const uint32_t off = warp_excl_scan(k, total);
+        uint32_t wbase = 0;
+        if (lane_id() == 0 && total) wbase = atomicAdd(b.item_count, total);
+        wbase = __shfl_sync(FULL, wbase, 0);
+        if (wbase + off + k > b.item_cap) {
+            if (k) atomicOr(g.err, ERR_LIST_OVERFLOW);
+            continue;
+        }
+        for (uint32_t j = 0; j < k; j++) b.items[wbase + off + j] = (unsigned long long)x | ((unsigned long long)j << 32);
     }
-    uint32_t total = 0;
-    const uint32_t off = warp_excl_scan(k, total);
-    uint32_t base = 0;
-    if (lane_id() == 0 && total) base = atomicAdd(b.item_count, total);
-    base = __shfl_sync(FULL, base, 0);
-    if (base + off + k > b.item_cap) {
-        if (k) atomicOr(g.err, ERR_LIST_OVERFLOW);
-        return;
-    }
-    for (uint32_t j = 0; j < k; j++) b.items[base + off + j] = (unsigned long long)x | ((unsigned long long)j << 32);
 }
-void launch_build_items(const Dev& g, const SweepBufs& b, cudaStream_t s) {
+void launch_build_items(const Dev& g, const SweepBufs& b, bool list, cudaStream_t s) {
     cudaMemsetAsync(b.item_count, 0, sizeof(uint32_t), s);
-    build_items_kernel<<<(g.n + 255) / 256, 256, 0, s>>>(g, b);
+    uint32_t blocks = (g.n + 255) / 256;
+    if (list && blocks > 148 * 8) blocks = 148 * 8;
+    build_items_kernel<<<blocks, 256, 0, s>>>(g, b, list ? 1 : 0);
 }
 
 // Ordered-pair hash for the symmetry checksum: the sum over all entries x->y
@@ -431,15 +446,14 @@ __global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b) {
     }
 }
 
-// Thread per vertex: short rows are swept here directly; long rows read the
+// One vertex of the finalize pass (warp-collective: every lane calls it; `valid`
+// lanes own a vertex). Short rows are swept here directly; long rows read the
 // accumulators. REBUILD writes bitmaps; TIER1 also decides the recolors.
-__global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b, int mode) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    bool fac_needed = false;
+__device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, int mode, bool valid, uint32_t x) {
+    bool fac_needed = false, pend = false, need = false;
     uint32_t pend_word = 0;
-    bool pend = false;
     unsigned long long sym = 0, live = 0;
-    if (x < g.n) {
+    if (valid) {
         const uint32_t len = g.hw[x];
         const uint32_t hd = __ldg(g.hdmap + x);
         const uint32_t w = __ldg(g.st + x);
@@ -450,8 +464,8 @@ __global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b,
         if (len <= SWEEP_TINY) {
             const uint64_t s = g.rp[x];
             const uint32_t mydeg = __ldg(g.deg + x);
-            for (uint32_t t = 0; t < len; t++) {
-                const uint32_t ng = __ldg(g.col + s + t);
+            for (uint32_t j = 0; j < len; j++) {
+                const uint32_t ng = __ldg(g.col + s + j);
                 if (ng >= g.n) continue;
                 if (ng != x) sym += sym_term(x, ng);
                 const uint16_t nc = color_of(__ldg(g.st + ng));
@@ -468,13 +482,19 @@ __global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b,
             if (hd == EMPTY) g.bm[x] = bits;
         } else {
             bool decide = false;
+            const bool indep = mode == SWEEP_INDEP;
             if (myc == 0) {
-                decide = len > 0;  // has_neighbors: any non-INV slot
+                decide = len > (g.holes ? g.holes[x] : 0u);  // has_neighbors: any non-INV slot
             } else if (conf) {
                 decide = true;
                 if (myc <= 64) bits |= 1ull << (myc - 1);
             }
-            if (hd == EMPTY) {
+            if (indep) {
+                if (hd == EMPTY) g.bm[x] = bits;
+                else if (decide && myc != 0 && myc <= 64) g.bm[x] |= 1ull << (myc - 1);
+                b.needf[x] = decide ? 1 : 0;
+                need = decide;
+            } else if (hd == EMPTY) {
                 g.bm[x] = bits;
                 if (decide) {
                     if (~bits) {
@@ -494,9 +514,18 @@ __global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b,
         sym += __shfl_xor_sync(FULL, sym, off);
         live += __shfl_xor_sync(FULL, live, off);
     }
+    const unsigned long long nv = __popc(__ballot_sync(FULL, valid));
     if (lane_id() == 0) {
         if (sym) atomicAdd(b.symsum, sym);
-        if (live) atomicAdd(b.live, live);
+        if (live) {
+            atomicAdd(b.live, live);
+            atomicAdd(b.swept, live);
+        }
+        if (nv) atomicAdd(b.swept + 1, nv);
+    }
+    if (mode == SWEEP_INDEP) {
+        const uint32_t ni = warp_append(b.need_count, need);
+        if (need) b.need_v[ni] = x;
     }
     if (mode == SWEEP_TIER1) {
         const uint32_t pi = warp_append(b.pend_count, pend);
@@ -506,6 +535,17 @@ __global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b,
         }
         const uint32_t fi = warp_append(b.fac_count, fac_needed);
         if (fac_needed) b.fac_v[fi] = x;
+    }
+}
+
+// Thread per vertex (every vertex, or the worklist).
+__global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b, int mode, int list) {
+    const uint32_t lim = list ? *b.wl_count : g.n;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < lim; base += stride) {  // warp-uniform trip count
+        const uint32_t t = base + threadIdx.x;
+        const bool valid = t < lim;
+        finalize_one(g, b, mode, valid, valid ? (list ? b.wl[t] : t) : 0);
     }
 }
 
@@ -527,23 +567,101 @@ __global__ void __launch_bounds__(256) sweep_fac_kernel(Dev g, SweepBufs b) {
     }
 }
 
+// Independent-set selection: warp per conflicted vertex. It recolors only when
+// no conflicted neighbor has higher priority, choosing the first color its
+// neighbors leave free (start-of-sweep colors; nothing is committed yet). Every
+// conflicted vertex is marked for the next sweep's worklist.
+__global__ void __launch_bounds__(256) sweep_indep_select_kernel(Dev g, SweepBufs b) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t cnt = *b.need_count;
+    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
+        const uint32_t x = b.need_v[k];
+        const uint32_t xd = __ldg(g.deg + x);
+        const uint64_t s = g.rp[x];
+        bool blocked = false;
+        warp_for_each(g.col, s, s + g.hw[x], [&](uint64_t, uint32_t y) {
+            if (y < g.n && y != x && b.needf[y] && prio_less(xd, x, __ldg(g.deg + y), y)) blocked = true;
+        });
+        blocked = __any_sync(FULL, blocked);
+        if (lane_id() == 0) atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
+        if (!blocked) {
+            const uint32_t w = ld_cg(g.st + x);
+            const uint16_t c = warp_fac(g, x, g.st);
+            if (lane_id() == 0) {
+                const uint32_t pi = atomicAdd(b.pend_count, 1u);
+                b.pend_v[pi] = x;
+                b.pend_w[pi] = pack(c, (uint16_t)(version_of(w) + 1));
+            }
+        }
+        __syncwarp();
+    }
+}
+
 __global__ void sweep_commit_kernel(Dev g, SweepBufs b) {
     const uint32_t cnt = *b.pend_count;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
         g.st[b.pend_v[k]] = b.pend_w[k];
 }
 
-void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s) {
-    if (mode == SWEEP_TIER1) {
+void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, int num_sms, cudaStream_t s) {
+    if (mode != SWEEP_REBUILD) {
         cudaMemsetAsync(b.pend_count, 0, sizeof(uint32_t), s);
         cudaMemsetAsync(b.fac_count, 0, sizeof(uint32_t), s);
+        cudaMemsetAsync(b.need_count, 0, sizeof(uint32_t), s);
     }
     sweep_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b);
-    sweep_finalize_kernel<<<(g.n + 255) / 256, 256, 0, s>>>(g, b, (int)mode);
+    uint32_t fblocks = (g.n + 255) / 256;
+    if (list && fblocks > (uint32_t)num_sms * 8) fblocks = num_sms * 8;
+    sweep_finalize_kernel<<<fblocks, 256, 0, s>>>(g, b, (int)mode, list ? 1 : 0);
     if (mode == SWEEP_TIER1) {
         sweep_fac_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
         sweep_commit_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
+    } else if (mode == SWEEP_INDEP) {
+        sweep_indep_select_kernel<<<num_sms * 4, 256, 0, s>>>(g, b);
+        sweep_commit_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
     }
+}
+
+// Marks every vertex recolored by the last sweep and all its live neighbors.
+__global__ void __launch_bounds__(256) mark_recolored_kernel(Dev g, SweepBufs b) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t cnt = *b.pend_count;
+    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
+        const uint32_t x = b.pend_v[k];
+        if (lane_id() == 0) atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
+        const uint64_t s = g.rp[x];
+        warp_for_each(g.col, s, s + g.hw[x], [&](uint64_t, uint32_t y) {
+            if (y < g.n) atomicOr(b.wmark + (y >> 5), 1u << (y & 31));
+        });
+    }
+}
+
+__global__ void collect_marks_kernel(uint32_t n, SweepBufs b) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nw = (n + 31) / 32;
+    uint32_t bits = 0;
+    if (w < nw) {
+        bits = b.wmark[w];
+        if (bits) b.wmark[w] = 0;
+    }
+    uint32_t total = 0;
+    const uint32_t off = warp_excl_scan(__popc(bits), total);
+    uint32_t base = 0;
+    if (lane_id() == 0 && total) base = atomicAdd(b.wl_count, total);
+    base = __shfl_sync(FULL, base, 0);
+    uint32_t k = base + off;
+    while (bits) {
+        const int i = __ffs(bits) - 1;
+        bits &= bits - 1;
+        b.wl[k++] = w * 32 + i;
+    }
+}
+
+void launch_next_worklist(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s) {
+    mark_recolored_kernel<<<num_sms * 4, 256, 0, s>>>(g, b);
+    cudaMemsetAsync(b.wl_count, 0, sizeof(uint32_t), s);
+    const uint32_t nw = (g.n + 31) / 32;
+    collect_marks_kernel<<<(nw + 255) / 256, 256, 0, s>>>(g.n, b);
 }
 
 }  // namespace sgc

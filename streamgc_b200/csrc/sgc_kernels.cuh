@@ -27,6 +27,15 @@ struct SweepBufs {
     uint32_t* fac_count;
     unsigned long long* symsum;  // sum over entries x->y (y != x, y < n) of H(x,y) - H(y,x)
     unsigned long long* live;    // live entries seen by the sweep
+    // worklist of the next sweep: vertices recolored by the last one and their neighbors
+    uint32_t* wmark;             // bitmask
+    uint32_t* wl;
+    uint32_t* wl_count;
+    unsigned long long* swept;   // [0] live entries, [1] vertices visited by the sweeps since reset
+    // independent-set sweeps: conflicted vertices of the current sweep
+    uint8_t* needf;              // per vertex: conflicted (or uncolored with neighbors) at the last visit
+    uint32_t* need_v;
+    uint32_t* need_count;
 };
 
 // Same-edge ordering for a concurrently applied batch.
@@ -41,7 +50,11 @@ struct EdgeOrder {
     uint32_t tmask;            // table size - 1
 };
 
-enum SweepMode : int { SWEEP_REBUILD = 0, SWEEP_TIER1 = 1 };
+// REBUILD: bitmaps only. TIER1: the reference rule (every conflicted vertex
+// recolors from start-of-sweep state). INDEP: conflicted vertices recolor only
+// when no conflicted neighbor has higher priority, so recolored vertices are
+// never adjacent and a sweep creates no conflict.
+enum SweepMode : int { SWEEP_REBUILD = 0, SWEEP_TIER1 = 1, SWEEP_INDEP = 2 };
 
 // ---- launchers (sgc_kernels.cu) ----
 void launch_det_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, cudaStream_t s);
@@ -52,8 +65,11 @@ void launch_compact(const Dev& g, const uint32_t* list, const uint32_t* count, u
 void launch_take_overflow(const Dev& g, uint32_t* drain_n, cudaStream_t s);
 void launch_drain(const Dev& g, const uint32_t* drain_n, bool ordered, unsigned long long* failed, cudaStream_t s);
 void launch_snapshot(const Dev& g, uint16_t* snap, cudaStream_t s);
-void launch_build_items(const Dev& g, const SweepBufs& b, cudaStream_t s);
-void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s);
+// list == false: every vertex; list == true: the vertices in b.wl.
+void launch_build_items(const Dev& g, const SweepBufs& b, bool list, cudaStream_t s);
+void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, int num_sms, cudaStream_t s);
+// After a TIER1 sweep: b.wl = the recolored vertices and their neighbors.
+void launch_next_worklist(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s);
 void launch_query(const uint16_t* snap, uint32_t n, const uint32_t* v, uint16_t* out, uint32_t k, cudaStream_t s);
 void launch_colors(const Dev& g, uint16_t* out, cudaStream_t s);
 

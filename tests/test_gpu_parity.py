@@ -80,6 +80,30 @@ def test_phase_end_repair_matches_oracle(name):
         g.close()
 
 
+@pytest.mark.parametrize("name", ["rmat11", "delaunay2k", "rmat11_thr16_a2"])
+def test_independent_set_repair_matches_oracle(name):
+    """Exact selection + independent-set Tier-1 (the concurrent configuration's
+    repair) on planted conflicts: bit-exact with the oracle, converged, proper."""
+    c = MG.build_case(name)
+    g = O.Oracle(c["rp"], c["col"], c["deg"], hist_threshold=c["thr"], slack_pct=c["slack"], exact=True)
+    h = S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"]), histogram_threshold=c["thr"], slack_pct=c["slack"],
+                   exact_select=True)
+    try:
+        st = np.random.default_rng(11).integers(0, 6, size=len(c["deg"])).astype(np.uint32)
+        g.set_states(st)
+        h.upload("states", st)
+        it, last, fixed = g.phase_end()
+        rep = h.repair()
+        assert (rep["tier1_iterations"], rep["tier1_last_count"], rep["tier2_fixed"]) == (it, last, fixed)
+        assert last == 0 and rep["tier2_ran"] == 0 and rep["proper"] == 1
+        assert np.array_equal(h.states(), g.states())
+        assert np.array_equal(h.bitmaps(), g.bitmaps())
+        assert h.validate()["violations"] == 0
+    finally:
+        h.close()
+        g.close()
+
+
 def test_tier2_exact_on_forced_conflicts():
     """Conflicts planted in the state: Tier-1 alone vs the oracle, then Tier-2."""
     c = MG.build_case("rmat11")
@@ -133,11 +157,11 @@ def test_concurrent_mode_publishes_proper_snapshots(name, exact):
         # row made an insert wait in the overflow buffer and then drop (which edge
         # loses the last slot depends on the order the inserts arrive in)
         st, oc = h.stats(), g.counters()
-        exact = st["drain_failed"] == 0 and st["overflow_lost"] == 0 and oc["drain_failed"] == 0 \
+        no_drop = st["drain_failed"] == 0 and st["overflow_lost"] == 0 and oc["drain_failed"] == 0 \
             and oc["overflow_lost"] == 0
         gr, gc = h.row_ptr(), h.col()
         orp, ocol = g.row_ptr(), g.col()
-        for x in range(len(c["deg"]) if exact else 0):
+        for x in range(len(c["deg"]) if no_drop else 0):
             a = np.sort(gc[gr[x]:gr[x + 1]])
             b = np.sort(ocol[orp[x]:orp[x + 1]])
             assert np.array_equal(a, b), f"row {x}"
