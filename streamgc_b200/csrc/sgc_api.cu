@@ -189,7 +189,7 @@ int drain(sgc_handle* h, bool ordered, unsigned long long* failed_counter) {
 }
 
 // Sweep with optional event timing around the edge passes.
-int sweep(sgc_handle* h, SweepMode mode, bool list = false) {
+int sweep(sgc_handle* h, SweepMode mode, bool list = false, bool with_sym = false) {
     const bool prof = (h->opt.flags & SGC_OPT_PROFILE) != 0 && mode != SWEEP_REBUILD;
     cudaEvent_t a = nullptr, b = nullptr;
     if (prof) {
@@ -197,7 +197,7 @@ int sweep(sgc_handle* h, SweepMode mode, bool list = false) {
         b = take_event(h);
         cudaEventRecord(a, h->stream);
     }
-    launch_sweep(h->g, h->sb, mode, list, h->num_sms, h->stream);
+    launch_sweep(h->g, h->sb, mode, list, with_sym, h->num_sms, h->stream);
     h->launches += mode == SWEEP_REBUILD ? 2 : 4;
     if (prof) {
         cudaEventRecord(b, h->stream);
@@ -241,12 +241,18 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep) {
         // under the independent-set rule, every vertex still conflicted):
         // every other vertex sees the colors it saw then, so its rebuilt bitmap
         // and its decision cannot change (the result equals a full sweep).
-        if (it > 0) {
+        // Worklists need mirror-complete rows (sweep 0's checksum is zero): a
+        // vertex re-checked after a neighbor y recolors is found through y's row.
+        const bool use_list = it > 0 && *(unsigned long long*)(h->h_small + 2) == 0;
+        if (use_list) {
             launch_next_worklist(h->g, h->sb, h->num_sms, h->stream);
             TRY(build_items(h, true));
             h->launches += 2;
+        } else if (it > 0) {
+            TRY(build_items(h, false));
+            CK(cudaMemsetAsync(h->sb.wmark, 0, ((h->n + 31) / 32) * 4, h->stream));
         }
-        TRY(sweep(h, mode, it > 0));
+        TRY(sweep(h, mode, use_list, it == 0));
         h->tier1_sweeps++;
         CK(cudaMemcpyAsync(h->h_small, count_ptr, 4, cudaMemcpyDeviceToHost, h->stream));
         if (it == 0) CK(cudaMemcpyAsync(h->h_small + 2, &h->ctl->symsum, 16, cudaMemcpyDeviceToHost, h->stream));

@@ -390,17 +390,26 @@ void launch_build_items(const Dev& g, const SweepBufs& b, bool list, cudaStream_
 // of H(x,y) - H(y,x) is 0 when every entry has its mirror (and otherwise is 0
 // only with probability ~2^-64).
 __device__ __forceinline__ unsigned long long pair_hash(uint32_t x, uint32_t y) {
-    unsigned long long z = ((unsigned long long)x << 32 | y) + 0x9E3779B97F4A7C15ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
+    const unsigned long long z = (((unsigned long long)x << 32) | y) * 0x9E3779B97F4A7C15ull;
+    return z ^ (z >> 29);
 }
 __device__ __forceinline__ unsigned long long sym_term(uint32_t x, uint32_t y) {
     return pair_hash(x, y) - pair_hash(y, x);
 }
 
-// Warp per item: up to SWEEP_CH live entries of one row. Nothing in the graph
-// changes during a sweep, so loads take the read-only path.
+// Sets color c's bit (colors 1..64) in a 64-bit mask kept as two 32-bit words;
+// c == 0 and c > 64 wrap out of both ranges.
+__device__ __forceinline__ void add_color_bit(uint32_t c, uint32_t& lo, uint32_t& hi) {
+    const uint32_t a = c - 1u, b = c - 33u;
+    lo |= a < 32u ? 1u << a : 0u;
+    hi |= b < 32u ? 1u << b : 0u;
+}
+
+// Warp per item: up to SWEEP_CH live slots of one row. Nothing in the graph
+// changes during a sweep, so loads take the read-only path. Each lane keeps two
+// 16-byte slot loads and their eight state gathers in flight per round.
+// SYM: also accumulate the mirror checksum (first sweep of a repair only).
+template <bool SYM>
 __global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
@@ -413,35 +422,42 @@ __global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b) {
         const uint64_t s = rs + (uint64_t)j * SWEEP_CH;
         const uint64_t re = rs + g.hw[x];
         const uint64_t e = s + SWEEP_CH < re ? s + SWEEP_CH : re;
-        const uint16_t myc = color_of(__ldg(g.st + x));
+        const uint32_t myc = color_of(__ldg(g.st + x));
         const uint32_t mydeg = __ldg(g.deg + x);
-        unsigned long long bits = 0, sym = 0;
+        uint32_t lo = 0, hi = 0;
+        unsigned long long sym = 0;
         bool conf = false;
-        for (uint64_t c = s & ~3ull; c < e; c += 128) {
-            const uint64_t i = c + 4ull * lane;
-            if (i < e) {
-                const uint4 q = __ldg(reinterpret_cast<const uint4*>(g.col + i));
-                const uint32_t vals[4] = {q.x, q.y, q.z, q.w};
+        for (uint64_t c = s & ~3ull; c < e; c += 256) {
+            const uint64_t i0 = c + 4ull * lane, i1 = i0 + 128;
+            uint4 q0 = make_uint4(INV, INV, INV, INV), q1 = q0;
+            if (i0 < e) q0 = __ldg(reinterpret_cast<const uint4*>(g.col + i0));
+            if (i1 < e) q1 = __ldg(reinterpret_cast<const uint4*>(g.col + i1));
+            uint32_t v[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+            uint32_t nc[8];
 #pragma unroll
-                for (int t = 0; t < 4; t++) {
-                    const uint32_t ng = vals[t];
-                    if (i + t < s || i + t >= e || ng >= g.n) continue;
-                    if (ng != x) sym += sym_term(x, ng);
-                    const uint16_t nc = color_of(__ldg(g.st + ng));
-                    if (nc != 0 && nc <= 64) bits |= 1ull << (nc - 1);
-                    if (nc == myc && nc != 0 && !conf && prio_less(mydeg, x, __ldg(g.deg + ng), ng)) conf = true;
-                }
+            for (int t = 0; t < 8; t++) {
+                const uint64_t p = (t < 4 ? i0 : i1) + (t & 3);
+                const bool in = p >= s && p < e && v[t] < g.n;
+                v[t] = in ? v[t] : INV;
+                nc[t] = in ? color_of(__ldg(g.st + v[t])) : 0u;
+            }
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                add_color_bit(nc[t], lo, hi);
+                if (nc[t] == myc && myc != 0 && !conf) conf = prio_less(mydeg, x, __ldg(g.deg + v[t]), v[t]);
+                if (SYM && v[t] != INV && v[t] != x) sym += sym_term(x, v[t]);
             }
         }
-        const uint32_t lo = __reduce_or_sync(FULL, (uint32_t)bits);
-        const uint32_t hi = __reduce_or_sync(FULL, (uint32_t)(bits >> 32));
+        lo = __reduce_or_sync(FULL, lo);
+        hi = __reduce_or_sync(FULL, hi);
         const bool anyc = __any_sync(FULL, conf);
-        for (int off = 16; off > 0; off >>= 1) sym += __shfl_xor_sync(FULL, sym, off);
+        if (SYM)
+            for (int off = 16; off > 0; off >>= 1) sym += __shfl_xor_sync(FULL, sym, off);
         if (lane == 0) {
             const unsigned long long m = ((unsigned long long)hi << 32) | lo;
             if (m) atomicOr(b.acc_bm + x, m);
             if (anyc) atomicOr(b.acc_fl + x, 1u);
-            if (sym) atomicAdd(b.symsum, sym);
+            if (SYM && sym) atomicAdd(b.symsum, sym);
         }
     }
 }
@@ -449,7 +465,8 @@ __global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b) {
 // One vertex of the finalize pass (warp-collective: every lane calls it; `valid`
 // lanes own a vertex). Short rows are swept here directly; long rows read the
 // accumulators. REBUILD writes bitmaps; TIER1 also decides the recolors.
-__device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, int mode, bool valid, uint32_t x) {
+__device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, int mode, bool valid, uint32_t x,
+                                             bool with_sym) {
     bool fac_needed = false, pend = false, need = false;
     uint32_t pend_word = 0;
     unsigned long long sym = 0, live = 0;
@@ -464,14 +481,16 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
         if (len <= SWEEP_TINY) {
             const uint64_t s = g.rp[x];
             const uint32_t mydeg = __ldg(g.deg + x);
+            uint32_t lo = 0, hi = 0;
             for (uint32_t j = 0; j < len; j++) {
                 const uint32_t ng = __ldg(g.col + s + j);
                 if (ng >= g.n) continue;
-                if (ng != x) sym += sym_term(x, ng);
-                const uint16_t nc = color_of(__ldg(g.st + ng));
-                if (nc != 0 && nc <= 64) bits |= 1ull << (nc - 1);
+                if (with_sym && ng != x) sym += sym_term(x, ng);
+                const uint32_t nc = color_of(__ldg(g.st + ng));
+                add_color_bit(nc, lo, hi);
                 if (nc == myc && nc != 0 && !conf && prio_less(mydeg, x, __ldg(g.deg + ng), ng)) conf = true;
             }
+            bits = ((unsigned long long)hi << 32) | lo;
         } else {
             bits = b.acc_bm[x];
             conf = b.acc_fl[x] != 0;
@@ -539,13 +558,13 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
 }
 
 // Thread per vertex (every vertex, or the worklist).
-__global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b, int mode, int list) {
+__global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b, int mode, int list, int with_sym) {
     const uint32_t lim = list ? *b.wl_count : g.n;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < lim; base += stride) {  // warp-uniform trip count
         const uint32_t t = base + threadIdx.x;
         const bool valid = t < lim;
-        finalize_one(g, b, mode, valid, valid ? (list ? b.wl[t] : t) : 0);
+        finalize_one(g, b, mode, valid, valid ? (list ? b.wl[t] : t) : 0, with_sym != 0);
     }
 }
 
@@ -603,16 +622,18 @@ __global__ void sweep_commit_kernel(Dev g, SweepBufs b) {
         g.st[b.pend_v[k]] = b.pend_w[k];
 }
 
-void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, int num_sms, cudaStream_t s) {
+void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, bool with_sym, int num_sms,
+                  cudaStream_t s) {
     if (mode != SWEEP_REBUILD) {
         cudaMemsetAsync(b.pend_count, 0, sizeof(uint32_t), s);
         cudaMemsetAsync(b.fac_count, 0, sizeof(uint32_t), s);
         cudaMemsetAsync(b.need_count, 0, sizeof(uint32_t), s);
     }
-    sweep_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b);
+    if (with_sym) sweep_items_kernel<true><<<num_sms * 8, 256, 0, s>>>(g, b);
+    else sweep_items_kernel<false><<<num_sms * 8, 256, 0, s>>>(g, b);
     uint32_t fblocks = (g.n + 255) / 256;
     if (list && fblocks > (uint32_t)num_sms * 8) fblocks = num_sms * 8;
-    sweep_finalize_kernel<<<fblocks, 256, 0, s>>>(g, b, (int)mode, list ? 1 : 0);
+    sweep_finalize_kernel<<<fblocks, 256, 0, s>>>(g, b, (int)mode, list ? 1 : 0, with_sym ? 1 : 0);
     if (mode == SWEEP_TIER1) {
         sweep_fac_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
         sweep_commit_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);

@@ -67,7 +67,9 @@ void launch_drain(const Dev& g, const uint32_t* drain_n, bool ordered, unsigned 
 void launch_snapshot(const Dev& g, uint16_t* snap, cudaStream_t s);
 // list == false: every vertex; list == true: the vertices in b.wl.
 void launch_build_items(const Dev& g, const SweepBufs& b, bool list, cudaStream_t s);
-void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, int num_sms, cudaStream_t s);
+// with_sym: accumulate the mirror checksum (b.symsum) over the visited entries.
+void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, bool with_sym, int num_sms,
+                  cudaStream_t s);
 // After a TIER1 sweep: b.wl = the recolored vertices and their neighbors.
 void launch_next_worklist(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s);
 void launch_query(const uint16_t* snap, uint32_t n, const uint32_t* v, uint16_t* out, uint32_t k, cudaStream_t s);

@@ -83,7 +83,10 @@ def test_phase_end_repair_matches_oracle(name):
 @pytest.mark.parametrize("name", ["rmat11", "delaunay2k", "rmat11_thr16_a2"])
 def test_independent_set_repair_matches_oracle(name):
     """Exact selection + independent-set Tier-1 (the concurrent configuration's
-    repair) on planted conflicts: bit-exact with the oracle, converged, proper."""
+    repair) on planted conflicts: bit-exact with the oracle (Tier-1 sweeps,
+    counts, Tier-2 fixes, states, bitmaps) and proper at the end. Random colors
+    from a 6-color palette on a dense graph can need more sweeps than Tier-1
+    allows; Tier-2 then finishes, identically on both sides."""
     c = MG.build_case(name)
     g = O.Oracle(c["rp"], c["col"], c["deg"], hist_threshold=c["thr"], slack_pct=c["slack"], exact=True)
     h = S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"]), histogram_threshold=c["thr"], slack_pct=c["slack"],
@@ -95,7 +98,7 @@ def test_independent_set_repair_matches_oracle(name):
         it, last, fixed = g.phase_end()
         rep = h.repair()
         assert (rep["tier1_iterations"], rep["tier1_last_count"], rep["tier2_fixed"]) == (it, last, fixed)
-        assert last == 0 and rep["tier2_ran"] == 0 and rep["proper"] == 1
+        assert rep["proper"] == 1 and rep["tier2_ran"] == (1 if last else 0)
         assert np.array_equal(h.states(), g.states())
         assert np.array_equal(h.bitmaps(), g.bitmaps())
         assert h.validate()["violations"] == 0
