@@ -431,7 +431,21 @@ struct Oracle {
     // rule would recolor, then recolor only those with no flagged neighbor of
     // higher priority, each to the first color its neighbors leave free
     // (start-of-sweep colors). Returns the number flagged.
-    uint32_t tier1_indep_sweep() {
+    // Selection order of the independent-set rule: the "lowbias32" mixer
+    // (C. Wellons, hash-prospector) of x ^ salt, id as tie-break; the salt is
+    // (sweep + 1) * 0x9E3779B9 for the sweep's index within its repair.
+    static uint64_t sel_rank(uint32_t x, uint32_t salt) {
+        uint32_t h = x ^ salt;
+        h ^= h >> 16;
+        h *= 0x7feb352du;
+        h ^= h >> 15;
+        h *= 0x846ca68bu;
+        h ^= h >> 16;
+        return ((uint64_t)h << 32) | x;
+    }
+
+    uint32_t tier1_indep_sweep(uint32_t sweep) {
+        const uint32_t salt = (sweep + 1u) * 0x9E3779B9u;
         std::vector<uint32_t> old = st;
         std::vector<uint8_t> need(n, 0);
         uint32_t count = 0;
@@ -466,7 +480,7 @@ struct Oracle {
                 uint32_t y = col[j];
                 b += 4;
                 if (y == INV || y >= n || y == x) continue;
-                if (need[y] && prio(x) < prio(y)) blocked = true;
+                if (need[y] && sel_rank(x, salt) < sel_rank(y, salt)) blocked = true;
             }
             if (blocked) continue;
             uint16_t c = fac(x, old, b);
@@ -483,7 +497,7 @@ struct Oracle {
             uint32_t cnt = 0;
             for (int it = 0; it < 64; it++) {
                 rebuild_all(bytes.tier1);
-                cnt = tier1_indep_sweep();
+                cnt = tier1_indep_sweep((uint32_t)it);
                 if (history && it < hist_cap) history[it] = cnt;
                 if (cnt == 0) { if (last_count) *last_count = 0; return it + 1; }
             }

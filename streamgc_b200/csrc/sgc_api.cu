@@ -54,7 +54,9 @@ struct Ctl {
     unsigned long long drain_failed;
     unsigned long long symsum;
     unsigned long long live;
-    unsigned long long pad[3];
+    uint32_t asym;
+    uint32_t pad32;
+    unsigned long long pad[2];
 };
 
 }  // namespace
@@ -189,7 +191,7 @@ int drain(sgc_handle* h, bool ordered, unsigned long long* failed_counter) {
 }
 
 // Sweep with optional event timing around the edge passes.
-int sweep(sgc_handle* h, SweepMode mode, bool list = false, bool with_sym = false) {
+int sweep(sgc_handle* h, SweepMode mode, bool list = false, bool with_sym = false, uint32_t index = 0) {
     const bool prof = (h->opt.flags & SGC_OPT_PROFILE) != 0 && mode != SWEEP_REBUILD;
     cudaEvent_t a = nullptr, b = nullptr;
     if (prof) {
@@ -197,8 +199,8 @@ int sweep(sgc_handle* h, SweepMode mode, bool list = false, bool with_sym = fals
         b = take_event(h);
         cudaEventRecord(a, h->stream);
     }
-    launch_sweep(h->g, h->sb, mode, list, with_sym, h->num_sms, h->stream);
-    h->launches += mode == SWEEP_REBUILD ? 2 : 4;
+    launch_sweep(h->g, h->sb, mode, list, with_sym, index, h->num_sms, h->stream);
+    h->launches += mode == SWEEP_REBUILD ? 2 : (mode == SWEEP_INDEP ? 6 : 4);
     if (prof) {
         cudaEventRecord(b, h->stream);
         h->ev_pending.push_back({a, b});
@@ -235,6 +237,9 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep) {
     int plateau = 0, it = 0;
     CK(cudaMemsetAsync(&h->ctl->symsum, 0, 16, h->stream));
     CK(cudaMemsetAsync(h->sb.swept, 0, 16, h->stream));
+    const size_t mwords = ((h->n + 31) / 32) * 4;
+    CK(cudaMemsetAsync(h->sb.wmark, 0, mwords, h->stream));
+    CK(cudaMemsetAsync(h->sb.rbits, 0, mwords, h->stream));
     for (it = 0; it < max_sweeps; it++) {
         // Sweep 0 visits every vertex. Later Jacobi sweeps visit only the
         // vertices recolored by the previous sweep and their neighbors (plus,
@@ -250,9 +255,10 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep) {
             h->launches += 2;
         } else if (it > 0) {
             TRY(build_items(h, false));
-            CK(cudaMemsetAsync(h->sb.wmark, 0, ((h->n + 31) / 32) * 4, h->stream));
+            CK(cudaMemsetAsync(h->sb.wmark, 0, mwords, h->stream));
+            CK(cudaMemsetAsync(h->sb.rbits, 0, mwords, h->stream));
         }
-        TRY(sweep(h, mode, use_list, it == 0));
+        TRY(sweep(h, mode, use_list, it == 0, (uint32_t)it));
         h->tier1_sweeps++;
         CK(cudaMemcpyAsync(h->h_small, count_ptr, 4, cudaMemcpyDeviceToHost, h->stream));
         if (it == 0) CK(cudaMemcpyAsync(h->h_small + 2, &h->ctl->symsum, 16, cudaMemcpyDeviceToHost, h->stream));
@@ -271,6 +277,10 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep) {
         prev = cnt;
     }
     const unsigned long long sym = *(unsigned long long*)(h->h_small + 2);
+    // Rows found mirror-complete stay so until an overflow, a drain failure or
+    // an update that found one direction only sets the flag again; until then
+    // the first sweep skips the checksum.
+    if (sym == 0) CK(cudaMemsetAsync(h->g.asym, 0, 4, h->stream));
     const uint32_t iters = it < max_sweeps ? it + 1 : max_sweeps;
     if (h->opt.flags & SGC_OPT_PROFILE) {
         unsigned long long sw[2];
@@ -438,6 +448,9 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     g.ovf_lost = &h->ctl->ovf_lost;
     g.nskip = &h->ctl->nskip;
     g.err = &h->ctl->err;
+    g.asym = &h->ctl->asym;
+    if (cudaMemsetAsync(g.asym, 0x01, 4, h->stream) != cudaSuccess)  // nothing known about the mirrors yet
+        return bail(fail(SGC_ECUDA, "control block init failed"));
     if (cudaMemcpyAsync(d_rp, rp.data(), rp.size() * 8, cudaMemcpyHostToDevice, h->stream) ||
         cudaMemcpyAsync(d_hdmap, hdmap.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) ||
         cudaMemcpyAsync(d_deg, degree, (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) ||
@@ -503,6 +516,9 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     A(&sb.needf, n, 0);
     A(&sb.need_v, n);
     A(&sb.need_count, 4, 0);
+    A(&sb.rbits, (n + 31) / 32 + 1, 0);
+    if (g.exact) A(&sb.hiused, (size_t)num_hd * 64, 0);
+    else sb.hiused = nullptr;
     A(&h->dirty_list, n);
     // tier-2 buffers
     Tier2Bufs& t2 = h->t2;

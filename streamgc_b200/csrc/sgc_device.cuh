@@ -61,6 +61,9 @@ struct Dev {
     unsigned long long* ovf_lost;  // overflows beyond OVF_CAP (edge dropped, as the reference does)
     unsigned long long* nskip;     // updates skipped: an endpoint outside [0, n) (hash miss)
     uint32_t* err;
+    uint32_t* asym;                // nonzero: an entry may have lost its mirror since rows were last
+                                   // found mirror-complete (set at creation, on every overflow, on a
+                                   // drain failure, and when an update found one direction only)
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -101,32 +104,28 @@ template <class P>
 __device__ __forceinline__ bool warp_find(const uint32_t* col, uint64_t s, uint64_t e, P pred,
                                           uint64_t& pos, uint32_t& val) {
     const uint32_t lane = lane_id();
-    for (uint64_t c = s & ~3ull; c < e; c += 256) {
-        const uint64_t i0 = c + 4ull * lane, i1 = i0 + 128;
-        uint4 a = make_uint4(INV, INV, INV, INV), b = a;
-        if (i0 < e) a = ld_cg4(col + i0);
-        if (i1 < e) b = ld_cg4(col + i1);
-        const uint32_t ma = mask4(a, i0, s, e, pred);
-        const uint32_t mb = mask4(b, i1, s, e, pred);
-        const uint32_t ba = __ballot_sync(FULL, ma != 0);
-        if (ba) {
-            const int src = __ffs(ba) - 1;
-            const int k = __ffs(ma) - 1;
-            const uint32_t v = ma ? pick4(a, k) : 0u;
-            const int ks = __shfl_sync(FULL, k, src);
-            val = __shfl_sync(FULL, v, src);
-            pos = c + 4ull * src + ks;
-            return true;
+    for (uint64_t c = s & ~3ull; c < e; c += 512) {  // four 16-byte loads per lane in flight
+        uint4 q[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint64_t i = c + 128ull * k + 4ull * lane;
+            q[k] = make_uint4(INV, INV, INV, INV);
+            if (i < e) q[k] = ld_cg4(col + i);
         }
-        const uint32_t bb = __ballot_sync(FULL, mb != 0);
-        if (bb) {
-            const int src = __ffs(bb) - 1;
-            const int k = __ffs(mb) - 1;
-            const uint32_t v = mb ? pick4(b, k) : 0u;
-            const int ks = __shfl_sync(FULL, k, src);
-            val = __shfl_sync(FULL, v, src);
-            pos = c + 128 + 4ull * src + ks;
-            return true;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint64_t i = c + 128ull * k + 4ull * lane;
+            const uint32_t m = mask4(q[k], i, s, e, pred);
+            const uint32_t b = __ballot_sync(FULL, m != 0);
+            if (b) {
+                const int src = __ffs(b) - 1;
+                const int kk = __ffs(m) - 1;
+                const uint32_t v = m ? pick4(q[k], kk) : 0u;
+                const int ks = __shfl_sync(FULL, kk, src);
+                val = __shfl_sync(FULL, v, src);
+                pos = c + 128ull * k + 4ull * src + ks;
+                return true;
+            }
         }
     }
     return false;
@@ -137,21 +136,65 @@ __device__ __forceinline__ bool warp_find(const uint32_t* col, uint64_t s, uint6
 template <class F>
 __device__ __forceinline__ void warp_for_each(const uint32_t* col, uint64_t s, uint64_t e, F f) {
     const uint32_t lane = lane_id();
-    for (uint64_t c = s & ~3ull; c < e; c += 128) {
-        const uint64_t i = c + 4ull * lane;
-        if (i < e) {
-            const uint4 q = ld_cg4(col + i);
-            if (i + 0 >= s) f(i + 0, q.x);
-            if (i + 1 >= s && i + 1 < e) f(i + 1, q.y);
-            if (i + 2 >= s && i + 2 < e) f(i + 2, q.z);
-            if (i + 3 >= s && i + 3 < e) f(i + 3, q.w);
+    for (uint64_t c = s & ~3ull; c < e; c += 512) {  // four 16-byte loads per lane in flight
+        uint4 q[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint64_t i = c + 128ull * k + 4ull * lane;
+            q[k] = make_uint4(INV, INV, INV, INV);
+            if (i < e) q[k] = ld_cg4(col + i);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint64_t i = c + 128ull * k + 4ull * lane;
+            if (i < e) {
+                if (i + 0 >= s) f(i + 0, q[k].x);
+                if (i + 1 >= s && i + 1 < e) f(i + 1, q[k].y);
+                if (i + 2 >= s && i + 2 < e) f(i + 2, q[k].z);
+                if (i + 3 >= s && i + 3 < e) f(i + 3, q[k].w);
+            }
         }
     }
+}
+
+// Warp-collective visit of every slot of [s, e) holding a vertex id y < n,
+// with arr[y] (a coherent load): a lane issues the loads of its 16 slots and
+// their 16 gathers before it uses any of them. f(y, arr[y]) runs once per slot.
+// With STOP, the scan ends after the first round in which f returned true on
+// any lane (warp vote); the return value says whether that happened.
+template <bool STOP, class F>
+__device__ __forceinline__ bool warp_gather_each(const uint32_t* col, uint64_t s, uint64_t e, uint32_t n,
+                                                 const uint32_t* arr, F f) {
+    const uint32_t lane = lane_id();
+    for (uint64_t c = s & ~3ull; c < e; c += 512) {
+        uint32_t y[16], w[16];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint64_t i = c + 128ull * k + 4ull * lane;
+            uint4 q = make_uint4(INV, INV, INV, INV);
+            if (i < e) q = ld_cg4(col + i);
+            y[4 * k + 0] = (i + 0 >= s && i + 0 < e) ? q.x : INV;
+            y[4 * k + 1] = (i + 1 >= s && i + 1 < e) ? q.y : INV;
+            y[4 * k + 2] = (i + 2 >= s && i + 2 < e) ? q.z : INV;
+            y[4 * k + 3] = (i + 3 >= s && i + 3 < e) ? q.w : INV;
+        }
+#pragma unroll
+        for (int t = 0; t < 16; t++) w[t] = y[t] < n ? ld_cg(arr + y[t]) : 0u;
+        bool hit = false;
+#pragma unroll
+        for (int t = 0; t < 16; t++)
+            if (y[t] < n) hit |= f(y[t], w[t]);
+        if (STOP && __any_sync(FULL, hit)) return true;
+    }
+    return false;
 }
 
 __device__ __forceinline__ void mark_dirty(const Dev& g, uint32_t x) {
     atomicOr(g.dirty + (x >> 5), 1u << (x & 31));
     if (!(ld_cg(g.edited + (x >> 5)) & (1u << (x & 31)))) atomicOr(g.edited + (x >> 5), 1u << (x & 31));
+}
+__device__ __forceinline__ void flag_asym(const Dev& g) {
+    if (!ld_cg(g.asym)) atomicOr(g.asym, 1u);
 }
 __device__ __forceinline__ bool pristine(const Dev& g, uint32_t x) {
     return !(ld_cg(g.edited + (x >> 5)) & (1u << (x & 31)));
@@ -194,7 +237,11 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
         // else at the first INV right after the base run.
         const uint64_t len = ld_cg(g.hw + x);
         if (warp_bsearch(g.col, s, s + len, nbr) != ~0ull) return ADD_PRESENT;
-        if (exact) from = s + len;  // one warp in stream order: the row cannot change under us
+        // Past the sorted run: in stream order nothing else changes the row; in
+        // a concurrent batch the updates of this edge are ordered, so nbr can
+        // only be in the row through an earlier update of the edge, and that
+        // one would have marked the row edited.
+        from = s + len;
     }
     for (;;) {
         uint64_t p = 0;
@@ -209,6 +256,7 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
                 } else {
                     atomicAdd(g.ovf_lost, 1ull);
                 }
+                flag_asym(g);
             }
             __syncwarp();
             return ADD_OVERFLOW;
@@ -231,7 +279,8 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
 }
 
 // remove_local_neighbor: first slot equal to nbr becomes INV (lazy delete).
-__device__ __forceinline__ void warp_remove_slot(const Dev& g, uint32_t x, uint32_t nbr, bool exact) {
+// Returns whether an entry was removed.
+__device__ __forceinline__ bool warp_remove_slot(const Dev& g, uint32_t x, uint32_t nbr, bool exact) {
     const uint64_t s = g.rp[x];
     const uint64_t e = s + ld_cg(g.hw + x);
     uint64_t from = s;
@@ -247,15 +296,15 @@ __device__ __forceinline__ void warp_remove_slot(const Dev& g, uint32_t x, uint3
                 }
             }
             old = __shfl_sync(FULL, old, 0);
-            if (old == nbr) return;
+            if (old == nbr) return true;
         } else if (exact) {
-            return;  // absent from the sorted run and nothing after it
+            return false;  // absent from the sorted run and nothing after it
         }
     }
     for (;;) {
         uint64_t p = 0;
         uint32_t v = 0;
-        if (!warp_find(g.col, from, e, [nbr](uint32_t t) { return t == nbr; }, p, v)) return;
+        if (!warp_find(g.col, from, e, [nbr](uint32_t t) { return t == nbr; }, p, v)) return false;
         uint32_t old = 0;
         if (lane_id() == 0) {
             old = atomicCAS(g.col + p, nbr, INV);
@@ -265,12 +314,22 @@ __device__ __forceinline__ void warp_remove_slot(const Dev& g, uint32_t x, uint3
             }
         }
         old = __shfl_sync(FULL, old, 0);
-        if (old == nbr) return;
+        if (old == nbr) return true;
         from = p + 1;
     }
 }
 
 // ---------------- color selection (color_select.cuh:10-115) ----------------
+
+// Sets color c's bit (colors 1..64) in a 64-bit mask kept as two 32-bit words;
+// c == 0 and c > 64 wrap out of both ranges.
+__device__ __forceinline__ void add_color_bit(uint32_t c, uint32_t& lo, uint32_t& hi) {
+    const uint32_t a = c - 1u, b = c - 33u;
+    lo |= a < 32u ? 1u << a : 0u;
+    hi |= b < 32u ? 1u << b : 0u;
+}
+
+
 
 // Histogram mode: first zero counter -> its color; else the first minimum.
 // Whole row (maxc counters) is loaded warp-wide, 16 bytes per lane per step.
@@ -311,14 +370,14 @@ __device__ __forceinline__ uint16_t warp_fac_hist(const uint32_t* h, uint32_t ma
 __device__ __forceinline__ uint16_t warp_fac_scan(const Dev& g, uint32_t x, const uint32_t* cols) {
     const uint64_t s = g.rp[x], e = s + ld_cg(g.hw + x);
     uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    warp_for_each(g.col, s, e, [&](uint64_t, uint32_t ng) {
-        if (ng == INV || ng >= g.n) return;
-        const uint16_t c = color_of(ld_cg(cols + ng));
+    warp_gather_each<false>(g.col, s, e, g.n, cols, [&](uint32_t, uint32_t sw) {
+        const uint16_t c = color_of(sw);
         if (c > 0 && c < 256) {
 #pragma unroll
             for (int k = 0; k < 8; k++)
                 if ((c >> 5) == k) w[k] |= 1u << (c & 31);
         }
+        return false;
     });
 #pragma unroll
     for (int k = 0; k < 8; k++) w[k] = __reduce_or_sync(FULL, w[k]);
@@ -340,16 +399,16 @@ __device__ __forceinline__ uint16_t warp_fac_exact(const Dev& g, uint32_t x, con
     used[lane] = 0;
     used[lane + 32] = 0;
     __syncwarp();
-    unsigned long long low = 0;
+    uint32_t lo = 0, hi = 0;
     const uint64_t s = g.rp[x], e = s + ld_cg(g.hw + x);
-    warp_for_each(g.col, s, e, [&](uint64_t, uint32_t ng) {
-        if (ng == INV || ng >= g.n) return;
-        const uint16_t c = color_of(ld_cg(cols + ng));
-        if (c == 0) return;
-        if (c <= 64) low |= 1ull << (c - 1);
-        else if (c < 2048) atomicOr(&used[c >> 5], 1u << (c & 31));
+    warp_gather_each<false>(g.col, s, e, g.n, cols, [&](uint32_t, uint32_t sw) {
+        const uint16_t c = color_of(sw);
+        add_color_bit(c, lo, hi);
+        if (c > 64 && c < 2048) atomicOr(&used[c >> 5], 1u << (c & 31));
+        return false;
     });
-    const uint32_t lo = __reduce_or_sync(FULL, (uint32_t)low), hi = __reduce_or_sync(FULL, (uint32_t)(low >> 32));
+    lo = __reduce_or_sync(FULL, lo);
+    hi = __reduce_or_sync(FULL, hi);
     const unsigned long long m = ((unsigned long long)hi << 32) | lo;
     __syncwarp();
     if (~m) return (uint16_t)__ffsll((long long)~m);
@@ -438,11 +497,26 @@ __device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x, uint16_t 
     __syncwarp();
 }
 
+// Warp-collective: does some live neighbor of x hold color c? Stops at the
+// first round that finds one.
+__device__ __forceinline__ bool warp_color_held(const Dev& g, uint32_t x, uint16_t c) {
+    const uint64_t s = g.rp[x], e = s + ld_cg(g.hw + x);
+    return warp_gather_each<true>(g.col, s, e, g.n, g.st, [c](uint32_t, uint32_t w) { return color_of(w) == c; });
+}
+
 // try_color_reduction: after a delete freed `freed`, move to a lower color if one is open.
-__device__ __forceinline__ void warp_try_reduce(const Dev& g, uint32_t x, uint16_t freed) {
+// `stream_order` false (a concurrent batch) with exact selection on a row above
+// the threshold: instead of the full first-free scan, x moves to `freed` when no
+// live neighbor holds it any more (an early-exit scan; the full scan of a
+// high-degree row would almost always confirm the current color).
+__device__ __forceinline__ void warp_try_reduce(const Dev& g, uint32_t x, uint16_t freed, bool stream_order) {
     const uint16_t cur = color_of(warp_load_state(g, x));
     if (cur == 0) return;
     if (freed >= cur) return;
+    if (!stream_order && g.exact && __ldg(g.hdmap + x) != EMPTY) {
+        if (freed != 0 && !warp_color_held(g, x, freed)) warp_recolor(g, x, freed);
+        return;
+    }
     const uint16_t best = warp_fac(g, x, g.st);
     if (best < cur) warp_recolor(g, x, best);
 }
@@ -464,8 +538,9 @@ __device__ __forceinline__ void warp_color_if_uncolored(const Dev& g, uint32_t x
 // to the linear scan whenever the search does not find the key.
 __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v, uint8_t type, bool exact) {
     if (type == SGC_UPDATE_ADD) {
-        warp_add_slot(g, u, v, exact);
-        warp_add_slot(g, v, u, exact);
+        const int ru = warp_add_slot(g, u, v, exact);
+        const int rv = warp_add_slot(g, v, u, exact);
+        if (ru != rv && lane_id() == 0) flag_asym(g);
         warp_color_if_uncolored(g, u);
         if (color_of(warp_load_state(g, v)) == 0) {
             if (lane_id() == 0) new_nbr(g, v, color_of(ld_cg(g.st + u)));
@@ -486,15 +561,16 @@ __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v,
     } else if (type == SGC_UPDATE_DEL) {
         const uint16_t fu = color_of(warp_load_state(g, v));
         const uint16_t fv = color_of(warp_load_state(g, u));
-        warp_remove_slot(g, u, v, exact);
-        warp_remove_slot(g, v, u, exact);
+        const bool du = warp_remove_slot(g, u, v, exact);
+        const bool dv = warp_remove_slot(g, v, u, exact);
         if (lane_id() == 0) {
+            if (du != dv) flag_asym(g);
             removed_nbr(g, u, fu);
             removed_nbr(g, v, fv);
         }
         __syncwarp();
-        warp_try_reduce(g, u, fu);
-        warp_try_reduce(g, v, fv);
+        warp_try_reduce(g, u, fu, exact);
+        warp_try_reduce(g, v, fv, exact);
     }
 }
 

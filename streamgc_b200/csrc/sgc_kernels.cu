@@ -319,7 +319,10 @@ __global__ void drain_kernel(Dev g, const uint32_t* __restrict__ drain_n, int or
     for (uint32_t k = w0; k < cnt; k += step) {
         const OverflowEdge oe = g.ovf[k];
         const bool ok = warp_drain_insert(g, oe.local_vertex_idx, oe.neighbor_global);
-        if (!ok && lane_id() == 0 && failed) atomicAdd(failed, 1ull);
+        if (!ok && lane_id() == 0) {
+            if (failed) atomicAdd(failed, 1ull);
+            flag_asym(g);
+        }
     }
 }
 void launch_drain(const Dev& g, const uint32_t* drain_n, bool ordered, unsigned long long* failed, cudaStream_t s) {
@@ -397,20 +400,13 @@ __device__ __forceinline__ unsigned long long sym_term(uint32_t x, uint32_t y) {
     return pair_hash(x, y) - pair_hash(y, x);
 }
 
-// Sets color c's bit (colors 1..64) in a 64-bit mask kept as two 32-bit words;
-// c == 0 and c > 64 wrap out of both ranges.
-__device__ __forceinline__ void add_color_bit(uint32_t c, uint32_t& lo, uint32_t& hi) {
-    const uint32_t a = c - 1u, b = c - 33u;
-    lo |= a < 32u ? 1u << a : 0u;
-    hi |= b < 32u ? 1u << b : 0u;
-}
-
 // Warp per item: up to SWEEP_CH live slots of one row. Nothing in the graph
 // changes during a sweep, so loads take the read-only path. Each lane keeps two
 // 16-byte slot loads and their eight state gathers in flight per round.
-// SYM: also accumulate the mirror checksum (first sweep of a repair only).
+// SYM: also accumulate the mirror checksum (first sweep of a repair, and only
+// while the rows are not known to be mirror-complete).
 template <bool SYM>
-__global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b) {
+__device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& b) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
     const uint32_t cnt = *b.item_count;
@@ -462,6 +458,12 @@ __global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b) {
     }
 }
 
+template <bool SYM>
+__global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b) {
+    if (SYM && ld_cg(g.asym)) sweep_items_body<true>(g, b);
+    else sweep_items_body<false>(g, b);  // mirror-complete rows: the checksum is known to be 0
+}
+
 // One vertex of the finalize pass (warp-collective: every lane calls it; `valid`
 // lanes own a vertex). Short rows are swept here directly; long rows read the
 // accumulators. REBUILD writes bitmaps; TIER1 also decides the recolors.
@@ -511,6 +513,7 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
             if (indep) {
                 if (hd == EMPTY) g.bm[x] = bits;
                 else if (decide && myc != 0 && myc <= 64) g.bm[x] |= 1ull << (myc - 1);
+                if (decide) b.acc_bm[x] = bits;  // the selection step reads and clears it
                 b.needf[x] = decide ? 1 : 0;
                 need = decide;
             } else if (hd == EMPTY) {
@@ -561,10 +564,11 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
 __global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b, int mode, int list, int with_sym) {
     const uint32_t lim = list ? *b.wl_count : g.n;
     const uint32_t stride = gridDim.x * blockDim.x;
+    const bool sym = with_sym && ld_cg(g.asym);
     for (uint32_t base = blockIdx.x * blockDim.x; base < lim; base += stride) {  // warp-uniform trip count
         const uint32_t t = base + threadIdx.x;
         const bool valid = t < lim;
-        finalize_one(g, b, mode, valid, valid ? (list ? b.wl[t] : t) : 0, with_sym != 0);
+        finalize_one(g, b, mode, valid, valid ? (list ? b.wl[t] : t) : 0, sym);
     }
 }
 
@@ -586,44 +590,149 @@ __global__ void __launch_bounds__(256) sweep_fac_kernel(Dev g, SweepBufs b) {
     }
 }
 
-// Independent-set selection: warp per conflicted vertex. It recolors only when
-// no conflicted neighbor has higher priority, choosing the first color its
-// neighbors leave free (start-of-sweep colors; nothing is committed yet). Every
-// conflicted vertex is marked for the next sweep's worklist.
-__global__ void __launch_bounds__(256) sweep_indep_select_kernel(Dev g, SweepBufs b) {
+// Independent-set selection, step 1: warp per item (chunk) of a conflicted
+// row. Sets the row's blocked flag (acc_fl) when a conflicted neighbor in the
+// chunk ranks above it; for a histogram-class row whose neighbors take every
+// color 1..64 (acc_bm, from the sweep) it also gathers the taken colors 65..2047
+// into the row's words of b.hiused. Colors are the start-of-sweep ones.
+__global__ void __launch_bounds__(256) indep_items_kernel(Dev g, SweepBufs b, uint32_t salt) {
+    __shared__ uint32_t s_used[8][64];
+    uint32_t* used = s_used[threadIdx.x >> 5];
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t cnt = *b.need_count;
+    const uint32_t lane = lane_id();
+    const uint32_t cnt = *b.item_count;
+    used[lane] = 0;
+    used[lane + 32] = 0;
+    __syncwarp();
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
-        const uint32_t x = b.need_v[k];
-        const uint32_t xd = __ldg(g.deg + x);
-        const uint64_t s = g.rp[x];
+        const unsigned long long it = b.items[k];
+        const uint32_t x = (uint32_t)it;
+        if (!__ldg(b.needf + x)) continue;
+        if (ld_cg(b.acc_fl + x)) continue;  // another chunk already found it blocked
+        const uint32_t hd = __ldg(g.hdmap + x);
+        const bool full = hd != EMPTY && g.exact && ~b.acc_bm[x] == 0ull;
+        const unsigned long long rx = sel_rank(x, salt);
+        const uint32_t j = (uint32_t)(it >> 32);
+        const uint64_t rs = g.rp[x];
+        const uint64_t s = rs + (uint64_t)j * SWEEP_CH;
+        const uint64_t re = rs + g.hw[x];
+        const uint64_t e = s + SWEEP_CH < re ? s + SWEEP_CH : re;
         bool blocked = false;
-        warp_for_each(g.col, s, s + g.hw[x], [&](uint64_t, uint32_t y) {
-            if (y < g.n && y != x && b.needf[y] && prio_less(xd, x, __ldg(g.deg + y), y)) blocked = true;
-        });
-        blocked = __any_sync(FULL, blocked);
-        if (lane_id() == 0) atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
-        if (!blocked) {
-            const uint32_t w = ld_cg(g.st + x);
-            const uint16_t c = warp_fac(g, x, g.st);
-            if (lane_id() == 0) {
-                const uint32_t pi = atomicAdd(b.pend_count, 1u);
-                b.pend_v[pi] = x;
-                b.pend_w[pi] = pack(c, (uint16_t)(version_of(w) + 1));
+        for (uint64_t c = s & ~3ull; c < e; c += 256) {
+            const uint64_t i0 = c + 4ull * lane, i1 = i0 + 128;
+            uint4 q0 = make_uint4(INV, INV, INV, INV), q1 = q0;
+            if (i0 < e) q0 = __ldg(reinterpret_cast<const uint4*>(g.col + i0));
+            if (i1 < e) q1 = __ldg(reinterpret_cast<const uint4*>(g.col + i1));
+            uint32_t v[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+            uint8_t nf[8];
+            uint32_t nc[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                const uint64_t p = (t < 4 ? i0 : i1) + (t & 3);
+                const bool in = p >= s && p < e && v[t] < g.n && v[t] != x;
+                v[t] = in ? v[t] : INV;
+                nf[t] = in ? __ldg(b.needf + v[t]) : (uint8_t)0;
+                nc[t] = (in && full) ? color_of(__ldg(g.st + v[t])) : 0u;
             }
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                if (nf[t] && sel_rank(v[t], salt) > rx) blocked = true;
+                if (full && nc[t] > 64 && nc[t] < 2048) atomicOr(&used[nc[t] >> 5], 1u << (nc[t] & 31));
+            }
+            if (__any_sync(FULL, blocked)) break;  // a blocked row needs nothing more
         }
-        __syncwarp();
+        blocked = __any_sync(FULL, blocked);
+        if (lane == 0 && blocked) atomicOr(b.acc_fl + x, 1u);
+        if (full) {
+            __syncwarp();
+            uint32_t* dst = b.hiused + (uint64_t)hd * 64;
+            const uint32_t w0 = used[lane], w1 = used[lane + 32];
+            if (w0) atomicOr(dst + lane, w0);
+            if (w1) atomicOr(dst + lane + 32, w1);
+            used[lane] = 0;
+            used[lane + 32] = 0;
+            __syncwarp();
+        }
     }
 }
 
-__global__ void sweep_commit_kernel(Dev g, SweepBufs b) {
-    const uint32_t cnt = *b.pend_count;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
-        g.st[b.pend_v[k]] = b.pend_w[k];
+// Independent-set selection, step 2: thread per conflicted vertex. A row of at
+// most SWEEP_TINY slots checks its neighbors here; longer rows read step 1's
+// flag. An unblocked vertex takes the first color its neighbors leave free:
+// from the sweep's 64-bit mask, else from the gathered 65..2047 set
+// (histogram-class rows), else through the warp scan of sweep_fac_kernel
+// (bitmap rows whose 64 low colors are all taken). Every conflicted vertex is
+// marked for the next sweep's worklist.
+__global__ void __launch_bounds__(256) indep_decide_kernel(Dev g, SweepBufs b, uint32_t salt) {
+    const uint32_t cnt = *b.need_count;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+        const uint32_t x = b.need_v[t];
+        atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
+        const uint32_t len = g.hw[x];
+        bool blocked = false;
+        if (len <= SWEEP_TINY) {
+            const uint64_t s = g.rp[x];
+            const unsigned long long rx = sel_rank(x, salt);
+            for (uint32_t j = 0; j < len && !blocked; j++) {
+                const uint32_t y = __ldg(g.col + s + j);
+                if (y < g.n && y != x && __ldg(b.needf + y) && sel_rank(y, salt) > rx) blocked = true;
+            }
+        } else if (b.acc_fl[x]) {
+            blocked = true;
+            b.acc_fl[x] = 0;
+        }
+        const unsigned long long mask = b.acc_bm[x];
+        if (mask) b.acc_bm[x] = 0;
+        const uint32_t hd = __ldg(g.hdmap + x);
+        const bool full = ~mask == 0ull;
+        uint32_t c = 0;
+        if (full && hd != EMPTY && g.exact && len > SWEEP_TINY) {
+            uint32_t* w = b.hiused + (uint64_t)hd * 64;
+            c = 2048;
+            for (uint32_t k = 2; k < 64; k++) {
+                const uint32_t word = w[k];
+                if (word) w[k] = 0;
+                const uint32_t freew = ~word & (k == 2 ? ~1u : FULL);  // color 64 is taken (full mask)
+                if (c == 2048 && freew) c = k * 32 + __ffs(freew) - 1;
+            }
+        }
+        if (blocked) continue;
+        if (!full) {
+            c = __ffsll((long long)~mask);
+        } else if (c == 0) {  // the scan over colors above 64 needs a warp
+            b.fac_v[atomicAdd(b.fac_count, 1u)] = x;
+            continue;
+        }
+        const uint32_t w = g.st[x];
+        const uint32_t pi = atomicAdd(b.pend_count, 1u);
+        b.pend_v[pi] = x;
+        b.pend_w[pi] = pack((uint16_t)c, (uint16_t)(version_of(w) + 1));
+    }
 }
 
-void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, bool with_sym, int num_sms,
-                  cudaStream_t s) {
+// Writes the chosen colors; marks each recolored vertex (rbits, wmark) and,
+// for a row of at most SWEEP_TINY slots, its neighbors (longer rows are marked
+// per item by mark_items_kernel).
+__global__ void sweep_commit_kernel(Dev g, SweepBufs b) {
+    const uint32_t cnt = *b.pend_count;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+        const uint32_t x = b.pend_v[k];
+        g.st[x] = b.pend_w[k];
+        atomicOr(b.rbits + (x >> 5), 1u << (x & 31));
+        atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
+        const uint32_t len = g.hw[x];
+        if (len <= SWEEP_TINY) {
+            const uint64_t s = g.rp[x];
+            for (uint32_t j = 0; j < len; j++) {
+                const uint32_t y = g.col[s + j];
+                if (y < g.n) atomicOr(b.wmark + (y >> 5), 1u << (y & 31));
+            }
+        }
+    }
+}
+
+void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, bool with_sym, uint32_t sweep,
+                  int num_sms, cudaStream_t s) {
     if (mode != SWEEP_REBUILD) {
         cudaMemsetAsync(b.pend_count, 0, sizeof(uint32_t), s);
         cudaMemsetAsync(b.fac_count, 0, sizeof(uint32_t), s);
@@ -634,29 +743,40 @@ void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, b
     uint32_t fblocks = (g.n + 255) / 256;
     if (list && fblocks > (uint32_t)num_sms * 8) fblocks = num_sms * 8;
     sweep_finalize_kernel<<<fblocks, 256, 0, s>>>(g, b, (int)mode, list ? 1 : 0, with_sym ? 1 : 0);
-    if (mode == SWEEP_TIER1) {
+    if (mode == SWEEP_INDEP) {
+        const uint32_t salt = sweep_salt(sweep);
+        indep_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b, salt);
+        indep_decide_kernel<<<num_sms * 2, 256, 0, s>>>(g, b, salt);
+    }
+    if (mode != SWEEP_REBUILD) {
         sweep_fac_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
         sweep_commit_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
-    } else if (mode == SWEEP_INDEP) {
-        sweep_indep_select_kernel<<<num_sms * 4, 256, 0, s>>>(g, b);
-        sweep_commit_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
     }
 }
 
-// Marks every vertex recolored by the last sweep and all its live neighbors.
-__global__ void __launch_bounds__(256) mark_recolored_kernel(Dev g, SweepBufs b) {
+// Warp per item of the last sweep whose row was recolored: marks the
+// neighbors in the item's slots.
+__global__ void __launch_bounds__(256) mark_items_kernel(Dev g, SweepBufs b) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t cnt = *b.pend_count;
+    const uint32_t lane = lane_id();
+    const uint32_t cnt = *b.item_count;
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
-        const uint32_t x = b.pend_v[k];
-        if (lane_id() == 0) atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
-        const uint64_t s = g.rp[x];
-        warp_for_each(g.col, s, s + g.hw[x], [&](uint64_t, uint32_t y) {
+        const unsigned long long it = b.items[k];
+        const uint32_t x = (uint32_t)it;
+        if (!(b.rbits[x >> 5] & (1u << (x & 31)))) continue;
+        const uint32_t j = (uint32_t)(it >> 32);
+        const uint64_t rs = g.rp[x];
+        const uint64_t s = rs + (uint64_t)j * SWEEP_CH;
+        const uint64_t re = rs + g.hw[x];
+        const uint64_t e = s + SWEEP_CH < re ? s + SWEEP_CH : re;
+        for (uint64_t p = s + lane; p < e; p += 32) {
+            const uint32_t y = g.col[p];
             if (y < g.n) atomicOr(b.wmark + (y >> 5), 1u << (y & 31));
-        });
+        }
     }
 }
 
+// Turns the marks into the next worklist and clears them (and rbits).
 __global__ void collect_marks_kernel(uint32_t n, SweepBufs b) {
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nw = (n + 31) / 32;
@@ -664,6 +784,7 @@ __global__ void collect_marks_kernel(uint32_t n, SweepBufs b) {
     if (w < nw) {
         bits = b.wmark[w];
         if (bits) b.wmark[w] = 0;
+        if (b.rbits[w]) b.rbits[w] = 0;
     }
     uint32_t total = 0;
     const uint32_t off = warp_excl_scan(__popc(bits), total);
@@ -679,7 +800,7 @@ __global__ void collect_marks_kernel(uint32_t n, SweepBufs b) {
 }
 
 void launch_next_worklist(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s) {
-    mark_recolored_kernel<<<num_sms * 4, 256, 0, s>>>(g, b);
+    mark_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b);
     cudaMemsetAsync(b.wl_count, 0, sizeof(uint32_t), s);
     const uint32_t nw = (g.n + 31) / 32;
     collect_marks_kernel<<<(nw + 255) / 256, 256, 0, s>>>(g.n, b);

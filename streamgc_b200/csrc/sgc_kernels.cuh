@@ -36,7 +36,24 @@ struct SweepBufs {
     uint8_t* needf;              // per vertex: conflicted (or uncolored with neighbors) at the last visit
     uint32_t* need_v;
     uint32_t* need_count;
+    uint32_t* rbits;             // bitmask: recolored by the last sweep (cleared with the worklist)
+    uint32_t* hiused;            // exact selection: 64 words per histogram-class row, colors 64..2047
+                                 // taken by its neighbors (filled and cleared within one sweep)
 };
+
+// Selection order of the independent-set rule: a 32-bit mix of (x, salt) with
+// the id as tie-break. The mixer is the "lowbias32" function published in C.
+// Wellons' hash-prospector; the salt changes with every sweep.
+__host__ __device__ __forceinline__ unsigned long long sel_rank(uint32_t x, uint32_t salt) {
+    uint32_t h = x ^ salt;
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    h *= 0x846ca68bu;
+    h ^= h >> 16;
+    return ((unsigned long long)h << 32) | x;
+}
+__host__ __device__ __forceinline__ uint32_t sweep_salt(uint32_t sweep) { return (sweep + 1u) * 0x9E3779B9u; }
 
 // Same-edge ordering for a concurrently applied batch.
 struct EdgeOrder {
@@ -51,9 +68,9 @@ struct EdgeOrder {
 };
 
 // REBUILD: bitmaps only. TIER1: the reference rule (every conflicted vertex
-// recolors from start-of-sweep state). INDEP: conflicted vertices recolor only
-// when no conflicted neighbor has higher priority, so recolored vertices are
-// never adjacent and a sweep creates no conflict.
+// recolors from start-of-sweep state). INDEP: a conflicted vertex recolors only
+// when no conflicted neighbor ranks above it (sel_rank of this sweep), so
+// recolored vertices are never adjacent and a sweep creates no conflict.
 enum SweepMode : int { SWEEP_REBUILD = 0, SWEEP_TIER1 = 1, SWEEP_INDEP = 2 };
 
 // ---- launchers (sgc_kernels.cu) ----
@@ -67,10 +84,14 @@ void launch_drain(const Dev& g, const uint32_t* drain_n, bool ordered, unsigned 
 void launch_snapshot(const Dev& g, uint16_t* snap, cudaStream_t s);
 // list == false: every vertex; list == true: the vertices in b.wl.
 void launch_build_items(const Dev& g, const SweepBufs& b, bool list, cudaStream_t s);
-// with_sym: accumulate the mirror checksum (b.symsum) over the visited entries.
-void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, bool with_sym, int num_sms,
-                  cudaStream_t s);
-// After a TIER1 sweep: b.wl = the recolored vertices and their neighbors.
+// with_sym: accumulate the mirror checksum (b.symsum) over the visited entries
+// when *g.asym is set (rows not known to be mirror-complete). `sweep` is the
+// sweep's index within its repair (the independent-set order's salt).
+void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, bool with_sym, uint32_t sweep,
+                  int num_sms, cudaStream_t s);
+// After a sweep: b.wl = the vertices it recolored, their neighbors, and (INDEP)
+// the vertices still conflicted. Reads the sweep's items: call before the next
+// launch_build_items.
 void launch_next_worklist(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s);
 void launch_query(const uint16_t* snap, uint32_t n, const uint32_t* v, uint16_t* out, uint32_t k, cudaStream_t s);
 void launch_colors(const Dev& g, uint16_t* out, cudaStream_t s);
