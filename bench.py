@@ -280,6 +280,8 @@ def cpu_baseline(g, h, bench, first_batch, nb, budget_s):
     from oracle import oracle as O
     o = O.Oracle(g.row_ptr, g.col_idx, g.degree, hist_threshold=HIST_THR, exact=True)
     o.load_state(h.col(), h.states(), h.bitmaps(), np.zeros(0, dtype=np.uint32))
+    # the GPU's last publish was proper on mirror-complete rows: same repair rules from here
+    o.set_repair_state(clean=True, asym=False)
     done = 0
     t0 = time.perf_counter()
     for k in range(nb):

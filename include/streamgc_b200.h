@@ -51,6 +51,9 @@ typedef struct sgc_options {
     uint32_t max_batch;        /* largest batch sgc_apply accepts (default 32768, the reference's host batch) */
     int32_t  device;           /* CUDA device ordinal */
     uint32_t flags;            /* SGC_OPT_* */
+    uint32_t full_repair_every;/* exact selection: every Nth repair visits every vertex (0 = only when
+                                  required, 1 = always); the others start from the touched vertices */
+    uint32_t repair_tile;      /* slots per warp work item in repair sweeps (0 = 512; >= 256) */
 } sgc_options;
 
 /* What one repair (sgc_repair / sgc_publish) did. */
@@ -63,7 +66,7 @@ typedef struct sgc_repair_report {
     uint32_t drained;            /* overflow entries re-inserted this call */
     uint64_t drain_failed;       /* overflow entries that still found no slot */
     uint32_t proper;             /* 1 when the result is a proper coloring of the live CSR */
-    uint32_t _pad;
+    uint32_t incremental;        /* 1 when the first sweep visited only the vertices touched since the last repair */
 } sgc_repair_report;
 
 typedef struct sgc_stats {

@@ -68,6 +68,9 @@ def lib():
             "og_process_stream_repaired": (C.c_uint32, [_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32]),
             "og_phase_end": (C.c_uint32, [_vp, C.POINTER(C.c_int), _u32p]),
             "og_load_state": (None, [_vp, _u32p, _u32p, _u64p, _u32p]),
+            "og_publish_repair": (None, [_vp, C.c_int, _u32p]),
+            "og_set_full_repair_every": (None, [_vp, C.c_uint32]),
+            "og_set_repair_state": (None, [_vp, C.c_int, C.c_int]),
             "og_get_states": (None, [_vp, _u32p]),
             "og_set_states": (None, [_vp, _u32p]),
             "og_get_bitmaps": (None, [_vp, _u64p]),
@@ -162,6 +165,20 @@ class Oracle:
         last = np.zeros(1, dtype=np.uint32)
         fixed = self.L.og_phase_end(self.h, C.byref(it), _p(last, _u32p))
         return it.value, int(last[0]), fixed
+
+    def publish_repair(self, force_full=False):
+        """Compact, drain, repair, snapshot as the library's sgc_publish does under
+        exact selection (incremental when allowed)."""
+        out = np.zeros(6, dtype=np.uint32)
+        self.L.og_publish_repair(self.h, 1 if force_full else 0, _p(out, _u32p))
+        keys = ("tier1_iterations", "tier1_last_count", "incremental", "tier2_ran", "proper", "tier2_fixed")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def set_full_repair_every(self, every):
+        self.L.og_set_full_repair_every(self.h, every)
+
+    def set_repair_state(self, clean, asym):
+        self.L.og_set_repair_state(self.h, 1 if clean else 0, 1 if asym else 0)
 
     def process_stream(self, ups, epoch_size, batch=32768):
         ups = np.ascontiguousarray(ups, dtype=EDGE_UPDATE)

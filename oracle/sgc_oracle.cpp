@@ -84,6 +84,14 @@ struct Oracle {
     uint64_t recolors = 0;
     uint64_t updates_applied = 0;
     uint64_t skipped_updates = 0;
+    // repair bookkeeping of the exact-selection configuration (the library's
+    // device flags): rows possibly not mirror-complete; last repair ended
+    // proper; endpoints touched since the last repair; full-repair cadence
+    bool asym = true;
+    bool clean = false;
+    std::vector<uint8_t> touched;
+    uint32_t full_every = 16;
+    uint64_t since_full = 0;
     Bytes bytes;
     std::string err;
 
@@ -194,32 +202,37 @@ struct Oracle {
     }
 
     // -------- slack CSR row edits (local_update.cu:12-56) --------
-    void add_slot(uint32_t x, uint32_t nbr, uint64_t& b) {
+    // Returns 0 inserted, 1 already present, 2 overflowed.
+    int add_slot(uint32_t x, uint32_t nbr, uint64_t& b) {
         uint64_t from = rp[x];
         if (!edited[x]) {
-            if (pristine_find(x, nbr, b) != ~0ull) return;
+            if (pristine_find(x, nbr, b) != ~0ull) return 1;
             from = rp[x] + base_len[x];
         }
         for (uint64_t j = from; j < rp[x + 1]; j++) {
             uint32_t s = col[j];
             b += 4;
-            if (s == INV) { col[j] = nbr; b += 4; edited[x] = 1; return; }
-            if (s == nbr) return;
+            if (s == INV) { col[j] = nbr; b += 4; edited[x] = 1; return 0; }
+            if (s == nbr) return 1;
         }
         uint32_t pos = ovf_count++;
         if (pos < OVF_CAP) { ovf[pos].local_vertex_idx = x; ovf[pos].neighbor_global = nbr; b += 8; }
         else ovf_lost++;
+        asym = true;
+        return 2;
     }
-    void remove_slot(uint32_t x, uint32_t nbr, uint64_t& b) {
+    // Returns whether an entry was removed.
+    bool remove_slot(uint32_t x, uint32_t nbr, uint64_t& b) {
         if (!edited[x]) {
             const uint64_t p = pristine_find(x, nbr, b);
-            if (p != ~0ull) { col[p] = INV; b += 4; edited[x] = 1; }
-            return;
+            if (p != ~0ull) { col[p] = INV; b += 4; edited[x] = 1; return true; }
+            return false;
         }
         for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
             b += 4;
-            if (col[j] == nbr) { col[j] = INV; b += 4; return; }
+            if (col[j] == nbr) { col[j] = INV; b += 4; return true; }
         }
+        return false;
     }
 
     // -------- recolor (recolor.cu:49-163) --------
@@ -256,9 +269,9 @@ struct Oracle {
         uint32_t u = e.u, v = e.v;
         if (u >= n || v >= n) { skipped_updates++; return; }  // hash miss -> continue
         updates_applied++;
+        if (exact && (e.type == SGC_UPDATE_ADD || e.type == SGC_UPDATE_DEL)) touched[u] = touched[v] = 1;
         if (e.type == SGC_UPDATE_ADD) {
-            add_slot(u, v, b);
-            add_slot(v, u, b);
+            if (add_slot(u, v, b) != add_slot(v, u, b)) asym = true;
             b += 4;
             if (color(u) == 0) {
                 uint16_t c = fac(u, st, b);
@@ -283,8 +296,9 @@ struct Oracle {
             uint16_t fu = color(v);
             uint16_t fv = color(u);
             b += 8;
-            remove_slot(u, v, b);
-            remove_slot(v, u, b);
+            const bool du = remove_slot(u, v, b);
+            const bool dv = remove_slot(v, u, b);
+            if (du != dv) asym = true;
             removed_nbr(u, fu, b);
             removed_nbr(v, fv, b);
             try_reduce(u, fu, b);
@@ -326,7 +340,7 @@ struct Oracle {
                 if (s == INV) { col[j] = nb; done = true; edited[x] = 1; break; }
                 if (s == nb) { done = true; break; }
             }
-            if (!done) failed++;
+            if (!done) { failed++; asym = true; }
         }
         drain_failed += failed;
         return failed;
@@ -524,6 +538,162 @@ struct Oracle {
         return 20;
     }
 
+    // -------- mirror checksum and properness --------
+    // Sum over live entries x->y (y < n, y != x) of H(x,y) - H(y,x): zero when
+    // every entry has its mirror (the library's first-sweep checksum).
+    static uint64_t pair_hash(uint32_t x, uint32_t y) {
+        const uint64_t z = (((uint64_t)x << 32) | y) * 0x9E3779B97F4A7C15ull;
+        return z ^ (z >> 29);
+    }
+    uint64_t mirror_sum() const {
+        uint64_t sum = 0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : sum)
+        for (int64_t xi = 0; xi < (int64_t)n; xi++) {
+            const uint32_t x = (uint32_t)xi;
+            for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                const uint32_t y = col[j];
+                if (y >= n || y == x) continue;
+                sum += pair_hash(x, y) - pair_hash(y, x);
+            }
+        }
+        return sum;
+    }
+    // No live edge joins two equal nonzero colors and no vertex with a live
+    // entry is uncolored.
+    bool is_proper() const {
+        for (uint32_t x = 0; x < n; x++)
+            for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                const uint32_t y = col[j];
+                if (y == INV) continue;
+                if (color(x) == 0) return false;
+                if (y < n && y != x && color(y) == color(x)) return false;
+            }
+        return true;
+    }
+
+    // -------- incremental independent-set repair --------
+    // First worklist: the vertices touched by updates since the last repair.
+    // A sweep visits its worklist only (start-of-sweep colors): it rebuilds
+    // their bitmaps and finds the conflicted ones; a same-colored neighbor that
+    // loses to a visited vertex joins the next worklist, as does every
+    // conflicted vertex the independent-set rule blocks. A recolored vertex ORs
+    // its new color (1..64) into its neighbors' bitmaps. Stops when the next
+    // worklist is empty (up to 64 sweeps). Returns sweeps run.
+    int tier1_incremental(uint32_t* last_count, bool* done) {
+        std::vector<uint32_t> W;
+        for (uint32_t x = 0; x < n; x++)
+            if (touched[x]) { W.push_back(x); touched[x] = 0; }
+        std::vector<uint8_t> needf(n, 0), nextf(n, 0);
+        *done = false;
+        uint32_t count = 0;
+        for (int it = 0; it < 64; it++) {
+            const std::vector<uint32_t> old = st;
+            std::vector<uint32_t> need;
+            for (uint32_t x : W) {
+                const uint16_t my = (uint16_t)(old[x] & 0xFFFFu);
+                uint64_t bits = 0;
+                bool has = false, conf = false;
+                for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                    const uint32_t ng = col[j];
+                    if (ng == INV) continue;
+                    has = true;
+                    if (ng >= n) continue;
+                    const uint16_t c = (uint16_t)(old[ng] & 0xFFFFu);
+                    if (c != 0 && c <= 64) bits |= 1ull << (c - 1);
+                    if (my != 0 && c == my) {
+                        if (prio(x) < prio(ng)) conf = true;
+                        else if (ng != x) nextf[ng] = 1;
+                    }
+                }
+                const bool d = (my == 0) ? has : conf;
+                const uint64_t own = (d && my != 0 && my <= 64) ? 1ull << (my - 1) : 0ull;
+                if (hdmap[x] == EMPTY) bm[x] = bits | own;
+                else bm[x] |= own;
+                needf[x] = d ? 1 : 0;
+                if (d) need.push_back(x);
+            }
+            count = (uint32_t)need.size();
+            const uint32_t salt = (uint32_t)(it + 1) * 0x9E3779B9u;
+            std::vector<uint32_t> recolored;
+            uint64_t b = 0;
+            for (uint32_t x : need) {
+                bool blocked = false;
+                for (uint64_t j = rp[x]; j < rp[x + 1] && !blocked; j++) {
+                    const uint32_t y = col[j];
+                    if (y >= n || y == x) continue;
+                    if (needf[y] && sel_rank(x, salt) < sel_rank(y, salt)) blocked = true;
+                }
+                if (blocked) { nextf[x] = 1; continue; }
+                const uint16_t c = fac(x, old, b);
+                st[x] = sgc_pack_state(c, (uint16_t)((old[x] >> 16) + 1));
+                recolored.push_back(x);
+            }
+            bytes.tier1 += b;
+            for (uint32_t x : recolored) {
+                needf[x] = 0;
+                const uint16_t c = color(x);
+                if (c == 0 || c > 64) continue;
+                for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                    const uint32_t y = col[j];
+                    if (y < n) bm[y] |= 1ull << (c - 1);
+                }
+            }
+            W.clear();
+            for (uint32_t x = 0; x < n; x++)
+                if (nextf[x]) { W.push_back(x); nextf[x] = 0; }
+            if (W.empty()) {
+                *done = true;
+                if (last_count) *last_count = count;
+                return it + 1;
+            }
+        }
+        if (last_count) *last_count = count;
+        return 64;
+    }
+
+    // One repair of the exact-selection configuration (the library's
+    // sgc_publish / sgc_repair): incremental when the last repair ended proper,
+    // the rows are known mirror-complete and no full repair is due or forced;
+    // else rebuild + full independent-set sweeps (with the mirror checksum when
+    // the rows are not known mirror-complete). Tier-2 runs unless the sweeps
+    // converged on mirror-complete rows. out: [sweeps, last count, incremental,
+    // tier2 ran, proper, tier2 fixes].
+    void repair_exact(bool force, uint32_t* out) {
+        const bool incr = clean && !force && !asym && !(full_every && since_full + 1 >= full_every);
+        uint32_t last = 0;
+        int iters = 0;
+        bool done = false, sym_bad = false;
+        if (incr) {
+            iters = tier1_incremental(&last, &done);
+        } else {
+            std::fill(touched.begin(), touched.end(), (uint8_t)0);
+            if (asym) {
+                sym_bad = mirror_sum() != 0;
+                if (!sym_bad) asym = false;
+            }
+            iters = tier1(nullptr, 0, &last);
+            done = last == 0;
+        }
+        since_full = incr ? since_full + 1 : 0;
+        bool proper = done && !sym_bad;
+        bool t2 = false;
+        uint32_t fixed = 0;
+        if (!proper) {
+            fixed = tier2();
+            t2 = true;
+            proper = is_proper();
+        }
+        clean = proper;
+        if (out) {
+            out[0] = (uint32_t)iters;
+            out[1] = last;
+            out[2] = incr ? 1 : 0;
+            out[3] = t2 ? 1 : 0;
+            out[4] = proper ? 1 : 0;
+            out[5] = fixed;
+        }
+    }
+
     // -------- Tier-2 (streamgc.cu:1057-1240) --------
     uint32_t tier2() {
         std::vector<std::vector<uint32_t>> adj(n);
@@ -640,6 +810,7 @@ void* og_create(uint32_t n, const uint64_t* row_ptr, const uint32_t* col_idx, co
     g->hist.assign(g->exact ? 0 : (size_t)g->num_hd * g->maxc, 0);
     g->snap.assign(n, 0);
     g->ovf.resize(OVF_CAP);
+    g->touched.assign(n, 0);
     return g;
 }
 
@@ -692,11 +863,37 @@ uint32_t og_process_stream(void* h, const EdgeUpdate* ups, uint64_t n, uint32_t 
 uint32_t og_phase_end(void* h, int* t1_iters, uint32_t* t1_last) {
     Oracle* g = (Oracle*)h;
     g->drain_and_compact();
+    if (g->exact) {  // the library's phase end: a forced full repair
+        uint32_t out[6];
+        g->repair_exact(true, out);
+        if (t1_iters) *t1_iters = (int)out[0];
+        if (t1_last) *t1_last = out[1];
+        return out[5];
+    }
     uint32_t last = 0;
     int it = g->tier1(nullptr, 0, &last);
     if (t1_iters) *t1_iters = it;
     if (t1_last) *t1_last = last;
     return g->tier2();
+}
+
+// One repair as the library's sgc_publish does it (exact selection only):
+// compact, drain, repair (incremental when allowed), snapshot. out: [sweeps,
+// last count, incremental, tier2 ran, proper, tier2 fixes].
+void og_publish_repair(void* h, int force_full, uint32_t* out) {
+    Oracle* g = (Oracle*)h;
+    g->compact_all();
+    g->drain_pending();
+    g->repair_exact(force_full != 0, out);
+    g->snapshot();
+}
+void og_set_full_repair_every(void* h, uint32_t every) { ((Oracle*)h)->full_every = every; }
+// Sets the repair bookkeeping (e.g. to continue from a state loaded with
+// og_load_state that a proper repair produced on mirror-complete rows).
+void og_set_repair_state(void* h, int clean, int asym) {
+    Oracle* g = (Oracle*)h;
+    g->clean = clean != 0;
+    g->asym = asym != 0;
 }
 
 // Epoch with repair-before-publish (the concurrent mode's epoch): compact,
@@ -716,8 +913,12 @@ uint32_t og_process_stream_repaired(void* h, const EdgeUpdate* ups, uint64_t n, 
         if (since >= epoch_size) {
             g->compact_all();
             g->drain_pending();
-            g->tier1(nullptr, 0, nullptr);
-            g->tier2();
+            if (g->exact) {
+                g->repair_exact(false, nullptr);
+            } else {
+                g->tier1(nullptr, 0, nullptr);
+                g->tier2();
+            }
             g->snapshot();
             since = 0;
             epochs++;
@@ -741,11 +942,17 @@ void og_load_state(void* h, const uint32_t* col, const uint32_t* states, const u
     std::memcpy(g->st.data(), states, g->n * 4ull);
     std::memcpy(g->bm.data(), bitmaps, g->n * 8ull);
     std::memcpy(g->hist.data(), hist, g->hist.size() * 4ull);
+    g->clean = false;
+    g->asym = true;
 }
 
 // ---------------- state access ----------------
 void og_get_states(void* h, uint32_t* out) { Oracle* g = (Oracle*)h; std::memcpy(out, g->st.data(), g->n * 4ull); }
-void og_set_states(void* h, const uint32_t* in) { Oracle* g = (Oracle*)h; std::memcpy(g->st.data(), in, g->n * 4ull); }
+void og_set_states(void* h, const uint32_t* in) {
+    Oracle* g = (Oracle*)h;
+    std::memcpy(g->st.data(), in, g->n * 4ull);
+    g->clean = false;  // colors from elsewhere: the next repair visits every vertex
+}
 void og_get_bitmaps(void* h, uint64_t* out) { Oracle* g = (Oracle*)h; std::memcpy(out, g->bm.data(), g->n * 8ull); }
 void og_get_hdmap(void* h, uint32_t* out) { Oracle* g = (Oracle*)h; std::memcpy(out, g->hdmap.data(), g->n * 4ull); }
 void og_get_hist(void* h, uint32_t* out) {

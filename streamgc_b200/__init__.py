@@ -47,13 +47,14 @@ class _Config(C.Structure):
 
 class _Options(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("slack_pct", C.c_uint32), ("max_hist_colors", C.c_uint32),
-                ("max_batch", C.c_uint32), ("device", C.c_int32), ("flags", C.c_uint32)]
+                ("max_batch", C.c_uint32), ("device", C.c_int32), ("flags", C.c_uint32),
+                ("full_repair_every", C.c_uint32), ("repair_tile", C.c_uint32)]
 
 
 class RepairReport(C.Structure):
     _fields_ = [("tier1_iterations", C.c_uint32), ("tier1_last_count", C.c_uint32), ("tier2_ran", C.c_uint32),
                 ("tier2_fixed", C.c_uint32), ("tier2_gave_up", C.c_uint32), ("drained", C.c_uint32),
-                ("drain_failed", C.c_uint64), ("proper", C.c_uint32), ("_pad", C.c_uint32)]
+                ("drain_failed", C.c_uint64), ("proper", C.c_uint32), ("incremental", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("_")}
@@ -279,13 +280,18 @@ class StreamGC:
     """One graph resident on one GPU (a handle of the C ABI)."""
 
     def __init__(self, graph: Graph, epoch_size=32768, histogram_threshold=64, slack_pct=300,
-                 max_hist_colors=1024, max_batch=32768, device=0, profile=False, exact_select=False):
+                 max_hist_colors=1024, max_batch=32768, device=0, profile=False, exact_select=False,
+                 full_repair_every=None, repair_tile=None):
         L = lib()
         cfg = _Config(1, graph.n, graph.nnz, 1 << 20, epoch_size, 100, histogram_threshold, 0.2)
         opt = _Options()
         L.sgc_default_options(C.byref(opt))
         opt.slack_pct, opt.max_hist_colors, opt.max_batch, opt.device = slack_pct, max_hist_colors, max_batch, device
         opt.flags = (1 if profile else 0) | (2 if exact_select else 0)
+        if full_repair_every is not None:
+            opt.full_repair_every = full_repair_every
+        if repair_tile is not None:
+            opt.repair_tile = repair_tile
         self.h = _vp()
         self.graph = graph
         self.n = graph.n

@@ -85,6 +85,9 @@ struct sgc_handle {
     uint32_t* dirty_list = nullptr;
     Tier2Bufs t2{};
     uint32_t* h_small = nullptr;    // pinned readback scratch
+    RepairCtl* h_rc_in = nullptr;   // pinned: host fields of the repair control block
+    RepairCtl* h_rc_out = nullptr;  // pinned: its readback
+    uint64_t repairs_since_full = 0;
     int last_mode = SGC_MODE_DETERMINISTIC;
     // host counters
     uint64_t updates = 0, epochs = 0, tier1_sweeps = 0, tier2_runs = 0, tier2_fixed = 0;
@@ -190,28 +193,21 @@ int drain(sgc_handle* h, bool ordered, unsigned long long* failed_counter) {
     return check_cuda("drain");
 }
 
-// Sweep with optional event timing around the edge passes.
-int sweep(sgc_handle* h, SweepMode mode, bool list = false, bool with_sym = false, uint32_t index = 0) {
-    const bool prof = (h->opt.flags & SGC_OPT_PROFILE) != 0 && mode != SWEEP_REBUILD;
-    cudaEvent_t a = nullptr, b = nullptr;
-    if (prof) {
-        a = take_event(h);
-        b = take_event(h);
-        cudaEventRecord(a, h->stream);
-    }
-    launch_sweep(h->g, h->sb, mode, list, with_sym, index, h->num_sms, h->stream);
-    h->launches += mode == SWEEP_REBUILD ? 2 : (mode == SWEEP_INDEP ? 6 : 4);
-    if (prof) {
-        cudaEventRecord(b, h->stream);
-        h->ev_pending.push_back({a, b});
-    }
-    return check_cuda("sweep");
+// A REBUILD sweep over every vertex (epoch maintenance), with optional event
+// timing.
+int rebuild_sweep(sgc_handle* h) {
+    launch_build_items(h->g, h->sb, 0, h->num_sms, h->stream);
+    launch_sweep(h->g, h->sb, SWEEP_REBUILD, 0, 0, h->num_sms, h->stream);
+    h->launches += 3;
+    return check_cuda("rebuild");
 }
 
-int build_items(sgc_handle* h, bool list = false) {
-    launch_build_items(h->g, h->sb, list, h->stream);
-    h->launches += 1;
-    return check_cuda("build_items");
+// The control block's `clean` flag: whether the next repair may start from the
+// touched vertices (the current colors are a proper coloring of the rows).
+int set_clean(sgc_handle* h, uint32_t v) {
+    CK(cudaMemsetAsync(&h->sb.rc->clean, 0, 4, h->stream));
+    if (v) CK(cudaMemsetAsync(&h->sb.rc->clean, 1, 1, h->stream));
+    return SGC_OK;
 }
 
 void publish_snapshot(sgc_handle* h) {
@@ -221,77 +217,69 @@ void publish_snapshot(sgc_handle* h) {
     h->front = back;
 }
 
-// Tier-1 loop of run_conflict_repair (streamgc.cu:1317-1393); rows compact and
-// items built. Tier-2 runs unless convergence on a mirror-complete CSR proves
-// it a no-op.
-int repair_loop(sgc_handle* h, sgc_repair_report* rep) {
-    // Reference rule (deterministic parity): at most 20 sweeps, stop at 0 or after
-    // 3 equal counts (streamgc.cu:1317-1393). Independent-set rule (exact color
-    // selection): each sweep resolves at least the highest-priority conflict and
-    // creates none, so the count only falls; up to 64 sweeps.
+// Tier-1 loop of run_conflict_repair (streamgc.cu:1317-1393) on compact rows,
+// driven by the device control block: the host starts it and reads the block
+// after each sweep. Tier-2 runs unless convergence on a mirror-complete CSR
+// proves it a no-op.
+//   Reference rule (deterministic parity): at most 20 sweeps, stop at 0 or after
+//   3 equal counts. Independent-set rule (exact color selection): each sweep
+//   resolves at least the highest-ranked conflict and creates none; up to 64
+//   sweeps. Under it a repair is incremental -- its first sweep visits only the
+//   vertices touched by updates since the last repair -- when that repair ended
+//   proper, the rows are mirror-complete and `force_full` is off: every new
+//   conflict then has an endpoint among the touched vertices.
+int repair_loop(sgc_handle* h, sgc_repair_report* rep, bool force_full) {
     const bool indep = h->g.exact != 0;
     const SweepMode mode = indep ? SWEEP_INDEP : SWEEP_TIER1;
-    const int max_sweeps = indep ? 64 : 20;
-    uint32_t* count_ptr = indep ? h->sb.need_count : &h->ctl->pend_count;
-    uint32_t prev = 0xFFFFFFFFu, cnt = 0;
-    int plateau = 0, it = 0;
-    CK(cudaMemsetAsync(&h->ctl->symsum, 0, 16, h->stream));
-    CK(cudaMemsetAsync(h->sb.swept, 0, 16, h->stream));
+    const uint32_t every = h->opt.full_repair_every;
+    if (every && h->repairs_since_full + 1 >= every) force_full = true;
+    RepairCtl* hin = h->h_rc_in;
+    hin->mode = (uint32_t)mode;
+    hin->max_sweeps = indep ? 64u : 20u;
+    hin->force_full = force_full ? 1u : 0u;
+    CK(cudaMemcpyAsync(h->sb.rc, hin, 12, cudaMemcpyHostToDevice, h->stream));
     const size_t mwords = ((h->n + 31) / 32) * 4;
     CK(cudaMemsetAsync(h->sb.wmark, 0, mwords, h->stream));
     CK(cudaMemsetAsync(h->sb.rbits, 0, mwords, h->stream));
-    for (it = 0; it < max_sweeps; it++) {
-        // Sweep 0 visits every vertex. Later Jacobi sweeps visit only the
-        // vertices recolored by the previous sweep and their neighbors (plus,
-        // under the independent-set rule, every vertex still conflicted):
-        // every other vertex sees the colors it saw then, so its rebuilt bitmap
-        // and its decision cannot change (the result equals a full sweep).
-        // Worklists need mirror-complete rows (sweep 0's checksum is zero): a
-        // vertex re-checked after a neighbor y recolors is found through y's row.
-        const bool use_list = it > 0 && *(unsigned long long*)(h->h_small + 2) == 0;
-        if (use_list) {
-            launch_next_worklist(h->g, h->sb, h->num_sms, h->stream);
-            TRY(build_items(h, true));
-            h->launches += 2;
-        } else if (it > 0) {
-            TRY(build_items(h, false));
-            CK(cudaMemsetAsync(h->sb.wmark, 0, mwords, h->stream));
-            CK(cudaMemsetAsync(h->sb.rbits, 0, mwords, h->stream));
+    CK(cudaMemsetAsync(h->sb.needf, 0, h->n, h->stream));  // no vertex starts conflicted
+    launch_repair_begin(h->g, h->sb, h->num_sms, h->stream);
+    h->launches += h->g.touched ? 2 : 1;
+    const bool prof = (h->opt.flags & SGC_OPT_PROFILE) != 0;
+    RepairCtl* rc = h->h_rc_out;
+    for (;;) {
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (prof) {
+            a = take_event(h);
+            b = take_event(h);
+            cudaEventRecord(a, h->stream);
         }
-        TRY(sweep(h, mode, use_list, it == 0, (uint32_t)it));
-        h->tier1_sweeps++;
-        CK(cudaMemcpyAsync(h->h_small, count_ptr, 4, cudaMemcpyDeviceToHost, h->stream));
-        if (it == 0) CK(cudaMemcpyAsync(h->h_small + 2, &h->ctl->symsum, 16, cudaMemcpyDeviceToHost, h->stream));
-        h->d2h_bytes += it == 0 ? 20 : 4;
+        launch_repair_sweep(h->g, h->sb, mode, h->num_sms, h->stream);
+        if (prof) {
+            cudaEventRecord(b, h->stream);
+            h->ev_pending.push_back({a, b});
+        }
+        launch_repair_step(h->g, h->sb, h->num_sms, h->stream, nullptr);
+        h->launches += 1 + (mode == SWEEP_INDEP ? 6 : 4) + 3;
+        CK(cudaMemcpyAsync(rc, h->sb.rc, sizeof(RepairCtl), cudaMemcpyDeviceToHost, h->stream));
+        h->d2h_bytes += sizeof(RepairCtl);
         TRY(sync(h));
-        cnt = h->h_small[0];
-        if (it == 0) h->live_entries = *(unsigned long long*)(h->h_small + 4);
-        if (cnt == 0) break;
-        if (!indep) {
-            if (cnt == prev) {
-                if (++plateau >= 3) break;
-            } else {
-                plateau = 0;
-            }
-        }
-        prev = cnt;
+        if (!rc->cont) break;
     }
-    const unsigned long long sym = *(unsigned long long*)(h->h_small + 2);
-    // Rows found mirror-complete stay so until an overflow, a drain failure or
-    // an update that found one direction only sets the flag again; until then
-    // the first sweep skips the checksum.
-    if (sym == 0) CK(cudaMemsetAsync(h->g.asym, 0, 4, h->stream));
-    const uint32_t iters = it < max_sweeps ? it + 1 : max_sweeps;
-    if (h->opt.flags & SGC_OPT_PROFILE) {
+    TRY(check_cuda("repair"));
+    h->tier1_sweeps += rc->it;
+    if (!rc->incr) h->live_entries = rc->live;
+    h->repairs_since_full = rc->incr ? h->repairs_since_full + 1 : 0;
+    if (prof) {
         unsigned long long sw[2];
         CK(cudaMemcpyAsync(sw, h->sb.swept, 16, cudaMemcpyDeviceToHost, h->stream));
         TRY(sync(h));
         h->sweep_bytes += 8ull * sw[0] + 28ull * sw[1];
     }
     sgc_repair_report r{};
-    r.tier1_iterations = iters;
-    r.tier1_last_count = cnt;
-    bool proper = (cnt == 0 && sym == 0);
+    r.tier1_iterations = rc->it;
+    r.tier1_last_count = rc->need;
+    r.incremental = rc->incr;
+    bool proper = rc->done && rc->sym == 0;
     if (!proper) {
         bool gave_up = false;
         const uint32_t fixed = run_tier2(h->g, h->t2, h->stream, h->h_small, &gave_up, &h->launches);
@@ -302,6 +290,7 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep) {
         h->tier2_runs++;
         h->tier2_fixed += fixed;
         proper = !gave_up;
+        if (proper) TRY(set_clean(h, 1));
     }
     r.proper = proper ? 1 : 0;
     if (rep) {
@@ -337,6 +326,8 @@ int sgc_default_options(sgc_options* o) {
     o->max_batch = SGC_HOST_BATCH_SIZE;
     o->device = 0;
     o->flags = 0;
+    o->full_repair_every = 16;
+    o->repair_tile = SWEEP_CH;
     return SGC_OK;
 }
 
@@ -347,6 +338,8 @@ int sgc_destroy(sgc_handle* h) {
     for (void* p : h->allocs) cudaFree(p);
     if (h->h_stage) cudaFreeHost(h->h_stage);
     if (h->h_small) cudaFreeHost(h->h_small);
+    if (h->h_rc_in) cudaFreeHost(h->h_rc_in);
+    if (h->h_rc_out) cudaFreeHost(h->h_rc_out);
     if (h->stage_free) cudaEventDestroy(h->stage_free);
     for (auto& pr : h->ev_pending) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     for (auto e : h->ev_pool) cudaEventDestroy(e);
@@ -372,6 +365,9 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     if (opt.max_hist_colors == 0 || opt.max_hist_colors % 4 || opt.max_hist_colors > 65535)
         return fail(SGC_EINVAL, "max_hist_colors must be a positive multiple of 4");
     if (opt.max_batch == 0) return fail(SGC_EINVAL, "max_batch must be positive");
+    if (opt.repair_tile == 0) opt.repair_tile = SWEEP_CH;
+    if (opt.repair_tile < SWEEP_CH_MIN || opt.repair_tile % 32 || opt.repair_tile > (1u << 20))
+        return fail(SGC_EINVAL, "repair_tile must be a multiple of 32 in [%u, 2^20]", SWEEP_CH_MIN);
     const uint32_t n = cfg->num_vertices;
     if (n == 0) return fail(SGC_EINVAL, "num_vertices is 0");
     if (row_ptr[0] != 0) return fail(SGC_EINVAL, "row_ptr[0] must be 0");
@@ -495,7 +491,7 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     eo.tmask = tsize - 1;
     // sweep buffers
     SweepBufs& sb = h->sb;
-    const uint64_t icap = h->total_slots / SWEEP_CH + (uint64_t)n + 1;
+    const uint64_t icap = h->total_slots / SWEEP_CH_MIN + (uint64_t)n + 1;
     if (icap > 0xFFFFFFF0ull) return bail(fail(SGC_ENOTSUP, "sweep item list beyond 2^32 entries"));
     sb.item_cap = (uint32_t)icap;
     A(&sb.items, icap);
@@ -517,6 +513,15 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     A(&sb.need_v, n);
     A(&sb.need_count, 4, 0);
     A(&sb.rbits, (n + 31) / 32 + 1, 0);
+    A(&sb.rc, 1, 0);
+    sb.tile = opt.repair_tile;
+    if (g.exact) A(&g.touched, (n + 31) / 32 + 1, 0);
+    else g.touched = nullptr;
+    if (cudaHostAlloc(&h->h_rc_in, sizeof(RepairCtl), cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc(&h->h_rc_out, sizeof(RepairCtl), cudaHostAllocDefault) != cudaSuccess)
+        return bail(fail(SGC_ENOMEM, "pinned control block allocation failed"));
+    std::memset(h->h_rc_in, 0, sizeof(RepairCtl));
+    std::memset(h->h_rc_out, 0, sizeof(RepairCtl));
     if (g.exact) A(&sb.hiused, (size_t)num_hd * 64, 0);
     else sb.hiused = nullptr;
     A(&h->dirty_list, n);
@@ -600,8 +605,7 @@ int sgc_epoch(sgc_handle* h) {
     publish_snapshot(h);
     TRY(compact_dirty(h));
     TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, nullptr));
-    TRY(build_items(h));
-    TRY(sweep(h, SWEEP_REBUILD));
+    TRY(rebuild_sweep(h));
     h->epochs++;
     return SGC_OK;
 }
@@ -614,8 +618,7 @@ int sgc_drain_and_compact(sgc_handle* h, sgc_repair_report* rep) {
     const unsigned long long before = *(unsigned long long*)(h->h_small + 8);
     TRY(compact_dirty(h));
     TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, &h->ctl->drain_failed));
-    TRY(build_items(h));
-    TRY(sweep(h, SWEEP_REBUILD));
+    TRY(rebuild_sweep(h));
     return read_drain(h, rep, before);
 }
 
@@ -628,10 +631,9 @@ int sgc_repair(sgc_handle* h, sgc_repair_report* rep) {
     const unsigned long long before = *(unsigned long long*)(h->h_small + 8);
     TRY(compact_dirty(h));
     TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, &h->ctl->drain_failed));
-    TRY(build_items(h));
-    // drain_and_compact's rebuild is subsumed: the first Tier-1 sweep rebuilds every bitmap first.
+    // drain_and_compact's rebuild is subsumed: the first (full) sweep rebuilds every bitmap first.
     TRY(read_drain(h, &r, before));
-    TRY(repair_loop(h, &r));
+    TRY(repair_loop(h, &r, true));
     if (rep) *rep = r;
     return SGC_OK;
 }
@@ -642,8 +644,7 @@ int sgc_publish(sgc_handle* h, sgc_repair_report* rep) {
     sgc_repair_report r{};
     TRY(compact_dirty(h));
     TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, &h->ctl->drain_failed));
-    TRY(build_items(h));
-    TRY(repair_loop(h, &r));
+    TRY(repair_loop(h, &r, false));
     publish_snapshot(h);
     h->epochs++;
     if (rep) *rep = r;
@@ -800,6 +801,7 @@ int sgc_upload(sgc_handle* h, int what, const void* src, uint64_t bytes) {
     }
     if (bytes != need) return fail(SGC_EINVAL, "upload target %d needs exactly %llu bytes", what, (unsigned long long)need);
     CK(cudaMemcpyAsync(dst, src, need, cudaMemcpyHostToDevice, h->stream));
+    TRY(set_clean(h, 0));  // colors from elsewhere: the next repair visits every vertex
     return sync(h);
 }
 

@@ -61,6 +61,8 @@ struct Dev {
     unsigned long long* ovf_lost;  // overflows beyond OVF_CAP (edge dropped, as the reference does)
     unsigned long long* nskip;     // updates skipped: an endpoint outside [0, n) (hash miss)
     uint32_t* err;
+    uint32_t* touched;             // exact selection: bitmask of update endpoints since the last repair
+                                   // (null otherwise)
     uint32_t* asym;                // nonzero: an entry may have lost its mirror since rows were last
                                    // found mirror-complete (set at creation, on every overflow, on a
                                    // drain failure, and when an update found one direction only)
@@ -537,6 +539,10 @@ __device__ __forceinline__ void warp_color_if_uncolored(const Dev& g, uint32_t x
 // pristine row's binary-search answer is final; concurrent callers fall back
 // to the linear scan whenever the search does not find the key.
 __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v, uint8_t type, bool exact) {
+    if (g.touched && lane_id() == 0 && (type == SGC_UPDATE_ADD || type == SGC_UPDATE_DEL)) {
+        atomicOr(g.touched + (u >> 5), 1u << (u & 31));
+        atomicOr(g.touched + (v >> 5), 1u << (v & 31));
+    }
     if (type == SGC_UPDATE_ADD) {
         const int ru = warp_add_slot(g, u, v, exact);
         const int rv = warp_add_slot(g, v, u, exact);

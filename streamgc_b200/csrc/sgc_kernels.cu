@@ -356,11 +356,25 @@ void launch_query(const uint16_t* snap, uint32_t n, const uint32_t* v, uint16_t*
 }
 
 // ---------------------------------------------------------------------------
-// degree-balanced sweep: rebuild + Tier-1 decision (Jacobi)
+// degree-balanced sweeps and the device-driven repair loop
 // ---------------------------------------------------------------------------
+//
+// A repair is a loop of sweeps whose state lives in the RepairCtl block on the
+// device: repair_begin_kernel starts it, each sweep reads its index and its
+// vertex set (every vertex, or the worklist b.wl) from there, and
+// repair_step_kernel decides whether another sweep runs. The host either reads
+// the block after each sweep (sgc_repair / sgc_publish) or lets a CUDA-graph
+// while-node run the loop (the batched engine): the kernels are the same.
 
-__global__ void build_items_kernel(Dev g, SweepBufs b, int list) {
+// list_mode of the per-vertex passes: 0 every vertex, 1 b.wl, 2 as RepairCtl says.
+__device__ __forceinline__ bool use_list(const SweepBufs& b, int list_mode) {
+    return list_mode == 2 ? ld_cg(&b.rc->list) != 0 : list_mode == 1;
+}
+
+__global__ void build_items_kernel(Dev g, SweepBufs b, int list_mode) {
+    const bool list = use_list(b, list_mode);
     const uint32_t lim = list ? *b.wl_count : g.n;
+    const uint32_t tile = b.tile;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < lim; base += stride) {  // warp-uniform trip count
         const uint32_t t = base + threadIdx.x;
@@ -368,7 +382,7 @@ __global__ void build_items_kernel(Dev g, SweepBufs b, int list) {
         if (t < lim) {
             x = list ? b.wl[t] : t;
             const uint32_t len = g.hw[x];
-            if (len > SWEEP_TINY) k = (len + SWEEP_CH - 1) / SWEEP_CH;
+            if (len > SWEEP_TINY) k = (len + tile - 1) / tile;
         }
         uint32_t total = 0;
         const uint32_t off = warp_excl_scan(k, total);
@@ -382,11 +396,11 @@ __global__ void build_items_kernel(Dev g, SweepBufs b, int list) {
         for (uint32_t j = 0; j < k; j++) b.items[wbase + off + j] = (unsigned long long)x | ((unsigned long long)j << 32);
     }
 }
-void launch_build_items(const Dev& g, const SweepBufs& b, bool list, cudaStream_t s) {
+void launch_build_items(const Dev& g, const SweepBufs& b, int list_mode, int num_sms, cudaStream_t s) {
     cudaMemsetAsync(b.item_count, 0, sizeof(uint32_t), s);
     uint32_t blocks = (g.n + 255) / 256;
-    if (list && blocks > 148 * 8) blocks = 148 * 8;
-    build_items_kernel<<<blocks, 256, 0, s>>>(g, b, list ? 1 : 0);
+    if (list_mode != 0 && blocks > (uint32_t)num_sms * 8) blocks = num_sms * 8;
+    build_items_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(g, b, list_mode);
 }
 
 // Ordered-pair hash for the symmetry checksum: the sum over all entries x->y
@@ -400,24 +414,32 @@ __device__ __forceinline__ unsigned long long sym_term(uint32_t x, uint32_t y) {
     return pair_hash(x, y) - pair_hash(y, x);
 }
 
-// Warp per item: up to SWEEP_CH live slots of one row. Nothing in the graph
+// The bounds of item `it` (row x, chunk j) in slot space.
+__device__ __forceinline__ void item_bounds(const Dev& g, const SweepBufs& b, unsigned long long it, uint32_t& x,
+                                            uint64_t& s, uint64_t& e) {
+    x = (uint32_t)it;
+    const uint32_t j = (uint32_t)(it >> 32);
+    const uint64_t rs = g.rp[x];
+    s = rs + (uint64_t)j * b.tile;
+    const uint64_t re = rs + g.hw[x];
+    e = s + b.tile < re ? s + b.tile : re;
+}
+
+// Warp per item: up to b.tile live slots of one row. Nothing in the graph
 // changes during a sweep, so loads take the read-only path. Each lane keeps two
 // 16-byte slot loads and their eight state gathers in flight per round.
-// SYM: also accumulate the mirror checksum (first sweep of a repair, and only
-// while the rows are not known to be mirror-complete).
-template <bool SYM>
+// SYM: also accumulate the mirror checksum. PUSH (incremental repairs): a
+// same-colored neighbor that loses to x (lower priority) is marked for the
+// next sweep, which decides it from its own row.
+template <bool SYM, bool PUSH>
 __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& b) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
     const uint32_t cnt = *b.item_count;
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
-        const unsigned long long it = b.items[k];
-        const uint32_t x = (uint32_t)it;
-        const uint32_t j = (uint32_t)(it >> 32);
-        const uint64_t rs = g.rp[x];
-        const uint64_t s = rs + (uint64_t)j * SWEEP_CH;
-        const uint64_t re = rs + g.hw[x];
-        const uint64_t e = s + SWEEP_CH < re ? s + SWEEP_CH : re;
+        uint32_t x;
+        uint64_t s, e;
+        item_bounds(g, b, b.items[k], x, s, e);
         const uint32_t myc = color_of(__ldg(g.st + x));
         const uint32_t mydeg = __ldg(g.deg + x);
         uint32_t lo = 0, hi = 0;
@@ -440,7 +462,14 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
 #pragma unroll
             for (int t = 0; t < 8; t++) {
                 add_color_bit(nc[t], lo, hi);
-                if (nc[t] == myc && myc != 0 && !conf) conf = prio_less(mydeg, x, __ldg(g.deg + v[t]), v[t]);
+                if (nc[t] == myc && myc != 0) {
+                    if (PUSH) {
+                        if (prio_less(mydeg, x, __ldg(g.deg + v[t]), v[t])) conf = true;
+                        else if (v[t] != x) atomicOr(b.wmark + (v[t] >> 5), 1u << (v[t] & 31));
+                    } else if (!conf) {
+                        conf = prio_less(mydeg, x, __ldg(g.deg + v[t]), v[t]);
+                    }
+                }
                 if (SYM && v[t] != INV && v[t] != x) sym += sym_term(x, v[t]);
             }
         }
@@ -458,17 +487,28 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
     }
 }
 
-template <bool SYM>
-__global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b) {
-    if (SYM && ld_cg(g.asym)) sweep_items_body<true>(g, b);
-    else sweep_items_body<false>(g, b);  // mirror-complete rows: the checksum is known to be 0
+// sym_mode 0: no checksum; 1: checksum when *g.asym is set; 2: as 1, and only
+// in the first sweep of the repair (RepairCtl).
+__device__ __forceinline__ bool want_sym(const Dev& g, const SweepBufs& b, int sym_mode) {
+    if (sym_mode == 0 || !ld_cg(g.asym)) return false;  // mirror-complete rows: the checksum is known to be 0
+    return sym_mode == 1 || ld_cg(&b.rc->it) == 0;
+}
+__device__ __forceinline__ bool want_push(const SweepBufs& b, int mode) {
+    return mode == SWEEP_INDEP && ld_cg(&b.rc->incr) != 0;
+}
+
+__global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b, int mode, int sym_mode) {
+    const bool sym = want_sym(g, b, sym_mode);
+    if (want_push(b, mode)) sweep_items_body<false, true>(g, b);  // incremental: rows are mirror-complete
+    else if (sym) sweep_items_body<true, false>(g, b);
+    else sweep_items_body<false, false>(g, b);
 }
 
 // One vertex of the finalize pass (warp-collective: every lane calls it; `valid`
 // lanes own a vertex). Short rows are swept here directly; long rows read the
-// accumulators. REBUILD writes bitmaps; TIER1 also decides the recolors.
+// accumulators. REBUILD writes bitmaps; TIER1 and INDEP also decide.
 __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, int mode, bool valid, uint32_t x,
-                                             bool with_sym) {
+                                             bool with_sym, bool push) {
     bool fac_needed = false, pend = false, need = false;
     uint32_t pend_word = 0;
     unsigned long long sym = 0, live = 0;
@@ -490,7 +530,10 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
                 if (with_sym && ng != x) sym += sym_term(x, ng);
                 const uint32_t nc = color_of(__ldg(g.st + ng));
                 add_color_bit(nc, lo, hi);
-                if (nc == myc && nc != 0 && !conf && prio_less(mydeg, x, __ldg(g.deg + ng), ng)) conf = true;
+                if (nc == myc && nc != 0) {
+                    if (prio_less(mydeg, x, __ldg(g.deg + ng), ng)) conf = true;
+                    else if (push && ng != x) atomicOr(b.wmark + (ng >> 5), 1u << (ng & 31));
+                }
             }
             bits = ((unsigned long long)hi << 32) | lo;
         } else {
@@ -561,14 +604,17 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
 }
 
 // Thread per vertex (every vertex, or the worklist).
-__global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b, int mode, int list, int with_sym) {
+__global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b, int mode, int list_mode,
+                                                             int sym_mode) {
+    const bool list = use_list(b, list_mode);
     const uint32_t lim = list ? *b.wl_count : g.n;
     const uint32_t stride = gridDim.x * blockDim.x;
-    const bool sym = with_sym && ld_cg(g.asym);
+    const bool sym = want_sym(g, b, sym_mode);
+    const bool push = want_push(b, mode);
     for (uint32_t base = blockIdx.x * blockDim.x; base < lim; base += stride) {  // warp-uniform trip count
         const uint32_t t = base + threadIdx.x;
         const bool valid = t < lim;
-        finalize_one(g, b, mode, valid, valid ? (list ? b.wl[t] : t) : 0, sym);
+        finalize_one(g, b, mode, valid, valid ? (list ? b.wl[t] : t) : 0, sym, push);
     }
 }
 
@@ -595,28 +641,26 @@ __global__ void __launch_bounds__(256) sweep_fac_kernel(Dev g, SweepBufs b) {
 // chunk ranks above it; for a histogram-class row whose neighbors take every
 // color 1..64 (acc_bm, from the sweep) it also gathers the taken colors 65..2047
 // into the row's words of b.hiused. Colors are the start-of-sweep ones.
-__global__ void __launch_bounds__(256) indep_items_kernel(Dev g, SweepBufs b, uint32_t salt) {
+__global__ void __launch_bounds__(256) indep_items_kernel(Dev g, SweepBufs b) {
     __shared__ uint32_t s_used[8][64];
     uint32_t* used = s_used[threadIdx.x >> 5];
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
     const uint32_t cnt = *b.item_count;
+    const uint32_t salt = sweep_salt(ld_cg(&b.rc->it));
     used[lane] = 0;
     used[lane + 32] = 0;
     __syncwarp();
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
         const unsigned long long it = b.items[k];
-        const uint32_t x = (uint32_t)it;
-        if (!__ldg(b.needf + x)) continue;
-        if (ld_cg(b.acc_fl + x)) continue;  // another chunk already found it blocked
+        if (!__ldg(b.needf + (uint32_t)it)) continue;
+        if (ld_cg(b.acc_fl + (uint32_t)it)) continue;  // another chunk already found it blocked
+        uint32_t x;
+        uint64_t s, e;
+        item_bounds(g, b, it, x, s, e);
         const uint32_t hd = __ldg(g.hdmap + x);
         const bool full = hd != EMPTY && g.exact && ~b.acc_bm[x] == 0ull;
         const unsigned long long rx = sel_rank(x, salt);
-        const uint32_t j = (uint32_t)(it >> 32);
-        const uint64_t rs = g.rp[x];
-        const uint64_t s = rs + (uint64_t)j * SWEEP_CH;
-        const uint64_t re = rs + g.hw[x];
-        const uint64_t e = s + SWEEP_CH < re ? s + SWEEP_CH : re;
         bool blocked = false;
         for (uint64_t c = s & ~3ull; c < e; c += 256) {
             const uint64_t i0 = c + 4ull * lane, i1 = i0 + 128;
@@ -661,13 +705,14 @@ __global__ void __launch_bounds__(256) indep_items_kernel(Dev g, SweepBufs b, ui
 // flag. An unblocked vertex takes the first color its neighbors leave free:
 // from the sweep's 64-bit mask, else from the gathered 65..2047 set
 // (histogram-class rows), else through the warp scan of sweep_fac_kernel
-// (bitmap rows whose 64 low colors are all taken). Every conflicted vertex is
-// marked for the next sweep's worklist.
-__global__ void __launch_bounds__(256) indep_decide_kernel(Dev g, SweepBufs b, uint32_t salt) {
+// (bitmap rows whose 64 low colors are all taken). Blocked vertices are marked
+// for the next sweep (a full repair marks every conflicted vertex).
+__global__ void __launch_bounds__(256) indep_decide_kernel(Dev g, SweepBufs b) {
     const uint32_t cnt = *b.need_count;
+    const uint32_t salt = sweep_salt(ld_cg(&b.rc->it));
+    const bool incr = ld_cg(&b.rc->incr) != 0;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
         const uint32_t x = b.need_v[t];
-        atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
         const uint32_t len = g.hw[x];
         bool blocked = false;
         if (len <= SWEEP_TINY) {
@@ -681,6 +726,7 @@ __global__ void __launch_bounds__(256) indep_decide_kernel(Dev g, SweepBufs b, u
             blocked = true;
             b.acc_fl[x] = 0;
         }
+        if (blocked || !incr) atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
         const unsigned long long mask = b.acc_bm[x];
         if (mask) b.acc_bm[x] = 0;
         const uint32_t hd = __ldg(g.hdmap + x);
@@ -710,92 +756,87 @@ __global__ void __launch_bounds__(256) indep_decide_kernel(Dev g, SweepBufs b, u
     }
 }
 
-// Writes the chosen colors; marks each recolored vertex (rbits, wmark) and,
-// for a row of at most SWEEP_TINY slots, its neighbors (longer rows are marked
-// per item by mark_items_kernel).
+// Writes the chosen colors and clears the recolored vertices' conflict flags.
+// A full repair marks each recolored vertex and, for rows of at most
+// SWEEP_TINY slots, its neighbors for the next worklist (longer rows: per item
+// in mark_items_kernel). An incremental repair instead ORs the new color into
+// the neighbors' bitmaps (the next sweep needs no neighbor of a recolored
+// vertex: under the independent-set rule a recolor creates no conflict).
 __global__ void sweep_commit_kernel(Dev g, SweepBufs b) {
     const uint32_t cnt = *b.pend_count;
+    const bool incr = ld_cg(&b.rc->incr) != 0;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
         const uint32_t x = b.pend_v[k];
-        g.st[x] = b.pend_w[k];
+        const uint32_t nw = b.pend_w[k];
+        g.st[x] = nw;
+        b.needf[x] = 0;
         atomicOr(b.rbits + (x >> 5), 1u << (x & 31));
-        atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
+        if (!incr) atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
         const uint32_t len = g.hw[x];
         if (len <= SWEEP_TINY) {
             const uint64_t s = g.rp[x];
+            const uint32_t c = color_of(nw);
             for (uint32_t j = 0; j < len; j++) {
                 const uint32_t y = g.col[s + j];
-                if (y < g.n) atomicOr(b.wmark + (y >> 5), 1u << (y & 31));
+                if (y >= g.n) continue;
+                if (!incr) atomicOr(b.wmark + (y >> 5), 1u << (y & 31));
+                else if (c != 0 && c <= 64) atomicOr((unsigned long long*)(g.bm + y), 1ull << (c - 1));
             }
         }
     }
 }
 
-void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, bool with_sym, uint32_t sweep,
-                  int num_sms, cudaStream_t s) {
-    if (mode != SWEEP_REBUILD) {
-        cudaMemsetAsync(b.pend_count, 0, sizeof(uint32_t), s);
-        cudaMemsetAsync(b.fac_count, 0, sizeof(uint32_t), s);
-        cudaMemsetAsync(b.need_count, 0, sizeof(uint32_t), s);
-    }
-    if (with_sym) sweep_items_kernel<true><<<num_sms * 8, 256, 0, s>>>(g, b);
-    else sweep_items_kernel<false><<<num_sms * 8, 256, 0, s>>>(g, b);
-    uint32_t fblocks = (g.n + 255) / 256;
-    if (list && fblocks > (uint32_t)num_sms * 8) fblocks = num_sms * 8;
-    sweep_finalize_kernel<<<fblocks, 256, 0, s>>>(g, b, (int)mode, list ? 1 : 0, with_sym ? 1 : 0);
-    if (mode == SWEEP_INDEP) {
-        const uint32_t salt = sweep_salt(sweep);
-        indep_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b, salt);
-        indep_decide_kernel<<<num_sms * 2, 256, 0, s>>>(g, b, salt);
-    }
-    if (mode != SWEEP_REBUILD) {
-        sweep_fac_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
-        sweep_commit_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
-    }
-}
-
 // Warp per item of the last sweep whose row was recolored: marks the
-// neighbors in the item's slots.
+// neighbors in the item's slots (full repair) or ORs the row's new color into
+// their bitmaps (incremental repair).
 __global__ void __launch_bounds__(256) mark_items_kernel(Dev g, SweepBufs b) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
     const uint32_t cnt = *b.item_count;
+    const bool incr = ld_cg(&b.rc->incr) != 0;
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
         const unsigned long long it = b.items[k];
-        const uint32_t x = (uint32_t)it;
-        if (!(b.rbits[x >> 5] & (1u << (x & 31)))) continue;
-        const uint32_t j = (uint32_t)(it >> 32);
-        const uint64_t rs = g.rp[x];
-        const uint64_t s = rs + (uint64_t)j * SWEEP_CH;
-        const uint64_t re = rs + g.hw[x];
-        const uint64_t e = s + SWEEP_CH < re ? s + SWEEP_CH : re;
+        const uint32_t x0 = (uint32_t)it;
+        if (!(b.rbits[x0 >> 5] & (1u << (x0 & 31)))) continue;
+        uint32_t x;
+        uint64_t s, e;
+        item_bounds(g, b, it, x, s, e);
+        const uint32_t c = color_of(g.st[x]);
+        const unsigned long long bit = (c != 0 && c <= 64) ? 1ull << (c - 1) : 0ull;
+        if (incr && !bit) continue;
         for (uint64_t p = s + lane; p < e; p += 32) {
             const uint32_t y = g.col[p];
-            if (y < g.n) atomicOr(b.wmark + (y >> 5), 1u << (y & 31));
+            if (y >= g.n) continue;
+            if (incr) atomicOr((unsigned long long*)(g.bm + y), bit);
+            else atomicOr(b.wmark + (y >> 5), 1u << (y & 31));
         }
     }
 }
 
-// Turns the marks into the next worklist and clears them (and rbits).
-__global__ void collect_marks_kernel(uint32_t n, SweepBufs b) {
+// Turns a bitmask into a list (appending at *count) and clears it; `clear2`
+// (optional) is cleared alongside. With `keep` zero the bits are only cleared.
+__global__ void collect_bits_kernel(uint32_t n, uint32_t* bits_arr, uint32_t* clear2, uint32_t* list, uint32_t* count,
+                                    const uint32_t* keep) {
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nw = (n + 31) / 32;
+    const bool k_on = keep == nullptr || ld_cg(keep) != 0;
     uint32_t bits = 0;
     if (w < nw) {
-        bits = b.wmark[w];
-        if (bits) b.wmark[w] = 0;
-        if (b.rbits[w]) b.rbits[w] = 0;
+        bits = bits_arr[w];
+        if (bits) bits_arr[w] = 0;
+        if (clear2 && clear2[w]) clear2[w] = 0;
     }
+    if (!k_on) bits = 0;
     uint32_t total = 0;
     const uint32_t off = warp_excl_scan(__popc(bits), total);
     uint32_t base = 0;
-    if (lane_id() == 0 && total) base = atomicAdd(b.wl_count, total);
+    if (lane_id() == 0 && total) base = atomicAdd(count, total);
     base = __shfl_sync(FULL, base, 0);
     uint32_t k = base + off;
     while (bits) {
         const int i = __ffs(bits) - 1;
         bits &= bits - 1;
-        b.wl[k++] = w * 32 + i;
+        list[k++] = w * 32 + i;
     }
 }
 
@@ -803,7 +844,113 @@ void launch_next_worklist(const Dev& g, const SweepBufs& b, int num_sms, cudaStr
     mark_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b);
     cudaMemsetAsync(b.wl_count, 0, sizeof(uint32_t), s);
     const uint32_t nw = (g.n + 31) / 32;
-    collect_marks_kernel<<<(nw + 255) / 256, 256, 0, s>>>(g.n, b);
+    collect_bits_kernel<<<(nw + 255) / 256, 256, 0, s>>>(g.n, b.wmark, b.rbits, b.wl, b.wl_count, nullptr);
+}
+
+void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int list_mode, int sym_mode, int num_sms,
+                  cudaStream_t s) {
+    if (mode != SWEEP_REBUILD) {
+        cudaMemsetAsync(b.pend_count, 0, sizeof(uint32_t), s);
+        cudaMemsetAsync(b.fac_count, 0, sizeof(uint32_t), s);
+        cudaMemsetAsync(b.need_count, 0, sizeof(uint32_t), s);
+    }
+    sweep_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b, (int)mode, sym_mode);
+    uint32_t fblocks = (g.n + 255) / 256;
+    if (list_mode != 0 && fblocks > (uint32_t)num_sms * 8) fblocks = num_sms * 8;
+    sweep_finalize_kernel<<<fblocks ? fblocks : 1, 256, 0, s>>>(g, b, (int)mode, list_mode, sym_mode);
+    if (mode == SWEEP_INDEP) {
+        indep_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b);
+        indep_decide_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
+    }
+    if (mode != SWEEP_REBUILD) {
+        sweep_fac_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
+        sweep_commit_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
+    }
+}
+
+// Starts a repair: chooses incremental (rows mirror-complete, the last repair
+// ended proper, not forced full, exact selection) or full, and resets the
+// loop state and accumulators.
+__global__ void repair_begin_kernel(Dev g, SweepBufs b) {
+    RepairCtl& rc = *b.rc;
+    const bool incr = rc.mode == SWEEP_INDEP && rc.clean && !rc.force_full && !ld_cg(g.asym) && g.touched;
+    rc.incr = incr ? 1u : 0u;
+    rc.list = rc.incr;
+    rc.it = 0;
+    rc.cont = 1;
+    rc.done = 0;
+    rc.need = 0;
+    rc.next = 0;
+    rc.prev = 0xFFFFFFFFu;
+    rc.plateau = 0;
+    rc.sym = 0;
+    rc.live = 0;
+    *b.symsum = 0;
+    *b.live = 0;
+    *b.wl_count = 0;
+    b.swept[0] = 0;
+    b.swept[1] = 0;
+}
+
+// After each sweep: reads the counts, decides whether another sweep runs,
+// advances the index. Reference rule (TIER1): stop at 0 conflicts, after 3
+// equal counts, or at max_sweeps (streamgc.cu:1317-1393). Independent-set
+// rule: stop when nothing is conflicted (full) or the next worklist is empty
+// (incremental). Later sweeps of a full repair visit the worklist only when
+// the first sweep found the rows mirror-complete. `cond` (graph mode): the
+// while-node's handle receives the decision.
+__global__ void repair_step_kernel(Dev g, SweepBufs b, cudaGraphConditionalHandle cond, int has_cond) {
+    RepairCtl& rc = *b.rc;
+    const uint32_t count = rc.mode == SWEEP_INDEP ? *b.need_count : *b.pend_count;
+    const uint32_t next = *b.wl_count;
+    if (rc.it == 0) {
+        rc.sym = *b.symsum;
+        rc.live = *b.live;
+        if (rc.sym == 0 && *g.asym) *g.asym = 0;  // found mirror-complete
+    }
+    rc.need = count;
+    rc.next = next;
+    bool done;
+    bool stop;
+    if (rc.mode == SWEEP_INDEP) {
+        done = rc.incr ? next == 0 : count == 0;
+        stop = done;
+    } else {
+        done = count == 0;
+        stop = done;
+        if (!done) {
+            if (count == rc.prev) stop = ++rc.plateau >= 3;
+            else rc.plateau = 0;
+        }
+        rc.prev = count;
+    }
+    rc.done = done ? 1u : 0u;
+    rc.list = (rc.incr || rc.sym == 0) ? 1u : 0u;
+    rc.it += 1;
+    rc.cont = (!stop && rc.it < rc.max_sweeps) ? 1u : 0u;
+    if (!rc.cont) rc.clean = (done && rc.sym == 0) ? 1u : 0u;
+    if (has_cond) cudaGraphSetConditional(cond, rc.cont);
+}
+
+void launch_repair_begin(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s) {
+    repair_begin_kernel<<<1, 1, 0, s>>>(g, b);
+    // first worklist: the vertices touched since the last repair (incremental);
+    // a full repair only clears their marks
+    const uint32_t nw = (g.n + 31) / 32;
+    if (g.touched)
+        collect_bits_kernel<<<(nw + 255) / 256, 256, 0, s>>>(g.n, g.touched, nullptr, b.wl, b.wl_count, &b.rc->incr);
+    (void)num_sms;
+}
+
+void launch_repair_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s) {
+    launch_build_items(g, b, 2, num_sms, s);
+    launch_sweep(g, b, mode, 2, 2, num_sms, s);
+}
+
+void launch_repair_step(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s,
+                        const cudaGraphConditionalHandle* cond) {
+    launch_next_worklist(g, b, num_sms, s);
+    repair_step_kernel<<<1, 1, 0, s>>>(g, b, cond ? *cond : (cudaGraphConditionalHandle)0, cond ? 1 : 0);
 }
 
 }  // namespace sgc

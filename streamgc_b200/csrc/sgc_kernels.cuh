@@ -7,10 +7,33 @@
 
 namespace sgc {
 
-constexpr uint32_t SWEEP_CH = 512;    // slots per warp work item in a sweep
-constexpr uint32_t SWEEP_TINY = 16;   // rows this short are swept by one thread
+constexpr uint32_t SWEEP_CH = 512;       // default slots per warp work item in a sweep (repair tile width)
+constexpr uint32_t SWEEP_CH_MIN = 256;   // smallest tile width (sizes the item list)
+constexpr uint32_t SWEEP_TINY = 16;      // rows this short are swept by one thread
 constexpr uint32_t NONE32 = 0xFFFFFFFFu;
 constexpr unsigned long long EMPTY64 = 0xFFFFFFFFFFFFFFFFull;
+
+// Loop state of one repair, on the device (written by repair_begin_kernel and
+// repair_step_kernel; fields marked host are set by the host before a repair).
+struct RepairCtl {
+    uint32_t mode;         // host: SWEEP_TIER1 or SWEEP_INDEP
+    uint32_t max_sweeps;   // host
+    uint32_t force_full;   // host: 1 = visit every vertex in the first sweep
+    uint32_t clean;        // 1: the last repair ended proper and only updates changed colors since
+                           // (the host clears it when it writes states)
+    uint32_t incr;         // this repair starts from the touched vertices
+    uint32_t list;         // the current sweep visits b.wl (else every vertex)
+    uint32_t it;           // index of the current sweep
+    uint32_t cont;         // another sweep runs
+    uint32_t done;         // the last sweep left nothing to do
+    uint32_t need;         // conflicted vertices counted by the last sweep
+    uint32_t next;         // size of the next worklist
+    uint32_t prev;         // reference rule: last count
+    uint32_t plateau;      // reference rule: equal counts in a row
+    uint32_t pad;
+    unsigned long long sym;   // first sweep's mirror checksum
+    unsigned long long live;  // first sweep's live entries
+};
 
 // Per-sweep work state: warp items for rows longer than SWEEP_TINY, per-vertex
 // accumulators, the Jacobi pending list and the FAC work list.
@@ -18,6 +41,8 @@ struct SweepBufs {
     unsigned long long* items;   // x | chunk << 32
     uint32_t* item_count;
     uint32_t item_cap;
+    uint32_t tile;               // slots per item (repair tile width, >= SWEEP_CH_MIN)
+    RepairCtl* rc;
     unsigned long long* acc_bm;  // OR of neighbor colors 1..64, per vertex
     uint32_t* acc_fl;            // bit0: a same-colored neighbor has higher priority
     uint32_t* pend_v;            // Jacobi commit list
@@ -82,17 +107,25 @@ void launch_compact(const Dev& g, const uint32_t* list, const uint32_t* count, u
 void launch_take_overflow(const Dev& g, uint32_t* drain_n, cudaStream_t s);
 void launch_drain(const Dev& g, const uint32_t* drain_n, bool ordered, unsigned long long* failed, cudaStream_t s);
 void launch_snapshot(const Dev& g, uint16_t* snap, cudaStream_t s);
-// list == false: every vertex; list == true: the vertices in b.wl.
-void launch_build_items(const Dev& g, const SweepBufs& b, bool list, cudaStream_t s);
-// with_sym: accumulate the mirror checksum (b.symsum) over the visited entries
-// when *g.asym is set (rows not known to be mirror-complete). `sweep` is the
-// sweep's index within its repair (the independent-set order's salt).
-void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, bool list, bool with_sym, uint32_t sweep,
-                  int num_sms, cudaStream_t s);
-// After a sweep: b.wl = the vertices it recolored, their neighbors, and (INDEP)
-// the vertices still conflicted. Reads the sweep's items: call before the next
-// launch_build_items.
+// list_mode 0: every vertex; 1: the vertices in b.wl; 2: as b.rc->list says.
+void launch_build_items(const Dev& g, const SweepBufs& b, int list_mode, int num_sms, cudaStream_t s);
+// sym_mode 0: no mirror checksum; 1: accumulate it (b.symsum) when *g.asym is
+// set; 2: as 1, first sweep of a repair only. The sweep index (the
+// independent-set order's salt) and whether pushes are on come from b.rc.
+void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int list_mode, int sym_mode, int num_sms,
+                  cudaStream_t s);
+// After a sweep: b.wl = the next worklist (full repair: the vertices the sweep
+// recolored, their neighbors and the vertices still conflicted; incremental:
+// the blocked and pushed vertices). Reads the sweep's items: call before the
+// next launch_build_items.
 void launch_next_worklist(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s);
+// The device-driven repair loop: begin (b.rc host fields set), then per sweep
+// launch_repair_sweep + launch_repair_step; b.rc->cont says whether another
+// sweep runs. With `cond`, the step also sets that graph conditional.
+void launch_repair_begin(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s);
+void launch_repair_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s);
+void launch_repair_step(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s,
+                        const cudaGraphConditionalHandle* cond);
 void launch_query(const uint16_t* snap, uint32_t n, const uint32_t* v, uint16_t* out, uint32_t k, cudaStream_t s);
 void launch_colors(const Dev& g, uint16_t* out, cudaStream_t s);
 
