@@ -571,18 +571,16 @@ struct Oracle {
         return true;
     }
 
-    // -------- incremental independent-set repair --------
-    // First worklist: the vertices touched by updates since the last repair.
-    // A sweep visits its worklist only (start-of-sweep colors): it rebuilds
-    // their bitmaps and finds the conflicted ones; a same-colored neighbor that
-    // loses to a visited vertex joins the next worklist, as does every
-    // conflicted vertex the independent-set rule blocks. A recolored vertex ORs
-    // its new color (1..64) into its neighbors' bitmaps. Stops when the next
-    // worklist is empty (up to 64 sweeps). Returns sweeps run.
-    int tier1_incremental(uint32_t* last_count, bool* done) {
-        std::vector<uint32_t> W;
-        for (uint32_t x = 0; x < n; x++)
-            if (touched[x]) { W.push_back(x); touched[x] = 0; }
+    // -------- independent-set repair (exact selection) --------
+    // Starts from worklist W (every vertex for a full repair, else the vertices
+    // touched by updates since the last repair). A sweep visits its worklist
+    // only (start-of-sweep colors): it rebuilds their bitmaps and finds the
+    // conflicted ones; a same-colored neighbor that loses to a visited vertex
+    // joins the next worklist, as does every conflicted vertex the
+    // independent-set rule blocks. A recolored vertex ORs its new color (1..64)
+    // into its neighbors' bitmaps. Stops when the next worklist is empty (up to
+    // 64 sweeps). Returns sweeps run.
+    int tier1_worklist(std::vector<uint32_t> W, uint32_t* last_count, bool* done) {
         std::vector<uint8_t> needf(n, 0), nextf(n, 0);
         *done = false;
         uint32_t count = 0;
@@ -654,26 +652,24 @@ struct Oracle {
     // One repair of the exact-selection configuration (the library's
     // sgc_publish / sgc_repair): incremental when the last repair ended proper,
     // the rows are known mirror-complete and no full repair is due or forced;
-    // else rebuild + full independent-set sweeps (with the mirror checksum when
-    // the rows are not known mirror-complete). Tier-2 runs unless the sweeps
-    // converged on mirror-complete rows. out: [sweeps, last count, incremental,
+    // else full: the first sweep visits every vertex (and computes the mirror
+    // checksum when the rows are not known mirror-complete). Tier-2 runs unless
+    // the sweeps converged on mirror-complete rows. out: [sweeps, last count, incremental,
     // tier2 ran, proper, tier2 fixes].
     void repair_exact(bool force, uint32_t* out) {
         const bool incr = clean && !force && !asym && !(full_every && since_full + 1 >= full_every);
         uint32_t last = 0;
         int iters = 0;
         bool done = false, sym_bad = false;
-        if (incr) {
-            iters = tier1_incremental(&last, &done);
-        } else {
-            std::fill(touched.begin(), touched.end(), (uint8_t)0);
-            if (asym) {
-                sym_bad = mirror_sum() != 0;
-                if (!sym_bad) asym = false;
-            }
-            iters = tier1(nullptr, 0, &last);
-            done = last == 0;
+        std::vector<uint32_t> W;
+        for (uint32_t x = 0; x < n; x++)
+            if (!incr || touched[x]) W.push_back(x);
+        std::fill(touched.begin(), touched.end(), (uint8_t)0);
+        if (!incr && asym) {
+            sym_bad = mirror_sum() != 0;
+            if (!sym_bad) asym = false;
         }
+        iters = tier1_worklist(std::move(W), &last, &done);
         since_full = incr ? since_full + 1 : 0;
         bool proper = done && !sym_bad;
         bool t2 = false;

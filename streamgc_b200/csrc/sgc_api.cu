@@ -54,9 +54,7 @@ struct Ctl {
     unsigned long long drain_failed;
     unsigned long long symsum;
     unsigned long long live;
-    uint32_t asym;
-    uint32_t pad32;
-    unsigned long long pad[2];
+    unsigned long long pad[3];
 };
 
 }  // namespace
@@ -178,10 +176,12 @@ int sync(sgc_handle* h) {
 
 // ---- epoch building blocks ----
 
-int compact_dirty(sgc_handle* h) {
+// force: compact every edited row (epoch maintenance and phase end, as the
+// reference does); publishes under exact selection leave rows with few holes.
+int compact_dirty(sgc_handle* h, bool force) {
     CK(cudaMemsetAsync(&h->ctl->dirty_count, 0, 4, h->stream));
     launch_dirty_list(h->g, h->dirty_list, &h->ctl->dirty_count, h->stream);
-    launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, h->stream);
+    launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, force, h->stream);
     h->launches += 2;
     return check_cuda("compact");
 }
@@ -205,8 +205,8 @@ int rebuild_sweep(sgc_handle* h) {
 // The control block's `clean` flag: whether the next repair may start from the
 // touched vertices (the current colors are a proper coloring of the rows).
 int set_clean(sgc_handle* h, uint32_t v) {
-    CK(cudaMemsetAsync(&h->sb.rc->clean, 0, 4, h->stream));
-    if (v) CK(cudaMemsetAsync(&h->sb.rc->clean, 1, 1, h->stream));
+    CK(cudaMemsetAsync(&h->g.gctl->clean, 0, 4, h->stream));
+    if (v) CK(cudaMemsetAsync(&h->g.gctl->clean, 1, 1, h->stream));
     return SGC_OK;
 }
 
@@ -236,14 +236,14 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep, bool force_full) {
     RepairCtl* hin = h->h_rc_in;
     hin->mode = (uint32_t)mode;
     hin->max_sweeps = indep ? 64u : 20u;
-    hin->force_full = force_full ? 1u : 0u;
+    hin->force_all = force_full ? 1u : 0u;
     CK(cudaMemcpyAsync(h->sb.rc, hin, 12, cudaMemcpyHostToDevice, h->stream));
     const size_t mwords = ((h->n + 31) / 32) * 4;
     CK(cudaMemsetAsync(h->sb.wmark, 0, mwords, h->stream));
     CK(cudaMemsetAsync(h->sb.rbits, 0, mwords, h->stream));
     CK(cudaMemsetAsync(h->sb.needf, 0, h->n, h->stream));  // no vertex starts conflicted
-    launch_repair_begin(h->g, h->sb, h->num_sms, h->stream);
-    h->launches += h->g.touched ? 2 : 1;
+    launch_repair_begin(h->g, h->sb, mode, h->num_sms, h->stream);
+    h->launches += (mode == SWEEP_INDEP && h->g.touched) ? 2 : 1;
     const bool prof = (h->opt.flags & SGC_OPT_PROFILE) != 0;
     RepairCtl* rc = h->h_rc_out;
     for (;;) {
@@ -389,8 +389,13 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
         hw[x] = cnt;
         if (degree[x] > cfg->histogram_threshold) hdmap[x] = num_hd++;
     }
-    for (uint64_t j = 0; j < nnz; j++)
+    const bool exact_sel = (opt.flags & SGC_OPT_EXACT_SELECT) != 0;
+    for (uint64_t j = 0; j < nnz; j++) {
         if (col_idx[j] == INV) return fail(SGC_EINVAL, "col_idx holds the INVALID sentinel at %llu", (unsigned long long)j);
+        if (exact_sel && (col_idx[j] & TOMB))  // the top bit marks deleted entries under exact selection
+            return fail(SGC_EINVAL, "col_idx[%llu] >= 2^31 (exact selection)", (unsigned long long)j);
+    }
+    if (exact_sel && n >= TOMB) return fail(SGC_EINVAL, "num_vertices >= 2^31 (exact selection)");
     // rows whose base entries are not strictly ascending start "edited": the
     // binary-search fast path only serves sorted, duplicate-free rows
     std::vector<uint32_t> edited((n + 31) / 32 + 1, 0);
@@ -444,8 +449,9 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     g.ovf_lost = &h->ctl->ovf_lost;
     g.nskip = &h->ctl->nskip;
     g.err = &h->ctl->err;
-    g.asym = &h->ctl->asym;
-    if (cudaMemsetAsync(g.asym, 0x01, 4, h->stream) != cudaSuccess)  // nothing known about the mirrors yet
+    A(&g.gctl, 1, 0);
+    g.gidw = nullptr;
+    if (cudaMemsetAsync(&g.gctl->asym, 0x01, 1, h->stream) != cudaSuccess)  // nothing known about the mirrors yet
         return bail(fail(SGC_ECUDA, "control block init failed"));
     if (cudaMemcpyAsync(d_rp, rp.data(), rp.size() * 8, cudaMemcpyHostToDevice, h->stream) ||
         cudaMemcpyAsync(d_hdmap, hdmap.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) ||
@@ -487,6 +493,7 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     A(&eo.tnext, mb);
     A(&eo.tprev, mb);
     A(&eo.done, mb, 0);
+    A(&eo.succ, mb, 0);
     eo.ticket = &h->ctl->ticket;
     eo.tmask = tsize - 1;
     // sweep buffers
@@ -503,7 +510,6 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     sb.pend_count = &h->ctl->pend_count;
     A(&sb.fac_v, n);
     sb.fac_count = &h->ctl->fac_count;
-    sb.symsum = &h->ctl->symsum;
     sb.live = &h->ctl->live;
     A(&sb.wmark, (n + 31) / 32 + 1, 0);
     A(&sb.wl, n);
@@ -515,8 +521,19 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     A(&sb.rbits, (n + 31) / 32 + 1, 0);
     A(&sb.rc, 1, 0);
     sb.tile = opt.repair_tile;
+    sb.G = 1;
     if (g.exact) A(&g.touched, (n + 31) / 32 + 1, 0);
     else g.touched = nullptr;
+    if (g.exact) {  // base runs: rows whose base entries are strictly ascending
+        std::vector<uint32_t> bl(n);
+        for (uint32_t x = 0; x < n; x++) bl[x] = (edited[x >> 5] >> (x & 31)) & 1u ? 0u : hw[x];
+        A(&g.blen, n);
+        if (cudaMemcpyAsync(g.blen, bl.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess)
+            return bail(fail(SGC_ECUDA, "base run upload failed"));
+    } else {
+        g.blen = nullptr;
+    }
     if (cudaHostAlloc(&h->h_rc_in, sizeof(RepairCtl), cudaHostAllocDefault) != cudaSuccess ||
         cudaHostAlloc(&h->h_rc_out, sizeof(RepairCtl), cudaHostAllocDefault) != cudaSuccess)
         return bail(fail(SGC_ENOMEM, "pinned control block allocation failed"));
@@ -603,7 +620,7 @@ int sgc_epoch(sgc_handle* h) {
     if (!h) return fail(SGC_EINVAL, "null handle");
     CK(cudaSetDevice(h->device));
     publish_snapshot(h);
-    TRY(compact_dirty(h));
+    TRY(compact_dirty(h, true));
     TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, nullptr));
     TRY(rebuild_sweep(h));
     h->epochs++;
@@ -616,7 +633,7 @@ int sgc_drain_and_compact(sgc_handle* h, sgc_repair_report* rep) {
     CK(cudaMemcpyAsync(h->h_small + 8, &h->ctl->drain_failed, 8, cudaMemcpyDeviceToHost, h->stream));
     TRY(sync(h));
     const unsigned long long before = *(unsigned long long*)(h->h_small + 8);
-    TRY(compact_dirty(h));
+    TRY(compact_dirty(h, true));
     TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, &h->ctl->drain_failed));
     TRY(rebuild_sweep(h));
     return read_drain(h, rep, before);
@@ -629,7 +646,7 @@ int sgc_repair(sgc_handle* h, sgc_repair_report* rep) {
     CK(cudaMemcpyAsync(h->h_small + 8, &h->ctl->drain_failed, 8, cudaMemcpyDeviceToHost, h->stream));
     TRY(sync(h));
     const unsigned long long before = *(unsigned long long*)(h->h_small + 8);
-    TRY(compact_dirty(h));
+    TRY(compact_dirty(h, true));
     TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, &h->ctl->drain_failed));
     // drain_and_compact's rebuild is subsumed: the first (full) sweep rebuilds every bitmap first.
     TRY(read_drain(h, &r, before));
@@ -642,7 +659,7 @@ int sgc_publish(sgc_handle* h, sgc_repair_report* rep) {
     if (!h) return fail(SGC_EINVAL, "null handle");
     CK(cudaSetDevice(h->device));
     sgc_repair_report r{};
-    TRY(compact_dirty(h));
+    TRY(compact_dirty(h, false));
     TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, &h->ctl->drain_failed));
     TRY(repair_loop(h, &r, false));
     publish_snapshot(h);

@@ -27,12 +27,24 @@ constexpr uint32_t INV = SGC_CSR_INVALID;
 constexpr uint32_t EMPTY = SGC_HASH_EMPTY;
 constexpr uint32_t FULL = 0xFFFFFFFFu;
 constexpr uint32_t OVF_CAP = SGC_OVERFLOW_CAPACITY;
+constexpr uint32_t TOMB = 0x80000000u;  // tombstone bit of a deleted base-run entry (exact selection)
 
 // Error bits written to the handle's device error word.
 enum : uint32_t {
     ERR_WAIT_TIMEOUT = 1u << 0,   // a same-edge predecessor wait ran out
     ERR_BAD_UPDATE = 1u << 1,     // update endpoint outside [0, n)
     ERR_LIST_OVERFLOW = 1u << 2,  // a work list exceeded its capacity
+};
+
+// Repair flags of one graph of a handle.
+struct GraphCtl {
+    uint32_t clean;   // the last repair ended proper and only updates changed colors since
+    uint32_t asym;    // an entry may have lost its mirror since the rows were last found
+                      // mirror-complete (set at creation, on every overflow, on a drain
+                      // failure, and when an update found one direction only)
+    uint32_t force;   // host: the next repair visits every vertex of the graph
+    uint32_t full;    // the current repair visits every vertex of the graph
+    unsigned long long sym;  // mirror checksum of the current repair (full repairs with asym set)
 };
 
 // Device view of one graph's state (handle layout). Row x owns logical slots
@@ -61,11 +73,13 @@ struct Dev {
     unsigned long long* ovf_lost;  // overflows beyond OVF_CAP (edge dropped, as the reference does)
     unsigned long long* nskip;     // updates skipped: an endpoint outside [0, n) (hash miss)
     uint32_t* err;
+    uint32_t* blen;                // exact selection: per row, length of the base run [rp, rp+blen):
+                                   // ids strictly ascending, deleted ones kept as id | TOMB (null otherwise)
     uint32_t* touched;             // exact selection: bitmask of update endpoints since the last repair
                                    // (null otherwise)
-    uint32_t* asym;                // nonzero: an entry may have lost its mirror since rows were last
-                                   // found mirror-complete (set at creation, on every overflow, on a
-                                   // drain failure, and when an update found one direction only)
+    GraphCtl* gctl;                // per graph: repair flags (one entry for a single-graph handle)
+    const uint32_t* gidw;          // graph of each 32-vertex word (graphs start at multiples of 32);
+                                   // null: one graph
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -195,8 +209,10 @@ __device__ __forceinline__ void mark_dirty(const Dev& g, uint32_t x) {
     atomicOr(g.dirty + (x >> 5), 1u << (x & 31));
     if (!(ld_cg(g.edited + (x >> 5)) & (1u << (x & 31)))) atomicOr(g.edited + (x >> 5), 1u << (x & 31));
 }
-__device__ __forceinline__ void flag_asym(const Dev& g) {
-    if (!ld_cg(g.asym)) atomicOr(g.asym, 1u);
+__device__ __forceinline__ uint32_t graph_of(const Dev& g, uint32_t x) { return g.gidw ? __ldg(g.gidw + (x >> 5)) : 0u; }
+__device__ __forceinline__ void flag_asym(const Dev& g, uint32_t x) {
+    uint32_t* a = &g.gctl[graph_of(g, x)].asym;
+    if (!ld_cg(a)) atomicOr(a, 1u);
 }
 __device__ __forceinline__ bool pristine(const Dev& g, uint32_t x) {
     return !(ld_cg(g.edited + (x >> 5)) & (1u << (x & 31)));
@@ -224,9 +240,74 @@ __device__ __forceinline__ uint64_t warp_bsearch(const uint32_t* col, uint64_t s
     return b ? lo + (__ffs(b) - 1) : ~0ull;
 }
 
+// 32-ary search by id in a base run (ascending ids, tombstones keep their id
+// under TOMB). Returns the slot index, or ~0 when the id is absent; `val` gets
+// the slot's value (the id, or id | TOMB).
+__device__ __forceinline__ uint64_t warp_bsearch_key(const uint32_t* col, uint64_t s, uint64_t e, uint32_t key,
+                                                     uint32_t& val) {
+    const uint32_t lane = lane_id();
+    uint64_t lo = s, hi = e;
+    while (hi - lo > 32) {
+        const uint64_t step = (hi - lo) / 32;
+        const uint32_t v = ld_cg(col + lo + lane * step) & ~TOMB;
+        const uint32_t b = __ballot_sync(FULL, v <= key);
+        if (!b) return ~0ull;
+        const uint32_t L = 31 - __clz(b);
+        const uint64_t nlo = lo + L * step;
+        hi = (L == 31) ? hi : nlo + step;
+        lo = nlo;
+    }
+    const uint64_t i = lo + lane;
+    const uint32_t v = i < hi ? ld_cg(col + i) : INV;
+    const uint32_t b = __ballot_sync(FULL, i < hi && (v & ~TOMB) == key);
+    if (!b) return ~0ull;
+    val = __shfl_sync(FULL, v, __ffs(b) - 1);
+    return lo + (__ffs(b) - 1);
+}
+
 // ---------------- slack-CSR row edits (local_update.cu:12-56) ----------------
 
 enum { ADD_INSERTED = 0, ADD_PRESENT = 1, ADD_OVERFLOW = 2 };
+
+// Concurrent batches under exact selection: rows keep their base run sorted
+// (a delete there leaves a tombstone, a re-insert of the same id revives it),
+// so an update finds a base entry by a 32-ary search; only entries inserted
+// since the row's last compaction (its tail) are scanned. The updates of one
+// edge are ordered, so no other warp touches the slot of `nbr` meanwhile.
+// Add: returns ADD_PRESENT / ADD_INSERTED when the run holds nbr (live or
+// tombstone), -1 when it does not.
+__device__ __forceinline__ int warp_run_add(const Dev& g, uint32_t x, uint32_t nbr, uint64_t s, uint32_t bl) {
+    uint32_t val = 0;
+    const uint64_t p = warp_bsearch_key(g.col, s, s + bl, nbr, val);
+    if (p == ~0ull) return -1;
+    if (val == nbr) return ADD_PRESENT;
+    uint32_t old = 0;
+    if (lane_id() == 0) {
+        old = atomicCAS(g.col + p, nbr | TOMB, nbr);
+        if (old == (nbr | TOMB)) {
+            atomicSub(g.holes + x, 1u);
+            mark_dirty(g, x);
+        }
+    }
+    old = __shfl_sync(FULL, old, 0);
+    return old == nbr ? ADD_PRESENT : ADD_INSERTED;
+}
+// Delete: true when the run held nbr live (now a tombstone).
+__device__ __forceinline__ bool warp_run_remove(const Dev& g, uint32_t x, uint32_t nbr, uint64_t s, uint32_t bl) {
+    uint32_t val = 0;
+    const uint64_t p = warp_bsearch_key(g.col, s, s + bl, nbr, val);
+    if (p == ~0ull || val != nbr) return false;
+    uint32_t old = 0;
+    if (lane_id() == 0) {
+        old = atomicCAS(g.col + p, nbr, nbr | TOMB);
+        if (old == nbr) {
+            atomicAdd(g.holes + x, 1u);
+            mark_dirty(g, x);
+        }
+    }
+    old = __shfl_sync(FULL, old, 0);
+    return old == nbr;
+}
 
 // add_local_neighbor: claim the first INV slot unless `nbr` shows up first;
 // a full row appends to the overflow buffer (counter always advances, entry
@@ -234,7 +315,14 @@ enum { ADD_INSERTED = 0, ADD_PRESENT = 1, ADD_OVERFLOW = 2 };
 __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t nbr, bool exact) {
     const uint64_t s = g.rp[x], e = g.rp[x + 1];
     uint64_t from = s;
-    if (pristine(g, x)) {
+    if (!exact && g.blen) {
+        const uint32_t bl = ld_cg(g.blen + x);
+        if (bl) {
+            const int r = warp_run_add(g, x, nbr, s, bl);
+            if (r >= 0) return r;
+        }
+        from = s + bl;  // the tail: first INV or nbr
+    } else if (pristine(g, x)) {
         // Sorted base entries, no holes: the scan would stop at nbr if present,
         // else at the first INV right after the base run.
         const uint64_t len = ld_cg(g.hw + x);
@@ -258,7 +346,7 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
                 } else {
                     atomicAdd(g.ovf_lost, 1ull);
                 }
-                flag_asym(g);
+                flag_asym(g, x);
             }
             __syncwarp();
             return ADD_OVERFLOW;
@@ -286,7 +374,11 @@ __device__ __forceinline__ bool warp_remove_slot(const Dev& g, uint32_t x, uint3
     const uint64_t s = g.rp[x];
     const uint64_t e = s + ld_cg(g.hw + x);
     uint64_t from = s;
-    if (pristine(g, x)) {
+    if (!exact && g.blen) {
+        const uint32_t bl = ld_cg(g.blen + x);
+        if (bl && warp_run_remove(g, x, nbr, s, bl)) return true;
+        from = s + bl;  // not live in the run: the tail
+    } else if (pristine(g, x)) {
         const uint64_t p = warp_bsearch(g.col, s, e, nbr);
         if (p != ~0ull) {
             uint32_t old = 0;
@@ -295,6 +387,7 @@ __device__ __forceinline__ bool warp_remove_slot(const Dev& g, uint32_t x, uint3
                 if (old == nbr) {
                     mark_dirty(g, x);
                     if (g.holes) atomicAdd(g.holes + x, 1u);
+                    if (g.blen) g.blen[x] = 0;  // an INV inside the run ends it
                 }
             }
             old = __shfl_sync(FULL, old, 0);
@@ -313,6 +406,7 @@ __device__ __forceinline__ bool warp_remove_slot(const Dev& g, uint32_t x, uint3
             if (old == nbr) {
                 mark_dirty(g, x);
                 if (g.holes) atomicAdd(g.holes + x, 1u);
+                if (g.blen && p < s + ld_cg(g.blen + x)) g.blen[x] = 0;  // an INV inside the run ends it
             }
         }
         old = __shfl_sync(FULL, old, 0);
@@ -546,7 +640,7 @@ __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v,
     if (type == SGC_UPDATE_ADD) {
         const int ru = warp_add_slot(g, u, v, exact);
         const int rv = warp_add_slot(g, v, u, exact);
-        if (ru != rv && lane_id() == 0) flag_asym(g);
+        if (ru != rv && lane_id() == 0) flag_asym(g, u);
         warp_color_if_uncolored(g, u);
         if (color_of(warp_load_state(g, v)) == 0) {
             if (lane_id() == 0) new_nbr(g, v, color_of(ld_cg(g.st + u)));
@@ -570,7 +664,7 @@ __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v,
         const bool du = warp_remove_slot(g, u, v, exact);
         const bool dv = warp_remove_slot(g, v, u, exact);
         if (lane_id() == 0) {
-            if (du != dv) flag_asym(g);
+            if (du != dv) flag_asym(g, u);
             removed_nbr(g, u, fu);
             removed_nbr(g, v, fv);
         }

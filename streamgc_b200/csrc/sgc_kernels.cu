@@ -97,6 +97,7 @@ __global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint
         eo.tslot[i] = NONE32;
         return;
     }
+    eo.succ[i] = 0;
     const unsigned long long key = edge_key(u, v);
     uint32_t h = key_hash(key) & eo.tmask;
     for (uint32_t probe = 0; probe <= eo.tmask; probe++) {
@@ -118,6 +119,7 @@ __global__ void conc_prep_prev(uint32_t n, EdgeOrder eo) {
             if (j < i && (best == NONE32 || j > best)) best = j;
     }
     eo.tprev[i] = best;
+    if (best != NONE32) eo.succ[best] = 1;  // best's done mark is awaited
 }
 
 // Bounded wait for the same-edge predecessor: ~2^22 polls with a sleep, then
@@ -137,13 +139,18 @@ __device__ __forceinline__ void wait_done(const EdgeOrder& eo, const Dev& g, uin
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(256) conc_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n,
+// Tickets are taken one update ahead, so the ticket's round trip overlaps the
+// current update. A warp's tickets rise, and a predecessor always has a lower
+// index than its successor, so no chain of waits closes on itself. Only an
+// update that a later one of the same edge waits for publishes its done mark.
+__global__ void __launch_bounds__(256, 4) conc_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n,
                                                          EdgeOrder eo, uint32_t seq) {
-    for (;;) {
-        uint32_t i = 0;
-        if (lane_id() == 0) i = atomicAdd(eo.ticket, 1u);
-        i = __shfl_sync(FULL, i, 0);
-        if (i >= n) break;
+    uint32_t i = 0;
+    if (lane_id() == 0) i = atomicAdd(eo.ticket, 1u);
+    i = __shfl_sync(FULL, i, 0);
+    while (i < n) {
+        uint32_t inext = 0;
+        if (lane_id() == 0) inext = atomicAdd(eo.ticket, 1u);
         const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
         const uint32_t u = r.x, v = r.y;
         const uint8_t type = (uint8_t)(r.z & 0xFFu);
@@ -159,12 +166,14 @@ __global__ void __launch_bounds__(256) conc_apply_kernel(Dev g, const EdgeUpdate
             if (h != NONE32) {  // no kernel reads the table during apply: reset it for the next batch
                 eo.tkey[h] = EMPTY64;
                 eo.thead[h] = NONE32;
+                if (eo.succ[i]) {
+                    __threadfence();
+                    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> d(eo.done[i]);
+                    d.store(seq, cuda::memory_order_release);
+                }
             }
-            __threadfence();
-            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> d(eo.done[i]);
-            d.store(seq, cuda::memory_order_release);
         }
-        __syncwarp();
+        i = __shfl_sync(FULL, inext, 0);
     }
 }
 
@@ -221,8 +230,10 @@ void launch_dirty_list(const Dev& g, uint32_t* list, uint32_t* count, cudaStream
 
 // Warp per edited row: stable in-place compaction of [rp, rp + hw), INV tail,
 // hw = live count.
+// Under exact selection a tombstone (id | TOMB) is a hole too, and the live
+// entries of the base run, which stay in front and in order, form the new run.
 __global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __restrict__ list,
-                                                      const uint32_t* __restrict__ count) {
+                                                      const uint32_t* __restrict__ count, int force) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
     const uint32_t cnt = *count;
@@ -231,19 +242,29 @@ __global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __r
         const uint64_t s = g.rp[x];
         const uint32_t hwx = g.hw[x];
         // Lazy mode: a row whose holes fill at most a quarter of its extent stays
-        // as it is (every reader skips INV slots); it is compacted later.
-        if (g.holes && 4u * g.holes[x] <= hwx) continue;
+        // as it is (every reader skips INV slots and tombstones); it is compacted later.
+        if (!force && g.holes && 4u * g.holes[x] <= hwx) {
+            if (g.holes[x] && lane == 0) atomicOr(g.dirty + (x >> 5), 1u << (x & 31));  // still a candidate
+            continue;
+        }
         const uint64_t e = s + hwx;
-        uint64_t w = s;
+        const uint64_t run_end = s + (g.blen ? g.blen[x] : 0u);
+        uint64_t w = s, run_live = 0;
         for (uint64_t c = s & ~3ull; c < e; c += 128) {
             const uint64_t i = c + 4ull * lane;
             uint4 q = make_uint4(INV, INV, INV, INV);
             if (i < e) q = ld_cg4(g.col + i);
             uint32_t vals[4] = {q.x, q.y, q.z, q.w};
-            uint32_t m = 0;
+            uint32_t m = 0, mr = 0;
 #pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (i + j >= s && i + j < e && vals[j] != INV) m |= 1u << j;
+            for (int j = 0; j < 4; j++) {
+                const bool live = g.blen ? (vals[j] & TOMB) == 0 : vals[j] != INV;
+                if (i + j >= s && i + j < e && live) {
+                    m |= 1u << j;
+                    if (i + j < run_end) mr |= 1u << j;
+                }
+            }
+            run_live += __reduce_add_sync(FULL, (uint32_t)__popc(mr));
             uint32_t total = 0;
             const uint32_t pre = warp_excl_scan(__popc(m), total);
             __syncwarp();
@@ -261,16 +282,18 @@ __global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __r
         if (lane == 0) {
             g.hw[x] = (uint32_t)(w - s);
             if (g.holes) g.holes[x] = 0;
+            if (g.blen) g.blen[x] = (uint32_t)run_live;
         }
         __syncwarp();
     }
 }
 
-void launch_compact(const Dev& g, const uint32_t* list, const uint32_t* count, uint32_t max_rows, cudaStream_t s) {
+void launch_compact(const Dev& g, const uint32_t* list, const uint32_t* count, uint32_t max_rows, bool force,
+                    cudaStream_t s) {
     if (!max_rows) return;
     uint32_t blocks = (max_rows + 7) / 8;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    compact_kernel<<<blocks, 256, 0, s>>>(g, list, count);
+    compact_kernel<<<blocks, 256, 0, s>>>(g, list, count, force ? 1 : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -287,9 +310,15 @@ void launch_take_overflow(const Dev& g, uint32_t* drain_n, cudaStream_t s) {
 }
 
 // Re-insert without re-appending: first INV or equal slot; none -> failure.
-__device__ __forceinline__ bool warp_drain_insert(const Dev& g, uint32_t x, uint32_t nbr) {
+// Unordered drains under exact selection look in the sorted base run first.
+__device__ __forceinline__ bool warp_drain_insert(const Dev& g, uint32_t x, uint32_t nbr, bool ordered) {
     const uint64_t s = g.rp[x], e = g.rp[x + 1];
     uint64_t from = s;
+    if (!ordered && g.blen) {
+        const uint32_t bl = ld_cg(g.blen + x);
+        if (bl && warp_run_add(g, x, nbr, s, bl) >= 0) return true;
+        from = s + bl;
+    }
     for (;;) {
         uint64_t p = 0;
         uint32_t v = 0;
@@ -318,10 +347,10 @@ __global__ void drain_kernel(Dev g, const uint32_t* __restrict__ drain_n, int or
     if (ordered && w0 != 0) return;
     for (uint32_t k = w0; k < cnt; k += step) {
         const OverflowEdge oe = g.ovf[k];
-        const bool ok = warp_drain_insert(g, oe.local_vertex_idx, oe.neighbor_global);
+        const bool ok = warp_drain_insert(g, oe.local_vertex_idx, oe.neighbor_global, ordered != 0);
         if (!ok && lane_id() == 0) {
             if (failed) atomicAdd(failed, 1ull);
-            flag_asym(g);
+            flag_asym(g, oe.local_vertex_idx);
         }
     }
 }
@@ -428,9 +457,9 @@ __device__ __forceinline__ void item_bounds(const Dev& g, const SweepBufs& b, un
 // Warp per item: up to b.tile live slots of one row. Nothing in the graph
 // changes during a sweep, so loads take the read-only path. Each lane keeps two
 // 16-byte slot loads and their eight state gathers in flight per round.
-// SYM: also accumulate the mirror checksum. PUSH (incremental repairs): a
-// same-colored neighbor that loses to x (lower priority) is marked for the
-// next sweep, which decides it from its own row.
+// SYM: accumulate the mirror checksum of rows whose graph wants it. PUSH
+// (independent-set rule): a same-colored neighbor that loses to x (lower
+// priority) is marked for the next sweep, which decides it from its own row.
 template <bool SYM, bool PUSH>
 __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& b) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -440,6 +469,8 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
         uint32_t x;
         uint64_t s, e;
         item_bounds(g, b, b.items[k], x, s, e);
+        GraphCtl* gc = SYM ? &g.gctl[graph_of(g, x)] : nullptr;
+        const bool symx = SYM && gc->full && ld_cg(&gc->asym);
         const uint32_t myc = color_of(__ldg(g.st + x));
         const uint32_t mydeg = __ldg(g.deg + x);
         uint32_t lo = 0, hi = 0;
@@ -470,7 +501,7 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
                         conf = prio_less(mydeg, x, __ldg(g.deg + v[t]), v[t]);
                     }
                 }
-                if (SYM && v[t] != INV && v[t] != x) sym += sym_term(x, v[t]);
+                if (SYM && symx && v[t] != INV && v[t] != x) sym += sym_term(x, v[t]);
             }
         }
         lo = __reduce_or_sync(FULL, lo);
@@ -482,26 +513,27 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
             const unsigned long long m = ((unsigned long long)hi << 32) | lo;
             if (m) atomicOr(b.acc_bm + x, m);
             if (anyc) atomicOr(b.acc_fl + x, 1u);
-            if (SYM && sym) atomicAdd(b.symsum, sym);
+            if (SYM && sym) atomicAdd(&gc->sym, sym);
         }
     }
 }
 
-// sym_mode 0: no checksum; 1: checksum when *g.asym is set; 2: as 1, and only
-// in the first sweep of the repair (RepairCtl).
-__device__ __forceinline__ bool want_sym(const Dev& g, const SweepBufs& b, int sym_mode) {
-    if (sym_mode == 0 || !ld_cg(g.asym)) return false;  // mirror-complete rows: the checksum is known to be 0
-    return sym_mode == 1 || ld_cg(&b.rc->it) == 0;
-}
-__device__ __forceinline__ bool want_push(const SweepBufs& b, int mode) {
-    return mode == SWEEP_INDEP && ld_cg(&b.rc->incr) != 0;
+// sym_mode 0: no checksum; 2: the first sweep of a repair accumulates it for
+// the graphs of this repair that visit every vertex with asym set (RepairCtl).
+__device__ __forceinline__ bool want_sym(const SweepBufs& b, int sym_mode) {
+    return sym_mode == 2 && ld_cg(&b.rc->it) == 0 && ld_cg(&b.rc->any_sym) != 0;
 }
 
 __global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b, int mode, int sym_mode) {
-    const bool sym = want_sym(g, b, sym_mode);
-    if (want_push(b, mode)) sweep_items_body<false, true>(g, b);  // incremental: rows are mirror-complete
-    else if (sym) sweep_items_body<true, false>(g, b);
-    else sweep_items_body<false, false>(g, b);
+    const bool sym = want_sym(b, sym_mode);
+    const bool push = mode == SWEEP_INDEP;
+    if (push) {
+        if (sym) sweep_items_body<true, true>(g, b);
+        else sweep_items_body<false, true>(g, b);
+    } else {
+        if (sym) sweep_items_body<true, false>(g, b);
+        else sweep_items_body<false, false>(g, b);
+    }
 }
 
 // One vertex of the finalize pass (warp-collective: every lane calls it; `valid`
@@ -513,6 +545,10 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
     uint32_t pend_word = 0;
     unsigned long long sym = 0, live = 0;
     if (valid) {
+        if (with_sym) {
+            const GraphCtl& gc = g.gctl[graph_of(g, x)];
+            with_sym = gc.full && ld_cg(&gc.asym);
+        }
         const uint32_t len = g.hw[x];
         const uint32_t hd = __ldg(g.hdmap + x);
         const uint32_t w = __ldg(g.st + x);
@@ -575,13 +611,10 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
             }
         }
     }
-    for (int off = 16; off > 0; off >>= 1) {
-        sym += __shfl_xor_sync(FULL, sym, off);
-        live += __shfl_xor_sync(FULL, live, off);
-    }
+    for (int off = 16; off > 0; off >>= 1) live += __shfl_xor_sync(FULL, live, off);
+    if (sym) atomicAdd(&g.gctl[graph_of(g, x)].sym, sym);  // per lane: the lanes' rows may sit in different graphs
     const unsigned long long nv = __popc(__ballot_sync(FULL, valid));
     if (lane_id() == 0) {
-        if (sym) atomicAdd(b.symsum, sym);
         if (live) {
             atomicAdd(b.live, live);
             atomicAdd(b.swept, live);
@@ -609,8 +642,8 @@ __global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b,
     const bool list = use_list(b, list_mode);
     const uint32_t lim = list ? *b.wl_count : g.n;
     const uint32_t stride = gridDim.x * blockDim.x;
-    const bool sym = want_sym(g, b, sym_mode);
-    const bool push = want_push(b, mode);
+    const bool sym = want_sym(b, sym_mode);
+    const bool push = mode == SWEEP_INDEP;
     for (uint32_t base = blockIdx.x * blockDim.x; base < lim; base += stride) {  // warp-uniform trip count
         const uint32_t t = base + threadIdx.x;
         const bool valid = t < lim;
@@ -706,11 +739,10 @@ __global__ void __launch_bounds__(256) indep_items_kernel(Dev g, SweepBufs b) {
 // from the sweep's 64-bit mask, else from the gathered 65..2047 set
 // (histogram-class rows), else through the warp scan of sweep_fac_kernel
 // (bitmap rows whose 64 low colors are all taken). Blocked vertices are marked
-// for the next sweep (a full repair marks every conflicted vertex).
+// for the next sweep.
 __global__ void __launch_bounds__(256) indep_decide_kernel(Dev g, SweepBufs b) {
     const uint32_t cnt = *b.need_count;
     const uint32_t salt = sweep_salt(ld_cg(&b.rc->it));
-    const bool incr = ld_cg(&b.rc->incr) != 0;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
         const uint32_t x = b.need_v[t];
         const uint32_t len = g.hw[x];
@@ -726,7 +758,7 @@ __global__ void __launch_bounds__(256) indep_decide_kernel(Dev g, SweepBufs b) {
             blocked = true;
             b.acc_fl[x] = 0;
         }
-        if (blocked || !incr) atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
+        if (blocked) atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
         const unsigned long long mask = b.acc_bm[x];
         if (mask) b.acc_bm[x] = 0;
         const uint32_t hd = __ldg(g.hdmap + x);
@@ -757,14 +789,14 @@ __global__ void __launch_bounds__(256) indep_decide_kernel(Dev g, SweepBufs b) {
 }
 
 // Writes the chosen colors and clears the recolored vertices' conflict flags.
-// A full repair marks each recolored vertex and, for rows of at most
+// Reference rule (TIER1): marks each recolored vertex and, for rows of at most
 // SWEEP_TINY slots, its neighbors for the next worklist (longer rows: per item
-// in mark_items_kernel). An incremental repair instead ORs the new color into
-// the neighbors' bitmaps (the next sweep needs no neighbor of a recolored
-// vertex: under the independent-set rule a recolor creates no conflict).
-__global__ void sweep_commit_kernel(Dev g, SweepBufs b) {
+// in mark_items_kernel). Independent-set rule: ORs the new color into the
+// neighbors' bitmaps instead (the next sweep needs no neighbor of a recolored
+// vertex: under that rule a recolor creates no conflict).
+__global__ void sweep_commit_kernel(Dev g, SweepBufs b, int mode) {
     const uint32_t cnt = *b.pend_count;
-    const bool incr = ld_cg(&b.rc->incr) != 0;
+    const bool incr = mode == SWEEP_INDEP;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
         const uint32_t x = b.pend_v[k];
         const uint32_t nw = b.pend_w[k];
@@ -787,13 +819,13 @@ __global__ void sweep_commit_kernel(Dev g, SweepBufs b) {
 }
 
 // Warp per item of the last sweep whose row was recolored: marks the
-// neighbors in the item's slots (full repair) or ORs the row's new color into
-// their bitmaps (incremental repair).
+// neighbors in the item's slots (reference rule) or ORs the row's new color
+// into their bitmaps (independent-set rule).
 __global__ void __launch_bounds__(256) mark_items_kernel(Dev g, SweepBufs b) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
     const uint32_t cnt = *b.item_count;
-    const bool incr = ld_cg(&b.rc->incr) != 0;
+    const bool incr = ld_cg(&b.rc->mode) == SWEEP_INDEP;
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
         const unsigned long long it = b.items[k];
         const uint32_t x0 = (uint32_t)it;
@@ -864,81 +896,149 @@ void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int list_mod
     }
     if (mode != SWEEP_REBUILD) {
         sweep_fac_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
-        sweep_commit_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
+        sweep_commit_kernel<<<num_sms * 2, 256, 0, s>>>(g, b, (int)mode);
     }
 }
 
-// Starts a repair: chooses incremental (rows mirror-complete, the last repair
-// ended proper, not forced full, exact selection) or full, and resets the
-// loop state and accumulators.
+// Starts a repair. Reference rule (TIER1, one graph): the first sweep visits
+// every vertex. Independent-set rule: per graph, the first worklist is every
+// vertex of the graph when it must be repaired in full (its last repair did
+// not end proper, its rows may miss mirror entries, or the host forces it),
+// else the vertices its updates touched since the last repair: every new
+// conflict then has a touched endpoint. One block.
 __global__ void repair_begin_kernel(Dev g, SweepBufs b) {
     RepairCtl& rc = *b.rc;
-    const bool incr = rc.mode == SWEEP_INDEP && rc.clean && !rc.force_full && !ld_cg(g.asym) && g.touched;
-    rc.incr = incr ? 1u : 0u;
-    rc.list = rc.incr;
-    rc.it = 0;
-    rc.cont = 1;
-    rc.done = 0;
-    rc.need = 0;
-    rc.next = 0;
-    rc.prev = 0xFFFFFFFFu;
-    rc.plateau = 0;
-    rc.sym = 0;
-    rc.live = 0;
-    *b.symsum = 0;
-    *b.live = 0;
-    *b.wl_count = 0;
-    b.swept[0] = 0;
-    b.swept[1] = 0;
+    const bool indep = rc.mode == SWEEP_INDEP;
+    uint32_t any_sym = 0, any_incr = 0;
+    for (uint32_t k = threadIdx.x; k < b.G; k += blockDim.x) {
+        GraphCtl& c = g.gctl[k];
+        const bool full = !indep || !c.clean || c.asym || c.force || rc.force_all || !g.touched;
+        c.full = full ? 1u : 0u;
+        c.force = 0;
+        c.sym = 0;
+        if (full && c.asym) any_sym = 1;
+        if (!full) any_incr = 1;
+    }
+    any_sym = __syncthreads_or(any_sym);
+    any_incr = __syncthreads_or(any_incr);
+    if (threadIdx.x == 0) {
+        rc.any_sym = any_sym;
+        rc.incr = any_incr;
+        rc.list = indep ? 1u : 0u;
+        rc.it = 0;
+        rc.cont = 1;
+        rc.done = 0;
+        rc.need = 0;
+        rc.next = 0;
+        rc.prev = 0xFFFFFFFFu;
+        rc.plateau = 0;
+        rc.sym = 0;
+        rc.live = 0;
+        *b.live = 0;
+        *b.wl_count = 0;
+        b.swept[0] = 0;
+        b.swept[1] = 0;
+    }
+}
+
+// First worklist of an independent-set repair: every vertex of the graphs
+// repaired in full, the touched vertices of the others; clears the touched
+// marks. Thread per 32-vertex word.
+__global__ void seed_worklist_kernel(Dev g, SweepBufs b) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nw = (g.n + 31) / 32;
+    uint32_t bits = 0;
+    if (w < nw) {
+        const uint32_t t = g.touched[w];
+        if (t) g.touched[w] = 0;
+        if (g.gctl[g.gidw ? g.gidw[w] : 0u].full) {
+            const uint32_t left = g.n - w * 32;
+            bits = left >= 32 ? FULL : (1u << left) - 1u;
+        } else {
+            bits = t;
+        }
+    }
+    uint32_t total = 0;
+    const uint32_t off = warp_excl_scan(__popc(bits), total);
+    uint32_t base = 0;
+    if (lane_id() == 0 && total) base = atomicAdd(b.wl_count, total);
+    base = __shfl_sync(FULL, base, 0);
+    uint32_t k = base + off;
+    while (bits) {
+        const int i = __ffs(bits) - 1;
+        bits &= bits - 1;
+        b.wl[k++] = w * 32 + i;
+    }
 }
 
 // After each sweep: reads the counts, decides whether another sweep runs,
 // advances the index. Reference rule (TIER1): stop at 0 conflicts, after 3
-// equal counts, or at max_sweeps (streamgc.cu:1317-1393). Independent-set
-// rule: stop when nothing is conflicted (full) or the next worklist is empty
-// (incremental). Later sweeps of a full repair visit the worklist only when
-// the first sweep found the rows mirror-complete. `cond` (graph mode): the
-// while-node's handle receives the decision.
+// equal counts, or at max_sweeps (streamgc.cu:1317-1393); later sweeps visit
+// the worklist only when the first found the rows mirror-complete.
+// Independent-set rule: stop when the next worklist is empty. After the first
+// sweep a graph whose checksum came out 0 is known mirror-complete; when the
+// loop ends every graph records whether it ended proper. `cond` (graph mode):
+// the while-node's handle receives the decision. One block.
 __global__ void repair_step_kernel(Dev g, SweepBufs b, cudaGraphConditionalHandle cond, int has_cond) {
     RepairCtl& rc = *b.rc;
-    const uint32_t count = rc.mode == SWEEP_INDEP ? *b.need_count : *b.pend_count;
-    const uint32_t next = *b.wl_count;
+    __shared__ uint32_t s_stop;
+    const bool indep = rc.mode == SWEEP_INDEP;
+    uint32_t sym_any = 0;
     if (rc.it == 0) {
-        rc.sym = *b.symsum;
-        rc.live = *b.live;
-        if (rc.sym == 0 && *g.asym) *g.asym = 0;  // found mirror-complete
-    }
-    rc.need = count;
-    rc.next = next;
-    bool done;
-    bool stop;
-    if (rc.mode == SWEEP_INDEP) {
-        done = rc.incr ? next == 0 : count == 0;
-        stop = done;
-    } else {
-        done = count == 0;
-        stop = done;
-        if (!done) {
-            if (count == rc.prev) stop = ++rc.plateau >= 3;
-            else rc.plateau = 0;
+        for (uint32_t k = threadIdx.x; k < b.G; k += blockDim.x) {
+            GraphCtl& c = g.gctl[k];
+            if (c.full && c.asym) {
+                if (c.sym == 0) c.asym = 0;  // found mirror-complete
+                else sym_any = 1;
+            }
         }
-        rc.prev = count;
     }
-    rc.done = done ? 1u : 0u;
-    rc.list = (rc.incr || rc.sym == 0) ? 1u : 0u;
-    rc.it += 1;
-    rc.cont = (!stop && rc.it < rc.max_sweeps) ? 1u : 0u;
-    if (!rc.cont) rc.clean = (done && rc.sym == 0) ? 1u : 0u;
-    if (has_cond) cudaGraphSetConditional(cond, rc.cont);
+    sym_any = __syncthreads_or(sym_any);
+    if (threadIdx.x == 0) {
+        const uint32_t count = indep ? *b.need_count : *b.pend_count;
+        const uint32_t next = *b.wl_count;
+        if (rc.it == 0) {
+            rc.sym = sym_any ? (g.gctl[0].sym ? g.gctl[0].sym : 1ull) : 0ull;
+            rc.live = *b.live;
+        }
+        rc.need = count;
+        rc.next = next;
+        bool done, stop;
+        if (indep) {
+            done = next == 0;
+            stop = done;
+        } else {
+            done = count == 0;
+            stop = done;
+            if (!done) {
+                if (count == rc.prev) stop = ++rc.plateau >= 3;
+                else rc.plateau = 0;
+            }
+            rc.prev = count;
+        }
+        rc.done = done ? 1u : 0u;
+        rc.list = (indep || rc.sym == 0) ? 1u : 0u;
+        rc.it += 1;
+        rc.cont = (!stop && rc.it < rc.max_sweeps) ? 1u : 0u;
+        s_stop = rc.cont ? 0u : 1u;
+        if (has_cond) cudaGraphSetConditional(cond, rc.cont);
+    }
+    __syncthreads();
+    if (s_stop) {
+        const bool done = rc.done != 0;
+        for (uint32_t k = threadIdx.x; k < b.G; k += blockDim.x) {
+            GraphCtl& c = g.gctl[k];
+            c.clean = (done && c.sym == 0) ? 1u : 0u;
+        }
+    }
 }
 
-void launch_repair_begin(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s) {
-    repair_begin_kernel<<<1, 1, 0, s>>>(g, b);
-    // first worklist: the vertices touched since the last repair (incremental);
-    // a full repair only clears their marks
-    const uint32_t nw = (g.n + 31) / 32;
-    if (g.touched)
-        collect_bits_kernel<<<(nw + 255) / 256, 256, 0, s>>>(g.n, g.touched, nullptr, b.wl, b.wl_count, &b.rc->incr);
+void launch_repair_begin(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s) {
+    repair_begin_kernel<<<1, 256, 0, s>>>(g, b);
+    if (mode == SWEEP_INDEP && g.touched) {
+        const uint32_t nw = (g.n + 31) / 32;
+        seed_worklist_kernel<<<(nw + 255) / 256, 256, 0, s>>>(g, b);
+    }
     (void)num_sms;
 }
 
@@ -950,7 +1050,7 @@ void launch_repair_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int n
 void launch_repair_step(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s,
                         const cudaGraphConditionalHandle* cond) {
     launch_next_worklist(g, b, num_sms, s);
-    repair_step_kernel<<<1, 1, 0, s>>>(g, b, cond ? *cond : (cudaGraphConditionalHandle)0, cond ? 1 : 0);
+    repair_step_kernel<<<1, 256, 0, s>>>(g, b, cond ? *cond : (cudaGraphConditionalHandle)0, cond ? 1 : 0);
 }
 
 }  // namespace sgc

@@ -18,10 +18,9 @@ constexpr unsigned long long EMPTY64 = 0xFFFFFFFFFFFFFFFFull;
 struct RepairCtl {
     uint32_t mode;         // host: SWEEP_TIER1 or SWEEP_INDEP
     uint32_t max_sweeps;   // host
-    uint32_t force_full;   // host: 1 = visit every vertex in the first sweep
-    uint32_t clean;        // 1: the last repair ended proper and only updates changed colors since
-                           // (the host clears it when it writes states)
-    uint32_t incr;         // this repair starts from the touched vertices
+    uint32_t force_all;    // host: 1 = every graph is repaired in full
+    uint32_t any_sym;      // some graph computes its mirror checksum in the first sweep
+    uint32_t incr;         // some graph starts from its touched vertices only
     uint32_t list;         // the current sweep visits b.wl (else every vertex)
     uint32_t it;           // index of the current sweep
     uint32_t cont;         // another sweep runs
@@ -30,8 +29,8 @@ struct RepairCtl {
     uint32_t next;         // size of the next worklist
     uint32_t prev;         // reference rule: last count
     uint32_t plateau;      // reference rule: equal counts in a row
-    uint32_t pad;
-    unsigned long long sym;   // first sweep's mirror checksum
+    uint32_t pad[3];
+    unsigned long long sym;   // nonzero: some graph's first-sweep checksum was not 0
     unsigned long long live;  // first sweep's live entries
 };
 
@@ -42,6 +41,7 @@ struct SweepBufs {
     uint32_t* item_count;
     uint32_t item_cap;
     uint32_t tile;               // slots per item (repair tile width, >= SWEEP_CH_MIN)
+    uint32_t G;                  // graphs of the handle (entries of g.gctl)
     RepairCtl* rc;
     unsigned long long* acc_bm;  // OR of neighbor colors 1..64, per vertex
     uint32_t* acc_fl;            // bit0: a same-colored neighbor has higher priority
@@ -50,7 +50,6 @@ struct SweepBufs {
     uint32_t* pend_count;
     uint32_t* fac_v;             // vertices whose new color needs a warp (histogram or >64 scan)
     uint32_t* fac_count;
-    unsigned long long* symsum;  // sum over entries x->y (y != x, y < n) of H(x,y) - H(y,x)
     unsigned long long* live;    // live entries seen by the sweep
     // worklist of the next sweep: vertices recolored by the last one and their neighbors
     uint32_t* wmark;             // bitmask
@@ -87,7 +86,8 @@ struct EdgeOrder {
     uint32_t* tslot;           // per update: its key slot (NONE32 = not an edge op)
     uint32_t* tnext;           // per update: next in the key's push list
     uint32_t* tprev;           // per update: previous update of the same edge (stream order)
-    uint32_t* done;            // per update: batch sequence number once applied
+    uint32_t* done;            // per update: batch sequence number once applied (when awaited)
+    uint8_t* succ;             // per update: a later update of the same edge waits for it
     uint32_t* ticket;          // work ticket of the persistent apply kernel
     uint32_t tmask;            // table size - 1
 };
@@ -103,26 +103,30 @@ void launch_det_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, cudaStrea
 void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const EdgeOrder& eo, uint32_t seq,
                        int num_sms, cudaStream_t s);
 void launch_dirty_list(const Dev& g, uint32_t* list, uint32_t* count, cudaStream_t s);
-void launch_compact(const Dev& g, const uint32_t* list, const uint32_t* count, uint32_t max_rows, cudaStream_t s);
+// force: compact every listed row (else rows whose holes fill at most a quarter
+// of their extent wait, under exact selection).
+void launch_compact(const Dev& g, const uint32_t* list, const uint32_t* count, uint32_t max_rows, bool force,
+                    cudaStream_t s);
 void launch_take_overflow(const Dev& g, uint32_t* drain_n, cudaStream_t s);
 void launch_drain(const Dev& g, const uint32_t* drain_n, bool ordered, unsigned long long* failed, cudaStream_t s);
 void launch_snapshot(const Dev& g, uint16_t* snap, cudaStream_t s);
 // list_mode 0: every vertex; 1: the vertices in b.wl; 2: as b.rc->list says.
 void launch_build_items(const Dev& g, const SweepBufs& b, int list_mode, int num_sms, cudaStream_t s);
-// sym_mode 0: no mirror checksum; 1: accumulate it (b.symsum) when *g.asym is
-// set; 2: as 1, first sweep of a repair only. The sweep index (the
-// independent-set order's salt) and whether pushes are on come from b.rc.
+// sym_mode 0: no mirror checksum; 2: in the first sweep of a repair, each graph
+// repaired in full with asym set accumulates its checksum (sum over entries
+// x->y, y != x, y < n, of H(x,y) - H(y,x)) in its GraphCtl. The sweep index
+// (the independent-set order's salt) comes from b.rc.
 void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int list_mode, int sym_mode, int num_sms,
                   cudaStream_t s);
-// After a sweep: b.wl = the next worklist (full repair: the vertices the sweep
-// recolored, their neighbors and the vertices still conflicted; incremental:
-// the blocked and pushed vertices). Reads the sweep's items: call before the
-// next launch_build_items.
+// After a sweep: b.wl = the next worklist (reference rule: the vertices the
+// sweep recolored and their neighbors; independent-set rule: the blocked and
+// pushed vertices). Reads the sweep's items: call before the next
+// launch_build_items.
 void launch_next_worklist(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s);
 // The device-driven repair loop: begin (b.rc host fields set), then per sweep
 // launch_repair_sweep + launch_repair_step; b.rc->cont says whether another
 // sweep runs. With `cond`, the step also sets that graph conditional.
-void launch_repair_begin(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s);
+void launch_repair_begin(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s);
 void launch_repair_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s);
 void launch_repair_step(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s,
                         const cudaGraphConditionalHandle* cond);

@@ -299,7 +299,7 @@ __global__ void validate_kernel(Dev g, unsigned long long* ekeys, uint32_t* ecou
         bool eff = false;
         unsigned long long oor = 0;
         warp_for_each(g.col, row_s(g, x), row_e(g, x), [&](uint64_t, uint32_t y) {
-            if (y == INV) return;
+            if (y == INV || (g.blen && (y & TOMB))) return;  // free slot or deleted run entry
             if (y >= g.n) { oor++; return; }
             eff = true;
             const uint32_t a = x < y ? x : y, b2 = x < y ? y : x;
