@@ -335,6 +335,152 @@ def run_reference(a):
     print(json.dumps(out), flush=True)
 
 
+def run_batched(a):
+    """Batched form: `--batch-graphs` seeded graphs (Delaunay / R-MAT / Chung-Lu,
+    vertex counts log-uniform in [1,024, 2,097,152], epoch sizes in {1,024,
+    8,192, 32,768}), each with its own churn stream (16x its edge count, the
+    first ticks' worth generated). A tick submits one epoch of every graph. The
+    same graphs and updates run twice: per-graph plain launches (one handle per
+    graph: apply + publish per epoch) and the batched engine (one tick: one
+    CUDA-graph launch). Both arms are wall-clock timed from host memory."""
+    import torch
+    import streamgc_b200 as S
+    from streamgc_b200 import workloads as W
+
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    ticks = a.warmup + a.steps
+    specs = W.batch_specs(a.batch_graphs, seed=42)
+    t = time.time()
+    data = W.build_all(specs, lambda sp: (ticks + (16 if a.autotune else 0)) * sp["epoch"])
+    log(f"batched: {len(data)} graphs generated in {time.time() - t:.1f}s; "
+        f"{sum(d['spec']['n'] for d in data)} vertices, {sum(int(d['row_ptr'][-1]) for d in data) // 2} edges")
+    graphs = [S.Graph(d["row_ptr"], d["col"]) for d in data]
+    epochs = [d["spec"]["epoch"] for d in data]
+
+    def tick_parts(k, t_):
+        ch = data[k]["churn"]
+        lo = t_ * epochs[k]
+        return ch[lo:lo + epochs[k]] if lo < len(ch) else None
+
+    # ---- arm 1: per-graph plain launches ----
+    t = time.time()
+    hs = [S.StreamGC(gr, epoch_size=epochs[k], histogram_threshold=HIST_THR, slack_pct=300,
+                     max_batch=max(epochs[k], 1 << 16), device=local, exact_select=True, full_repair_every=0)
+          for k, gr in enumerate(graphs)]
+    for k, h in enumerate(hs):
+        init = data[k]["init"]
+        for s in range(0, len(init), 1 << 16):
+            h.apply(init[s:s + (1 << 16)], S.MODE_CONCURRENT)
+        h.publish()
+    torch.cuda.synchronize()
+    log(f"plain arm: {len(hs)} handles created and colored in {time.time() - t:.1f}s")
+    plain_ticks, plain_updates, plain_ok = [], 0, True
+    for t_ in range(ticks):
+        t0 = time.perf_counter()
+        n_up = 0
+        for k, h in enumerate(hs):
+            part = tick_parts(k, t_)
+            if part is None or len(part) == 0:
+                continue
+            h.apply(part, S.MODE_CONCURRENT)
+            r = h.publish()
+            plain_ok &= r["proper"] == 1
+            n_up += len(part)
+        torch.cuda.synchronize()
+        if t_ >= a.warmup:
+            plain_ticks.append(time.perf_counter() - t0)
+            plain_updates += n_up
+    plain_launches = sum(h.stats()["kernel_launches"] for h in hs)
+    for h in hs:
+        h.close()
+    del hs
+    torch.cuda.synchronize()
+
+    # ---- arm 2: the batched engine ----
+    t = time.time()
+    cap = max(sum(epochs), 1 << 20)
+    b = S.Batch(graphs, epoch_sizes=epochs, max_tick_updates=cap, device=local, profile=True)
+    pos = [0] * len(graphs)
+    while True:  # initial coloring: every graph's init stream, in ticks of at most `cap` updates
+        room, any_left = cap, False
+        for k in range(len(graphs)):
+            init = data[k]["init"]
+            if pos[k] < len(init) and room > 0:
+                m = min(room, len(init) - pos[k])
+                b.submit(k, init[pos[k]:pos[k] + m])
+                pos[k] += m
+                room -= m
+            any_left |= pos[k] < len(data[k]["init"])
+        b.close_epochs()
+        r = b.tick()
+        if not r["proper"]:
+            raise SystemExit("batched init not proper")
+        if not any_left:
+            break
+    log(f"batched arm: created and colored in {time.time() - t:.1f}s")
+    tuning = b.tuning()
+    tstate = {"t": 0}
+    if a.autotune:
+        def feed():
+            for k in range(len(graphs)):
+                part = tick_parts(k, tstate["t"])
+                if part is not None and len(part):
+                    b.submit(k, part)
+            tstate["t"] += 1
+        tuning = b.autotune(feed, ticks_per_candidate=1)
+        log(f"tuner chose {tuning} in {tstate['t']} ticks")
+    st0 = b.stats()
+    lat, dev_ms, b_updates, b_ok = [], [], 0, True
+    base_t = tstate["t"]  # ticks the tuner consumed
+    with ClockSampler(local) as clk:
+        for t_ in range(ticks):
+            t0 = time.perf_counter()
+            n_up = 0
+            for k in range(len(graphs)):
+                part = tick_parts(k, base_t + t_)
+                if part is None or len(part) == 0:
+                    continue
+                b.submit(k, part)
+                n_up += len(part)
+            r = b.tick()
+            b_ok &= r["proper"] == 1
+            if t_ >= a.warmup:
+                lat.append(time.perf_counter() - t0)
+                dev_ms.append(r["device_ms"])
+                b_updates += n_up
+    st1 = b.stats()
+    val = b.validate()
+    b.close()
+    plain_v = plain_updates / sum(plain_ticks)
+    batch_v = b_updates / sum(lat)
+    ls = sorted(lat)
+    fam = {f: sum(1 for d in data if d["spec"]["family"] == f) for f in W.FAMILIES}
+    out = {
+        "metric": METRIC, "form": "batched", "value": batch_v, "unit": "updates/s", "n_gpus": 1,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sum(lat) / len(lat), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"batched_{len(graphs)}_graphs", "families": fam,
+                   "vertices": sum(d["spec"]["n"] for d in data),
+                   "undirected_edges": sum(int(d["row_ptr"][-1]) for d in data) // 2,
+                   "epoch_sizes": "per graph in {1024, 8192, 32768}", "tick": "one epoch of every graph",
+                   "mode": "concurrent apply, independent-set repair, CUDA-graph tick", "tuning": tuning,
+                   "autotuned": bool(a.autotune), "all_ticks_proper": bool(b_ok and plain_ok),
+                   "valid_after_run": val["violations"] == 0 and val["uncolored_with_edges"] == 0},
+        "plain_per_graph": {"value": plain_v, "unit": "updates/s", "ms_per_tick": 1e3 * sum(plain_ticks) / len(plain_ticks),
+                            "launches": plain_launches},
+        "speedup_vs_plain": batch_v / plain_v,
+        "latency_ms": {"update_to_visible_p50": 1e3 * ls[len(ls) // 2],
+                       "update_to_visible_p99": 1e3 * ls[min(len(ls) - 1, int(round(0.99 * (len(ls) - 1))))],
+                       "tick_device_ms_p50": sorted(dev_ms)[len(dev_ms) // 2]},
+        "gpu_launches": st1["kernel_launches"] - st0["kernel_launches"],
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -346,11 +492,17 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--profile-window", action="store_true",
                     help="bracket the device-timed steps with cudaProfilerStart/Stop (for ncu)")
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "served"],
+                    help="plain: one graph (the headline); batched: many graphs per tick; served: request loop")
+    ap.add_argument("--batch-graphs", type=int, default=256)
+    ap.add_argument("--autotune", action="store_true", help="batched: run the tuner on the warm-up ticks first")
     a = ap.parse_args()
     if a.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
     if a.impl == "reference":
         run_reference(a)
+    elif a.form == "batched":
+        run_batched(a)
     else:
         run_ours(a)
 

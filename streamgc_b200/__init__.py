@@ -92,6 +92,31 @@ _u8p, _u16p, _u32p, _u64p, _vp = (C.POINTER(C.c_uint8), C.POINTER(C.c_uint16), C
 _lib = None
 
 # every exported entry point of include/streamgc_b200.h and csrc/sgc_host.h
+class BatchGraph(C.Structure):
+    _fields_ = [("num_vertices", C.c_uint32), ("epoch_size", C.c_uint32), ("histogram_threshold", C.c_uint32),
+                ("_reserved", C.c_uint32), ("row_ptr", _u64p), ("col_idx", _u32p), ("degree", _u32p)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("slack_pct", C.c_uint32), ("max_tick_updates", C.c_uint32),
+                ("device", C.c_int32), ("flags", C.c_uint32), ("repair_tile", C.c_uint32),
+                ("apply_blocks_per_sm", C.c_uint32), ("_reserved", C.c_uint32)]
+
+
+class TickReport(C.Structure):
+    _fields_ = [("updates", C.c_uint32), ("published", C.c_uint32), ("tier1_iterations", C.c_uint32),
+                ("tier2_ran", C.c_uint32), ("proper", C.c_uint32), ("_pad", C.c_uint32), ("device_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("_")}
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("repair_tile", C.c_uint32), ("apply_blocks_per_sm", C.c_uint32)]
+
+
+BATCH_FEED = C.CFUNCTYPE(C.c_int, _vp, _vp)
+
 SIGNATURES = {
     "sgc_default_options": (C.c_int, [C.POINTER(_Options)]),
     "sgc_create": (C.c_int, [C.POINTER(_Config), _u32p, _u32p, _u32p, C.POINTER(_vp)]),
@@ -128,6 +153,24 @@ SIGNATURES = {
     "sgc_gen_chung_lu": (C.c_int, [C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64, C.POINTER(_CSR)]),
     "sgc_static_greedy": (C.c_uint32, [C.POINTER(_CSR)]),
     "sgc_write_coloring": (C.c_int, [C.c_char_p, _u16p, C.c_uint32]),
+    "sgc_batch_default_options": (C.c_int, [C.POINTER(BatchOptions)]),
+    "sgc_batch_create": (C.c_int, [C.POINTER(BatchGraph), C.c_uint32, C.POINTER(BatchOptions), C.POINTER(_vp)]),
+    "sgc_batch_destroy": (C.c_int, [_vp]),
+    "sgc_batch_num_graphs": (C.c_uint32, [_vp]),
+    "sgc_batch_epoch_size": (C.c_uint32, [_vp, C.c_uint32]),
+    "sgc_batch_submit": (C.c_int, [_vp, C.c_uint32, _vp, C.c_uint32]),
+    "sgc_batch_pending": (C.c_uint64, [_vp]),
+    "sgc_batch_tick": (C.c_int, [_vp, C.POINTER(TickReport)]),
+    "sgc_batch_close_epochs": (C.c_int, [_vp]),
+    "sgc_batch_query": (C.c_int, [_vp, C.c_uint32, _u32p, _u16p, C.c_uint32]),
+    "sgc_batch_snapshot": (C.c_int, [_vp, C.c_uint32, _u16p]),
+    "sgc_batch_rows": (C.c_int, [_vp, C.c_uint32, _u64p, _u32p, C.c_uint64]),
+    "sgc_batch_validate": (C.c_int, [_vp, C.POINTER(Validation)]),
+    "sgc_batch_set_thresholds": (C.c_int, [_vp, C.c_uint32]),
+    "sgc_batch_get_tuning": (C.c_int, [_vp, C.POINTER(BatchTuning)]),
+    "sgc_batch_set_tuning": (C.c_int, [_vp, C.POINTER(BatchTuning)]),
+    "sgc_batch_autotune": (C.c_int, [_vp, BATCH_FEED, _vp, C.c_uint32, C.POINTER(BatchTuning)]),
+    "sgc_batch_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
 }
 
 
@@ -439,3 +482,128 @@ class StreamGC:
 
 def version():
     return lib().sgc_version().decode()
+
+
+BATCH_CUDA_GRAPH = 1
+BATCH_STREAM_ORDER = 2
+BATCH_PROFILE = 4
+
+
+class Batch:
+    """Many graphs resident on one GPU (include/streamgc_batch.h): updates are
+    submitted per graph in the graph's own ids; tick() applies everything
+    submitted in one persistent launch, repairs, and publishes each graph whose
+    epoch closed."""
+
+    def __init__(self, graphs, epoch_sizes=None, thresholds=None, max_tick_updates=1 << 20, slack_pct=300,
+                 device=0, cuda_graph=True, stream_order=False, profile=False, repair_tile=0, apply_blocks_per_sm=0):
+        L = lib()
+        self.graphs = list(graphs)
+        G = len(self.graphs)
+        arr = (BatchGraph * G)()
+        for k, g in enumerate(self.graphs):
+            arr[k].num_vertices = g.n
+            arr[k].epoch_size = int(epoch_sizes[k]) if epoch_sizes is not None else 0
+            arr[k].histogram_threshold = int(thresholds[k]) if thresholds is not None else 0
+            arr[k].row_ptr = _p(g.row_ptr, _u64p)
+            arr[k].col_idx = _p(g.col_idx, _u32p)
+            arr[k].degree = _p(g.degree, _u32p)
+        opt = BatchOptions()
+        L.sgc_batch_default_options(C.byref(opt))
+        opt.slack_pct, opt.max_tick_updates, opt.device = slack_pct, max_tick_updates, device
+        opt.flags = (BATCH_CUDA_GRAPH if cuda_graph else 0) | (BATCH_STREAM_ORDER if stream_order else 0) | \
+            (BATCH_PROFILE if profile else 0)
+        opt.repair_tile, opt.apply_blocks_per_sm = repair_tile, apply_blocks_per_sm
+        self.b = _vp()
+        _check(L.sgc_batch_create(arr, G, C.byref(opt), C.byref(self.b)), "sgc_batch_create")
+        self.G = G
+
+    def close(self):
+        if getattr(self, "b", None):
+            lib().sgc_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def epoch_size(self, k):
+        return lib().sgc_batch_epoch_size(self.b, k)
+
+    def submit(self, k, ups):
+        ups = np.ascontiguousarray(ups, dtype=EDGE_UPDATE)
+        _check(lib().sgc_batch_submit(self.b, k, ups.ctypes.data, len(ups)), "sgc_batch_submit")
+
+    def pending(self):
+        return lib().sgc_batch_pending(self.b)
+
+    def tick(self):
+        r = TickReport()
+        _check(lib().sgc_batch_tick(self.b, C.byref(r)), "sgc_batch_tick")
+        return r.as_dict()
+
+    def close_epochs(self):
+        _check(lib().sgc_batch_close_epochs(self.b), "sgc_batch_close_epochs")
+
+    def query(self, k, vertices):
+        v = np.ascontiguousarray(vertices, dtype=np.uint32)
+        out = np.zeros(len(v), dtype=np.uint16)
+        _check(lib().sgc_batch_query(self.b, k, _p(v, _u32p), _p(out, _u16p), len(v)), "sgc_batch_query")
+        return out
+
+    def snapshot(self, k):
+        out = np.zeros(self.graphs[k].n, dtype=np.uint16)
+        _check(lib().sgc_batch_snapshot(self.b, k, _p(out, _u16p)), "sgc_batch_snapshot")
+        return out
+
+    def rows(self, k):
+        """The graph's live rows (its own ids): (row_ptr, col)."""
+        n = self.graphs[k].n
+        rp = np.zeros(n + 1, dtype=np.uint64)
+        _check(lib().sgc_batch_rows(self.b, k, _p(rp, _u64p), None, 0), "sgc_batch_rows")
+        col = np.zeros(max(int(rp[-1]), 1), dtype=np.uint32)
+        _check(lib().sgc_batch_rows(self.b, k, _p(rp, _u64p), _p(col, _u32p), len(col)), "sgc_batch_rows")
+        return rp, col[: int(rp[-1])]
+
+    def validate(self):
+        v = Validation()
+        _check(lib().sgc_batch_validate(self.b, C.byref(v)), "sgc_batch_validate")
+        return v.as_dict()
+
+    def set_thresholds(self, thr):
+        _check(lib().sgc_batch_set_thresholds(self.b, thr), "sgc_batch_set_thresholds")
+
+    def tuning(self):
+        t = BatchTuning()
+        _check(lib().sgc_batch_get_tuning(self.b, C.byref(t)), "sgc_batch_get_tuning")
+        return {"repair_tile": t.repair_tile, "apply_blocks_per_sm": t.apply_blocks_per_sm}
+
+    def set_tuning(self, repair_tile, apply_blocks_per_sm):
+        t = BatchTuning(repair_tile, apply_blocks_per_sm)
+        _check(lib().sgc_batch_set_tuning(self.b, C.byref(t)), "sgc_batch_set_tuning")
+
+    def autotune(self, feed, ticks_per_candidate=2):
+        """feed(): stages one tick's updates. Returns the chosen tuning."""
+        def _cb(_b, _ctx):
+            try:
+                feed()
+                return 0
+            except Exception:
+                return -1
+        cb = BATCH_FEED(_cb)
+        t = BatchTuning()
+        _check(lib().sgc_batch_autotune(self.b, cb, None, ticks_per_candidate, C.byref(t)), "sgc_batch_autotune")
+        return {"repair_tile": t.repair_tile, "apply_blocks_per_sm": t.apply_blocks_per_sm}
+
+    def stats(self):
+        st = Stats()
+        _check(lib().sgc_batch_stats(self.b, C.byref(st)), "sgc_batch_stats")
+        return st.as_dict()

@@ -13,15 +13,14 @@
 #include <vector>
 
 #include "../../include/streamgc_b200.h"
-#include "sgc_kernels.cuh"
+#include "sgc_internal.h"
 
 using namespace sgc;
 
-namespace {
+namespace sgci {
 
 thread_local std::string g_err;
 
-int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
 int fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;
@@ -31,96 +30,6 @@ int fail(int code, const char* fmt, ...) {
     g_err = buf;
     return code;
 }
-
-#define CK(call)                                                                                      \
-    do {                                                                                              \
-        cudaError_t e_ = (call);                                                                      \
-        if (e_ != cudaSuccess)                                                                        \
-            return fail(SGC_ECUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
-    } while (0)
-
-// Control block on the device: counters every kernel family writes.
-struct Ctl {
-    uint32_t ovf_count;
-    uint32_t err;
-    uint32_t drain_n;
-    uint32_t dirty_count;
-    uint32_t item_count;
-    uint32_t pend_count;
-    uint32_t fac_count;
-    uint32_t ticket;
-    unsigned long long ovf_lost;
-    unsigned long long nskip;
-    unsigned long long drain_failed;
-    unsigned long long symsum;
-    unsigned long long live;
-    unsigned long long pad[3];
-};
-
-}  // namespace
-
-struct sgc_handle {
-    int device = 0;
-    int num_sms = 148;
-    cudaStream_t stream = nullptr;
-    sgc_options opt{};
-    StreamGCConfig cfg{};
-    uint32_t n = 0, num_hd = 0, maxc = 1024, hist_rows = 0;
-    uint64_t total_slots = 0;
-    uint64_t device_bytes = 0;
-    Dev g{};
-    // owned device buffers
-    std::vector<void*> allocs;
-    Ctl* ctl = nullptr;
-    uint16_t* snap[2] = {nullptr, nullptr};
-    int front = 0;
-    EdgeUpdate* d_batch = nullptr;
-    EdgeUpdate* h_stage = nullptr;  // pinned staging for pageable inputs
-    cudaEvent_t stage_free = nullptr;
-    EdgeOrder eo{};
-    uint32_t seq = 0;
-    SweepBufs sb{};
-    uint32_t* dirty_list = nullptr;
-    Tier2Bufs t2{};
-    uint32_t* h_small = nullptr;    // pinned readback scratch
-    RepairCtl* h_rc_in = nullptr;   // pinned: host fields of the repair control block
-    RepairCtl* h_rc_out = nullptr;  // pinned: its readback
-    uint64_t repairs_since_full = 0;
-    int last_mode = SGC_MODE_DETERMINISTIC;
-    // host counters
-    uint64_t updates = 0, epochs = 0, tier1_sweeps = 0, tier2_runs = 0, tier2_fixed = 0;
-    // profiling
-    std::vector<cudaEvent_t> ev_pool;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
-    double sweep_ms = 0;
-    uint64_t sweep_count = 0, sweep_bytes = 0, live_entries = 0;
-    uint64_t launches = 0;          // kernels this handle launched
-    uint64_t h2d_bytes = 0, d2h_bytes = 0;  // bytes the library moved across PCIe / C2C
-};
-
-namespace {
-
-template <class T>
-int dalloc(sgc_handle* h, T** p, size_t count, int fill = -1) {
-    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return fail(SGC_ENOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
-    }
-    h->allocs.push_back(q);
-    h->device_bytes += bytes;
-    if (fill >= 0) CK(cudaMemsetAsync(q, fill, bytes, h->stream));
-    *p = (T*)q;
-    return SGC_OK;
-}
-
-#define TRY(x)                   \
-    do {                         \
-        int r_ = (x);            \
-        if (r_ != SGC_OK) return r_; \
-    } while (0)
 
 // Scatters the base CSR into the slack layout: warp per row.
 __global__ void scatter_base_kernel(uint32_t n, const uint64_t* __restrict__ brp, const uint32_t* __restrict__ bcol,
@@ -313,7 +222,9 @@ int read_drain(sgc_handle* h, sgc_repair_report* rep, unsigned long long before_
     return SGC_OK;
 }
 
-}  // namespace
+}  // namespace sgci
+
+using namespace sgci;
 
 extern "C" {
 
@@ -351,8 +262,10 @@ int sgc_destroy(sgc_handle* h) {
     return SGC_OK;
 }
 
-int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const uint64_t* row_ptr,
-                  const uint32_t* col_idx, const uint32_t* degree, sgc_handle** out) {
+}  // extern "C"
+
+int sgci::create_internal(const StreamGCConfig* cfg, const sgc_options* opt_in, const uint64_t* row_ptr,
+                          const uint32_t* col_idx, const uint32_t* degree, const CreateExtra* ex, sgc_handle** out) {
     if (!cfg || !row_ptr || !degree || !out) return fail(SGC_EINVAL, "null argument");
     *out = nullptr;
     sgc_options opt;
@@ -387,7 +300,8 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
         const uint32_t cap = std::max<uint32_t>(cnt + extra, 8u);
         rp[x + 1] = rp[x] + cap;
         hw[x] = cnt;
-        if (degree[x] > cfg->histogram_threshold) hdmap[x] = num_hd++;
+        const uint32_t thr = (ex && ex->thr_word) ? ex->thr_word[x >> 5] : cfg->histogram_threshold;
+        if (degree[x] > thr) hdmap[x] = num_hd++;
     }
     const bool exact_sel = (opt.flags & SGC_OPT_EXACT_SELECT) != 0;
     for (uint64_t j = 0; j < nnz; j++) {
@@ -449,10 +363,28 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     g.ovf_lost = &h->ctl->ovf_lost;
     g.nskip = &h->ctl->nskip;
     g.err = &h->ctl->err;
-    A(&g.gctl, 1, 0);
+    const uint32_t G = (ex && ex->G) ? ex->G : 1u;
+    {
+        std::vector<GraphCtl> gc(G);
+        for (uint32_t k = 0; k < G; k++) {
+            std::memset(&gc[k], 0, sizeof(GraphCtl));
+            gc[k].asym = 1;  // nothing known about the mirrors yet
+            gc[k].base = (ex && ex->base) ? ex->base[k] : 0u;
+        }
+        A(&g.gctl, G);
+        if (cudaMemcpyAsync(g.gctl, gc.data(), G * sizeof(GraphCtl), cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess)
+            return bail(fail(SGC_ECUDA, "control block init failed"));
+    }
     g.gidw = nullptr;
-    if (cudaMemsetAsync(&g.gctl->asym, 0x01, 1, h->stream) != cudaSuccess)  // nothing known about the mirrors yet
-        return bail(fail(SGC_ECUDA, "control block init failed"));
+    if (ex && ex->gidw) {
+        uint32_t* d_gidw;
+        A(&d_gidw, (n + 31) / 32);
+        if (cudaMemcpyAsync(d_gidw, ex->gidw, ((n + 31) / 32) * 4ull, cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess)
+            return bail(fail(SGC_ECUDA, "graph map upload failed"));
+        g.gidw = d_gidw;
+    }
     if (cudaMemcpyAsync(d_rp, rp.data(), rp.size() * 8, cudaMemcpyHostToDevice, h->stream) ||
         cudaMemcpyAsync(d_hdmap, hdmap.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) ||
         cudaMemcpyAsync(d_deg, degree, (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) ||
@@ -521,7 +453,7 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     A(&sb.rbits, (n + 31) / 32 + 1, 0);
     A(&sb.rc, 1, 0);
     sb.tile = opt.repair_tile;
-    sb.G = 1;
+    sb.G = G;
     if (g.exact) A(&g.touched, (n + 31) / 32 + 1, 0);
     else g.touched = nullptr;
     if (g.exact) {  // base runs: rows whose base entries are strictly ascending
@@ -565,6 +497,13 @@ int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const ui
     if ((r = check_cuda("create"))) return bail(r);
     *out = h;
     return SGC_OK;
+}
+
+extern "C" {
+
+int sgc_create_ex(const StreamGCConfig* cfg, const sgc_options* opt_in, const uint64_t* row_ptr,
+                  const uint32_t* col_idx, const uint32_t* degree, sgc_handle** out) {
+    return create_internal(cfg, opt_in, row_ptr, col_idx, degree, nullptr, out);
 }
 
 int sgc_create(const StreamGCConfig* cfg, const uint32_t* row_ptr, const uint32_t* col_idx, const uint32_t* degree,

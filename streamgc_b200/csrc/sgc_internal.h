@@ -1,0 +1,131 @@
+// sgc_internal.h -- internals shared by the handle API (sgc_api.cu) and the
+// batched engine (sgc_batch.cu): the handle layout and the host-side building
+// blocks of an epoch. Not part of the public interface.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <utility>
+#include <vector>
+
+#include "../../include/streamgc_b200.h"
+#include "sgc_kernels.cuh"
+
+namespace sgci {
+using namespace sgc;
+
+// Records the message returned by sgc_last_error(); returns `code`.
+int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+
+#define CK(call)                                                                                      \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return fail(SGC_ECUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// Control block on the device: counters every kernel family writes.
+struct Ctl {
+    uint32_t ovf_count;
+    uint32_t err;
+    uint32_t drain_n;
+    uint32_t dirty_count;
+    uint32_t item_count;
+    uint32_t pend_count;
+    uint32_t fac_count;
+    uint32_t ticket;
+    unsigned long long ovf_lost;
+    unsigned long long nskip;
+    unsigned long long drain_failed;
+    unsigned long long symsum;
+    unsigned long long live;
+    unsigned long long pad[3];
+};
+
+}  // namespace sgci
+
+// One handle: a graph (or several, side by side) resident on one GPU.
+struct sgc_handle {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    sgc_options opt{};
+    StreamGCConfig cfg{};
+    uint32_t n = 0, num_hd = 0, maxc = 1024, hist_rows = 0;
+    uint64_t total_slots = 0;
+    uint64_t device_bytes = 0;
+    sgc::Dev g{};
+    // owned device buffers
+    std::vector<void*> allocs;
+    sgci::Ctl* ctl = nullptr;
+    uint16_t* snap[2] = {nullptr, nullptr};
+    int front = 0;
+    EdgeUpdate* d_batch = nullptr;
+    EdgeUpdate* h_stage = nullptr;  // pinned staging for pageable inputs
+    cudaEvent_t stage_free = nullptr;
+    sgc::EdgeOrder eo{};
+    uint32_t seq = 0;
+    sgc::SweepBufs sb{};
+    uint32_t* dirty_list = nullptr;
+    sgc::Tier2Bufs t2{};
+    uint32_t* h_small = nullptr;         // pinned readback scratch
+    sgc::RepairCtl* h_rc_in = nullptr;   // pinned: host fields of the repair control block
+    sgc::RepairCtl* h_rc_out = nullptr;  // pinned: its readback
+    uint64_t repairs_since_full = 0;
+    int last_mode = SGC_MODE_DETERMINISTIC;
+    // host counters
+    uint64_t updates = 0, epochs = 0, tier1_sweeps = 0, tier2_runs = 0, tier2_fixed = 0;
+    // profiling
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
+    double sweep_ms = 0;
+    uint64_t sweep_count = 0, sweep_bytes = 0, live_entries = 0;
+    uint64_t launches = 0;          // kernels this handle launched
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;  // bytes the library moved across PCIe / C2C
+};
+
+namespace sgci {
+
+template <class T>
+int dalloc(sgc_handle* h, T** p, size_t count, int fill = -1) {
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SGC_ENOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    }
+    h->allocs.push_back(q);
+    h->device_bytes += bytes;
+    if (fill >= 0) CK(cudaMemsetAsync(q, fill, bytes, h->stream));
+    *p = (T*)q;
+    return SGC_OK;
+}
+
+#define TRY(x)                   \
+    do {                         \
+        int r_ = (x);            \
+        if (r_ != SGC_OK) return r_; \
+    } while (0)
+
+
+int check_cuda(const char* where);
+cudaEvent_t take_event(sgc_handle* h);
+int sync(sgc_handle* h);
+int compact_dirty(sgc_handle* h, bool force);
+int drain(sgc_handle* h, bool ordered, unsigned long long* failed_counter);
+int set_clean(sgc_handle* h, uint32_t v);
+int repair_loop(sgc_handle* h, sgc_repair_report* rep, bool force_full);
+// Extra layout of a handle that holds several graphs (the batched engine).
+struct CreateExtra {
+    const uint32_t* thr_word;  // per 32-vertex word: histogram threshold (null: cfg->histogram_threshold)
+    const uint32_t* gidw;      // per 32-vertex word: graph id (null: one graph)
+    uint32_t G;                // graphs
+    const uint32_t* base;      // per graph: first vertex (null: 0)
+};
+int create_internal(const StreamGCConfig* cfg, const sgc_options* opt_in, const uint64_t* row_ptr,
+                    const uint32_t* col_idx, const uint32_t* degree, const CreateExtra* ex, sgc_handle** out);
+
+}  // namespace sgci
+

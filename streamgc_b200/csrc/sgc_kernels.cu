@@ -86,40 +86,48 @@ __device__ __forceinline__ uint32_t key_hash(unsigned long long k) {
     return (uint32_t)k;
 }
 
-__global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n, EdgeOrder eo) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) *eo.ticket = 0;
-    if (i >= n) return;
-    const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
-    const uint32_t u = r.x, v = r.y;
-    const uint8_t type = (uint8_t)(r.z & 0xFFu);
-    if ((type != SGC_UPDATE_ADD && type != SGC_UPDATE_DEL) || u >= g.n || v >= g.n) {
-        eo.tslot[i] = NONE32;
-        return;
+// `dyn` (device words, optional): [0] the batch size, [1] the batch sequence
+// number; they replace the `n` / `seq` arguments so that a captured CUDA graph
+// can replay the launches on every tick. Grid-stride loops.
+__device__ __forceinline__ uint32_t batch_n(uint32_t n, const uint32_t* dyn) { return dyn ? ld_cg(dyn) : n; }
+
+__global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg, EdgeOrder eo,
+                                 const uint32_t* dyn) {
+    const uint32_t n = batch_n(n_arg, dyn);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *eo.ticket = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
+        const uint32_t u = r.x, v = r.y;
+        const uint8_t type = (uint8_t)(r.z & 0xFFu);
+        if ((type != SGC_UPDATE_ADD && type != SGC_UPDATE_DEL) || u >= g.n || v >= g.n) {
+            eo.tslot[i] = NONE32;
+            continue;
+        }
+        eo.succ[i] = 0;
+        const unsigned long long key = edge_key(u, v);
+        uint32_t h = key_hash(key) & eo.tmask;
+        for (uint32_t probe = 0; probe <= eo.tmask; probe++) {
+            const unsigned long long k = atomicCAS(eo.tkey + h, EMPTY64, key);
+            if (k == EMPTY64 || k == key) break;
+            h = (h + 1) & eo.tmask;
+        }
+        eo.tslot[i] = h;
+        eo.tnext[i] = atomicExch(eo.thead + h, i);
     }
-    eo.succ[i] = 0;
-    const unsigned long long key = edge_key(u, v);
-    uint32_t h = key_hash(key) & eo.tmask;
-    for (uint32_t probe = 0; probe <= eo.tmask; probe++) {
-        const unsigned long long k = atomicCAS(eo.tkey + h, EMPTY64, key);
-        if (k == EMPTY64 || k == key) break;
-        h = (h + 1) & eo.tmask;
-    }
-    eo.tslot[i] = h;
-    eo.tnext[i] = atomicExch(eo.thead + h, i);
 }
 
-__global__ void conc_prep_prev(uint32_t n, EdgeOrder eo) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t h = eo.tslot[i];
-    uint32_t best = NONE32;
-    if (h != NONE32) {
-        for (uint32_t j = eo.thead[h]; j != NONE32; j = eo.tnext[j])
-            if (j < i && (best == NONE32 || j > best)) best = j;
+__global__ void conc_prep_prev(uint32_t n_arg, EdgeOrder eo, const uint32_t* dyn) {
+    const uint32_t n = batch_n(n_arg, dyn);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t h = eo.tslot[i];
+        uint32_t best = NONE32;
+        if (h != NONE32) {
+            for (uint32_t j = eo.thead[h]; j != NONE32; j = eo.tnext[j])
+                if (j < i && (best == NONE32 || j > best)) best = j;
+        }
+        eo.tprev[i] = best;
+        if (best != NONE32) eo.succ[best] = 1;  // best's done mark is awaited
     }
-    eo.tprev[i] = best;
-    if (best != NONE32) eo.succ[best] = 1;  // best's done mark is awaited
 }
 
 // Bounded wait for the same-edge predecessor: ~2^22 polls with a sleep, then
@@ -143,8 +151,10 @@ __device__ __forceinline__ void wait_done(const EdgeOrder& eo, const Dev& g, uin
 // current update. A warp's tickets rise, and a predecessor always has a lower
 // index than its successor, so no chain of waits closes on itself. Only an
 // update that a later one of the same edge waits for publishes its done mark.
-__global__ void __launch_bounds__(256, 4) conc_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n,
-                                                         EdgeOrder eo, uint32_t seq) {
+__global__ void __launch_bounds__(256, 4) conc_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg,
+                                                            EdgeOrder eo, uint32_t seq_arg, const uint32_t* dyn) {
+    const uint32_t n = batch_n(n_arg, dyn);
+    const uint32_t seq = dyn ? ld_cg(dyn + 1) : seq_arg;
     uint32_t i = 0;
     if (lane_id() == 0) i = atomicAdd(eo.ticket, 1u);
     i = __shfl_sync(FULL, i, 0);
@@ -181,21 +191,64 @@ void launch_det_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, cudaStrea
     if (n) det_apply_kernel<<<1, 32, 0, s>>>(g, ups, n);
 }
 
-void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const EdgeOrder& eo, uint32_t seq,
-                       int num_sms, cudaStream_t s) {
-    if (!n) return;
-    const uint32_t blk = (n + 255) / 256;
-    conc_prep_insert<<<blk, 256, 0, s>>>(g, ups, n, eo);
-    conc_prep_prev<<<blk, 256, 0, s>>>(n, eo);
+int conc_apply_occupancy() {
     static int occ = 0;
     if (!occ) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, conc_apply_kernel, 256, 0);
         if (occ < 1) occ = 1;
     }
-    uint32_t grid = (uint32_t)(num_sms * occ);
+    return occ;
+}
+
+void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const EdgeOrder& eo, uint32_t seq,
+                       int num_sms, cudaStream_t s) {
+    if (!n) return;
+    uint32_t blk = (n + 255) / 256;
+    if (blk > (uint32_t)num_sms * 16) blk = num_sms * 16;
+    conc_prep_insert<<<blk, 256, 0, s>>>(g, ups, n, eo, nullptr);
+    conc_prep_prev<<<blk, 256, 0, s>>>(n, eo, nullptr);
+    uint32_t grid = (uint32_t)(num_sms * conc_apply_occupancy());
     const uint32_t need = (n + 7) / 8;  // 8 warps per block
     if (grid > need) grid = need;
-    conc_apply_kernel<<<grid, 256, 0, s>>>(g, ups, n, eo, seq);
+    conc_apply_kernel<<<grid, 256, 0, s>>>(g, ups, n, eo, seq, nullptr);
+}
+
+void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* dyn, const EdgeOrder& eo,
+                           int num_sms, int blocks_per_sm, cudaStream_t s) {
+    conc_prep_insert<<<num_sms * 16, 256, 0, s>>>(g, ups, 0, eo, dyn);
+    conc_prep_prev<<<num_sms * 16, 256, 0, s>>>(0, eo, dyn);
+    const int occ = conc_apply_occupancy();
+    const int bps = (blocks_per_sm > 0 && blocks_per_sm < occ) ? blocks_per_sm : occ;
+    conc_apply_kernel<<<num_sms * bps, 256, 0, s>>>(g, ups, 0, eo, 0, dyn);
+}
+
+// Stream order per graph, graphs side by side: warp per segment
+// [segs[k], segs[k+1]) of the batch (one graph's updates in submission order),
+// so each graph's result does not depend on the others. The segment count
+// comes from dyn[2].
+__global__ void __launch_bounds__(256) seg_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups,
+                                                        const uint32_t* __restrict__ segs, const uint32_t* dyn) {
+    const uint32_t nseg = ld_cg(dyn + 2);
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < nseg; k += warps) {
+        const uint32_t a = segs[k], e = segs[k + 1];
+        for (uint32_t i = a; i < e; i++) {
+            const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
+            const uint32_t u = r.x, v = r.y;
+            const uint8_t type = (uint8_t)(r.z & 0xFFu);
+            if (u >= g.n || v >= g.n) {
+                if (lane_id() == 0) atomicAdd(g.nskip, 1ull);
+                continue;
+            }
+            warp_apply(g, u, v, type, true);
+        }
+    }
+}
+void launch_seg_apply(const Dev& g, const EdgeUpdate* ups, const uint32_t* segs, const uint32_t* dyn, uint32_t max_segs,
+                      int num_sms, cudaStream_t s) {
+    uint32_t blocks = (max_segs + 7) / 8;
+    if (blocks > (uint32_t)num_sms * 4) blocks = num_sms * 4;
+    seg_apply_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(g, ups, segs, dyn);
 }
 
 // ---------------------------------------------------------------------------
@@ -693,7 +746,8 @@ __global__ void __launch_bounds__(256) indep_items_kernel(Dev g, SweepBufs b) {
         item_bounds(g, b, it, x, s, e);
         const uint32_t hd = __ldg(g.hdmap + x);
         const bool full = hd != EMPTY && g.exact && ~b.acc_bm[x] == 0ull;
-        const unsigned long long rx = sel_rank(x, salt);
+        const uint32_t base = g.gctl[graph_of(g, x)].base;  // ranks use the graph's own ids
+        const unsigned long long rx = sel_rank(x - base, salt);
         bool blocked = false;
         for (uint64_t c = s & ~3ull; c < e; c += 256) {
             const uint64_t i0 = c + 4ull * lane, i1 = i0 + 128;
@@ -713,7 +767,7 @@ __global__ void __launch_bounds__(256) indep_items_kernel(Dev g, SweepBufs b) {
             }
 #pragma unroll
             for (int t = 0; t < 8; t++) {
-                if (nf[t] && sel_rank(v[t], salt) > rx) blocked = true;
+                if (nf[t] && sel_rank(v[t] - base, salt) > rx) blocked = true;
                 if (full && nc[t] > 64 && nc[t] < 2048) atomicOr(&used[nc[t] >> 5], 1u << (nc[t] & 31));
             }
             if (__any_sync(FULL, blocked)) break;  // a blocked row needs nothing more
@@ -749,10 +803,11 @@ __global__ void __launch_bounds__(256) indep_decide_kernel(Dev g, SweepBufs b) {
         bool blocked = false;
         if (len <= SWEEP_TINY) {
             const uint64_t s = g.rp[x];
-            const unsigned long long rx = sel_rank(x, salt);
+            const uint32_t base = g.gctl[graph_of(g, x)].base;  // ranks use the graph's own ids
+            const unsigned long long rx = sel_rank(x - base, salt);
             for (uint32_t j = 0; j < len && !blocked; j++) {
                 const uint32_t y = __ldg(g.col + s + j);
-                if (y < g.n && y != x && __ldg(b.needf + y) && sel_rank(y, salt) > rx) blocked = true;
+                if (y < g.n && y != x && __ldg(b.needf + y) && sel_rank(y - base, salt) > rx) blocked = true;
             }
         } else if (b.acc_fl[x]) {
             blocked = true;

@@ -102,6 +102,15 @@ enum SweepMode : int { SWEEP_REBUILD = 0, SWEEP_TIER1 = 1, SWEEP_INDEP = 2 };
 void launch_det_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, cudaStream_t s);
 void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const EdgeOrder& eo, uint32_t seq,
                        int num_sms, cudaStream_t s);
+// The same with the batch size and sequence number read from device words
+// dyn[0], dyn[1] (replayable in a CUDA graph); fixed grids. blocks_per_sm <= 0:
+// as many resident apply blocks as fit.
+void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* dyn, const EdgeOrder& eo,
+                           int num_sms, int blocks_per_sm, cudaStream_t s);
+int conc_apply_occupancy();
+// One warp per segment [segs[k], segs[k+1]), k < dyn[2]: each segment in stream order.
+void launch_seg_apply(const Dev& g, const EdgeUpdate* ups, const uint32_t* segs, const uint32_t* dyn, uint32_t max_segs,
+                      int num_sms, cudaStream_t s);
 void launch_dirty_list(const Dev& g, uint32_t* list, uint32_t* count, cudaStream_t s);
 // force: compact every listed row (else rows whose holes fill at most a quarter
 // of their extent wait, under exact selection).
