@@ -91,8 +91,17 @@ int sgc_batch_submit(sgc_batch* b, uint32_t graph, const EdgeUpdate* ups, uint32
 uint64_t sgc_batch_pending(const sgc_batch* b);
 /* Applies everything staged, repairs, publishes the graphs whose epoch closed. */
 int sgc_batch_tick(sgc_batch* b, sgc_batch_tick_report* rep);
+/* The same in two halves: begin launches the tick on the batch's stream and
+ * returns; end waits for it (ticks of several batches then overlap on the
+ * device). No submit between them. */
+int sgc_batch_tick_begin(sgc_batch* b);
+int sgc_batch_tick_end(sgc_batch* b, sgc_batch_tick_report* rep);
 /* Publishes every graph's current colors (closes all epochs) on the next tick. */
 int sgc_batch_close_epochs(sgc_batch* b);
+/* Closes one graph's epoch on the next tick. */
+int sgc_batch_close_epoch(sgc_batch* b, uint32_t graph);
+/* Snapshots the graph has published so far. */
+uint64_t sgc_batch_publish_count(const sgc_batch* b, uint32_t graph);
 
 /* Colors from the graph's last published snapshot (safe while a tick runs). */
 int sgc_batch_query(sgc_batch* b, uint32_t graph, const uint32_t* v, uint16_t* out, uint32_t k);

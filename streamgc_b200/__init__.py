@@ -117,6 +117,32 @@ class BatchTuning(C.Structure):
 
 BATCH_FEED = C.CFUNCTYPE(C.c_int, _vp, _vp)
 
+
+class ServerOptions(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("flags", C.c_uint32), ("hbm_budget_bytes", C.c_uint64),
+                ("max_tick_updates", C.c_uint32), ("max_staleness_us", C.c_uint32), ("device", C.c_int32),
+                ("slack_pct", C.c_uint32)]
+
+
+class StepReport(C.Structure):
+    _fields_ = [("admitted", C.c_uint32), ("groups_ticked", C.c_uint32), ("updates", C.c_uint32),
+                ("published", C.c_uint32), ("requests_visible", C.c_uint32), ("proper", C.c_uint32),
+                ("step_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("tenants_resident", C.c_uint64), ("tenants_queued", C.c_uint64), ("groups", C.c_uint64),
+                ("resident_bytes", C.c_uint64), ("budget_bytes", C.c_uint64), ("update_requests", C.c_uint64),
+                ("updates_applied", C.c_uint64), ("requests_visible", C.c_uint64), ("queries", C.c_uint64),
+                ("query_vertices", C.c_uint64), ("visible_p50_ms", C.c_double), ("visible_p99_ms", C.c_double),
+                ("query_p50_ms", C.c_double), ("query_p99_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
 SIGNATURES = {
     "sgc_default_options": (C.c_int, [C.POINTER(_Options)]),
     "sgc_create": (C.c_int, [C.POINTER(_Config), _u32p, _u32p, _u32p, C.POINTER(_vp)]),
@@ -171,6 +197,23 @@ SIGNATURES = {
     "sgc_batch_set_tuning": (C.c_int, [_vp, C.POINTER(BatchTuning)]),
     "sgc_batch_autotune": (C.c_int, [_vp, BATCH_FEED, _vp, C.c_uint32, C.POINTER(BatchTuning)]),
     "sgc_batch_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
+    "sgc_batch_tick_begin": (C.c_int, [_vp]),
+    "sgc_batch_tick_end": (C.c_int, [_vp, C.POINTER(TickReport)]),
+    "sgc_batch_close_epoch": (C.c_int, [_vp, C.c_uint32]),
+    "sgc_batch_publish_count": (C.c_uint64, [_vp, C.c_uint32]),
+    "sgc_server_default_options": (C.c_int, [C.POINTER(ServerOptions)]),
+    "sgc_server_create": (C.c_int, [C.POINTER(ServerOptions), C.POINTER(_vp)]),
+    "sgc_server_destroy": (C.c_int, [_vp]),
+    "sgc_tenant_footprint": (C.c_uint64, [C.c_uint32, C.c_uint64, C.c_uint32]),
+    "sgc_server_add_tenant": (C.c_int, [_vp, C.POINTER(BatchGraph), _u32p]),
+    "sgc_server_remove_tenant": (C.c_int, [_vp, C.c_uint32]),
+    "sgc_server_tenant_state": (C.c_int, [_vp, C.c_uint32]),
+    "sgc_server_submit": (C.c_int, [_vp, C.c_uint32, _vp, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "sgc_server_query": (C.c_int, [_vp, C.c_uint32, _u32p, _u16p, C.c_uint32]),
+    "sgc_server_step": (C.c_int, [_vp, C.POINTER(StepReport)]),
+    "sgc_server_request_visible": (C.c_int, [_vp, C.c_uint64]),
+    "sgc_server_snapshot": (C.c_int, [_vp, C.c_uint32, _u16p]),
+    "sgc_server_get_stats": (C.c_int, [_vp, C.POINTER(ServerStats)]),
 }
 
 
@@ -606,4 +649,91 @@ class Batch:
     def stats(self):
         st = Stats()
         _check(lib().sgc_batch_stats(self.b, C.byref(st)), "sgc_batch_stats")
+        return st.as_dict()
+
+
+TENANT_QUEUED, TENANT_RESIDENT, TENANT_REMOVED = 0, 1, 2
+
+
+class Server:
+    """Request loop over many tenant graphs on one GPU (include/streamgc_server.h).
+    submit() and query() may be called from other threads while step() runs."""
+
+    def __init__(self, hbm_budget_bytes=150 << 30, max_tick_updates=1 << 20, max_staleness_us=0, device=0,
+                 slack_pct=300, cuda_graph=True, stream_order=False):
+        L = lib()
+        opt = ServerOptions()
+        L.sgc_server_default_options(C.byref(opt))
+        opt.hbm_budget_bytes = hbm_budget_bytes
+        opt.max_tick_updates = max_tick_updates
+        opt.max_staleness_us = max_staleness_us
+        opt.device, opt.slack_pct = device, slack_pct
+        opt.flags = (BATCH_CUDA_GRAPH if cuda_graph else 0) | (BATCH_STREAM_ORDER if stream_order else 0)
+        self.s = _vp()
+        _check(L.sgc_server_create(C.byref(opt), C.byref(self.s)), "sgc_server_create")
+        self.n = {}
+
+    def close(self):
+        if getattr(self, "s", None):
+            lib().sgc_server_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @staticmethod
+    def footprint(n, entries, slack_pct=300):
+        return lib().sgc_tenant_footprint(n, entries, slack_pct)
+
+    def add_tenant(self, graph, epoch_size=0, histogram_threshold=0):
+        g = BatchGraph(graph.n, epoch_size, histogram_threshold, 0, _p(graph.row_ptr, _u64p),
+                       _p(graph.col_idx, _u32p), _p(graph.degree, _u32p))
+        t = np.zeros(1, dtype=np.uint32)
+        _check(lib().sgc_server_add_tenant(self.s, C.byref(g), _p(t, _u32p)), "sgc_server_add_tenant")
+        self.n[int(t[0])] = graph.n
+        return int(t[0])
+
+    def remove_tenant(self, t):
+        _check(lib().sgc_server_remove_tenant(self.s, t), "sgc_server_remove_tenant")
+
+    def state(self, t):
+        return lib().sgc_server_tenant_state(self.s, t)
+
+    def submit(self, t, ups):
+        ups = np.ascontiguousarray(ups, dtype=EDGE_UPDATE)
+        rid = C.c_uint64(0)
+        _check(lib().sgc_server_submit(self.s, t, ups.ctypes.data, len(ups), C.byref(rid)), "sgc_server_submit")
+        return rid.value
+
+    def query(self, t, vertices):
+        v = np.ascontiguousarray(vertices, dtype=np.uint32)
+        out = np.zeros(len(v), dtype=np.uint16)
+        _check(lib().sgc_server_query(self.s, t, _p(v, _u32p), _p(out, _u16p), len(v)), "sgc_server_query")
+        return out
+
+    def step(self):
+        r = StepReport()
+        _check(lib().sgc_server_step(self.s, C.byref(r)), "sgc_server_step")
+        return r.as_dict()
+
+    def visible(self, request):
+        return lib().sgc_server_request_visible(self.s, request) == 1
+
+    def snapshot(self, t):
+        out = np.zeros(self.n[t], dtype=np.uint16)
+        _check(lib().sgc_server_snapshot(self.s, t, _p(out, _u16p)), "sgc_server_snapshot")
+        return out
+
+    def stats(self):
+        st = ServerStats()
+        _check(lib().sgc_server_get_stats(self.s, C.byref(st)), "sgc_server_get_stats")
         return st.as_dict()

@@ -97,6 +97,11 @@ struct sgc_batch {
     std::mutex qmu;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint64_t ticks = 0, tier2_ticks = 0;
+    // tick in flight (begin .. end)
+    bool in_tick = false;
+    uint32_t tick_updates = 0, tick_published = 0;
+    std::vector<uint8_t> close_one;    // per graph: close its epoch at the next tick
+    std::vector<uint64_t> publishes;   // per graph: snapshots published so far
 };
 
 namespace {
@@ -340,6 +345,8 @@ int sgc_batch_create(const sgc_batch_graph* graphs, uint32_t count, const sgc_ba
     b->since.assign(count, 0);
     b->pending.assign(count, 0);
     b->front.assign(count, 0);
+    b->close_one.assign(count, 0);
+    b->publishes.assign(count, 0);
     b->per_graph.resize(count);
     // hdmap as created (threshold 32 where tunable) is the index source for re-thresholding
     if (cudaMalloc(&b->d_hdidx, (size_t)n * 4) || cudaMalloc(&b->d_thr, (size_t)count * 4) ||
@@ -384,6 +391,7 @@ uint64_t sgc_batch_pending(const sgc_batch* b) { return b ? b->staged : 0; }
 int sgc_batch_submit(sgc_batch* b, uint32_t graph, const EdgeUpdate* ups, uint32_t n) {
     if (!b || (n && !ups)) return fail(SGC_EINVAL, "null argument");
     if (graph >= b->G) return fail(SGC_EINVAL, "graph %u out of range", graph);
+    if (b->in_tick) return fail(SGC_EINVAL, "submit while a tick runs: end it first");
     if ((uint64_t)b->staged + n > b->cap) return fail(SGC_EINVAL, "tick buffer full (%u updates)", b->cap);
     const uint32_t off = b->voff[graph], lim = b->nv[graph];
     auto translate = [&](const EdgeUpdate& e) {
@@ -410,22 +418,41 @@ int sgc_batch_close_epochs(sgc_batch* b) {
     return SGC_OK;
 }
 
-int sgc_batch_tick(sgc_batch* b, sgc_batch_tick_report* rep) {
+int sgc_batch_close_epoch(sgc_batch* b, uint32_t graph) {
     if (!b) return fail(SGC_EINVAL, "null batch");
+    if (graph >= b->G) return fail(SGC_EINVAL, "graph %u out of range", graph);
+    b->close_one[graph] = 1;
+    return SGC_OK;
+}
+
+uint64_t sgc_batch_publish_count(const sgc_batch* b, uint32_t graph) {
+    return (b && graph < b->G) ? b->publishes[graph] : 0;
+}
+
+int sgc_batch_tick(sgc_batch* b, sgc_batch_tick_report* rep) {
+    TRY(sgc_batch_tick_begin(b));
+    return sgc_batch_tick_end(b, rep);
+}
+
+int sgc_batch_tick_begin(sgc_batch* b) {
+    if (!b) return fail(SGC_EINVAL, "null batch");
+    if (b->in_tick) return fail(SGC_EINVAL, "a tick is already running");
     sgc_handle* h = b->h;
     CK(cudaSetDevice(h->device));
     const uint32_t G = b->G;
     uint32_t published = 0;
     for (uint32_t k = 0; k < G; k++) {
         b->since[k] += b->pending[k];
-        const bool pub = b->close_all || b->since[k] >= b->epoch[k];
+        const bool pub = b->close_all || b->close_one[k] || b->since[k] >= b->epoch[k];
         b->h_target[k] = pub ? (uint8_t)(1 - b->front[k]) : 2;
+        b->close_one[k] = 0;
         if (pub) {
             b->since[k] = 0;
             published++;
         }
     }
     b->close_all = false;
+    b->tick_published = published;
     uint32_t nup = b->staged;
     if (b->flags & SGC_BATCH_STREAM_ORDER) {
         uint32_t pos = 0;
@@ -455,6 +482,20 @@ int sgc_batch_tick(sgc_batch* b, sgc_batch_tick_report* rep) {
         TRY(run_tick_eager(b));
     }
     if (prof) CK(cudaEventRecord(b->ev1, h->stream));
+    b->tick_updates = nup;
+    b->in_tick = true;
+    return SGC_OK;
+}
+
+int sgc_batch_tick_end(sgc_batch* b, sgc_batch_tick_report* rep) {
+    if (!b) return fail(SGC_EINVAL, "null batch");
+    if (!b->in_tick) return fail(SGC_EINVAL, "no tick is running");
+    b->in_tick = false;
+    sgc_handle* h = b->h;
+    CK(cudaSetDevice(h->device));
+    const uint32_t G = b->G;
+    const uint32_t nup = b->tick_updates, published = b->tick_published;
+    const bool prof = (b->flags & SGC_BATCH_PROFILE) != 0;
     CK(cudaStreamSynchronize(h->stream));
     TRY(check_cuda("batch tick"));
     const RepairCtl rc = *h->h_rc_out;
@@ -478,7 +519,10 @@ int sgc_batch_tick(sgc_batch* b, sgc_batch_tick_report* rep) {
     {
         std::lock_guard<std::mutex> lk(b->front_mu);
         for (uint32_t k = 0; k < G; k++)
-            if (b->h_target[k] < 2) b->front[k] = b->h_target[k];
+            if (b->h_target[k] < 2) {
+                b->front[k] = b->h_target[k];
+                b->publishes[k]++;
+            }
     }
     for (uint32_t k = 0; k < G; k++) b->pending[k] = 0;
     b->staged = 0;

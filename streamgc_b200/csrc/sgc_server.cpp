@@ -1,0 +1,440 @@
+// sgc_server.cpp -- the request loop of the served form (include/streamgc_server.h).
+//
+// Host-side scheduling only: tenants live in groups, each group one batched
+// engine (sgc_batch) holding the tenants admitted together. Submissions are
+// held on the host per tenant; a step frees the groups whose tenants all left,
+// admits queued tenants that fit the HBM budget (one new group per step),
+// forwards the held requests to their groups, closes the epochs that reached
+// their staleness deadline, and ticks every group with work: all ticks are
+// launched first and waited for afterwards (with the lock released, so
+// queries and submits go on), so the groups' kernels overlap on the device.
+// Lock order: `life` (group lifetime) before `mu` (tables).
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <shared_mutex>
+#include <vector>
+
+#include "../../include/streamgc_server.h"
+
+namespace sgci {
+int fail(int code, const char* fmt, ...);  // sgc_api.cu: sets the message sgc_last_error() returns
+}
+
+namespace {
+
+int bad(const char* what) { return sgci::fail(SGC_EINVAL, "%s", what); }
+
+using clk = std::chrono::steady_clock;
+
+double ms_since(clk::time_point t0, clk::time_point t1) {
+    return std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
+// Device bytes of a handle per vertex (row offsets, states, bitmaps, maps,
+// sweep and fallback work arrays, two snapshot halves) and per slot, and of a
+// group per update of its tick capacity (staging and same-edge tables).
+constexpr uint64_t kBytesPerVertex = 176;
+constexpr uint64_t kBytesPerSlot = 4;
+constexpr uint64_t kBytesPerTickUpdate = 64;
+
+struct Request {
+    uint64_t id;
+    clk::time_point arrival;
+    uint32_t n;  // updates
+};
+
+struct Tenant {
+    int state = SGC_TENANT_QUEUED;
+    uint32_t n = 0;
+    uint32_t epoch = 0, threshold = 0;
+    std::vector<uint64_t> rp;  // the CSR until the tenant is resident
+    std::vector<uint32_t> col, deg;
+    uint64_t footprint = 0;
+    int group = -1;
+    uint32_t local = 0;
+    std::vector<EdgeUpdate> held;    // submitted, not yet forwarded to the group
+    std::deque<Request> held_reqs;
+    std::deque<Request> waiting;     // forwarded to the group, not yet visible
+    uint64_t seen_publishes = 0;
+};
+
+struct Group {
+    sgc_batch* b = nullptr;
+    std::vector<uint32_t> tenants;   // by local index
+    uint64_t bytes = 0;
+    uint32_t alive = 0;
+    bool has_work = false;
+    bool retired = false;            // all tenants removed: freed at the next step
+};
+
+double pct(std::vector<double> v, double q) {
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    const size_t i = std::min(v.size() - 1, (size_t)(q * (double)(v.size() - 1) + 0.5));
+    return v[i];
+}
+
+}  // namespace
+
+struct sgc_server {
+    sgc_server_options opt{};
+    std::shared_mutex life;  // queries read a group under it; freeing a group excludes them
+    std::mutex mu;
+    std::vector<Tenant> tenants;
+    std::vector<Group> groups;
+    std::deque<uint32_t> queue;      // tenants waiting for admission, in arrival order
+    uint64_t resident_bytes = 0;
+    uint64_t next_request = 1;
+    std::vector<uint8_t> visible;    // by request id
+    std::vector<double> vis_ms, query_ms;
+    uint64_t update_requests = 0, updates_applied = 0, queries = 0, query_vertices = 0;
+};
+
+namespace {
+
+// Moves a resident tenant's held requests, whole and in order, into its
+// group's next tick as far as the tick's capacity allows; the rest waits.
+int forward_held(sgc_server* s, Tenant& t) {
+    if (t.held_reqs.empty()) return SGC_OK;
+    Group& g = s->groups[t.group];
+    const uint64_t room = s->opt.max_tick_updates - sgc_batch_pending(g.b);
+    uint64_t take = 0;
+    size_t k = 0;
+    while (k < t.held_reqs.size() && take + t.held_reqs[k].n <= room) take += t.held_reqs[k++].n;
+    if (k == 0) return SGC_OK;
+    if (take) {
+        const int rc = sgc_batch_submit(g.b, t.local, t.held.data(), (uint32_t)take);
+        if (rc != SGC_OK) return rc;
+        s->updates_applied += take;
+    }
+    for (size_t i = 0; i < k; i++) t.waiting.push_back(t.held_reqs[i]);
+    t.held.erase(t.held.begin(), t.held.begin() + (ptrdiff_t)take);
+    t.held_reqs.erase(t.held_reqs.begin(), t.held_reqs.begin() + (ptrdiff_t)k);
+    g.has_work = true;
+    return SGC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t sgc_tenant_footprint(uint32_t num_vertices, uint64_t num_entries, uint32_t slack_pct) {
+    // rows get max(d + d*slack/100, 8) slots: at least 8 per vertex
+    const uint64_t slots = std::max<uint64_t>(num_entries + num_entries * slack_pct / 100, 8ull * num_vertices);
+    const uint64_t nv = ((uint64_t)num_vertices + 31) & ~31ull;
+    return slots * kBytesPerSlot + nv * kBytesPerVertex + (slots / 256) * 8;
+}
+
+int sgc_server_default_options(sgc_server_options* o) {
+    if (!o) return SGC_EINVAL;
+    std::memset(o, 0, sizeof(*o));
+    o->struct_size = sizeof(sgc_server_options);
+    o->flags = SGC_BATCH_CUDA_GRAPH;
+    o->hbm_budget_bytes = 150ull << 30;
+    o->max_tick_updates = 1u << 20;
+    o->slack_pct = SGC_CSR_EXTRA_SLACK_PCT_DEFAULT;
+    return SGC_OK;
+}
+
+int sgc_server_create(const sgc_server_options* opt, sgc_server** out) {
+    if (!out) return bad("null argument");
+    if (opt && opt->struct_size != sizeof(sgc_server_options)) return bad("sgc_server_options.struct_size mismatch");
+    sgc_server* s = new sgc_server();
+    sgc_server_default_options(&s->opt);
+    if (opt) s->opt = *opt;
+    s->visible.push_back(0);
+    *out = s;
+    return SGC_OK;
+}
+
+int sgc_server_destroy(sgc_server* s) {
+    if (!s) return SGC_OK;
+    for (auto& g : s->groups)
+        if (g.b) sgc_batch_destroy(g.b);
+    delete s;
+    return SGC_OK;
+}
+
+int sgc_server_add_tenant(sgc_server* s, const sgc_batch_graph* g, uint32_t* tenant) {
+    if (!s || !g || !tenant || !g->row_ptr || !g->num_vertices) return bad("null argument or empty graph");
+    const uint64_t m = g->row_ptr[g->num_vertices];
+    if (m && !g->col_idx) return bad("col_idx is null");
+    Tenant t;
+    t.n = g->num_vertices;
+    t.epoch = g->epoch_size;
+    t.threshold = g->histogram_threshold;
+    t.rp.assign(g->row_ptr, g->row_ptr + (size_t)g->num_vertices + 1);
+    if (m) t.col.assign(g->col_idx, g->col_idx + m);
+    if (g->degree) t.deg.assign(g->degree, g->degree + g->num_vertices);
+    std::lock_guard<std::mutex> lk(s->mu);
+    t.footprint = sgc_tenant_footprint(t.n, m, s->opt.slack_pct);
+    *tenant = (uint32_t)s->tenants.size();
+    s->tenants.push_back(std::move(t));
+    s->queue.push_back(*tenant);
+    return SGC_OK;
+}
+
+int sgc_server_tenant_state(sgc_server* s, uint32_t tenant) {
+    if (!s) return SGC_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (tenant >= s->tenants.size()) return bad("tenant out of range");
+    return s->tenants[tenant].state;
+}
+
+int sgc_server_remove_tenant(sgc_server* s, uint32_t tenant) {
+    if (!s) return SGC_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (tenant >= s->tenants.size()) return bad("tenant out of range");
+    Tenant& t = s->tenants[tenant];
+    if (t.state == SGC_TENANT_REMOVED) return SGC_OK;
+    if (t.state == SGC_TENANT_QUEUED) {
+        s->queue.erase(std::remove(s->queue.begin(), s->queue.end(), tenant), s->queue.end());
+    } else {
+        Group& g = s->groups[t.group];
+        if (--g.alive == 0) g.retired = true;  // its memory goes back to the budget at the next step
+    }
+    t.state = SGC_TENANT_REMOVED;
+    std::vector<uint64_t>().swap(t.rp);
+    std::vector<uint32_t>().swap(t.col);
+    std::vector<uint32_t>().swap(t.deg);
+    t.held.clear();
+    t.held_reqs.clear();
+    t.waiting.clear();
+    return SGC_OK;
+}
+
+int sgc_server_submit(sgc_server* s, uint32_t tenant, const EdgeUpdate* ups, uint32_t n, uint64_t* request) {
+    if (!s || (n && !ups)) return bad("null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (tenant >= s->tenants.size()) return bad("tenant out of range");
+    Tenant& t = s->tenants[tenant];
+    if (t.state == SGC_TENANT_REMOVED) return bad("tenant was removed");
+    if (n > s->opt.max_tick_updates) return bad("request larger than max_tick_updates");
+    Request r{s->next_request++, clk::now(), n};
+    s->visible.push_back(0);
+    s->update_requests++;
+    // held on the host until the next step forwards it (a step may be running)
+    t.held.insert(t.held.end(), ups, ups + n);
+    t.held_reqs.push_back(r);
+    if (request) *request = r.id;
+    return SGC_OK;
+}
+
+int sgc_server_query(sgc_server* s, uint32_t tenant, const uint32_t* v, uint16_t* out, uint32_t k) {
+    if (!s || (k && (!v || !out))) return bad("null argument");
+    const auto t0 = clk::now();
+    sgc_batch* b = nullptr;
+    uint32_t local = 0;
+    std::shared_lock<std::shared_mutex> sl(s->life);  // the group stays alive until the answer is back
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (tenant >= s->tenants.size()) return bad("tenant out of range");
+        Tenant& t = s->tenants[tenant];
+        if (t.state == SGC_TENANT_RESIDENT && s->groups[t.group].b) {
+            b = s->groups[t.group].b;
+            local = t.local;
+        }
+    }
+    int rc = SGC_OK;
+    if (b) rc = sgc_batch_query(b, local, v, out, k);
+    else std::memset(out, 0, (size_t)k * 2);  // nothing published yet
+    sl.unlock();
+    const double ms = ms_since(t0, clk::now());
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->queries++;
+    s->query_vertices += k;
+    s->query_ms.push_back(ms);
+    return rc;
+}
+
+int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
+    if (!s) return SGC_EINVAL;
+    const auto t0 = clk::now();
+    {  // 0. groups whose tenants all left: free them
+        std::unique_lock<std::shared_mutex> xl(s->life);
+        std::lock_guard<std::mutex> lk0(s->mu);
+        for (auto& g : s->groups) {
+            if (!g.retired || !g.b) continue;
+            sgc_batch_destroy(g.b);
+            g.b = nullptr;
+            s->resident_bytes -= g.bytes;
+        }
+    }
+    std::unique_lock<std::mutex> lk(s->mu);
+    sgc_server_step_report r{};
+    r.proper = 1;
+    // 1. admission: first come first served against the budget
+    std::vector<uint32_t> admit;
+    uint64_t add_bytes = (uint64_t)s->opt.max_tick_updates * kBytesPerTickUpdate;
+    while (!s->queue.empty()) {
+        const Tenant& t = s->tenants[s->queue.front()];
+        if (s->resident_bytes + add_bytes + t.footprint > s->opt.hbm_budget_bytes) break;
+        add_bytes += t.footprint;
+        admit.push_back(s->queue.front());
+        s->queue.pop_front();
+    }
+    if (!admit.empty()) {
+        std::vector<sgc_batch_graph> gs(admit.size());
+        for (size_t i = 0; i < admit.size(); i++) {
+            Tenant& t = s->tenants[admit[i]];
+            gs[i] = sgc_batch_graph{t.n, t.epoch, t.threshold, 0, t.rp.data(), t.col.empty() ? nullptr : t.col.data(),
+                                    t.deg.empty() ? nullptr : t.deg.data()};
+        }
+        sgc_batch_options bo;
+        sgc_batch_default_options(&bo);
+        bo.slack_pct = s->opt.slack_pct;
+        bo.max_tick_updates = s->opt.max_tick_updates;
+        bo.device = s->opt.device;
+        bo.flags = s->opt.flags;
+        Group g;
+        const int rc = sgc_batch_create(gs.data(), (uint32_t)gs.size(), &bo, &g.b);
+        if (rc != SGC_OK) {  // back to the head of the queue
+            for (auto it = admit.rbegin(); it != admit.rend(); ++it) s->queue.push_front(*it);
+            return rc;
+        }
+        g.tenants = admit;
+        g.bytes = add_bytes;
+        g.alive = (uint32_t)admit.size();
+        g.has_work = true;
+        s->resident_bytes += add_bytes;
+        const int gi = (int)s->groups.size();
+        for (size_t i = 0; i < admit.size(); i++) {
+            Tenant& t = s->tenants[admit[i]];
+            t.state = SGC_TENANT_RESIDENT;
+            t.group = gi;
+            t.local = (uint32_t)i;
+            std::vector<uint64_t>().swap(t.rp);  // the CSR lives on the device now
+            std::vector<uint32_t>().swap(t.col);
+            std::vector<uint32_t>().swap(t.deg);
+        }
+        // the first tick colors the new tenants' graphs and publishes them
+        sgc_batch_close_epochs(g.b);
+        s->groups.push_back(g);
+        r.admitted = (uint32_t)admit.size();
+    }
+    // 2. everything submitted since the last step goes into this step's ticks
+    for (auto& t : s->tenants) {
+        if (t.state != SGC_TENANT_RESIDENT) continue;
+        const int rc = forward_held(s, t);
+        if (rc != SGC_OK) return rc;
+    }
+    // 3. staleness deadlines
+    if (s->opt.max_staleness_us) {
+        const auto now = clk::now();
+        for (auto& t : s->tenants) {
+            if (t.state != SGC_TENANT_RESIDENT || t.waiting.empty()) continue;
+            if (1e3 * ms_since(t.waiting.front().arrival, now) >= (double)s->opt.max_staleness_us) {
+                sgc_batch_close_epoch(s->groups[t.group].b, t.local);
+                s->groups[t.group].has_work = true;
+            }
+        }
+    }
+    // 4. tick every group with work: launch all, then wait for all. Groups are
+    //    created, ticked and freed only by steps, so the batches stay valid
+    //    while the lock is released.
+    std::vector<int> ticking;
+    std::vector<sgc_batch*> tb;
+    for (size_t gi = 0; gi < s->groups.size(); gi++) {
+        Group& g = s->groups[gi];
+        if (!g.b || !g.has_work) continue;
+        const int rc = sgc_batch_tick_begin(g.b);
+        if (rc != SGC_OK) return rc;
+        ticking.push_back((int)gi);
+        tb.push_back(g.b);
+    }
+    std::vector<sgc_batch_tick_report> trs(ticking.size());
+    lk.unlock();
+    int end_rc = SGC_OK;
+    for (size_t i = 0; i < tb.size(); i++) {
+        const int rc = sgc_batch_tick_end(tb[i], &trs[i]);
+        if (rc != SGC_OK && end_rc == SGC_OK) end_rc = rc;
+    }
+    lk.lock();
+    if (end_rc != SGC_OK) return end_rc;
+    const auto now = clk::now();
+    for (size_t i = 0; i < ticking.size(); i++) {
+        Group& g = s->groups[ticking[i]];
+        const sgc_batch_tick_report& tr = trs[i];
+        g.has_work = false;
+        r.groups_ticked++;
+        r.updates += tr.updates;
+        r.published += tr.published;
+        if (!tr.proper) r.proper = 0;
+        for (uint32_t tid : g.tenants) {
+            Tenant& t = s->tenants[tid];
+            if (t.state != SGC_TENANT_RESIDENT) continue;
+            const uint64_t p = sgc_batch_publish_count(g.b, t.local);
+            if (p != t.seen_publishes) {  // everything forwarded so far is in this snapshot
+                t.seen_publishes = p;
+                for (auto& q : t.waiting) {
+                    s->visible[q.id] = 1;
+                    s->vis_ms.push_back(ms_since(q.arrival, now));
+                    r.requests_visible++;
+                }
+                t.waiting.clear();
+            }
+            // a deadline still to come, or requests held back by the capacity, need another tick
+            if ((!t.waiting.empty() && s->opt.max_staleness_us) || !t.held_reqs.empty()) g.has_work = true;
+        }
+    }
+    r.step_ms = ms_since(t0, clk::now());
+    if (rep) *rep = r;
+    return SGC_OK;
+}
+
+int sgc_server_request_visible(sgc_server* s, uint64_t request) {
+    if (!s) return SGC_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    return request < s->visible.size() ? s->visible[request] : 0;
+}
+
+int sgc_server_snapshot(sgc_server* s, uint32_t tenant, uint16_t* out) {
+    if (!s || !out) return SGC_EINVAL;
+    sgc_batch* b = nullptr;
+    uint32_t local = 0, n = 0;
+    std::shared_lock<std::shared_mutex> sl(s->life);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (tenant >= s->tenants.size()) return bad("tenant out of range");
+        Tenant& t = s->tenants[tenant];
+        n = t.n;
+        if (t.state == SGC_TENANT_RESIDENT && s->groups[t.group].b) {
+            b = s->groups[t.group].b;
+            local = t.local;
+        }
+    }
+    if (!b) {
+        std::memset(out, 0, (size_t)n * 2);
+        return SGC_OK;
+    }
+    return sgc_batch_snapshot(b, local, out);
+}
+
+int sgc_server_get_stats(sgc_server* s, sgc_server_stats* o) {
+    if (!s || !o) return SGC_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    std::memset(o, 0, sizeof(*o));
+    for (auto& t : s->tenants) {
+        if (t.state == SGC_TENANT_RESIDENT) o->tenants_resident++;
+        if (t.state == SGC_TENANT_QUEUED) o->tenants_queued++;
+    }
+    for (auto& g : s->groups)
+        if (g.b) o->groups++;
+    o->resident_bytes = s->resident_bytes;
+    o->budget_bytes = s->opt.hbm_budget_bytes;
+    o->update_requests = s->update_requests;
+    o->updates_applied = s->updates_applied;
+    o->requests_visible = s->vis_ms.size();
+    o->queries = s->queries;
+    o->query_vertices = s->query_vertices;
+    o->visible_p50_ms = pct(s->vis_ms, 0.50);
+    o->visible_p99_ms = pct(s->vis_ms, 0.99);
+    o->query_p50_ms = pct(s->query_ms, 0.50);
+    o->query_p99_ms = pct(s->query_ms, 0.99);
+    return SGC_OK;
+}
+
+}  // extern "C"

@@ -26,6 +26,7 @@ def test_library_exports_every_declared_symbol():
     L = S.lib()
     heads = [os.path.join(ROOT, "include", "streamgc_b200.h"),
              os.path.join(ROOT, "include", "streamgc_batch.h"),
+             os.path.join(ROOT, "include", "streamgc_server.h"),
              os.path.join(ROOT, "streamgc_b200", "csrc", "sgc_host.h")]
     for h in heads:
         for name in header_symbols(h):

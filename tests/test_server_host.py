@@ -1,0 +1,37 @@
+"""Host-side rules of the served form that need no GPU: the footprint the
+admission control charges, and the queue before the first step."""
+import pytest
+
+import streamgc_b200 as S
+from tests.golden import make_golden as MG
+
+
+def test_footprint_counts_slack_slots_and_vertex_state():
+    # rows get max(d + 3d, 8) slots of 4 bytes under alpha = 4
+    assert S.Server.footprint(1000, 0) >= 1000 * 8 * 4
+    a = S.Server.footprint(1 << 20, 10 << 20)
+    b = S.Server.footprint(1 << 20, 20 << 20)
+    assert b - a >= 4 * (40 << 20)  # 10M more entries -> 40M more slots of 4 bytes
+    assert S.Server.footprint(1 << 20, 10 << 20, slack_pct=100) < a
+
+
+def test_tenants_queue_until_a_step_and_can_leave():
+    c = MG.build_case("delaunay2k")
+    g = S.Graph(c["rp"], c["col"], c["deg"])
+    srv = S.Server(hbm_budget_bytes=1 << 30, max_tick_updates=1 << 12)
+    try:
+        t0 = srv.add_tenant(g, epoch_size=1024)
+        t1 = srv.add_tenant(g, epoch_size=1024)
+        assert srv.state(t0) == srv.state(t1) == S.TENANT_QUEUED
+        rid = srv.submit(t1, c["bench"][:10])
+        assert rid > 0 and not srv.visible(rid)
+        with pytest.raises(S.StreamGCError, match="max_tick_updates"):
+            srv.submit(t1, c["bench"][:5000])
+        srv.remove_tenant(t0)
+        assert srv.state(t0) == S.TENANT_REMOVED
+        with pytest.raises(S.StreamGCError, match="removed"):
+            srv.submit(t0, c["bench"][:10])
+        st = srv.stats()
+        assert st["tenants_queued"] == 1 and st["tenants_resident"] == 0 and st["update_requests"] == 1
+    finally:
+        srv.close()
