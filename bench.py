@@ -25,6 +25,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -126,14 +127,29 @@ class ClockSampler:
 
 
 def read_traffic():
-    """dram bytes per launch of the sweep kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
-    if os.path.exists(p):
-        try:
-            return json.load(open(p)).get("sweep_dram_bytes_per_sweep")
-        except Exception:
-            return None
+    """DRAM bytes per launch of the sweep's main kernel, from the committed ncu
+    summary (its `sweep_dram_bytes_per_launch` row), if present."""
+    p = os.path.join(ROOT, "profiles", "sweep_items_skewed_rmat20.md")
+    try:
+        for line in open(p):
+            if line.startswith("| sweep_dram_bytes_per_launch |"):
+                return int(line.split("|")[2])
+    except (OSError, ValueError):
+        pass
     return None
+
+
+def max_over_ranks(dist, values, device):
+    """Element-wise maximum of per-rank timings over all ranks (every rank gets it)."""
+    import torch
+    t = torch.tensor(list(values), device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def job_rate(units_per_rank, world, seconds):
+    """Whole-job throughput of `world` replicas timed by the slowest rank."""
+    return world * units_per_rank / seconds
 
 
 def dist_setup():
@@ -223,9 +239,7 @@ def run_ours(a):
         d1 = h.stats()
     total_ms = sum(step_ms)
     if dist:
-        tt = torch.tensor([total_ms, e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms, e2e_s = float(tt[0]), float(tt[1])
+        total_ms, e2e_s = max_over_ranks(dist, [total_ms, e2e_s], f"cuda:{local}")
     val = h.validate()
     cpu = None
     if rank == 0 and world == 1 and a.cpu_batches > 0:
@@ -250,7 +264,7 @@ def run_ours(a):
                     tier2_runs_in_timed=sum(r["tier2_ran"] for r in reps),
                     all_published_proper=all(r["proper"] for r in reps))
         out = {
-            "metric": METRIC, "value": updates / (total_ms / 1e3), "unit": "updates/s", "n_gpus": world,
+            "metric": METRIC, "value": job_rate(a.steps * E, world, total_ms / 1e3), "unit": "updates/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": conf,
             "latency_ms": {"update_to_visible_p50": p50, "update_to_visible_p99": p99},
@@ -481,6 +495,138 @@ def run_batched(a):
     print(json.dumps(out), flush=True)
 
 
+def run_served(a):
+    """Served form: 64 tenants (63 drawn as in the batched form, plus an R-MAT
+    graph with 2^22 vertices and edge factor 16) behind the request loop. Each
+    tenant's update requests arrive as a Poisson process, sizes log-uniform in
+    [1, 32,768], 50/50 insert/delete; single-vertex queries are 20% of the
+    requests. A client thread replays the arrivals in real time (submits and
+    queries), a second thread steps the server; the offered load is
+    `--served-rate` updates/s over `--served-seconds`."""
+    import threading
+    import torch
+    import streamgc_b200 as S
+    from streamgc_b200 import workloads as W
+
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    rate, dur = a.served_rate, a.served_seconds
+    specs = W.batch_specs(63, seed=43)
+    specs.append(dict(index=63, family="rmat22", n=1 << 22, epoch=32768, seed=43 * 100003 + 63))
+    T = len(specs)
+    rng = np.random.default_rng(43)
+    max_b = 32768
+    mean_b = (max_b - 1) / math.log(max_b + 1)
+    req_rate = rate / (T * mean_b)  # update requests per second per tenant
+    events = []
+    need = [0] * T
+    for k in range(T):
+        t_ = 0.0
+        while True:
+            t_ += rng.exponential(1.0 / (req_rate / 0.8))  # updates are 80% of the requests
+            if t_ >= dur:
+                break
+            if rng.random() < 0.2:
+                events.append((t_, k, 0, 0))
+            else:
+                m = int(min(max_b, math.floor(math.exp(rng.uniform(0.0, math.log(max_b + 1))))))
+                m = max(1, m)
+                events.append((t_, k, 1, m))
+                need[k] += m
+    events.sort()
+
+    def stream_len(sp):
+        return need[sp["index"]] + 1
+
+    t = time.time()
+    big = specs[-1]
+    data = W.build_all(specs[:-1], stream_len)
+    g22 = S.Graph.rmat(22, 16, 0.57, 0.19, 0.19, seed=big["seed"])
+    data.append(dict(spec=big, row_ptr=g22.row_ptr, col=g22.col_idx, init=None,
+                     churn=g22.churn_stream(need[63] + 1, 50, big["seed"])))
+    log(f"served: {T} tenants generated in {time.time() - t:.1f}s; {len(events)} requests over {dur}s")
+    srv = S.Server(hbm_budget_bytes=150 << 30, max_tick_updates=1 << 22, max_staleness_us=a.served_staleness_us,
+                   device=local)
+    tids = [srv.add_tenant(S.Graph(d["row_ptr"], d["col"]), epoch_size=d["spec"]["epoch"]) for d in data]
+    t = time.time()
+    r0 = srv.step()  # admission: every tenant colored and published
+    log(f"admitted {r0['admitted']} tenants in {time.time() - t:.1f}s (proper={r0['proper']})")
+    st0 = srv.stats()
+    pos = [0] * T
+    stop = threading.Event()
+    errors = []
+    steps = []
+
+    def stepper():
+        try:
+            while not stop.is_set():
+                r = srv.step()
+                if not r["proper"]:
+                    raise RuntimeError("improper step")
+                if r["groups_ticked"]:
+                    steps.append(r["step_ms"])
+                else:
+                    time.sleep(0.0002)
+        except Exception as e:
+            errors.append(e)
+
+    th = threading.Thread(target=stepper)
+    qv = np.zeros(1, dtype=np.uint32)
+    with ClockSampler(local) as clk:
+        th.start()
+        t0 = time.perf_counter()
+        late = 0.0
+        for (te, k, kind, m) in events:
+            now = time.perf_counter() - t0
+            if te > now:
+                time.sleep(te - now)
+            else:
+                late = max(late, now - te)
+            if kind == 0:
+                qv[0] = rng.integers(0, data[k]["spec"]["n"])
+                srv.query(tids[k], qv)
+            else:
+                ch = data[k]["churn"]
+                srv.submit(tids[k], ch[pos[k]:pos[k] + m])
+                pos[k] += m
+        t_sub = time.perf_counter() - t0
+        deadline = time.time() + 60
+        while time.time() < deadline:  # let every request become visible
+            st = srv.stats()
+            if st["requests_visible"] - st0["requests_visible"] >= st["update_requests"] - st0["update_requests"]:
+                break
+            time.sleep(0.01)
+        t_end = time.perf_counter() - t0
+        stop.set()
+        th.join()
+    if errors:
+        raise SystemExit(f"served run failed: {errors[0]}")
+    st = srv.stats()
+    srv.close()
+    applied = st["updates_applied"] - st0["updates_applied"]
+    ls = sorted(steps)
+    out = {
+        "metric": METRIC, "form": "served", "value": applied / t_end, "unit": "updates/s", "n_gpus": 1,
+        "steps": len(steps), "warmup": 1, "ms_per_step": sum(steps) / max(1, len(steps)), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": "served_64_tenants", "offered_updates_per_s": rate, "seconds": dur,
+                   "tenants": T, "vertices": sum(d["spec"]["n"] for d in data),
+                   "undirected_edges": sum(int(d["row_ptr"][-1]) for d in data) // 2,
+                   "requests": len(events), "queries": sum(1 for e in events if e[2] == 0),
+                   "batch_sizes": "log-uniform [1, 32768]", "max_staleness_us": a.served_staleness_us,
+                   "hbm_budget_gb": 150, "resident_gb": round(st["resident_bytes"] / 2**30, 2),
+                   "client_max_lag_s": round(late, 4), "submit_window_s": round(t_sub, 3)},
+        "latency_ms": {"update_to_visible_p50": st["visible_p50_ms"], "update_to_visible_p99": st["visible_p99_ms"],
+                       "query_p50": st["query_p50_ms"], "query_p99": st["query_p99_ms"],
+                       "step_p50": ls[len(ls) // 2] if ls else None,
+                       "step_p99": ls[min(len(ls) - 1, int(round(0.99 * (len(ls) - 1))))] if ls else None},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -496,6 +642,9 @@ def main():
                     help="plain: one graph (the headline); batched: many graphs per tick; served: request loop")
     ap.add_argument("--batch-graphs", type=int, default=256)
     ap.add_argument("--autotune", action="store_true", help="batched: run the tuner on the warm-up ticks first")
+    ap.add_argument("--served-rate", type=float, default=20e6, help="served: offered updates per second")
+    ap.add_argument("--served-seconds", type=float, default=8.0)
+    ap.add_argument("--served-staleness-us", type=int, default=2000)
     a = ap.parse_args()
     if a.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -503,6 +652,8 @@ def main():
         run_reference(a)
     elif a.form == "batched":
         run_batched(a)
+    elif a.form == "served":
+        run_served(a)
     else:
         run_ours(a)
 

@@ -147,20 +147,19 @@ __device__ __forceinline__ void wait_done(const EdgeOrder& eo, const Dev& g, uin
     __syncwarp();
 }
 
-// Tickets are taken one update ahead, so the ticket's round trip overlaps the
-// current update. A warp's tickets rise, and a predecessor always has a lower
-// index than its successor, so no chain of waits closes on itself. Only an
-// update that a later one of the same edge waits for publishes its done mark.
-__global__ void __launch_bounds__(256, 4) conc_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg,
+// Warp per update, tickets handed out in stream order: a predecessor always
+// has a lower ticket than its successor and was handed out first, so no chain
+// of waits closes on itself. Only an update that a later one of the same edge
+// waits for publishes its done mark (fence + release store).
+__global__ void __launch_bounds__(256) conc_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg,
                                                             EdgeOrder eo, uint32_t seq_arg, const uint32_t* dyn) {
     const uint32_t n = batch_n(n_arg, dyn);
     const uint32_t seq = dyn ? ld_cg(dyn + 1) : seq_arg;
-    uint32_t i = 0;
-    if (lane_id() == 0) i = atomicAdd(eo.ticket, 1u);
-    i = __shfl_sync(FULL, i, 0);
-    while (i < n) {
-        uint32_t inext = 0;
-        if (lane_id() == 0) inext = atomicAdd(eo.ticket, 1u);
+    for (;;) {
+        uint32_t i = 0;
+        if (lane_id() == 0) i = atomicAdd(eo.ticket, 1u);
+        i = __shfl_sync(FULL, i, 0);
+        if (i >= n) break;
         const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
         const uint32_t u = r.x, v = r.y;
         const uint8_t type = (uint8_t)(r.z & 0xFFu);
@@ -183,7 +182,7 @@ __global__ void __launch_bounds__(256, 4) conc_apply_kernel(Dev g, const EdgeUpd
                 }
             }
         }
-        i = __shfl_sync(FULL, inext, 0);
+        __syncwarp();
     }
 }
 

@@ -98,7 +98,8 @@ def test_independent_set_repair_matches_oracle(name):
         it, last, fixed = g.phase_end()
         rep = h.repair()
         assert (rep["tier1_iterations"], rep["tier1_last_count"], rep["tier2_fixed"]) == (it, last, fixed)
-        assert rep["proper"] == 1 and rep["tier2_ran"] == (1 if last else 0)
+        # the loop ends when nothing is left to visit; Tier-2 runs only after 64 unconverged sweeps
+        assert rep["proper"] == 1 and rep["tier2_ran"] == (1 if fixed else 0)
         assert np.array_equal(h.states(), g.states())
         assert np.array_equal(h.bitmaps(), g.bitmaps())
         assert h.validate()["violations"] == 0
