@@ -385,10 +385,11 @@ def run_batched(a):
                      max_batch=max(epochs[k], 1 << 16), device=local, exact_select=True, full_repair_every=0)
           for k, gr in enumerate(graphs)]
     for k, h in enumerate(hs):
-        init = data[k]["init"]
+        init = W.init_stream(data[k])
         for s in range(0, len(init), 1 << 16):
             h.apply(init[s:s + (1 << 16)], S.MODE_CONCURRENT)
         h.publish()
+        del init
     torch.cuda.synchronize()
     log(f"plain arm: {len(hs)} handles created and colored in {time.time() - t:.1f}s")
     plain_ticks, plain_updates, plain_ok = [], 0, True
@@ -417,23 +418,23 @@ def run_batched(a):
     t = time.time()
     cap = max(sum(epochs), 1 << 20)
     b = S.Batch(graphs, epoch_sizes=epochs, max_tick_updates=cap, device=local, profile=True)
-    pos = [0] * len(graphs)
-    while True:  # initial coloring: every graph's init stream, in ticks of at most `cap` updates
-        room, any_left = cap, False
-        for k in range(len(graphs)):
-            init = data[k]["init"]
-            if pos[k] < len(init) and room > 0:
-                m = min(room, len(init) - pos[k])
-                b.submit(k, init[pos[k]:pos[k] + m])
-                pos[k] += m
-                room -= m
-            any_left |= pos[k] < len(data[k]["init"])
-        b.close_epochs()
-        r = b.tick()
-        if not r["proper"]:
-            raise SystemExit("batched init not proper")
-        if not any_left:
-            break
+    room = cap  # initial coloring: every graph's init stream, in ticks of at most `cap` updates
+    for k in range(len(graphs)):
+        init = W.init_stream(data[k])
+        s0 = 0
+        while s0 < len(init):
+            m = min(room, len(init) - s0)
+            b.submit(k, init[s0:s0 + m])
+            s0 += m
+            room -= m
+            if room == 0:
+                if not b.tick()["proper"]:
+                    raise SystemExit("batched init not proper")
+                room = cap
+        del init
+    b.close_epochs()
+    if not b.tick()["proper"]:
+        raise SystemExit("batched init not proper")
     log(f"batched arm: created and colored in {time.time() - t:.1f}s")
     tuning = b.tuning()
     tstate = {"t": 0}
@@ -544,7 +545,7 @@ def run_served(a):
     big = specs[-1]
     data = W.build_all(specs[:-1], stream_len)
     g22 = S.Graph.rmat(22, 16, 0.57, 0.19, 0.19, seed=big["seed"])
-    data.append(dict(spec=big, row_ptr=g22.row_ptr, col=g22.col_idx, init=None,
+    data.append(dict(spec=big, row_ptr=g22.row_ptr, col=g22.col_idx,
                      churn=g22.churn_stream(need[63] + 1, 50, big["seed"])))
     log(f"served: {T} tenants generated in {time.time() - t:.1f}s; {len(events)} requests over {dur}s")
     srv = S.Server(hbm_budget_bytes=150 << 30, max_tick_updates=1 << 22, max_staleness_us=a.served_staleness_us,

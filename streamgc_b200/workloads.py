@@ -63,23 +63,31 @@ def _build(args):
     import streamgc_b200 as S
     rp, col = make_graph(spec)
     g = S.Graph(rp, col)
-    init = g.init_stream()
     m = int(rp[-1]) // 2
     size = min(16 * m, stream_len) if stream_len is not None else 16 * m
-    churn = g.churn_stream(max(size, 0), 50, spec["seed"]) if size > 0 else g.churn_stream(0, 50, spec["seed"])
-    return spec["index"], rp, col, init, churn
+    churn = g.churn_stream(max(size, 0), 50, spec["seed"])
+    return spec["index"], rp, col, churn
 
 
 def build_all(specs, stream_len_of, procs=None):
-    """Graphs and streams for every spec, in worker processes. stream_len_of(spec)
-    bounds each churn stream (the full stream is 16x the graph's edge count).
-    Returns a list of dicts (spec, row_ptr, col, init, churn) in spec order."""
+    """Graphs and churn streams for every spec, in worker processes.
+    stream_len_of(spec) bounds each churn stream (the full stream is 16x the
+    graph's edge count; its prefix is the same). Returns a list of dicts
+    (spec, row_ptr, col, churn) in spec order; a graph's init stream (every
+    edge as an ADD) comes from init_stream(d) when needed."""
     procs = procs or max(1, min(8, (os.cpu_count() or 2)))
     order = sorted(specs, key=lambda s: -s["n"])
     jobs = [(s, stream_len_of(s)) for s in order]
+    pos = {s["index"]: i for i, s in enumerate(specs)}
     out = [None] * len(specs)
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
-        for idx, rp, col, init, churn in pool.imap_unordered(_build, jobs):
-            out[idx] = dict(spec=specs[idx], row_ptr=rp, col=col, init=init, churn=churn)
+        for idx, rp, col, churn in pool.imap_unordered(_build, jobs):
+            out[pos[idx]] = dict(spec=specs[pos[idx]], row_ptr=rp, col=col, churn=churn)
     return out
+
+
+def init_stream(d):
+    """Every edge of a built graph as an ADD, in the reference's init order."""
+    import streamgc_b200 as S
+    return S.Graph(d["row_ptr"], d["col"]).init_stream()
