@@ -71,14 +71,15 @@ __global__ void iota_kernel(uint32_t* out, const uint32_t* count) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) out[i] = i;
 }
 
-// Reverse entries into the list: (y << 32 | x) for x -> y with inL[y].
+// Reverse entries into the list: (y << 32 | x) for x -> y with inL[y]. Counts
+// every entry but stores only `cap`: the host grows the buffer to the count
+// and collects again.
 __global__ void rev_collect_kernel(Dev g, const uint8_t* inL, unsigned long long* keys, uint32_t* count,
                                    uint32_t cap) {
     for_all_entries(g, [&](uint32_t x, uint32_t y) {
         if (y >= g.n || y == x || !inL[y]) return;
         const uint32_t k = atomicAdd(count, 1u);
         if (k < cap) keys[k] = ((unsigned long long)y << 32) | x;
-        else atomicOr(g.err, ERR_LIST_OVERFLOW);
     });
 }
 
@@ -187,6 +188,8 @@ uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, 
         cudaFree(b.rev_keys);
         cudaFree(b.rev_keys2);
         cudaFree(b.cub_tmp);
+        b.rev_keys = b.rev_keys2 = nullptr;
+        b.cub_tmp = nullptr;
         b.rev_cap = nrev + nrev / 4;
         b.cub_tmp_bytes = tier2_cub_bytes(g.n, b.rev_cap);
         if (cudaMalloc(&b.rev_keys, (size_t)b.rev_cap * 8) || cudaMalloc(&b.rev_keys2, (size_t)b.rev_cap * 8) ||
