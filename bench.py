@@ -549,7 +549,7 @@ def run_served(a):
                      churn=g22.churn_stream(need[63] + 1, 50, big["seed"])))
     log(f"served: {T} tenants generated in {time.time() - t:.1f}s; {len(events)} requests over {dur}s")
     srv = S.Server(hbm_budget_bytes=150 << 30, max_tick_updates=1 << 22, max_staleness_us=a.served_staleness_us,
-                   device=local)
+                   device=local, profile=True)
     tids = [srv.add_tenant(S.Graph(d["row_ptr"], d["col"]), epoch_size=d["spec"]["epoch"]) for d in data]
     t = time.time()
     r0 = srv.step()  # admission: every tenant colored and published
@@ -618,7 +618,11 @@ def run_served(a):
                    "requests": len(events), "queries": sum(1 for e in events if e[2] == 0),
                    "batch_sizes": "log-uniform [1, 32768]", "max_staleness_us": a.served_staleness_us,
                    "hbm_budget_gb": 150, "resident_gb": round(st["resident_bytes"] / 2**30, 2),
-                   "client_max_lag_s": round(late, 4), "submit_window_s": round(t_sub, 3)},
+                   "client_max_lag_s": round(late, 4), "submit_window_s": round(t_sub, 3),
+                   "ticks": st["ticks"] - st0["ticks"], "tier2_ticks": st["tier2_ticks"] - st0["tier2_ticks"],
+                   "sweeps_per_tick": round((st["tier1_sweeps"] - st0["tier1_sweeps"]) /
+                                            max(1, st["ticks"] - st0["ticks"]), 2),
+                   "tick_device_ms_total": round(st["tick_device_ms"] - st0["tick_device_ms"], 1)},
         "latency_ms": {"update_to_visible_p50": st["visible_p50_ms"], "update_to_visible_p99": st["visible_p99_ms"],
                        "query_p50": st["query_p50_ms"], "query_p99": st["query_p99_ms"],
                        "step_p50": ls[len(ls) // 2] if ls else None,

@@ -63,6 +63,8 @@ typedef struct sgc_server_stats {
     uint64_t update_requests, updates_applied, requests_visible, queries, query_vertices;
     double   visible_p50_ms, visible_p99_ms;  /* update-to-visible */
     double   query_p50_ms, query_p99_ms;
+    uint64_t ticks, tier1_sweeps, tier2_ticks;  /* group ticks, their repair sweeps, ticks that needed Tier-2 */
+    double   tick_device_ms;                    /* device time of the ticks (SGC_BATCH_PROFILE groups), else 0 */
 } sgc_server_stats;
 
 int sgc_server_default_options(sgc_server_options* opt);

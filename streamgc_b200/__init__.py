@@ -138,7 +138,8 @@ class ServerStats(C.Structure):
                 ("resident_bytes", C.c_uint64), ("budget_bytes", C.c_uint64), ("update_requests", C.c_uint64),
                 ("updates_applied", C.c_uint64), ("requests_visible", C.c_uint64), ("queries", C.c_uint64),
                 ("query_vertices", C.c_uint64), ("visible_p50_ms", C.c_double), ("visible_p99_ms", C.c_double),
-                ("query_p50_ms", C.c_double), ("query_p99_ms", C.c_double)]
+                ("query_p50_ms", C.c_double), ("query_p99_ms", C.c_double), ("ticks", C.c_uint64),
+                ("tier1_sweeps", C.c_uint64), ("tier2_ticks", C.c_uint64), ("tick_device_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -660,7 +661,7 @@ class Server:
     submit() and query() may be called from other threads while step() runs."""
 
     def __init__(self, hbm_budget_bytes=150 << 30, max_tick_updates=1 << 20, max_staleness_us=0, device=0,
-                 slack_pct=300, cuda_graph=True, stream_order=False):
+                 slack_pct=300, cuda_graph=True, stream_order=False, profile=False):
         L = lib()
         opt = ServerOptions()
         L.sgc_server_default_options(C.byref(opt))
@@ -668,7 +669,8 @@ class Server:
         opt.max_tick_updates = max_tick_updates
         opt.max_staleness_us = max_staleness_us
         opt.device, opt.slack_pct = device, slack_pct
-        opt.flags = (BATCH_CUDA_GRAPH if cuda_graph else 0) | (BATCH_STREAM_ORDER if stream_order else 0)
+        opt.flags = (BATCH_CUDA_GRAPH if cuda_graph else 0) | (BATCH_STREAM_ORDER if stream_order else 0) | \
+            (BATCH_PROFILE if profile else 0)
         self.s = _vp()
         _check(L.sgc_server_create(C.byref(opt), C.byref(self.s)), "sgc_server_create")
         self.n = {}

@@ -8,7 +8,8 @@
 // their staleness deadline, and ticks every group with work: all ticks are
 // launched first and waited for afterwards (with the lock released, so
 // queries and submits go on), so the groups' kernels overlap on the device.
-// Lock order: `life` (group lifetime) before `mu` (tables).
+// Lock order: `life` (group lifetime) before `mu` (tables). Tenants removed
+// while their group is being created end when the creation is done.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -59,6 +60,8 @@ struct Tenant {
     std::deque<Request> held_reqs;
     std::deque<Request> waiting;     // forwarded to the group, not yet visible
     uint64_t seen_publishes = 0;
+    bool admitting = false;          // its group is being created (its CSR is in use)
+    bool remove_pending = false;     // removed while admitting: ends once admission is done
 };
 
 struct Group {
@@ -91,31 +94,11 @@ struct sgc_server {
     std::vector<uint8_t> visible;    // by request id
     std::vector<double> vis_ms, query_ms;
     uint64_t update_requests = 0, updates_applied = 0, queries = 0, query_vertices = 0;
+    uint64_t ticks = 0, tier1_sweeps = 0, tier2_ticks = 0;
+    double tick_device_ms = 0;
 };
 
 namespace {
-
-// Moves a resident tenant's held requests, whole and in order, into its
-// group's next tick as far as the tick's capacity allows; the rest waits.
-int forward_held(sgc_server* s, Tenant& t) {
-    if (t.held_reqs.empty()) return SGC_OK;
-    Group& g = s->groups[t.group];
-    const uint64_t room = s->opt.max_tick_updates - sgc_batch_pending(g.b);
-    uint64_t take = 0;
-    size_t k = 0;
-    while (k < t.held_reqs.size() && take + t.held_reqs[k].n <= room) take += t.held_reqs[k++].n;
-    if (k == 0) return SGC_OK;
-    if (take) {
-        const int rc = sgc_batch_submit(g.b, t.local, t.held.data(), (uint32_t)take);
-        if (rc != SGC_OK) return rc;
-        s->updates_applied += take;
-    }
-    for (size_t i = 0; i < k; i++) t.waiting.push_back(t.held_reqs[i]);
-    t.held.erase(t.held.begin(), t.held.begin() + (ptrdiff_t)take);
-    t.held_reqs.erase(t.held_reqs.begin(), t.held_reqs.begin() + (ptrdiff_t)k);
-    g.has_work = true;
-    return SGC_OK;
-}
 
 }  // namespace
 
@@ -190,6 +173,10 @@ int sgc_server_remove_tenant(sgc_server* s, uint32_t tenant) {
     if (tenant >= s->tenants.size()) return bad("tenant out of range");
     Tenant& t = s->tenants[tenant];
     if (t.state == SGC_TENANT_REMOVED) return SGC_OK;
+    if (t.admitting) {  // the step creating its group ends it afterwards
+        t.remove_pending = true;
+        return SGC_OK;
+    }
     if (t.state == SGC_TENANT_QUEUED) {
         s->queue.erase(std::remove(s->queue.begin(), s->queue.end(), tenant), s->queue.end());
     } else {
@@ -250,10 +237,25 @@ int sgc_server_query(sgc_server* s, uint32_t tenant, const uint32_t* v, uint16_t
     return rc;
 }
 
+namespace {
+
+// One tenant's requests moved out of its held buffer by a step.
+struct Forward {
+    sgc_batch* b;
+    uint32_t local;
+    std::vector<EdgeUpdate> ups;
+};
+
+}  // namespace
+
+// The table lock (`mu`) is held only for bookkeeping: creating a group,
+// copying updates into the groups' staging and the ticks themselves run
+// without it. Batches are touched by the stepping thread only (and, for
+// snapshot reads, by queries under `life`).
 int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
     if (!s) return SGC_EINVAL;
     const auto t0 = clk::now();
-    {  // 0. groups whose tenants all left: free them
+    {  // 0. groups whose tenants all left: free them (lock order: life, then mu)
         std::unique_lock<std::shared_mutex> xl(s->life);
         std::lock_guard<std::mutex> lk0(s->mu);
         for (auto& g : s->groups) {
@@ -263,26 +265,30 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
             s->resident_bytes -= g.bytes;
         }
     }
-    std::unique_lock<std::mutex> lk(s->mu);
     sgc_server_step_report r{};
     r.proper = 1;
     // 1. admission: first come first served against the budget
     std::vector<uint32_t> admit;
     uint64_t add_bytes = (uint64_t)s->opt.max_tick_updates * kBytesPerTickUpdate;
-    while (!s->queue.empty()) {
-        const Tenant& t = s->tenants[s->queue.front()];
-        if (s->resident_bytes + add_bytes + t.footprint > s->opt.hbm_budget_bytes) break;
-        add_bytes += t.footprint;
-        admit.push_back(s->queue.front());
-        s->queue.pop_front();
+    std::vector<sgc_batch_graph> gs;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        while (!s->queue.empty()) {
+            Tenant& t = s->tenants[s->queue.front()];
+            if (s->resident_bytes + add_bytes + t.footprint > s->opt.hbm_budget_bytes) break;
+            add_bytes += t.footprint;
+            t.admitting = true;
+            admit.push_back(s->queue.front());
+            s->queue.pop_front();
+        }
+        for (uint32_t tid : admit) {
+            Tenant& t = s->tenants[tid];
+            gs.push_back(sgc_batch_graph{t.n, t.epoch, t.threshold, 0, t.rp.data(),
+                                         t.col.empty() ? nullptr : t.col.data(), t.deg.empty() ? nullptr : t.deg.data()});
+        }
+        if (!admit.empty()) s->resident_bytes += add_bytes;  // reserved while the group is built
     }
     if (!admit.empty()) {
-        std::vector<sgc_batch_graph> gs(admit.size());
-        for (size_t i = 0; i < admit.size(); i++) {
-            Tenant& t = s->tenants[admit[i]];
-            gs[i] = sgc_batch_graph{t.n, t.epoch, t.threshold, 0, t.rp.data(), t.col.empty() ? nullptr : t.col.data(),
-                                    t.deg.empty() ? nullptr : t.deg.data()};
-        }
         sgc_batch_options bo;
         sgc_batch_default_options(&bo);
         bo.slack_pct = s->opt.slack_pct;
@@ -291,77 +297,127 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
         bo.flags = s->opt.flags;
         Group g;
         const int rc = sgc_batch_create(gs.data(), (uint32_t)gs.size(), &bo, &g.b);
+        std::lock_guard<std::mutex> lk(s->mu);
         if (rc != SGC_OK) {  // back to the head of the queue
-            for (auto it = admit.rbegin(); it != admit.rend(); ++it) s->queue.push_front(*it);
+            s->resident_bytes -= add_bytes;
+            for (auto it = admit.rbegin(); it != admit.rend(); ++it) {
+                Tenant& t = s->tenants[*it];
+                t.admitting = false;
+                if (t.remove_pending) {
+                    t.state = SGC_TENANT_REMOVED;
+                    continue;
+                }
+                s->queue.push_front(*it);
+            }
             return rc;
         }
+        sgc_batch_close_epochs(g.b);  // the first tick colors the new tenants' graphs and publishes them
         g.tenants = admit;
         g.bytes = add_bytes;
-        g.alive = (uint32_t)admit.size();
         g.has_work = true;
-        s->resident_bytes += add_bytes;
         const int gi = (int)s->groups.size();
         for (size_t i = 0; i < admit.size(); i++) {
             Tenant& t = s->tenants[admit[i]];
-            t.state = SGC_TENANT_RESIDENT;
+            t.admitting = false;
             t.group = gi;
             t.local = (uint32_t)i;
             std::vector<uint64_t>().swap(t.rp);  // the CSR lives on the device now
             std::vector<uint32_t>().swap(t.col);
             std::vector<uint32_t>().swap(t.deg);
+            if (t.remove_pending) {
+                t.state = SGC_TENANT_REMOVED;
+                t.held.clear();
+                t.held_reqs.clear();
+            } else {
+                t.state = SGC_TENANT_RESIDENT;
+                g.alive++;
+            }
         }
-        // the first tick colors the new tenants' graphs and publishes them
-        sgc_batch_close_epochs(g.b);
+        if (g.alive == 0) g.retired = true;
         s->groups.push_back(g);
         r.admitted = (uint32_t)admit.size();
     }
-    // 2. everything submitted since the last step goes into this step's ticks
-    for (auto& t : s->tenants) {
-        if (t.state != SGC_TENANT_RESIDENT) continue;
-        const int rc = forward_held(s, t);
-        if (rc != SGC_OK) return rc;
-    }
-    // 3. staleness deadlines
-    if (s->opt.max_staleness_us) {
-        const auto now = clk::now();
-        for (auto& t : s->tenants) {
-            if (t.state != SGC_TENANT_RESIDENT || t.waiting.empty()) continue;
-            if (1e3 * ms_since(t.waiting.front().arrival, now) >= (double)s->opt.max_staleness_us) {
-                sgc_batch_close_epoch(s->groups[t.group].b, t.local);
-                s->groups[t.group].has_work = true;
-            }
-        }
-    }
-    // 4. tick every group with work: launch all, then wait for all. Groups are
-    //    created, ticked and freed only by steps, so the batches stay valid
-    //    while the lock is released.
+    // 2. requests submitted since the last step: whole and in order, as far as
+    //    each group's tick capacity allows (the rest waits for the next step)
+    std::vector<Forward> fw;
+    std::vector<sgc_batch*> closes_b;
+    std::vector<uint32_t> closes_l;
     std::vector<int> ticking;
     std::vector<sgc_batch*> tb;
-    for (size_t gi = 0; gi < s->groups.size(); gi++) {
-        Group& g = s->groups[gi];
-        if (!g.b || !g.has_work) continue;
-        const int rc = sgc_batch_tick_begin(g.b);
-        if (rc != SGC_OK) return rc;
-        ticking.push_back((int)gi);
-        tb.push_back(g.b);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        std::vector<uint64_t> room(s->groups.size());
+        for (size_t gi = 0; gi < s->groups.size(); gi++)
+            if (s->groups[gi].b) room[gi] = s->opt.max_tick_updates - sgc_batch_pending(s->groups[gi].b);
+        const auto now = clk::now();
+        for (auto& t : s->tenants) {
+            if (t.state != SGC_TENANT_RESIDENT) continue;
+            Group& g = s->groups[t.group];
+            if (!t.held_reqs.empty()) {
+                uint64_t take = 0;
+                size_t k = 0;
+                while (k < t.held_reqs.size() && take + t.held_reqs[k].n <= room[t.group]) take += t.held_reqs[k++].n;
+                if (k) {
+                    Forward f{g.b, t.local, {}};
+                    if (take == t.held.size()) {
+                        f.ups.swap(t.held);
+                    } else {
+                        f.ups.assign(t.held.begin(), t.held.begin() + (ptrdiff_t)take);
+                        t.held.erase(t.held.begin(), t.held.begin() + (ptrdiff_t)take);
+                    }
+                    room[t.group] -= take;
+                    s->updates_applied += take;
+                    for (size_t i = 0; i < k; i++) t.waiting.push_back(t.held_reqs[i]);
+                    t.held_reqs.erase(t.held_reqs.begin(), t.held_reqs.begin() + (ptrdiff_t)k);
+                    g.has_work = true;
+                    if (!f.ups.empty()) fw.push_back(std::move(f));
+                }
+            }
+            // 3. staleness deadline
+            if (s->opt.max_staleness_us && !t.waiting.empty() &&
+                1e3 * ms_since(t.waiting.front().arrival, now) >= (double)s->opt.max_staleness_us) {
+                closes_b.push_back(g.b);
+                closes_l.push_back(t.local);
+                g.has_work = true;
+            }
+        }
+        for (size_t gi = 0; gi < s->groups.size(); gi++) {
+            Group& g = s->groups[gi];
+            if (!g.b || !g.has_work) continue;
+            ticking.push_back((int)gi);
+            tb.push_back(g.b);
+            g.has_work = false;
+        }
     }
-    std::vector<sgc_batch_tick_report> trs(ticking.size());
-    lk.unlock();
+    // 4. staging copies and ticks without the lock: launch all, then wait for all
+    for (auto& f : fw) {
+        const int rc = sgc_batch_submit(f.b, f.local, f.ups.data(), (uint32_t)f.ups.size());
+        if (rc != SGC_OK) return rc;
+    }
+    for (size_t i = 0; i < closes_b.size(); i++) sgc_batch_close_epoch(closes_b[i], closes_l[i]);
+    for (sgc_batch* b : tb) {
+        const int rc = sgc_batch_tick_begin(b);
+        if (rc != SGC_OK) return rc;
+    }
+    std::vector<sgc_batch_tick_report> trs(tb.size());
     int end_rc = SGC_OK;
     for (size_t i = 0; i < tb.size(); i++) {
         const int rc = sgc_batch_tick_end(tb[i], &trs[i]);
         if (rc != SGC_OK && end_rc == SGC_OK) end_rc = rc;
     }
-    lk.lock();
     if (end_rc != SGC_OK) return end_rc;
+    std::lock_guard<std::mutex> lk(s->mu);
     const auto now = clk::now();
     for (size_t i = 0; i < ticking.size(); i++) {
         Group& g = s->groups[ticking[i]];
         const sgc_batch_tick_report& tr = trs[i];
-        g.has_work = false;
         r.groups_ticked++;
         r.updates += tr.updates;
         r.published += tr.published;
+        s->ticks++;
+        s->tier1_sweeps += tr.tier1_iterations;
+        s->tier2_ticks += tr.tier2_ran;
+        s->tick_device_ms += tr.device_ms;
         if (!tr.proper) r.proper = 0;
         for (uint32_t tid : g.tenants) {
             Tenant& t = s->tenants[tid];
@@ -434,6 +490,10 @@ int sgc_server_get_stats(sgc_server* s, sgc_server_stats* o) {
     o->visible_p99_ms = pct(s->vis_ms, 0.99);
     o->query_p50_ms = pct(s->query_ms, 0.50);
     o->query_p99_ms = pct(s->query_ms, 0.99);
+    o->ticks = s->ticks;
+    o->tier1_sweeps = s->tier1_sweeps;
+    o->tier2_ticks = s->tier2_ticks;
+    o->tick_device_ms = s->tick_device_ms;
     return SGC_OK;
 }
 
