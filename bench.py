@@ -620,6 +620,7 @@ def run_served(a):
                    "hbm_budget_gb": 150, "resident_gb": round(st["resident_bytes"] / 2**30, 2),
                    "client_max_lag_s": round(late, 4), "submit_window_s": round(t_sub, 3),
                    "ticks": st["ticks"] - st0["ticks"], "tier2_ticks": st["tier2_ticks"] - st0["tier2_ticks"],
+                   "tier2_mirror_ticks": st["tier2_mirror_ticks"] - st0["tier2_mirror_ticks"],
                    "sweeps_per_tick": round((st["tier1_sweeps"] - st0["tier1_sweeps"]) /
                                             max(1, st["ticks"] - st0["ticks"]), 2),
                    "tick_device_ms_total": round(st["tick_device_ms"] - st0["tick_device_ms"], 1)},

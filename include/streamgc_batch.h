@@ -67,7 +67,8 @@ typedef struct sgc_batch_tick_report {
     uint32_t tier1_iterations;     /* repair sweeps */
     uint32_t tier2_ran;            /* 1 when the sequential fallback had to run */
     uint32_t proper;               /* 1 when every graph's coloring is proper */
-    uint32_t _pad;
+    uint32_t tier2_reason;         /* bit 0: some graph's rows may miss mirror entries; bit 1: the repair
+                                      did not converge in 64 sweeps (Tier-2 visits only those graphs) */
     double   device_ms;            /* tick time on the device (SGC_BATCH_PROFILE), else 0 */
 } sgc_batch_tick_report;
 

@@ -64,6 +64,7 @@ typedef struct sgc_server_stats {
     double   visible_p50_ms, visible_p99_ms;  /* update-to-visible */
     double   query_p50_ms, query_p99_ms;
     uint64_t ticks, tier1_sweeps, tier2_ticks;  /* group ticks, their repair sweeps, ticks that needed Tier-2 */
+    uint64_t tier2_mirror_ticks;                /* ... of which because some tenant's rows may miss mirror entries */
     double   tick_device_ms;                    /* device time of the ticks (SGC_BATCH_PROFILE groups), else 0 */
 } sgc_server_stats;
 

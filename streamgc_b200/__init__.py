@@ -105,7 +105,8 @@ class BatchOptions(C.Structure):
 
 class TickReport(C.Structure):
     _fields_ = [("updates", C.c_uint32), ("published", C.c_uint32), ("tier1_iterations", C.c_uint32),
-                ("tier2_ran", C.c_uint32), ("proper", C.c_uint32), ("_pad", C.c_uint32), ("device_ms", C.c_double)]
+                ("tier2_ran", C.c_uint32), ("proper", C.c_uint32), ("tier2_reason", C.c_uint32),
+                ("device_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("_")}
@@ -139,7 +140,8 @@ class ServerStats(C.Structure):
                 ("updates_applied", C.c_uint64), ("requests_visible", C.c_uint64), ("queries", C.c_uint64),
                 ("query_vertices", C.c_uint64), ("visible_p50_ms", C.c_double), ("visible_p99_ms", C.c_double),
                 ("query_p50_ms", C.c_double), ("query_p99_ms", C.c_double), ("ticks", C.c_uint64),
-                ("tier1_sweeps", C.c_uint64), ("tier2_ticks", C.c_uint64), ("tick_device_ms", C.c_double)]
+                ("tier1_sweeps", C.c_uint64), ("tier2_ticks", C.c_uint64), ("tier2_mirror_ticks", C.c_uint64),
+                ("tick_device_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -504,7 +504,8 @@ int sgc_batch_tick_end(sgc_batch* b, sgc_batch_tick_report* rep) {
     uint32_t t2 = 0;
     if (!proper) {  // sequential fallback, then publish again
         bool gave_up = false;
-        const uint32_t fixed = run_tier2(h->g, h->t2, h->stream, h->h_small, &gave_up, &h->launches);
+        // only the graphs the repair left unresolved (repair_step_kernel sets GraphCtl.t2)
+        const uint32_t fixed = run_tier2(h->g, h->t2, h->stream, h->h_small, &gave_up, &h->launches, true);
         TRY(check_cuda("batch tier2"));
         h->tier2_runs++;
         h->tier2_fixed += fixed;
@@ -536,6 +537,7 @@ int sgc_batch_tick_end(sgc_batch* b, sgc_batch_tick_report* rep) {
         rep->published = published;
         rep->tier1_iterations = rc.it;
         rep->tier2_ran = t2;
+        rep->tier2_reason = (rc.sym != 0 ? 1u : 0u) | (rc.done ? 0u : 2u);
         rep->proper = proper ? 1 : 0;
         if (prof) {
             float ms = 0;

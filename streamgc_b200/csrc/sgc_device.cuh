@@ -46,7 +46,7 @@ struct GraphCtl {
     uint32_t full;    // the current repair visits every vertex of the graph
     unsigned long long sym;  // mirror checksum of the current repair (full repairs with asym set)
     uint32_t base;    // first vertex of the graph in the handle (ids minus base are the graph's own)
-    uint32_t pad;
+    uint32_t t2;      // the last repair left this graph to Tier-2 (rows missing mirrors, or not converged)
 };
 
 // Device view of one graph's state (handle layout). Row x owns logical slots

@@ -1083,6 +1083,12 @@ __global__ void repair_step_kernel(Dev g, SweepBufs b, cudaGraphConditionalHandl
         for (uint32_t k = threadIdx.x; k < b.G; k += blockDim.x) {
             GraphCtl& c = g.gctl[k];
             c.clean = (done && c.sym == 0) ? 1u : 0u;
+            c.t2 = c.sym != 0 ? 1u : 0u;
+        }
+        __syncthreads();
+        if (!done) {  // the graphs of the vertices still to visit hold the unresolved conflicts
+            const uint32_t nx = *b.wl_count;
+            for (uint32_t i = threadIdx.x; i < nx; i += blockDim.x) g.gctl[graph_of(g, b.wl[i])].t2 = 1;
         }
     }
 }

@@ -162,9 +162,11 @@ struct Tier2Bufs {
     uint32_t* pend_w;
 };
 // Runs the reference's Tier-2 (streamgc.cu:1057-1240) exactly; returns fixes.
-// Rows must be compact (after compaction + drain).
+// Readers skip holes and deleted run entries. `masked`: only the rows of graphs
+// whose GraphCtl.t2 is set (every other graph converged on mirror-complete
+// rows, so Tier-2 would change nothing there).
 uint32_t run_tier2(const Dev& g, Tier2Bufs& b, cudaStream_t s, uint32_t* host_scratch, bool* gave_up,
-                   uint64_t* launches);
+                   uint64_t* launches, bool masked = false);
 size_t tier2_cub_bytes(uint32_t n, uint32_t rev_cap);
 
 // Validator (sgc_tier2.cu): [violations, uncolored_with_edges, distinct_edges, max_color, out_of_range]

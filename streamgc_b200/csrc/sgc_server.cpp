@@ -94,7 +94,7 @@ struct sgc_server {
     std::vector<uint8_t> visible;    // by request id
     std::vector<double> vis_ms, query_ms;
     uint64_t update_requests = 0, updates_applied = 0, queries = 0, query_vertices = 0;
-    uint64_t ticks = 0, tier1_sweeps = 0, tier2_ticks = 0;
+    uint64_t ticks = 0, tier1_sweeps = 0, tier2_ticks = 0, tier2_mirror_ticks = 0;
     double tick_device_ms = 0;
 };
 
@@ -417,6 +417,7 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
         s->ticks++;
         s->tier1_sweeps += tr.tier1_iterations;
         s->tier2_ticks += tr.tier2_ran;
+        s->tier2_mirror_ticks += (tr.tier2_reason & 1u) ? 1 : 0;
         s->tick_device_ms += tr.device_ms;
         if (!tr.proper) r.proper = 0;
         for (uint32_t tid : g.tenants) {
@@ -493,6 +494,7 @@ int sgc_server_get_stats(sgc_server* s, sgc_server_stats* o) {
     o->ticks = s->ticks;
     o->tier1_sweeps = s->tier1_sweeps;
     o->tier2_ticks = s->tier2_ticks;
+    o->tier2_mirror_ticks = s->tier2_mirror_ticks;
     o->tick_device_ms = s->tick_device_ms;
     return SGC_OK;
 }

@@ -33,27 +33,29 @@ namespace {
 __device__ __forceinline__ uint64_t row_s(const Dev& g, uint32_t x) { return g.rp[x]; }
 __device__ __forceinline__ uint64_t row_e(const Dev& g, uint32_t x) { return g.rp[x] + g.hw[x]; }
 
-// Warp per vertex over live rows: f(x, y) for every entry y != INV.
+// Warp per vertex over live rows: f(x, y) for every entry y != INV. masked:
+// only rows of graphs whose GraphCtl.t2 is set.
 template <class F>
-__device__ __forceinline__ void for_all_entries(const Dev& g, F f) {
+__device__ __forceinline__ void for_all_entries(const Dev& g, int masked, F f) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t x = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; x < g.n; x += warps) {
+        if (masked && !g.gctl[graph_of(g, x)].t2) continue;
         warp_for_each(g.col, row_s(g, x), row_e(g, x), [&](uint64_t, uint32_t y) {
             if (y != INV) f(x, y);
         });
     }
 }
 
-__global__ void mark_uncolored_kernel(Dev g, uint8_t* inU) {
-    for_all_entries(g, [&](uint32_t x, uint32_t y) {
+__global__ void mark_uncolored_kernel(Dev g, uint8_t* inU, int masked) {
+    for_all_entries(g, masked, [&](uint32_t x, uint32_t y) {
         if (y >= g.n || y == x) return;
         if (color_of(g.st[x]) == 0) inU[x] = 1;
         if (color_of(g.st[y]) == 0) inU[y] = 1;
     });
 }
 
-__global__ void mark_conflict_kernel(Dev g, uint8_t* inF) {
-    for_all_entries(g, [&](uint32_t x, uint32_t y) {
+__global__ void mark_conflict_kernel(Dev g, uint8_t* inF, int masked) {
+    for_all_entries(g, masked, [&](uint32_t x, uint32_t y) {
         if (y >= g.n || y == x) return;
         const uint16_t a = color_of(g.st[x]), b = color_of(g.st[y]);
         if (a == b && a != 0) inF[x > y ? x : y] = 1;
@@ -75,8 +77,8 @@ __global__ void iota_kernel(uint32_t* out, const uint32_t* count) {
 // every entry but stores only `cap`: the host grows the buffer to the count
 // and collects again.
 __global__ void rev_collect_kernel(Dev g, const uint8_t* inL, unsigned long long* keys, uint32_t* count,
-                                   uint32_t cap) {
-    for_all_entries(g, [&](uint32_t x, uint32_t y) {
+                                   uint32_t cap, int masked) {
+    for_all_entries(g, masked, [&](uint32_t x, uint32_t y) {
         if (y >= g.n || y == x || !inL[y]) return;
         const uint32_t k = atomicAdd(count, 1u);
         if (k < cap) keys[k] = ((unsigned long long)y << 32) | x;
@@ -170,7 +172,8 @@ uint32_t grid_for(uint32_t items, uint32_t per_block) {
 }
 
 // Sequential ascending greedy over the ordered list in b.list (count in b.count[4]).
-uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, uint32_t* hs, uint64_t* nl) {
+uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, uint32_t* hs, uint64_t* nl,
+                        int masked) {
     const uint32_t n = g.n;
     uint32_t* cnt = b.count;  // [0] rem count, [1] next count, [2] fixed, [3] rev count, [4] list count, [5] proc count
     cudaMemsetAsync(b.inL, 0, n, s);
@@ -179,7 +182,7 @@ uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, 
     uint32_t nrev = 0;
     for (int attempt = 0; attempt < 2; attempt++) {
         cudaMemsetAsync(cnt + 3, 0, sizeof(uint32_t), s);
-        rev_collect_kernel<<<148 * 8, 256, 0, s>>>(g, b.inL, b.rev_keys, cnt + 3, b.rev_cap);
+        rev_collect_kernel<<<148 * 8, 256, 0, s>>>(g, b.inL, b.rev_keys, cnt + 3, b.rev_cap, masked);
         cudaMemcpyAsync(hs, cnt + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
         cudaStreamSynchronize(s);
         nrev = hs[0];
@@ -260,25 +263,27 @@ size_t tier2_cub_bytes(uint32_t n, uint32_t rev_cap) {
     return a > c ? a : c;
 }
 
-uint32_t run_tier2(const Dev& g, Tier2Bufs& b, cudaStream_t s, uint32_t* hs, bool* gave_up, uint64_t* launches) {
+uint32_t run_tier2(const Dev& g, Tier2Bufs& b, cudaStream_t s, uint32_t* hs, bool* gave_up, uint64_t* launches,
+                   bool masked) {
+    const int mk = masked ? 1 : 0;
     const uint32_t n = g.n;
     uint32_t total = 0;
     if (gave_up) *gave_up = false;
     // step 1: uncolored vertices with a non-empty adjacency
     cudaMemsetAsync(b.inU, 0, n, s);
-    mark_uncolored_kernel<<<148 * 8, 256, 0, s>>>(g, b.inU);
+    mark_uncolored_kernel<<<148 * 8, 256, 0, s>>>(g, b.inU, mk);
     uint32_t m = select_flagged(n, b, b.inU, s, hs);
     uint64_t nl = 2;
-    if (m) total += ordered_greedy(g, b, m, s, hs, &nl);
+    if (m) total += ordered_greedy(g, b, m, s, hs, &nl, mk);
     // step 2: up to 30 detect / fix passes
     bool clean = false;
     for (int pass = 0; pass < 30; pass++) {
         cudaMemsetAsync(b.inF, 0, n, s);
-        mark_conflict_kernel<<<148 * 8, 256, 0, s>>>(g, b.inF);
+        mark_conflict_kernel<<<148 * 8, 256, 0, s>>>(g, b.inF, mk);
         m = select_flagged(n, b, b.inF, s, hs);
         nl += 2;
         if (!m) { clean = true; break; }
-        const uint32_t fixed = ordered_greedy(g, b, m, s, hs, &nl);
+        const uint32_t fixed = ordered_greedy(g, b, m, s, hs, &nl, mk);
         total += fixed;
         if (!fixed) break;
     }
