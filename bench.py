@@ -355,7 +355,8 @@ def run_batched(a):
     8,192, 32,768}), each with its own churn stream (16x its edge count, the
     first ticks' worth generated). A tick submits one epoch of every graph. The
     same graphs and updates run twice: per-graph plain launches (one handle per
-    graph: apply + publish per epoch) and the batched engine (one tick: one
+    graph, colored by its init stream: apply + publish per epoch) and the
+    batched engine (colored from scratch by its first tick; then one tick = one
     CUDA-graph launch). Both arms are wall-clock timed from host memory."""
     import torch
     import streamgc_b200 as S
@@ -408,6 +409,7 @@ def run_batched(a):
         if t_ >= a.warmup:
             plain_ticks.append(time.perf_counter() - t0)
             plain_updates += n_up
+    log(f"plain arm: {ticks} ticks in {time.time() - t:.1f}s since creation")
     plain_launches = sum(h.stats()["kernel_launches"] for h in hs)
     for h in hs:
         h.close()
@@ -418,20 +420,8 @@ def run_batched(a):
     t = time.time()
     cap = max(sum(epochs), 1 << 20)
     b = S.Batch(graphs, epoch_sizes=epochs, max_tick_updates=cap, device=local, profile=True)
-    room = cap  # initial coloring: every graph's init stream, in ticks of at most `cap` updates
-    for k in range(len(graphs)):
-        init = W.init_stream(data[k])
-        s0 = 0
-        while s0 < len(init):
-            m = min(room, len(init) - s0)
-            b.submit(k, init[s0:s0 + m])
-            s0 += m
-            room -= m
-            if room == 0:
-                if not b.tick()["proper"]:
-                    raise SystemExit("batched init not proper")
-                room = cap
-        del init
+    # the rows hold every edge from creation; the first tick colors all graphs
+    # from scratch and publishes them (as the served form admits tenants)
     b.close_epochs()
     if not b.tick()["proper"]:
         raise SystemExit("batched init not proper")
@@ -496,12 +486,24 @@ def run_batched(a):
     print(json.dumps(out), flush=True)
 
 
+def mirror_checksum(rp, col):
+    """Sum over entries x->y of H(x,y) - H(y,x) (mod 2^64): 0 when every entry has its mirror."""
+    n = len(rp) - 1
+    x = np.repeat(np.arange(n, dtype=np.uint64), np.diff(rp.astype(np.int64)))
+    y = col.astype(np.uint64)
+    with np.errstate(over="ignore"):
+        ha = ((x << np.uint64(32)) | y) * np.uint64(0x9E3779B97F4A7C15)
+        hb = ((y << np.uint64(32)) | x) * np.uint64(0x9E3779B97F4A7C15)
+        d = (ha ^ (ha >> np.uint64(29))).sum(dtype=np.uint64) - (hb ^ (hb >> np.uint64(29))).sum(dtype=np.uint64)
+    return int(d)
+
+
 def run_served(a):
     """Served form: 64 tenants (63 drawn as in the batched form, plus an R-MAT
     graph with 2^22 vertices and edge factor 16) behind the request loop. Each
-    tenant's update requests arrive as a Poisson process, sizes log-uniform in
-    [1, 32,768], 50/50 insert/delete; single-vertex queries are 20% of the
-    requests. A client thread replays the arrivals in real time (submits and
+    tenant's update requests arrive as a Poisson process at a rate proportional
+    to its edge count, sizes log-uniform in [1, 32,768], 50/50 insert/delete;
+    single-vertex queries are 20% of the requests. A client thread replays the arrivals in real time (submits and
     queries), a second thread steps the server; the offered load is
     `--served-rate` updates/s over `--served-seconds`."""
     import threading
@@ -517,13 +519,19 @@ def run_served(a):
     specs = W.batch_specs(63, seed=43)
     specs.append(dict(index=63, family="rmat22", n=1 << 22, epoch=32768, seed=43 * 100003 + 63))
     T = len(specs)
+    t = time.time()
+    big = specs[-1]
+    data = W.build_all(specs[:-1], lambda sp: None, churn_per_edge=(0.5, 1 << 17))
+    g22 = S.Graph.rmat(22, 16, 0.57, 0.19, 0.19, seed=big["seed"])
+    data.append(dict(spec=big, row_ptr=g22.row_ptr, col=g22.col_idx, churn=None))
+    edges = np.array([int(d["row_ptr"][-1]) // 2 for d in data], dtype=np.float64)
     rng = np.random.default_rng(43)
     max_b = 32768
     mean_b = (max_b - 1) / math.log(max_b + 1)
-    req_rate = rate / (T * mean_b)  # update requests per second per tenant
     events = []
     need = [0] * T
     for k in range(T):
+        req_rate = rate * edges[k] / edges.sum() / mean_b  # update requests per second of this tenant
         t_ = 0.0
         while True:
             t_ += rng.exponential(1.0 / (req_rate / 0.8))  # updates are 80% of the requests
@@ -538,15 +546,10 @@ def run_served(a):
                 need[k] += m
     events.sort()
 
-    def stream_len(sp):
-        return need[sp["index"]] + 1
-
-    t = time.time()
-    big = specs[-1]
-    data = W.build_all(specs[:-1], stream_len)
-    g22 = S.Graph.rmat(22, 16, 0.57, 0.19, 0.19, seed=big["seed"])
-    data.append(dict(spec=big, row_ptr=g22.row_ptr, col=g22.col_idx,
-                     churn=g22.churn_stream(need[63] + 1, 50, big["seed"])))
+    data[-1]["churn"] = g22.churn_stream(need[63] + 1, 50, big["seed"])
+    short = [k for k in range(T - 1) if len(data[k]["churn"]) < need[k]]
+    if short:
+        raise SystemExit(f"served: churn streams of tenants {short} are shorter than their offered updates")
     log(f"served: {T} tenants generated in {time.time() - t:.1f}s; {len(events)} requests over {dur}s")
     srv = S.Server(hbm_budget_bytes=150 << 30, max_tick_updates=1 << 22, max_staleness_us=a.served_staleness_us,
                    device=local, profile=True)
@@ -605,6 +608,13 @@ def run_served(a):
     if errors:
         raise SystemExit(f"served run failed: {errors[0]}")
     st = srv.stats()
+    asym = None
+    if a.served_check:  # every tenant's live rows must still hold each entry's mirror
+        asym = []
+        for k in range(T):
+            rp_, col_ = srv.rows(tids[k])
+            if mirror_checksum(rp_, col_):
+                asym.append(k)
     srv.close()
     applied = st["updates_applied"] - st0["updates_applied"]
     ls = sorted(steps)
@@ -619,11 +629,14 @@ def run_served(a):
                    "batch_sizes": "log-uniform [1, 32768]", "max_staleness_us": a.served_staleness_us,
                    "hbm_budget_gb": 150, "resident_gb": round(st["resident_bytes"] / 2**30, 2),
                    "client_max_lag_s": round(late, 4), "submit_window_s": round(t_sub, 3),
+                   "timed_s": round(t_end, 3),
                    "ticks": st["ticks"] - st0["ticks"], "tier2_ticks": st["tier2_ticks"] - st0["tier2_ticks"],
                    "tier2_mirror_ticks": st["tier2_mirror_ticks"] - st0["tier2_mirror_ticks"],
                    "sweeps_per_tick": round((st["tier1_sweeps"] - st0["tier1_sweeps"]) /
                                             max(1, st["ticks"] - st0["ticks"]), 2),
-                   "tick_device_ms_total": round(st["tick_device_ms"] - st0["tick_device_ms"], 1)},
+                   "tick_device_ms_total": round(st["tick_device_ms"] - st0["tick_device_ms"], 1),
+                   "offered_updates": int(sum(need)), "overflows": st["overflows"], "drain_failed": st["drain_failed"],
+                   "device_errors": st["device_errors"], "asymmetric_tenants": asym},
         "latency_ms": {"update_to_visible_p50": st["visible_p50_ms"], "update_to_visible_p99": st["visible_p99_ms"],
                        "query_p50": st["query_p50_ms"], "query_p99": st["query_p99_ms"],
                        "step_p50": ls[len(ls) // 2] if ls else None,
@@ -651,6 +664,7 @@ def main():
     ap.add_argument("--served-rate", type=float, default=20e6, help="served: offered updates per second")
     ap.add_argument("--served-seconds", type=float, default=8.0)
     ap.add_argument("--served-staleness-us", type=int, default=2000)
+    ap.add_argument("--served-check", action="store_true", help="served: check every tenant's rows for mirrors after the run")
     a = ap.parse_args()
     if a.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

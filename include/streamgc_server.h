@@ -66,6 +66,8 @@ typedef struct sgc_server_stats {
     uint64_t ticks, tier1_sweeps, tier2_ticks;  /* group ticks, their repair sweeps, ticks that needed Tier-2 */
     uint64_t tier2_mirror_ticks;                /* ... of which because some tenant's rows may miss mirror entries */
     double   tick_device_ms;                    /* device time of the ticks (SGC_BATCH_PROFILE groups), else 0 */
+    uint64_t overflows, drain_failed;           /* row overflows (pending + lost) and failed drains, all groups */
+    uint64_t device_errors;                     /* groups whose device error word is set */
 } sgc_server_stats;
 
 int sgc_server_default_options(sgc_server_options* opt);
@@ -90,6 +92,9 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep);
 /* 1 once the request's updates are in a published snapshot. */
 int sgc_server_request_visible(sgc_server* s, uint64_t request);
 int sgc_server_snapshot(sgc_server* s, uint32_t tenant, uint16_t* out);
+/* A resident tenant's live rows in its own ids (as sgc_batch_rows); call
+ * between steps. */
+int sgc_server_rows(sgc_server* s, uint32_t tenant, uint64_t* row_ptr, uint32_t* col, uint64_t col_cap);
 int sgc_server_get_stats(sgc_server* s, sgc_server_stats* out);
 
 #ifdef __cplusplus

@@ -141,7 +141,8 @@ class ServerStats(C.Structure):
                 ("query_vertices", C.c_uint64), ("visible_p50_ms", C.c_double), ("visible_p99_ms", C.c_double),
                 ("query_p50_ms", C.c_double), ("query_p99_ms", C.c_double), ("ticks", C.c_uint64),
                 ("tier1_sweeps", C.c_uint64), ("tier2_ticks", C.c_uint64), ("tier2_mirror_ticks", C.c_uint64),
-                ("tick_device_ms", C.c_double)]
+                ("tick_device_ms", C.c_double), ("overflows", C.c_uint64), ("drain_failed", C.c_uint64),
+                ("device_errors", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -217,6 +218,7 @@ SIGNATURES = {
     "sgc_server_request_visible": (C.c_int, [_vp, C.c_uint64]),
     "sgc_server_snapshot": (C.c_int, [_vp, C.c_uint32, _u16p]),
     "sgc_server_get_stats": (C.c_int, [_vp, C.POINTER(ServerStats)]),
+    "sgc_server_rows": (C.c_int, [_vp, C.c_uint32, _u64p, _u32p, C.c_uint64]),
 }
 
 
@@ -736,6 +738,15 @@ class Server:
         out = np.zeros(self.n[t], dtype=np.uint16)
         _check(lib().sgc_server_snapshot(self.s, t, _p(out, _u16p)), "sgc_server_snapshot")
         return out
+
+    def rows(self, t):
+        """A resident tenant's live rows (its own ids): (row_ptr, col). Between steps."""
+        n = self.n[t]
+        rp = np.zeros(n + 1, dtype=np.uint64)
+        _check(lib().sgc_server_rows(self.s, t, _p(rp, _u64p), None, 0), "sgc_server_rows")
+        col = np.zeros(max(int(rp[-1]), 1), dtype=np.uint32)
+        _check(lib().sgc_server_rows(self.s, t, _p(rp, _u64p), _p(col, _u32p), len(col)), "sgc_server_rows")
+        return rp, col[: int(rp[-1])]
 
     def stats(self):
         st = ServerStats()

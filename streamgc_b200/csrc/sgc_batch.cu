@@ -74,7 +74,7 @@ struct sgc_batch {
     uint32_t staged = 0;
     bool close_all = false;
     // per-tick control (device + pinned mirrors)
-    uint32_t* d_dyn = nullptr;   // [0] updates, [1] sequence number, [2] segments
+    uint32_t* d_dyn = nullptr;   // [0] updates, [1] sequence number, [2] segments, [4..5] Tier-2 span
     uint32_t* h_dyn = nullptr;
     uint32_t* d_segs = nullptr;  // G + 1
     uint32_t* h_segs = nullptr;
@@ -350,7 +350,7 @@ int sgc_batch_create(const sgc_batch_graph* graphs, uint32_t count, const sgc_ba
     b->per_graph.resize(count);
     // hdmap as created (threshold 32 where tunable) is the index source for re-thresholding
     if (cudaMalloc(&b->d_hdidx, (size_t)n * 4) || cudaMalloc(&b->d_thr, (size_t)count * 4) ||
-        cudaMalloc(&b->d_dyn, 16) || cudaMalloc(&b->d_segs, ((size_t)count + 1) * 4) || cudaMalloc(&b->d_target, count) ||
+        cudaMalloc(&b->d_dyn, 32) || cudaMalloc(&b->d_segs, ((size_t)count + 1) * 4) || cudaMalloc(&b->d_target, count) ||
         cudaMalloc(&b->d_qv, kQueryCap * 4) || cudaMalloc(&b->d_qout, kQueryCap * 2)) {
         cudaGetLastError();
         return bail(fail(SGC_ENOMEM, "batch control allocation failed"));
@@ -504,8 +504,14 @@ int sgc_batch_tick_end(sgc_batch* b, sgc_batch_tick_report* rep) {
     uint32_t t2 = 0;
     if (!proper) {  // sequential fallback, then publish again
         bool gave_up = false;
-        // only the graphs the repair left unresolved (repair_step_kernel sets GraphCtl.t2)
-        const uint32_t fixed = run_tier2(h->g, h->t2, h->stream, h->h_small, &gave_up, &h->launches, true);
+        // only the graphs the repair left unresolved (repair_step_kernel sets GraphCtl.t2),
+        // over the vertex span from the first to the last of them
+        launch_t2_span(h->g, G, b->d_dyn + 4, h->stream);
+        h->launches++;
+        CK(cudaMemcpyAsync(h->h_small, b->d_dyn + 4, 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        const uint32_t lo = h->h_small[0], hi = h->h_small[1];
+        const uint32_t fixed = run_tier2(h->g, h->t2, h->stream, h->h_small, &gave_up, &h->launches, true, lo, hi);
         TRY(check_cuda("batch tier2"));
         h->tier2_runs++;
         h->tier2_fixed += fixed;

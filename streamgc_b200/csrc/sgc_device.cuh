@@ -34,6 +34,10 @@ enum : uint32_t {
     ERR_WAIT_TIMEOUT = 1u << 0,   // a same-edge predecessor wait ran out
     ERR_BAD_UPDATE = 1u << 1,     // update endpoint outside [0, n)
     ERR_LIST_OVERFLOW = 1u << 2,  // a work list exceeded its capacity
+    ERR_CHAIN = 1u << 3,          // same-edge ordering words inconsistent with the batch (chain past
+                                  // the batch, or an update whose prep record does not match it)
+    ERR_RETRY = 1u << 4,          // a color compare-and-swap kept failing past its retry bound
+    ERR_ROW = 1u << 5,            // a row's high-water mark lay past its capacity (scans clamped)
 };
 
 // Repair flags of one graph of a handle.
@@ -212,6 +216,15 @@ __device__ __forceinline__ void mark_dirty(const Dev& g, uint32_t x) {
     if (!(ld_cg(g.edited + (x >> 5)) & (1u << (x & 31)))) atomicOr(g.edited + (x >> 5), 1u << (x & 31));
 }
 __device__ __forceinline__ uint32_t graph_of(const Dev& g, uint32_t x) { return g.gidw ? __ldg(g.gidw + (x >> 5)) : 0u; }
+// End of the slots of row x that scans visit, [s, s + hw), clamped to the
+// row's capacity (a larger mark sets ERR_ROW).
+__device__ __forceinline__ uint64_t live_end(const Dev& g, uint32_t x, uint64_t s) {
+    const uint64_t e = s + ld_cg(g.hw + x), cap = g.rp[x + 1];
+    if (e <= cap) return e;
+    if (lane_id() == 0) atomicOr(g.err, ERR_ROW);
+    return cap;
+}
+
 __device__ __forceinline__ void flag_asym(const Dev& g, uint32_t x) {
     uint32_t* a = &g.gctl[graph_of(g, x)].asym;
     if (!ld_cg(a)) atomicOr(a, 1u);
@@ -327,7 +340,7 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
     } else if (pristine(g, x)) {
         // Sorted base entries, no holes: the scan would stop at nbr if present,
         // else at the first INV right after the base run.
-        const uint64_t len = ld_cg(g.hw + x);
+        const uint64_t len = live_end(g, x, s) - s;
         if (warp_bsearch(g.col, s, s + len, nbr) != ~0ull) return ADD_PRESENT;
         // Past the sorted run: in stream order nothing else changes the row; in
         // a concurrent batch the updates of this edge are ordered, so nbr can
@@ -374,7 +387,7 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
 // Returns whether an entry was removed.
 __device__ __forceinline__ bool warp_remove_slot(const Dev& g, uint32_t x, uint32_t nbr, bool exact) {
     const uint64_t s = g.rp[x];
-    const uint64_t e = s + ld_cg(g.hw + x);
+    const uint64_t e = live_end(g, x, s);
     uint64_t from = s;
     if (!exact && g.blen) {
         const uint32_t bl = ld_cg(g.blen + x);
@@ -466,7 +479,7 @@ __device__ __forceinline__ uint16_t warp_fac_hist(const uint32_t* h, uint32_t ma
 // Bitmap mode fallback when all 64 bits are set: first color in 1..255 no live
 // neighbor holds (reading neighbor colors from `cols`), else 256.
 __device__ __forceinline__ uint16_t warp_fac_scan(const Dev& g, uint32_t x, const uint32_t* cols) {
-    const uint64_t s = g.rp[x], e = s + ld_cg(g.hw + x);
+    const uint64_t s = g.rp[x], e = live_end(g, x, s);
     uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     warp_gather_each<false>(g.col, s, e, g.n, cols, [&](uint32_t, uint32_t sw) {
         const uint16_t c = color_of(sw);
@@ -498,7 +511,7 @@ __device__ __forceinline__ uint16_t warp_fac_exact(const Dev& g, uint32_t x, con
     used[lane + 32] = 0;
     __syncwarp();
     uint32_t lo = 0, hi = 0;
-    const uint64_t s = g.rp[x], e = s + ld_cg(g.hw + x);
+    const uint64_t s = g.rp[x], e = live_end(g, x, s);
     warp_gather_each<false>(g.col, s, e, g.n, cols, [&](uint32_t, uint32_t sw) {
         const uint16_t c = color_of(sw);
         add_color_bit(c, lo, hi);
@@ -576,18 +589,22 @@ __device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x, uint16_t 
     uint32_t cur = warp_load_state(g, x);
     uint16_t newc = chosen ? chosen : warp_fac(g, x, g.st);
     if (newc == color_of(cur)) return;
-    for (;;) {
+    for (uint32_t tries = 0;; tries++) {
         const uint32_t want = pack(newc, (uint16_t)(version_of(cur) + 1));
         uint32_t got = 0;
         if (lane_id() == 0) got = atomicCAS(g.st + x, cur, want);
         got = __shfl_sync(FULL, got, 0);
         if (got == cur) break;
+        if (tries >= (1u << 20)) {  // the repair after the batch settles x
+            if (lane_id() == 0) atomicOr(g.err, ERR_RETRY);
+            return;
+        }
         cur = got;
         newc = warp_fac(g, x, g.st);
         if (newc == color_of(cur)) return;
     }
     const uint16_t oldc = color_of(cur);
-    const uint64_t s = g.rp[x], e = s + ld_cg(g.hw + x);
+    const uint64_t s = g.rp[x], e = live_end(g, x, s);
     warp_for_each(g.col, s, e, [&](uint64_t, uint32_t ng) {
         if (ng == INV || ng >= g.n) return;
         nbr_color_change(g, ng, oldc, newc);
@@ -598,7 +615,7 @@ __device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x, uint16_t 
 // Warp-collective: does some live neighbor of x hold color c? Stops at the
 // first round that finds one.
 __device__ __forceinline__ bool warp_color_held(const Dev& g, uint32_t x, uint16_t c) {
-    const uint64_t s = g.rp[x], e = s + ld_cg(g.hw + x);
+    const uint64_t s = g.rp[x], e = live_end(g, x, s);
     return warp_gather_each<true>(g.col, s, e, g.n, g.st, [c](uint32_t, uint32_t w) { return color_of(w) == c; });
 }
 

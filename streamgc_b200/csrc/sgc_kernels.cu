@@ -62,7 +62,7 @@ __device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t& total) 
 
 __global__ void __launch_bounds__(32) det_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n) {
     for (uint32_t i = 0; i < n; i++) {
-        const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
+        const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
         const uint32_t u = r.x, v = r.y;
         const uint8_t type = (uint8_t)(r.z & 0xFFu);
         if (u >= g.n || v >= g.n) {
@@ -96,7 +96,7 @@ __global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint
     const uint32_t n = batch_n(n_arg, dyn);
     if (blockIdx.x == 0 && threadIdx.x == 0) *eo.ticket = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
+        const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
         const uint32_t u = r.x, v = r.y;
         const uint8_t type = (uint8_t)(r.z & 0xFFu);
         if ((type != SGC_UPDATE_ADD && type != SGC_UPDATE_DEL) || u >= g.n || v >= g.n) {
@@ -116,28 +116,36 @@ __global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint
     }
 }
 
-__global__ void conc_prep_prev(uint32_t n_arg, EdgeOrder eo, const uint32_t* dyn) {
+__global__ void conc_prep_prev(uint32_t n_arg, EdgeOrder eo, const uint32_t* dyn, uint32_t* err) {
     const uint32_t n = batch_n(n_arg, dyn);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t h = eo.tslot[i];
+        const uint32_t h = ld_cg(eo.tslot + i);
         uint32_t best = NONE32;
         if (h != NONE32) {
-            for (uint32_t j = eo.thead[h]; j != NONE32; j = eo.tnext[j])
+            // a chain holds distinct positions of this batch: at most n links
+            uint32_t links = 0;
+            for (uint32_t j = ld_cg(eo.thead + h); j != NONE32; j = ld_cg(eo.tnext + j)) {
+                if (j >= n || ++links > n) {
+                    atomicOr(err, ERR_CHAIN);
+                    break;
+                }
                 if (j < i && (best == NONE32 || j > best)) best = j;
+            }
         }
         eo.tprev[i] = best;
         if (best != NONE32) eo.succ[best] = 1;  // best's done mark is awaited
     }
 }
 
-// Bounded wait for the same-edge predecessor: ~2^22 polls with a sleep, then
-// the error word records a timeout and the update proceeds.
+// Bounded wait for the same-edge predecessor: 2^16 polls with a sleep (tens
+// of milliseconds; a predecessor takes microseconds), then the error word
+// records a timeout and the update proceeds.
 __device__ __forceinline__ void wait_done(const EdgeOrder& eo, const Dev& g, uint32_t p, uint32_t seq) {
     if (lane_id() == 0) {
         cuda::atomic_ref<uint32_t, cuda::thread_scope_device> d(eo.done[p]);
         uint32_t polls = 0;
         while (d.load(cuda::memory_order_acquire) != seq) {
-            if (++polls > (1u << 22)) {
+            if (++polls > (1u << 16)) {
                 atomicOr(g.err, ERR_WAIT_TIMEOUT);
                 break;
             }
@@ -160,22 +168,29 @@ __global__ void __launch_bounds__(256) conc_apply_kernel(Dev g, const EdgeUpdate
         if (lane_id() == 0) i = atomicAdd(eo.ticket, 1u);
         i = __shfl_sync(FULL, i, 0);
         if (i >= n) break;
-        const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
+        // The batch and the ordering words were written by the copy and the
+        // prep kernels before this launch: L2-coherent loads.
+        const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
         const uint32_t u = r.x, v = r.y;
         const uint8_t type = (uint8_t)(r.z & 0xFFu);
-        const uint32_t h = eo.tslot[i];
+        const uint32_t h = ld_cg(eo.tslot + i);
         if (h == NONE32) {
             if ((u >= g.n || v >= g.n) && lane_id() == 0) atomicAdd(g.nskip, 1ull);
         } else {
-            const uint32_t p = eo.tprev[i];
-            if (p != NONE32) wait_done(eo, g, p, seq);
-            warp_apply(g, u, v, type, false);
+            const uint32_t p = ld_cg(eo.tprev + i);
+            if (u >= g.n || v >= g.n || h > eo.tmask || (p != NONE32 && p >= i)) {
+                // the prep kernels saw a different update here: record it, apply nothing
+                if (lane_id() == 0) atomicOr(g.err, ERR_CHAIN);
+            } else {
+                if (p != NONE32) wait_done(eo, g, p, seq);
+                warp_apply(g, u, v, type, false);
+            }
         }
         if (lane_id() == 0) {
-            if (h != NONE32) {  // no kernel reads the table during apply: reset it for the next batch
+            if (h != NONE32 && h <= eo.tmask) {  // no kernel reads the table during apply: reset it for the next batch
                 eo.tkey[h] = EMPTY64;
                 eo.thead[h] = NONE32;
-                if (eo.succ[i]) {
+                if (__ldcg(eo.succ + i)) {
                     __threadfence();
                     cuda::atomic_ref<uint32_t, cuda::thread_scope_device> d(eo.done[i]);
                     d.store(seq, cuda::memory_order_release);
@@ -205,7 +220,7 @@ void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const Ed
     uint32_t blk = (n + 255) / 256;
     if (blk > (uint32_t)num_sms * 16) blk = num_sms * 16;
     conc_prep_insert<<<blk, 256, 0, s>>>(g, ups, n, eo, nullptr);
-    conc_prep_prev<<<blk, 256, 0, s>>>(n, eo, nullptr);
+    conc_prep_prev<<<blk, 256, 0, s>>>(n, eo, nullptr, g.err);
     uint32_t grid = (uint32_t)(num_sms * conc_apply_occupancy());
     const uint32_t need = (n + 7) / 8;  // 8 warps per block
     if (grid > need) grid = need;
@@ -215,7 +230,7 @@ void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const Ed
 void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* dyn, const EdgeOrder& eo,
                            int num_sms, int blocks_per_sm, cudaStream_t s) {
     conc_prep_insert<<<num_sms * 16, 256, 0, s>>>(g, ups, 0, eo, dyn);
-    conc_prep_prev<<<num_sms * 16, 256, 0, s>>>(0, eo, dyn);
+    conc_prep_prev<<<num_sms * 16, 256, 0, s>>>(0, eo, dyn, g.err);
     const int occ = conc_apply_occupancy();
     const int bps = (blocks_per_sm > 0 && blocks_per_sm < occ) ? blocks_per_sm : occ;
     conc_apply_kernel<<<num_sms * bps, 256, 0, s>>>(g, ups, 0, eo, 0, dyn);
@@ -232,7 +247,7 @@ __global__ void __launch_bounds__(256) seg_apply_kernel(Dev g, const EdgeUpdate*
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < nseg; k += warps) {
         const uint32_t a = segs[k], e = segs[k + 1];
         for (uint32_t i = a; i < e; i++) {
-            const uint4 r = __ldg(reinterpret_cast<const uint4*>(ups + i));
+            const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
             const uint32_t u = r.x, v = r.y;
             const uint8_t type = (uint8_t)(r.z & 0xFFu);
             if (u >= g.n || v >= g.n) {

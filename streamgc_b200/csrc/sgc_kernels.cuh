@@ -165,8 +165,17 @@ struct Tier2Bufs {
 // Readers skip holes and deleted run entries. `masked`: only the rows of graphs
 // whose GraphCtl.t2 is set (every other graph converged on mirror-complete
 // rows, so Tier-2 would change nothing there).
+// Vertices [lo, hi) that a Tier-2 pass visits (whole graphs); masked: only
+// graphs whose GraphCtl.t2 is set.
+struct Tier2Span {
+    uint32_t lo, hi;
+    int masked;
+};
 uint32_t run_tier2(const Dev& g, Tier2Bufs& b, cudaStream_t s, uint32_t* host_scratch, bool* gave_up,
-                   uint64_t* launches, bool masked = false);
+                   uint64_t* launches, bool masked = false, uint32_t lo = 0, uint32_t hi = 0xFFFFFFFFu);
+// [first vertex, end) of the graphs whose GraphCtl.t2 is set, into span[0..1]
+// ({n, 0} when none); one block.
+void launch_t2_span(const Dev& g, uint32_t G, uint32_t* span, cudaStream_t s);
 size_t tier2_cub_bytes(uint32_t n, uint32_t rev_cap);
 
 // Validator (sgc_tier2.cu): [violations, uncolored_with_edges, distinct_edges, max_color, out_of_range]

@@ -470,6 +470,15 @@ int sgc_server_snapshot(sgc_server* s, uint32_t tenant, uint16_t* out) {
     return sgc_batch_snapshot(b, local, out);
 }
 
+int sgc_server_rows(sgc_server* s, uint32_t tenant, uint64_t* row_ptr, uint32_t* col, uint64_t col_cap) {
+    if (!s || !row_ptr) return bad("null argument");
+    std::lock_guard<std::mutex> lk(s->mu);  // excludes steps' bookkeeping; the rows are read between ticks
+    if (tenant >= s->tenants.size()) return bad("tenant out of range");
+    Tenant& t = s->tenants[tenant];
+    if (t.state != SGC_TENANT_RESIDENT || !s->groups[t.group].b) return bad("tenant is not resident");
+    return sgc_batch_rows(s->groups[t.group].b, t.local, row_ptr, col, col_cap);
+}
+
 int sgc_server_get_stats(sgc_server* s, sgc_server_stats* o) {
     if (!s || !o) return SGC_EINVAL;
     std::lock_guard<std::mutex> lk(s->mu);
@@ -478,8 +487,15 @@ int sgc_server_get_stats(sgc_server* s, sgc_server_stats* o) {
         if (t.state == SGC_TENANT_RESIDENT) o->tenants_resident++;
         if (t.state == SGC_TENANT_QUEUED) o->tenants_queued++;
     }
-    for (auto& g : s->groups)
-        if (g.b) o->groups++;
+    for (auto& g : s->groups) {
+        if (!g.b) continue;
+        o->groups++;
+        sgc_stats bs;
+        const int rc = sgc_batch_stats(g.b, &bs);
+        o->overflows += bs.overflow_pending + bs.overflow_lost;
+        o->drain_failed += bs.drain_failed;
+        if (rc != SGC_OK || bs.device_error) o->device_errors++;
+    }
     o->resident_bytes = s->resident_bytes;
     o->budget_bytes = s->opt.hbm_budget_bytes;
     o->update_requests = s->update_requests;

@@ -33,29 +33,31 @@ namespace {
 __device__ __forceinline__ uint64_t row_s(const Dev& g, uint32_t x) { return g.rp[x]; }
 __device__ __forceinline__ uint64_t row_e(const Dev& g, uint32_t x) { return g.rp[x] + g.hw[x]; }
 
-// Warp per vertex over live rows: f(x, y) for every entry y != INV. masked:
-// only rows of graphs whose GraphCtl.t2 is set.
+// Warp per vertex over the live rows of the vertices in [sp.lo, sp.hi): f(x, y)
+// for every entry y != INV. With sp.masked only rows of graphs whose
+// GraphCtl.t2 is set. A span always covers whole graphs, so every neighbor of
+// a visited vertex lies inside it too.
 template <class F>
-__device__ __forceinline__ void for_all_entries(const Dev& g, int masked, F f) {
+__device__ __forceinline__ void for_all_entries(const Dev& g, Tier2Span sp, F f) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t x = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; x < g.n; x += warps) {
-        if (masked && !g.gctl[graph_of(g, x)].t2) continue;
+    for (uint32_t x = sp.lo + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); x < sp.hi; x += warps) {
+        if (sp.masked && !g.gctl[graph_of(g, x)].t2) continue;
         warp_for_each(g.col, row_s(g, x), row_e(g, x), [&](uint64_t, uint32_t y) {
             if (y != INV) f(x, y);
         });
     }
 }
 
-__global__ void mark_uncolored_kernel(Dev g, uint8_t* inU, int masked) {
-    for_all_entries(g, masked, [&](uint32_t x, uint32_t y) {
+__global__ void mark_uncolored_kernel(Dev g, uint8_t* inU, Tier2Span sp) {
+    for_all_entries(g, sp, [&](uint32_t x, uint32_t y) {
         if (y >= g.n || y == x) return;
         if (color_of(g.st[x]) == 0) inU[x] = 1;
         if (color_of(g.st[y]) == 0) inU[y] = 1;
     });
 }
 
-__global__ void mark_conflict_kernel(Dev g, uint8_t* inF, int masked) {
-    for_all_entries(g, masked, [&](uint32_t x, uint32_t y) {
+__global__ void mark_conflict_kernel(Dev g, uint8_t* inF, Tier2Span sp) {
+    for_all_entries(g, sp, [&](uint32_t x, uint32_t y) {
         if (y >= g.n || y == x) return;
         const uint16_t a = color_of(g.st[x]), b = color_of(g.st[y]);
         if (a == b && a != 0) inF[x > y ? x : y] = 1;
@@ -77,8 +79,8 @@ __global__ void iota_kernel(uint32_t* out, const uint32_t* count) {
 // every entry but stores only `cap`: the host grows the buffer to the count
 // and collects again.
 __global__ void rev_collect_kernel(Dev g, const uint8_t* inL, unsigned long long* keys, uint32_t* count,
-                                   uint32_t cap, int masked) {
-    for_all_entries(g, masked, [&](uint32_t x, uint32_t y) {
+                                   uint32_t cap, Tier2Span sp) {
+    for_all_entries(g, sp, [&](uint32_t x, uint32_t y) {
         if (y >= g.n || y == x || !inL[y]) return;
         const uint32_t k = atomicAdd(count, 1u);
         if (k < cap) keys[k] = ((unsigned long long)y << 32) | x;
@@ -164,6 +166,12 @@ __global__ void __launch_bounds__(256) greedy_round_kernel(Dev g, const uint32_t
     }
 }
 
+// Warp per vertex of the span, at most 8 blocks per SM.
+uint32_t span_grid(Tier2Span sp) {
+    const uint32_t b = (sp.hi - sp.lo + 7) / 8;
+    return b < 1 ? 1 : (b > 148 * 8 ? 148 * 8 : b);
+}
+
 uint32_t grid_for(uint32_t items, uint32_t per_block) {
     uint32_t b = (items + per_block - 1) / per_block;
     if (b < 1) b = 1;
@@ -173,16 +181,15 @@ uint32_t grid_for(uint32_t items, uint32_t per_block) {
 
 // Sequential ascending greedy over the ordered list in b.list (count in b.count[4]).
 uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, uint32_t* hs, uint64_t* nl,
-                        int masked) {
-    const uint32_t n = g.n;
+                        Tier2Span sp) {
     uint32_t* cnt = b.count;  // [0] rem count, [1] next count, [2] fixed, [3] rev count, [4] list count, [5] proc count
-    cudaMemsetAsync(b.inL, 0, n, s);
-    cudaMemsetAsync(b.done, 0, n, s);
+    cudaMemsetAsync(b.inL + sp.lo, 0, sp.hi - sp.lo, s);
+    cudaMemsetAsync(b.done + sp.lo, 0, sp.hi - sp.lo, s);
     set_flags_kernel<<<grid_for(m, 256), 256, 0, s>>>(b.list, cnt + 4, b.inL, 1);
     uint32_t nrev = 0;
     for (int attempt = 0; attempt < 2; attempt++) {
         cudaMemsetAsync(cnt + 3, 0, sizeof(uint32_t), s);
-        rev_collect_kernel<<<148 * 8, 256, 0, s>>>(g, b.inL, b.rev_keys, cnt + 3, b.rev_cap, masked);
+        rev_collect_kernel<<<span_grid(sp), 256, 0, s>>>(g, b.inL, b.rev_keys, cnt + 3, b.rev_cap, sp);
         cudaMemcpyAsync(hs, cnt + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
         cudaStreamSynchronize(s);
         nrev = hs[0];
@@ -242,17 +249,44 @@ uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, 
     return hs[0];
 }
 
-// Ordered selection of flagged vertex ids into b.list; count to b.count[4].
-uint32_t select_flagged(uint32_t n, Tier2Bufs& b, const uint8_t* flags, cudaStream_t s, uint32_t* hs) {
+// Ordered selection of the flagged vertex ids of the span into b.list; count to b.count[4].
+uint32_t select_flagged(Tier2Span sp, Tier2Bufs& b, const uint8_t* flags, cudaStream_t s, uint32_t* hs) {
     size_t tb = b.cub_tmp_bytes;
-    thrust::counting_iterator<uint32_t> it(0);
-    cub::DeviceSelect::Flagged(b.cub_tmp, tb, it, flags, b.list, b.count + 4, (int)n, s);
+    thrust::counting_iterator<uint32_t> it(sp.lo);
+    cub::DeviceSelect::Flagged(b.cub_tmp, tb, it, flags + sp.lo, b.list, b.count + 4, (int)(sp.hi - sp.lo), s);
     cudaMemcpyAsync(hs, b.count + 4, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     return hs[0];
 }
 
 }  // namespace
+
+namespace {
+
+__global__ void t2_span_kernel(const GraphCtl* gc, uint32_t G, uint32_t n, uint32_t* span) {
+    __shared__ uint32_t lo, hi;
+    if (threadIdx.x == 0) {
+        lo = n;
+        hi = 0;
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < G; k += blockDim.x)
+        if (gc[k].t2) {
+            atomicMin(&lo, gc[k].base);
+            atomicMax(&hi, k + 1 < G ? gc[k + 1].base : n);
+        }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        span[0] = lo;
+        span[1] = hi;
+    }
+}
+
+}  // namespace
+
+void launch_t2_span(const Dev& g, uint32_t G, uint32_t* span, cudaStream_t s) {
+    t2_span_kernel<<<1, 256, 0, s>>>(g.gctl, G, g.n, span);
+}
 
 size_t tier2_cub_bytes(uint32_t n, uint32_t rev_cap) {
     size_t a = 0, c = 0;
@@ -264,26 +298,27 @@ size_t tier2_cub_bytes(uint32_t n, uint32_t rev_cap) {
 }
 
 uint32_t run_tier2(const Dev& g, Tier2Bufs& b, cudaStream_t s, uint32_t* hs, bool* gave_up, uint64_t* launches,
-                   bool masked) {
-    const int mk = masked ? 1 : 0;
-    const uint32_t n = g.n;
+                   bool masked, uint32_t lo, uint32_t hi) {
+    Tier2Span sp{lo, hi < g.n ? hi : g.n, masked ? 1 : 0};
     uint32_t total = 0;
     if (gave_up) *gave_up = false;
+    if (sp.lo >= sp.hi) return 0;
+    const uint32_t nsp = sp.hi - sp.lo;
     // step 1: uncolored vertices with a non-empty adjacency
-    cudaMemsetAsync(b.inU, 0, n, s);
-    mark_uncolored_kernel<<<148 * 8, 256, 0, s>>>(g, b.inU, mk);
-    uint32_t m = select_flagged(n, b, b.inU, s, hs);
+    cudaMemsetAsync(b.inU + sp.lo, 0, nsp, s);
+    mark_uncolored_kernel<<<span_grid(sp), 256, 0, s>>>(g, b.inU, sp);
+    uint32_t m = select_flagged(sp, b, b.inU, s, hs);
     uint64_t nl = 2;
-    if (m) total += ordered_greedy(g, b, m, s, hs, &nl, mk);
+    if (m) total += ordered_greedy(g, b, m, s, hs, &nl, sp);
     // step 2: up to 30 detect / fix passes
     bool clean = false;
     for (int pass = 0; pass < 30; pass++) {
-        cudaMemsetAsync(b.inF, 0, n, s);
-        mark_conflict_kernel<<<148 * 8, 256, 0, s>>>(g, b.inF, mk);
-        m = select_flagged(n, b, b.inF, s, hs);
+        cudaMemsetAsync(b.inF + sp.lo, 0, nsp, s);
+        mark_conflict_kernel<<<span_grid(sp), 256, 0, s>>>(g, b.inF, sp);
+        m = select_flagged(sp, b, b.inF, s, hs);
         nl += 2;
         if (!m) { clean = true; break; }
-        const uint32_t fixed = ordered_greedy(g, b, m, s, hs, &nl, mk);
+        const uint32_t fixed = ordered_greedy(g, b, m, s, hs, &nl, sp);
         total += fixed;
         if (!fixed) break;
     }
