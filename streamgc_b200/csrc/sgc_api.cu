@@ -155,7 +155,8 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep, bool force_full) {
     h->launches += (mode == SWEEP_INDEP && h->g.touched) ? 2 : 1;
     const bool prof = (h->opt.flags & SGC_OPT_PROFILE) != 0;
     RepairCtl* rc = h->h_rc_out;
-    for (;;) {
+    for (uint32_t sweeps = 0;; sweeps++) {
+        if (sweeps > hin->max_sweeps) return fail(SGC_EDEVICE, "repair loop ran past %u sweeps", hin->max_sweeps);
         cudaEvent_t a = nullptr, b = nullptr;
         if (prof) {
             a = take_event(h);
@@ -424,8 +425,7 @@ int sgci::create_internal(const StreamGCConfig* cfg, const sgc_options* opt_in, 
     A(&eo.tslot, mb);
     A(&eo.tnext, mb);
     A(&eo.tprev, mb);
-    A(&eo.done, mb, 0);
-    A(&eo.succ, mb, 0);
+    A(&eo.tsucc, mb);
     eo.ticket = &h->ctl->ticket;
     eo.tmask = tsize - 1;
     // sweep buffers
@@ -542,12 +542,7 @@ int sgc_apply(sgc_handle* h, const EdgeUpdate* ups, uint32_t n, int mode) {
         launch_det_apply(h->g, src, n, h->stream);
         h->launches += 1;
     } else {
-        h->seq++;
-        if (h->seq == 0) {  // wrapped: clear the done marks before reuse
-            CK(cudaMemsetAsync(h->eo.done, 0, (size_t)h->opt.max_batch * 4, h->stream));
-            h->seq = 1;
-        }
-        launch_conc_apply(h->g, src, n, h->eo, h->seq, h->num_sms, h->stream);
+        launch_conc_apply(h->g, src, n, h->eo, h->num_sms, h->stream);
         h->launches += 3;
     }
     h->last_mode = mode;

@@ -3,9 +3,9 @@
 // The graphs share one handle: their rows sit side by side in one slack CSR
 // (graph k's vertex ids are offset by voff[k], a multiple of 32, so every
 // 32-vertex word belongs to one graph and gidw maps words to graphs). A tick
-//   1. bumps the batch sequence number and applies the staged updates in one
-//      persistent launch fed by the device ticket queue (or, in stream-order
-//      mode, one warp per graph walks that graph's updates in order);
+//   1. applies the staged updates in one persistent launch fed by the device
+//      ticket queue, a warp per edge (or, in stream-order mode, one warp per
+//      graph walks that graph's updates in order);
 //   2. compacts edited rows and drains the overflow buffer;
 //   3. repairs with the independent-set rule, each graph starting from its
 //      touched vertices (or from all of them when its repair must be full);
@@ -29,11 +29,6 @@ using namespace sgc;
 using namespace sgci;
 
 namespace {
-
-__global__ void bump_seq_kernel(uint32_t* dyn) {
-    dyn[1] += 1;
-    if (dyn[1] == 0) dyn[1] = 1;  // the done marks start at 0: never reuse it
-}
 
 // Writes the colors of every graph whose target is 0 or 1 into that half of
 // the snapshot double buffer. Thread per vertex.
@@ -74,7 +69,7 @@ struct sgc_batch {
     uint32_t staged = 0;
     bool close_all = false;
     // per-tick control (device + pinned mirrors)
-    uint32_t* d_dyn = nullptr;   // [0] updates, [1] sequence number, [2] segments, [4..5] Tier-2 span
+    uint32_t* d_dyn = nullptr;   // [0] updates, [2] segments, [4..5] Tier-2 span
     uint32_t* h_dyn = nullptr;
     uint32_t* d_segs = nullptr;  // G + 1
     uint32_t* h_segs = nullptr;
@@ -123,7 +118,6 @@ void drop_graph(sgc_batch* b) {
 // Everything of a tick before the repair loop.
 void enqueue_head(sgc_batch* b, cudaStream_t s) {
     sgc_handle* h = b->h;
-    bump_seq_kernel<<<1, 1, 0, s>>>(b->d_dyn);
     if (b->flags & SGC_BATCH_STREAM_ORDER)
         launch_seg_apply(h->g, h->d_batch, b->d_segs, b->d_dyn, b->G, h->num_sms, s);
     else

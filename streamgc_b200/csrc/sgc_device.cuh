@@ -31,7 +31,7 @@ constexpr uint32_t TOMB = 0x80000000u;  // tombstone bit of a deleted base-run e
 
 // Error bits written to the handle's device error word.
 enum : uint32_t {
-    ERR_WAIT_TIMEOUT = 1u << 0,   // a same-edge predecessor wait ran out
+    ERR_RESERVED0 = 1u << 0,      // not set (formerly a same-edge wait timeout)
     ERR_BAD_UPDATE = 1u << 1,     // update endpoint outside [0, n)
     ERR_LIST_OVERFLOW = 1u << 2,  // a work list exceeded its capacity
     ERR_CHAIN = 1u << 3,          // same-edge ordering words inconsistent with the batch (chain past

@@ -65,7 +65,6 @@ struct sgc_handle {
     EdgeUpdate* h_stage = nullptr;  // pinned staging for pageable inputs
     cudaEvent_t stage_free = nullptr;
     sgc::EdgeOrder eo{};
-    uint32_t seq = 0;
     sgc::SweepBufs sb{};
     uint32_t* dirty_list = nullptr;
     sgc::Tier2Bufs t2{};

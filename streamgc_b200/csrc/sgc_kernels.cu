@@ -86,9 +86,9 @@ __device__ __forceinline__ uint32_t key_hash(unsigned long long k) {
     return (uint32_t)k;
 }
 
-// `dyn` (device words, optional): [0] the batch size, [1] the batch sequence
-// number; they replace the `n` / `seq` arguments so that a captured CUDA graph
-// can replay the launches on every tick. Grid-stride loops.
+// `dyn` (device words, optional): [0] the batch size; it replaces the `n`
+// argument so that a captured CUDA graph can replay the launches on every
+// tick. Grid-stride loops.
 __device__ __forceinline__ uint32_t batch_n(uint32_t n, const uint32_t* dyn) { return dyn ? ld_cg(dyn) : n; }
 
 __global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg, EdgeOrder eo,
@@ -103,7 +103,6 @@ __global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint
             eo.tslot[i] = NONE32;
             continue;
         }
-        eo.succ[i] = 0;
         const unsigned long long key = edge_key(u, v);
         uint32_t h = key_hash(key) & eo.tmask;
         for (uint32_t probe = 0; probe <= eo.tmask; probe++) {
@@ -116,86 +115,68 @@ __global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint
     }
 }
 
+// Per update: the previous and the next update of the same edge in stream
+// order (NONE32 at the ends), from the slot's push list.
 __global__ void conc_prep_prev(uint32_t n_arg, EdgeOrder eo, const uint32_t* dyn, uint32_t* err) {
     const uint32_t n = batch_n(n_arg, dyn);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t h = ld_cg(eo.tslot + i);
-        uint32_t best = NONE32;
+        uint32_t prev = NONE32, next = NONE32;
         if (h != NONE32) {
-            // a chain holds distinct positions of this batch: at most n links
+            // a list holds distinct positions of this batch: at most n links
             uint32_t links = 0;
             for (uint32_t j = ld_cg(eo.thead + h); j != NONE32; j = ld_cg(eo.tnext + j)) {
                 if (j >= n || ++links > n) {
                     atomicOr(err, ERR_CHAIN);
                     break;
                 }
-                if (j < i && (best == NONE32 || j > best)) best = j;
+                if (j < i && (prev == NONE32 || j > prev)) prev = j;
+                if (j > i && (next == NONE32 || j < next)) next = j;
             }
         }
-        eo.tprev[i] = best;
-        if (best != NONE32) eo.succ[best] = 1;  // best's done mark is awaited
+        eo.tprev[i] = prev;
+        eo.tsucc[i] = next;
     }
 }
 
-// Bounded wait for the same-edge predecessor: 2^16 polls with a sleep (tens
-// of milliseconds; a predecessor takes microseconds), then the error word
-// records a timeout and the update proceeds.
-__device__ __forceinline__ void wait_done(const EdgeOrder& eo, const Dev& g, uint32_t p, uint32_t seq) {
-    if (lane_id() == 0) {
-        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> d(eo.done[p]);
-        uint32_t polls = 0;
-        while (d.load(cuda::memory_order_acquire) != seq) {
-            if (++polls > (1u << 16)) {
-                atomicOr(g.err, ERR_WAIT_TIMEOUT);
-                break;
-            }
-            __nanosleep(64);
-        }
-    }
-    __syncwarp();
-}
-
-// Warp per update, tickets handed out in stream order: a predecessor always
-// has a lower ticket than its successor and was handed out first, so no chain
-// of waits closes on itself. Only an update that a later one of the same edge
-// waits for publishes its done mark (fence + release store).
+// Warp per edge: a warp takes tickets (update positions) and, when the update
+// is the first of its edge in the batch, applies every update of that edge in
+// stream order; the later ones are skipped at their own tickets. So the
+// updates of one edge never run concurrently and no warp waits for another.
+// The batch and the ordering words were written by the copy and the prep
+// kernels before this launch: L2-coherent loads.
 __global__ void __launch_bounds__(256) conc_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg,
-                                                            EdgeOrder eo, uint32_t seq_arg, const uint32_t* dyn) {
+                                                            EdgeOrder eo, const uint32_t* dyn) {
     const uint32_t n = batch_n(n_arg, dyn);
-    const uint32_t seq = dyn ? ld_cg(dyn + 1) : seq_arg;
     for (;;) {
         uint32_t i = 0;
         if (lane_id() == 0) i = atomicAdd(eo.ticket, 1u);
         i = __shfl_sync(FULL, i, 0);
         if (i >= n) break;
-        // The batch and the ordering words were written by the copy and the
-        // prep kernels before this launch: L2-coherent loads.
-        const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
-        const uint32_t u = r.x, v = r.y;
-        const uint8_t type = (uint8_t)(r.z & 0xFFu);
         const uint32_t h = ld_cg(eo.tslot + i);
         if (h == NONE32) {
-            if ((u >= g.n || v >= g.n) && lane_id() == 0) atomicAdd(g.nskip, 1ull);
-        } else {
-            const uint32_t p = ld_cg(eo.tprev + i);
-            if (u >= g.n || v >= g.n || h > eo.tmask || (p != NONE32 && p >= i)) {
-                // the prep kernels saw a different update here: record it, apply nothing
-                if (lane_id() == 0) atomicOr(g.err, ERR_CHAIN);
-            } else {
-                if (p != NONE32) wait_done(eo, g, p, seq);
-                warp_apply(g, u, v, type, false);
-            }
+            const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
+            if ((r.x >= g.n || r.y >= g.n) && lane_id() == 0) atomicAdd(g.nskip, 1ull);
+            continue;
         }
-        if (lane_id() == 0) {
-            if (h != NONE32 && h <= eo.tmask) {  // no kernel reads the table during apply: reset it for the next batch
-                eo.tkey[h] = EMPTY64;
-                eo.thead[h] = NONE32;
-                if (__ldcg(eo.succ + i)) {
-                    __threadfence();
-                    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> d(eo.done[i]);
-                    d.store(seq, cuda::memory_order_release);
-                }
+        if (ld_cg(eo.tprev + i) != NONE32) continue;  // applied with the first update of its edge
+        uint32_t steps = 0;
+        for (uint32_t j = i; j != NONE32; j = ld_cg(eo.tsucc + j)) {
+            if (j >= n || j < i || ++steps > n) {  // ordering words inconsistent with the batch
+                if (lane_id() == 0) atomicOr(g.err, ERR_CHAIN);
+                break;
             }
+            const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + j));
+            const uint32_t u = r.x, v = r.y;
+            if (u >= g.n || v >= g.n) {
+                if (lane_id() == 0) atomicOr(g.err, ERR_CHAIN);
+                break;
+            }
+            warp_apply(g, u, v, (uint8_t)(r.z & 0xFFu), false);
+        }
+        if (lane_id() == 0 && h <= eo.tmask) {  // no kernel reads the table during apply: reset it for the next batch
+            eo.tkey[h] = EMPTY64;
+            eo.thead[h] = NONE32;
         }
         __syncwarp();
     }
@@ -214,8 +195,8 @@ int conc_apply_occupancy() {
     return occ;
 }
 
-void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const EdgeOrder& eo, uint32_t seq,
-                       int num_sms, cudaStream_t s) {
+void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const EdgeOrder& eo, int num_sms,
+                       cudaStream_t s) {
     if (!n) return;
     uint32_t blk = (n + 255) / 256;
     if (blk > (uint32_t)num_sms * 16) blk = num_sms * 16;
@@ -224,7 +205,7 @@ void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const Ed
     uint32_t grid = (uint32_t)(num_sms * conc_apply_occupancy());
     const uint32_t need = (n + 7) / 8;  // 8 warps per block
     if (grid > need) grid = need;
-    conc_apply_kernel<<<grid, 256, 0, s>>>(g, ups, n, eo, seq, nullptr);
+    conc_apply_kernel<<<grid, 256, 0, s>>>(g, ups, n, eo, nullptr);
 }
 
 void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* dyn, const EdgeOrder& eo,
@@ -233,7 +214,7 @@ void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* 
     conc_prep_prev<<<num_sms * 16, 256, 0, s>>>(0, eo, dyn, g.err);
     const int occ = conc_apply_occupancy();
     const int bps = (blocks_per_sm > 0 && blocks_per_sm < occ) ? blocks_per_sm : occ;
-    conc_apply_kernel<<<num_sms * bps, 256, 0, s>>>(g, ups, 0, eo, 0, dyn);
+    conc_apply_kernel<<<num_sms * bps, 256, 0, s>>>(g, ups, 0, eo, dyn);
 }
 
 // Stream order per graph, graphs side by side: warp per segment

@@ -86,8 +86,7 @@ struct EdgeOrder {
     uint32_t* tslot;           // per update: its key slot (NONE32 = not an edge op)
     uint32_t* tnext;           // per update: next in the key's push list
     uint32_t* tprev;           // per update: previous update of the same edge (stream order)
-    uint32_t* done;            // per update: batch sequence number once applied (when awaited)
-    uint8_t* succ;             // per update: a later update of the same edge waits for it
+    uint32_t* tsucc;           // per update: next update of the same edge (stream order)
     uint32_t* ticket;          // work ticket of the persistent apply kernel
     uint32_t tmask;            // table size - 1
 };
@@ -100,10 +99,10 @@ enum SweepMode : int { SWEEP_REBUILD = 0, SWEEP_TIER1 = 1, SWEEP_INDEP = 2 };
 
 // ---- launchers (sgc_kernels.cu) ----
 void launch_det_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, cudaStream_t s);
-void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const EdgeOrder& eo, uint32_t seq,
-                       int num_sms, cudaStream_t s);
-// The same with the batch size and sequence number read from device words
-// dyn[0], dyn[1] (replayable in a CUDA graph); fixed grids. blocks_per_sm <= 0:
+void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const EdgeOrder& eo, int num_sms,
+                       cudaStream_t s);
+// The same with the batch size read from the device word dyn[0] (replayable
+// in a CUDA graph); fixed grids. blocks_per_sm <= 0:
 // as many resident apply blocks as fit.
 void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* dyn, const EdgeOrder& eo,
                            int num_sms, int blocks_per_sm, cudaStream_t s);

@@ -103,6 +103,41 @@ __global__ void rev_bounds_kernel(const uint32_t* list, const uint32_t* count, c
     }
 }
 
+// Greedy color of list vertex v from its row and its reverse entries
+// rkeys[r0, r1): the smallest color in 1..1023 no neighbor holds (version + 1
+// when it changes). Warp-collective; `used` is the warp's 32-word scratch.
+__device__ __forceinline__ void greedy_color(const Dev& g, uint32_t v, const unsigned long long* rkeys, uint32_t r0,
+                                             uint32_t r1, uint32_t* used, uint32_t* fixed) {
+    const uint32_t lane = lane_id();
+    used[lane] = 0;
+    __syncwarp();
+    auto mark = [&](uint32_t w) {
+        if (w == INV || w >= g.n || w == v) return;
+        const uint16_t nc = color_of(ld_cg(g.st + w));
+        if (nc != 0 && nc < 1024) atomicOr(&used[nc >> 5], 1u << (nc & 31));
+    };
+    warp_for_each(g.col, row_s(g, v), row_e(g, v), [&](uint64_t, uint32_t w) { mark(w); });
+    for (uint32_t t = r0 + lane; t < r1; t += 32) mark((uint32_t)rkeys[t]);
+    __syncwarp();
+    uint32_t freew = ~used[lane];
+    if (lane == 0) freew &= ~1u;  // color 0 is not a candidate
+    const uint32_t bal = __ballot_sync(FULL, freew != 0);
+    uint32_t c = 0;
+    if (bal) {
+        const int src = __ffs(bal) - 1;
+        const uint32_t bit = __shfl_sync(FULL, __ffs(freew) - 1, src);
+        c = (uint32_t)src * 32 + bit;
+    }
+    if (lane == 0) {
+        const uint32_t w = ld_cg(g.st + v);
+        if (c != 0 && c != color_of(w)) {
+            g.st[v] = pack((uint16_t)c, (uint16_t)(version_of(w) + 1));
+            atomicAdd(fixed, 1u);
+        }
+    }
+    __syncwarp();
+}
+
 // One round: warp per remaining list position. Ready vertices greedy-recolor
 // in place and are listed as processed; the rest carry over.
 __global__ void __launch_bounds__(256) greedy_round_kernel(Dev g, const uint32_t* L, const uint32_t* rem,
@@ -135,34 +170,23 @@ __global__ void __launch_bounds__(256) greedy_round_kernel(Dev g, const uint32_t
             __syncwarp();
             continue;
         }
-        used[lane] = 0;
+        greedy_color(g, v, rkeys, rs[pos], re[pos], used, fixed);
+        if (lane == 0) proc[atomicAdd(proc_count, 1u)] = v;
         __syncwarp();
-        auto mark = [&](uint32_t w) {
-            if (w == INV || w >= g.n || w == v) return;
-            const uint16_t nc = color_of(ld_cg(g.st + w));
-            if (nc != 0 && nc < 1024) atomicOr(&used[nc >> 5], 1u << (nc & 31));
-        };
-        warp_for_each(g.col, row_s(g, v), row_e(g, v), [&](uint64_t, uint32_t w) { mark(w); });
-        for (uint32_t t = rs[pos] + lane; t < re[pos]; t += 32) mark((uint32_t)rkeys[t]);
-        __syncwarp();
-        uint32_t freew = ~used[lane];
-        if (lane == 0) freew &= ~1u;  // color 0 is not a candidate
-        const uint32_t bal = __ballot_sync(FULL, freew != 0);
-        uint32_t c = 0;
-        if (bal) {
-            const int src = __ffs(bal) - 1;
-            const uint32_t bit = __shfl_sync(FULL, __ffs(freew) - 1, src);
-            c = (uint32_t)src * 32 + bit;
-        }
-        if (lane == 0) {
-            const uint32_t w = ld_cg(g.st + v);
-            if (c != 0 && c != color_of(w)) {
-                g.st[v] = pack((uint16_t)c, (uint16_t)(version_of(w) + 1));
-                atomicAdd(fixed, 1u);
-            }
-            proc[atomicAdd(proc_count, 1u)] = v;
-        }
-        __syncwarp();
+    }
+}
+
+// One warp, after the round cap: the list positions still pending, in
+// ascending order (every lower-id list neighbor is final when a vertex is
+// reached, as in the rounds).
+__global__ void __launch_bounds__(32) greedy_tail_kernel(Dev g, const uint32_t* L, uint32_t m, const uint8_t* done,
+                                                         const unsigned long long* rkeys, const uint32_t* rs,
+                                                         const uint32_t* re, uint32_t* fixed) {
+    __shared__ uint32_t used[32];
+    for (uint32_t pos = 0; pos < m; pos++) {
+        const uint32_t v = L[pos];
+        if (done[v]) continue;
+        greedy_color(g, v, rkeys, rs[pos], re[pos], used, fixed);
     }
 }
 
@@ -171,6 +195,10 @@ uint32_t span_grid(Tier2Span sp) {
     const uint32_t b = (sp.hi - sp.lo + 7) / 8;
     return b < 1 ? 1 : (b > 148 * 8 ? 148 * 8 : b);
 }
+
+// Host-synchronized rounds of the ordered greedy before the rest of the list
+// goes to one warp in order (the same result, bounded time).
+constexpr uint32_t kMaxRounds = 1024;
 
 uint32_t grid_for(uint32_t items, uint32_t per_block) {
     uint32_t b = (items + per_block - 1) / per_block;
@@ -228,7 +256,7 @@ uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, 
     iota_kernel<<<grid_for(m, 256), 256, 0, s>>>(rem, cnt + 0);
     cudaMemsetAsync(cnt + 2, 0, sizeof(uint32_t), s);
     uint32_t left = m;
-    for (uint32_t round = 0; round < m && left; round++) {
+    for (uint32_t round = 0; round < m && round < kMaxRounds && left; round++) {
         cudaMemsetAsync(cnt + 1, 0, sizeof(uint32_t), s);
         cudaMemsetAsync(cnt + 5, 0, sizeof(uint32_t), s);
         greedy_round_kernel<<<grid_for(left, 8), 256, 0, s>>>(g, b.list, rem, cnt + 0, nxt, cnt + 1, proc, cnt + 5,
@@ -243,6 +271,10 @@ uint32_t ordered_greedy(const Dev& g, Tier2Bufs& b, uint32_t m, cudaStream_t s, 
         uint32_t* t = rem;
         rem = nxt;
         nxt = t;
+    }
+    if (left) {  // round cap reached: the rest in order on one warp
+        greedy_tail_kernel<<<1, 32, 0, s>>>(g, b.list, m, b.done, b.rev_keys, b.rev_start, b.rev_end, cnt + 2);
+        *nl += 1;
     }
     cudaMemcpyAsync(hs, cnt + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
