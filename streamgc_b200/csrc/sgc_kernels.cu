@@ -3,12 +3,12 @@
 //   det_apply_kernel      one warp applies a batch in stream order: the
 //                         reference's local_update_kernel run as a single warp
 //                         (local_update.cu:61-147), bit-exact.
-//   conc_*                a batch applied by one warp per update. A hash pre-pass
-//                         links each update to the previous update of the same
-//                         edge in the batch, and the persistent apply kernel hands
-//                         out updates in stream order and waits (bounded) for
-//                         that predecessor, so every edge sees its own updates in
-//                         stream order and the edge set after a batch equals the
+//   conc_*                a batch applied by one warp per edge. A hash pre-pass
+//                         links each update to the previous and the next update
+//                         of the same edge in the batch; the persistent apply
+//                         kernel hands out update tickets and the first update
+//                         of each edge applies that edge's updates in stream
+//                         order, so the edge set after a batch equals the
 //                         sequential one; updates of different edges overlap.
 //   dirty list + compact  stable per-row compaction (epoch_maintenance.cu:20-61)
 //                         of only the rows edited since their last compaction
