@@ -147,6 +147,24 @@ def max_over_ranks(dist, values, device):
     return [float(x) for x in t]
 
 
+def sum_over_ranks(dist, values, device):
+    """Element-wise sum of per-rank counts over all ranks (every rank gets it)."""
+    import torch
+    t = torch.tensor(list(values), device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return [float(x) for x in t]
+
+
+def init_dist(world):
+    """The process group of a multi-rank run (NCCL, short timeout), else None."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
 def job_rate(units_per_rank, world, seconds):
     """Whole-job throughput of `world` replicas timed by the slowest rank."""
     return world * units_per_rank / seconds
@@ -362,14 +380,20 @@ def run_batched(a):
     import streamgc_b200 as S
     from streamgc_b200 import workloads as W
 
+    from streamgc_b200 import placement as P
+
     world, rank, local = dist_setup()
-    if rank != 0:
-        return
     torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    dist = init_dist(world)
     ticks = a.warmup + a.steps
-    specs = W.batch_specs(a.batch_graphs, seed=42)
+    specs_all = W.batch_specs(a.batch_graphs, seed=42)
+    # independent graphs: each rank holds a share balanced by resident bytes
+    share = P.place([P.spec_footprint(sp) for sp in specs_all], world)[rank]
+    specs = [specs_all[i] for i in share]
     t = time.time()
-    data = W.build_all(specs, lambda sp: (ticks + (16 if a.autotune else 0)) * sp["epoch"])
+    data = W.build_all(specs, lambda sp: (ticks + (16 if a.autotune else 0)) * sp["epoch"],
+                       procs=max(1, min(8, (os.cpu_count() or 2) // world)))
     log(f"batched: {len(data)} graphs generated in {time.time() - t:.1f}s; "
         f"{sum(d['spec']['n'] for d in data)} vertices, {sum(int(d['row_ptr'][-1]) for d in data) // 2} edges")
     graphs = [S.Graph(d["row_ptr"], d["col"]) for d in data]
@@ -394,6 +418,8 @@ def run_batched(a):
     torch.cuda.synchronize()
     log(f"plain arm: {len(hs)} handles created and colored in {time.time() - t:.1f}s")
     plain_ticks, plain_updates, plain_ok = [], 0, True
+    if dist:
+        dist.barrier()
     for t_ in range(ticks):
         t0 = time.perf_counter()
         n_up = 0
@@ -440,6 +466,8 @@ def run_batched(a):
     st0 = b.stats()
     lat, dev_ms, b_updates, b_ok = [], [], 0, True
     base_t = tstate["t"]  # ticks the tuner consumed
+    if dist:
+        dist.barrier()
     with ClockSampler(local) as clk:
         for t_ in range(ticks):
             t0 = time.perf_counter()
@@ -459,28 +487,46 @@ def run_batched(a):
     st1 = b.stats()
     val = b.validate()
     b.close()
-    plain_v = plain_updates / sum(plain_ticks)
-    batch_v = b_updates / sum(lat)
     ls = sorted(lat)
+    p50, p99 = ls[len(ls) // 2], ls[min(len(ls) - 1, int(round(0.99 * (len(ls) - 1))))]
+    dev_p50 = sorted(dev_ms)[len(dev_ms) // 2]
     fam = {f: sum(1 for d in data if d["spec"]["family"] == f) for f in W.FAMILIES}
+    nv = sum(d["spec"]["n"] for d in data)
+    ne = sum(int(d["row_ptr"][-1]) for d in data) // 2
+    ok = int(b_ok and plain_ok)
+    valid = int(val["violations"] == 0 and val["uncolored_with_edges"] == 0)
+    launches = st1["kernel_launches"] - st0["kernel_launches"]
+    plain_time, batch_time = sum(plain_ticks), sum(lat)
+    if dist:  # every rank ran its own share: slowest rank's time, every rank's work
+        plain_time, batch_time, p50, p99, dev_p50 = max_over_ranks(dist, [plain_time, batch_time, p50, p99, dev_p50], dev)
+        sums = sum_over_ranks(dist, [plain_updates, b_updates, plain_launches, launches, nv, ne,
+                                     *[fam[f] for f in W.FAMILIES]], dev)
+        plain_updates, b_updates, plain_launches, launches, nv, ne = (int(x) for x in sums[:6])
+        fam = {f: int(x) for f, x in zip(W.FAMILIES, sums[6:])}
+        ok, valid = (int(x) for x in sum_over_ranks(dist, [ok, valid], dev))
+        ok, valid = ok == world, valid == world
+        dist.destroy_process_group()
+        if rank != 0:
+            return
+    plain_v = plain_updates / plain_time
+    batch_v = b_updates / batch_time
     out = {
-        "metric": METRIC, "form": "batched", "value": batch_v, "unit": "updates/s", "n_gpus": 1,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sum(lat) / len(lat), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"batched_{len(graphs)}_graphs", "families": fam,
-                   "vertices": sum(d["spec"]["n"] for d in data),
-                   "undirected_edges": sum(int(d["row_ptr"][-1]) for d in data) // 2,
+        "metric": METRIC, "form": "batched", "value": batch_v, "unit": "updates/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * batch_time / len(lat), "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"batched_{len(specs_all)}_graphs", "families": fam,
+                   "vertices": nv, "undirected_edges": ne,
+                   "placement": f"{world} ranks, graphs balanced by resident bytes" if world > 1 else "one GPU",
                    "epoch_sizes": "per graph in {1024, 8192, 32768}", "tick": "one epoch of every graph",
                    "mode": "concurrent apply, independent-set repair, CUDA-graph tick", "tuning": tuning,
-                   "autotuned": bool(a.autotune), "all_ticks_proper": bool(b_ok and plain_ok),
-                   "valid_after_run": val["violations"] == 0 and val["uncolored_with_edges"] == 0},
-        "plain_per_graph": {"value": plain_v, "unit": "updates/s", "ms_per_tick": 1e3 * sum(plain_ticks) / len(plain_ticks),
+                   "autotuned": bool(a.autotune), "all_ticks_proper": bool(ok),
+                   "valid_after_run": bool(valid)},
+        "plain_per_graph": {"value": plain_v, "unit": "updates/s", "ms_per_tick": 1e3 * plain_time / len(plain_ticks),
                             "launches": plain_launches},
         "speedup_vs_plain": batch_v / plain_v,
-        "latency_ms": {"update_to_visible_p50": 1e3 * ls[len(ls) // 2],
-                       "update_to_visible_p99": 1e3 * ls[min(len(ls) - 1, int(round(0.99 * (len(ls) - 1))))],
-                       "tick_device_ms_p50": sorted(dev_ms)[len(dev_ms) // 2]},
-        "gpu_launches": st1["kernel_launches"] - st0["kernel_launches"],
+        "latency_ms": {"update_to_visible_p50": 1e3 * p50, "update_to_visible_p99": 1e3 * p99,
+                       "tick_device_ms_p50": dev_p50},
+        "gpu_launches": launches,
         "clocks": clk.summary(),
     }
     print(json.dumps(out), flush=True)
@@ -502,36 +548,36 @@ def run_served(a):
     """Served form: 64 tenants (63 drawn as in the batched form, plus an R-MAT
     graph with 2^22 vertices and edge factor 16) behind the request loop. Each
     tenant's update requests arrive as a Poisson process at a rate proportional
-    to its edge count, sizes log-uniform in [1, 32,768], 50/50 insert/delete;
-    single-vertex queries are 20% of the requests. A client thread replays the arrivals in real time (submits and
-    queries), a second thread steps the server; the offered load is
-    `--served-rate` updates/s over `--served-seconds`."""
+    to its expected edge count, sizes log-uniform in [1, 32,768], 50/50
+    insert/delete; single-vertex queries are 20% of the requests. A client
+    thread replays the arrivals in real time (submits and queries), a second
+    thread steps the server; the offered load is `--served-rate` updates/s over
+    `--served-seconds`. Under torchrun every rank serves the tenants placed on
+    its GPU (balanced by resident bytes) with their own arrivals."""
     import threading
     import torch
     import streamgc_b200 as S
+    from streamgc_b200 import placement as P
     from streamgc_b200 import workloads as W
 
     world, rank, local = dist_setup()
-    if rank != 0:
-        return
     torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    dist = init_dist(world)
     rate, dur = a.served_rate, a.served_seconds
     specs = W.batch_specs(63, seed=43)
-    specs.append(dict(index=63, family="rmat22", n=1 << 22, epoch=32768, seed=43 * 100003 + 63))
+    specs.append(dict(index=63, family="rmat22", n=1 << 22, edge_factor=16, epoch=32768, seed=43 * 100003 + 63))
     T = len(specs)
-    t = time.time()
-    big = specs[-1]
-    data = W.build_all(specs[:-1], lambda sp: None, churn_per_edge=(0.5, 1 << 17))
-    g22 = S.Graph.rmat(22, 16, 0.57, 0.19, 0.19, seed=big["seed"])
-    data.append(dict(spec=big, row_ptr=g22.row_ptr, col=g22.col_idx, churn=None))
-    edges = np.array([int(d["row_ptr"][-1]) // 2 for d in data], dtype=np.float64)
+    est = [P.expected_entries(sp) for sp in specs]
+    mine = P.place([P.footprint(sp["n"], e) for sp, e in zip(specs, est)], world)[rank]
+    # arrivals of every tenant (the same on every rank), from expected sizes
     rng = np.random.default_rng(43)
     max_b = 32768
     mean_b = (max_b - 1) / math.log(max_b + 1)
     events = []
     need = [0] * T
     for k in range(T):
-        req_rate = rate * edges[k] / edges.sum() / mean_b  # update requests per second of this tenant
+        req_rate = rate * est[k] / sum(est) / mean_b  # update requests per second of this tenant
         t_ = 0.0
         while True:
             t_ += rng.exponential(1.0 / (req_rate / 0.8))  # updates are 80% of the requests
@@ -545,20 +591,33 @@ def run_served(a):
                 events.append((t_, k, 1, m))
                 need[k] += m
     events.sort()
+    mset = set(mine)
+    events = [e for e in events if e[1] in mset]
 
-    data[-1]["churn"] = g22.churn_stream(need[63] + 1, 50, big["seed"])
-    short = [k for k in range(T - 1) if len(data[k]["churn"]) < need[k]]
+    t = time.time()
+    small = [specs[k] for k in mine if k < T - 1]
+    built = W.build_all(small, lambda sp: need[sp["index"]] + 1,
+                        procs=max(1, min(8, (os.cpu_count() or 2) // world))) if small else []
+    data = {d["spec"]["index"]: d for d in built}
+    if T - 1 in mset:
+        big = specs[-1]
+        g22 = S.Graph.rmat(22, 16, 0.57, 0.19, 0.19, seed=big["seed"])
+        data[T - 1] = dict(spec=big, row_ptr=g22.row_ptr, col=g22.col_idx,
+                           churn=g22.churn_stream(need[T - 1] + 1, 50, big["seed"]))
+    short = [k for k in mine if len(data[k]["churn"]) < need[k]]
     if short:
         raise SystemExit(f"served: churn streams of tenants {short} are shorter than their offered updates")
-    log(f"served: {T} tenants generated in {time.time() - t:.1f}s; {len(events)} requests over {dur}s")
+    log(f"served (rank {rank}): {len(mine)} of {T} tenants generated in {time.time() - t:.1f}s; "
+        f"{len(events)} requests over {dur}s")
     srv = S.Server(hbm_budget_bytes=150 << 30, max_tick_updates=1 << 22, max_staleness_us=a.served_staleness_us,
                    device=local, profile=True)
-    tids = [srv.add_tenant(S.Graph(d["row_ptr"], d["col"]), epoch_size=d["spec"]["epoch"]) for d in data]
+    tids = {k: srv.add_tenant(S.Graph(data[k]["row_ptr"], data[k]["col"]), epoch_size=data[k]["spec"]["epoch"])
+            for k in mine}
     t = time.time()
     r0 = srv.step()  # admission: every tenant colored and published
     log(f"admitted {r0['admitted']} tenants in {time.time() - t:.1f}s (proper={r0['proper']})")
     st0 = srv.stats()
-    pos = [0] * T
+    pos = {k: 0 for k in mine}
     stop = threading.Event()
     errors = []
     steps = []
@@ -578,6 +637,8 @@ def run_served(a):
 
     th = threading.Thread(target=stepper)
     qv = np.zeros(1, dtype=np.uint32)
+    if dist:
+        dist.barrier()
     with ClockSampler(local) as clk:
         th.start()
         t0 = time.perf_counter()
@@ -592,8 +653,7 @@ def run_served(a):
                 qv[0] = rng.integers(0, data[k]["spec"]["n"])
                 srv.query(tids[k], qv)
             else:
-                ch = data[k]["churn"]
-                srv.submit(tids[k], ch[pos[k]:pos[k] + m])
+                srv.submit(tids[k], data[k]["churn"][pos[k]:pos[k] + m])
                 pos[k] += m
         t_sub = time.perf_counter() - t0
         deadline = time.time() + 60
@@ -610,37 +670,52 @@ def run_served(a):
     st = srv.stats()
     asym = None
     if a.served_check:  # every tenant's live rows must still hold each entry's mirror
-        asym = []
-        for k in range(T):
-            rp_, col_ = srv.rows(tids[k])
-            if mirror_checksum(rp_, col_):
-                asym.append(k)
+        asym = [k for k in mine if mirror_checksum(*srv.rows(tids[k]))]
     srv.close()
     applied = st["updates_applied"] - st0["updates_applied"]
     ls = sorted(steps)
+    step_p50 = ls[len(ls) // 2] if ls else 0.0
+    step_p99 = ls[min(len(ls) - 1, int(round(0.99 * (len(ls) - 1))))] if ls else 0.0
+    nv = sum(data[k]["spec"]["n"] for k in mine)
+    ne = sum(int(data[k]["row_ptr"][-1]) for k in mine) // 2
+    cnt = [applied, len(events), sum(1 for e in events if e[2] == 0), st["resident_bytes"], nv, ne,
+           st["ticks"] - st0["ticks"], st["tier2_ticks"] - st0["tier2_ticks"],
+           st["tier2_mirror_ticks"] - st0["tier2_mirror_ticks"], st["tier1_sweeps"] - st0["tier1_sweeps"],
+           st["tick_device_ms"] - st0["tick_device_ms"], sum(need[k] for k in mine), st["overflows"],
+           st["drain_failed"], st["device_errors"], len(steps), sum(steps)]
+    worst = [t_end, t_sub, late, st["visible_p50_ms"], st["visible_p99_ms"], st["query_p50_ms"], st["query_p99_ms"],
+             step_p50, step_p99]
+    if dist:  # tenants on every rank: every rank's work, the slowest rank's times and latencies
+        cnt = sum_over_ranks(dist, cnt, dev)
+        worst = max_over_ranks(dist, worst, dev)
+        if asym is not None:
+            flags = sum_over_ranks(dist, [1.0 if k in asym else 0.0 for k in range(T)], dev)
+            asym = [k for k in range(T) if flags[k]]
+        dist.destroy_process_group()
+        if rank != 0:
+            return
+    (applied, nreq, nq, resident, nv, ne, ticks, t2, t2m, sweeps, tick_ms, offered, ovf, dfail, derr,
+     nsteps, steps_ms) = cnt
+    t_end, t_sub, late, v50, v99, q50, q99, step_p50, step_p99 = worst
     out = {
-        "metric": METRIC, "form": "served", "value": applied / t_end, "unit": "updates/s", "n_gpus": 1,
-        "steps": len(steps), "warmup": 1, "ms_per_step": sum(steps) / max(1, len(steps)), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "metric": METRIC, "form": "served", "value": applied / t_end, "unit": "updates/s", "n_gpus": world,
+        "steps": int(nsteps), "warmup": 1, "ms_per_step": steps_ms / max(1, nsteps), "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": "served_64_tenants", "offered_updates_per_s": rate, "seconds": dur,
-                   "tenants": T, "vertices": sum(d["spec"]["n"] for d in data),
-                   "undirected_edges": sum(int(d["row_ptr"][-1]) for d in data) // 2,
-                   "requests": len(events), "queries": sum(1 for e in events if e[2] == 0),
-                   "batch_sizes": "log-uniform [1, 32768]", "max_staleness_us": a.served_staleness_us,
-                   "hbm_budget_gb": 150, "resident_gb": round(st["resident_bytes"] / 2**30, 2),
+                   "tenants": T, "vertices": int(nv), "undirected_edges": int(ne),
+                   "placement": f"{world} ranks, tenants balanced by resident bytes" if world > 1 else "one GPU",
+                   "requests": int(nreq), "queries": int(nq),
+                   "batch_sizes": "log-uniform [1, 32768]", "arrival_rate": "proportional to expected edges",
+                   "max_staleness_us": a.served_staleness_us,
+                   "hbm_budget_gb": 150, "resident_gb": round(resident / 2**30, 2),
                    "client_max_lag_s": round(late, 4), "submit_window_s": round(t_sub, 3),
-                   "timed_s": round(t_end, 3),
-                   "ticks": st["ticks"] - st0["ticks"], "tier2_ticks": st["tier2_ticks"] - st0["tier2_ticks"],
-                   "tier2_mirror_ticks": st["tier2_mirror_ticks"] - st0["tier2_mirror_ticks"],
-                   "sweeps_per_tick": round((st["tier1_sweeps"] - st0["tier1_sweeps"]) /
-                                            max(1, st["ticks"] - st0["ticks"]), 2),
-                   "tick_device_ms_total": round(st["tick_device_ms"] - st0["tick_device_ms"], 1),
-                   "offered_updates": int(sum(need)), "overflows": st["overflows"], "drain_failed": st["drain_failed"],
-                   "device_errors": st["device_errors"], "asymmetric_tenants": asym},
-        "latency_ms": {"update_to_visible_p50": st["visible_p50_ms"], "update_to_visible_p99": st["visible_p99_ms"],
-                       "query_p50": st["query_p50_ms"], "query_p99": st["query_p99_ms"],
-                       "step_p50": ls[len(ls) // 2] if ls else None,
-                       "step_p99": ls[min(len(ls) - 1, int(round(0.99 * (len(ls) - 1))))] if ls else None},
+                   "timed_s": round(t_end, 3), "ticks": int(ticks), "tier2_ticks": int(t2),
+                   "tier2_mirror_ticks": int(t2m), "sweeps_per_tick": round(sweeps / max(1, ticks), 2),
+                   "tick_device_ms_total": round(tick_ms, 1), "offered_updates": int(offered),
+                   "overflows": int(ovf), "drain_failed": int(dfail), "device_errors": int(derr),
+                   "asymmetric_tenants": asym},
+        "latency_ms": {"update_to_visible_p50": v50, "update_to_visible_p99": v99,
+                       "query_p50": q50, "query_p99": q99, "step_p50": step_p50, "step_p99": step_p99},
         "clocks": clk.summary(),
     }
     print(json.dumps(out), flush=True)

@@ -59,28 +59,27 @@ def make_graph(spec):
 
 
 def _build(args):
-    spec, stream_len, per_edge = args
+    spec, stream_len = args
     import streamgc_b200 as S
     rp, col = make_graph(spec)
     g = S.Graph(rp, col)
     m = int(rp[-1]) // 2
     size = min(16 * m, stream_len) if stream_len is not None else 16 * m
-    if per_edge is not None:
-        size = min(size, max(int(per_edge[0] * m), per_edge[1]))
     churn = g.churn_stream(max(size, 0), 50, spec["seed"])
     return spec["index"], rp, col, churn
 
 
-def build_all(specs, stream_len_of, procs=None, churn_per_edge=None):
+def build_all(specs, stream_len_of, procs=None):
     """Graphs and churn streams for every spec, in worker processes.
-    stream_len_of(spec) bounds each churn stream (the full stream is 16x the
-    graph's edge count; its prefix is the same; None: no bound), and so does
-    churn_per_edge = (f, floor): max(f x edges, floor) updates. Returns a list of dicts
-    (spec, row_ptr, col, churn) in spec order; a graph's init stream (every
-    edge as an ADD) comes from init_stream(d) when needed."""
+
+    Each churn stream is 16x the graph's edge count; stream_len_of(spec)
+    bounds it (None: no bound), and a shorter stream is a prefix of a longer
+    one. Returns a list of dicts (spec, row_ptr, col, churn) in spec order; a
+    graph's init stream (every edge as an ADD) comes from init_stream(d) when
+    needed."""
     procs = procs or max(1, min(8, (os.cpu_count() or 2)))
     order = sorted(specs, key=lambda s: -s["n"])
-    jobs = [(s, stream_len_of(s), churn_per_edge) for s in order]
+    jobs = [(s, stream_len_of(s)) for s in order]
     pos = {s["index"]: i for i, s in enumerate(specs)}
     out = [None] * len(specs)
     ctx = mp.get_context("spawn")

@@ -1,6 +1,7 @@
 """The bench's multi-rank path on CPU: two gloo ranks (one per process, as
-torchrun runs replicas) agree on the slowest rank's timings, and the whole-job
-rate counts every replica's work over that time."""
+torchrun runs replicas or shards) agree on the slowest rank's timings and on
+the sum of their counts, and the whole-job rate counts every replica's work
+over that time."""
 import os
 import socket
 
@@ -22,7 +23,7 @@ def _rank(rank, world, port, q):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         mine = [10.0 + 5 * rank, 3.0 - rank]  # rank 1 is slower on the first timing, faster on the second
-        q.put((rank, bench.max_over_ranks(dist, mine, "cpu")))
+        q.put((rank, (bench.max_over_ranks(dist, mine, "cpu"), bench.sum_over_ranks(dist, [1.0 + rank, 7.0], "cpu"))))
     finally:
         dist.destroy_process_group()
 
@@ -39,7 +40,7 @@ def test_two_ranks_take_the_slowest_timing():
     for p in procs:
         p.join(30)
         assert p.exitcode == 0
-    assert got[0] == got[1] == [15.0, 3.0]
+    assert got[0] == got[1] == ([15.0, 3.0], [3.0, 14.0])
 
 
 def test_job_rate_counts_every_replica():
