@@ -102,6 +102,21 @@ typedef struct sgc_validation {
     uint64_t out_of_range;          /* live entries naming a vertex >= n */
 } sgc_validation;
 
+/* Layout invariants of the rows (sgc_check_state). */
+#define SGC_STATE_HW     0x1u   /* high-water mark beyond the row's capacity (or row offsets decreasing) */
+#define SGC_STATE_TAIL   0x2u   /* a slot at or past the high-water mark that is not free */
+#define SGC_STATE_ID     0x4u   /* an entry naming a vertex >= n */
+#define SGC_STATE_RUN    0x8u   /* sorted prefix (base run / never-edited row) not strictly ascending */
+#define SGC_STATE_HOLES  0x10u  /* hole counter above the row's extent (wrapped below zero) */
+#define SGC_STATE_COLOR  0x20u  /* a color above 2048 */
+
+typedef struct sgc_state_report {
+    uint64_t rows;        /* rows checked (the handle's vertices) */
+    uint64_t bad_rows;    /* rows breaking at least one invariant */
+    uint32_t flags;       /* SGC_STATE_* bits seen */
+    uint32_t first_bad;   /* lowest such row, 0xFFFFFFFF when none */
+} sgc_state_report;
+
 /* sgc_download / sgc_upload targets */
 #define SGC_DL_STATES    0   /* uint32[n] packed (color | version << 16) */
 #define SGC_DL_COLORS    1   /* uint16[n] current colors */
@@ -179,6 +194,9 @@ int sgc_upload(sgc_handle* h, int what, const void* src, uint64_t bytes);   /* S
 int sgc_find_color(sgc_handle* h, uint32_t x, uint16_t* color);
 
 int sgc_validate(sgc_handle* h, sgc_validation* out);   /* check_coloring_valid, streamgc.cu:448-556 */
+/* Checks every row's layout invariants on the device (a debugging aid with no
+ * reference counterpart); call between batches. */
+int sgc_check_state(sgc_handle* h, sgc_state_report* out);
 int sgc_get_stats(sgc_handle* h, sgc_stats* out);
 int sgc_synchronize(sgc_handle* h);
 /* The handle's cudaStream_t, for callers that time or order work around it. */

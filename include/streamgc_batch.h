@@ -113,6 +113,8 @@ int sgc_batch_snapshot(sgc_batch* b, uint32_t graph, uint16_t* out);  /* num_ver
 int sgc_batch_rows(sgc_batch* b, uint32_t graph, uint64_t* row_ptr, uint32_t* col, uint64_t col_cap);
 /* Validator over all graphs (the reference's, streamgc.cu:448-556). */
 int sgc_batch_validate(sgc_batch* b, sgc_validation* out);
+/* Layout invariants of every graph's rows (sgc_check_state); between ticks. */
+int sgc_batch_check_state(sgc_batch* b, sgc_state_report* out);
 
 /* Histogram threshold of every graph created without one (32, 64 or 128 ...). */
 int sgc_batch_set_thresholds(sgc_batch* b, uint32_t threshold);

@@ -82,6 +82,17 @@ class Validation(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class StateReport(C.Structure):
+    _fields_ = [("rows", C.c_uint64), ("bad_rows", C.c_uint64), ("flags", C.c_uint32), ("first_bad", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# sgc_state_report.flags bits
+STATE_HW, STATE_TAIL, STATE_ID, STATE_RUN, STATE_HOLES, STATE_COLOR = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20
+
+
 class _CSR(C.Structure):
     _fields_ = [("n", C.c_uint32), ("nnz", C.c_uint64), ("row_ptr", C.POINTER(C.c_uint64)),
                 ("col_idx", C.POINTER(C.c_uint32)), ("degree", C.POINTER(C.c_uint32))]
@@ -164,6 +175,7 @@ SIGNATURES = {
     "sgc_upload": (C.c_int, [_vp, C.c_int, _vp, C.c_uint64]),
     "sgc_find_color": (C.c_int, [_vp, C.c_uint32, _u16p]),
     "sgc_validate": (C.c_int, [_vp, C.POINTER(Validation)]),
+    "sgc_check_state": (C.c_int, [_vp, C.POINTER(StateReport)]),
     "sgc_get_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
     "sgc_synchronize": (C.c_int, [_vp]),
     "sgc_cuda_stream": (_vp, [_vp]),
@@ -196,6 +208,7 @@ SIGNATURES = {
     "sgc_batch_snapshot": (C.c_int, [_vp, C.c_uint32, _u16p]),
     "sgc_batch_rows": (C.c_int, [_vp, C.c_uint32, _u64p, _u32p, C.c_uint64]),
     "sgc_batch_validate": (C.c_int, [_vp, C.POINTER(Validation)]),
+    "sgc_batch_check_state": (C.c_int, [_vp, C.POINTER(StateReport)]),
     "sgc_batch_set_thresholds": (C.c_int, [_vp, C.c_uint32]),
     "sgc_batch_get_tuning": (C.c_int, [_vp, C.POINTER(BatchTuning)]),
     "sgc_batch_set_tuning": (C.c_int, [_vp, C.POINTER(BatchTuning)]),
@@ -527,6 +540,12 @@ class StreamGC:
         _check(lib().sgc_validate(self.h, C.byref(v)), "sgc_validate")
         return v.as_dict()
 
+    def check_state(self):
+        """Layout invariants of every row (STATE_* bits in `flags`)."""
+        r = StateReport()
+        _check(lib().sgc_check_state(self.h, C.byref(r)), "sgc_check_state")
+        return r.as_dict()
+
 
 def version():
     return lib().sgc_version().decode()
@@ -625,6 +644,11 @@ class Batch:
         v = Validation()
         _check(lib().sgc_batch_validate(self.b, C.byref(v)), "sgc_batch_validate")
         return v.as_dict()
+
+    def check_state(self):
+        r = StateReport()
+        _check(lib().sgc_batch_check_state(self.b, C.byref(r)), "sgc_batch_check_state")
+        return r.as_dict()
 
     def set_thresholds(self, thr):
         _check(lib().sgc_batch_set_thresholds(self.b, thr), "sgc_batch_set_thresholds")

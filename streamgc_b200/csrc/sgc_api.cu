@@ -782,6 +782,18 @@ int sgc_validate(sgc_handle* h, sgc_validation* out) {
     return SGC_OK;
 }
 
+int sgc_check_state(sgc_handle* h, sgc_state_report* out) {
+    if (!h || !out) return fail(SGC_EINVAL, "null argument");
+    CK(cudaSetDevice(h->device));
+    uint64_t v[3] = {0, 0, 0};
+    if (run_check_state(h->g, h->stream, v) < 0) return fail(SGC_ECUDA, "state check failed: %s", cudaGetErrorString(cudaGetLastError()));
+    out->rows = h->n;
+    out->bad_rows = v[0];
+    out->flags = (uint32_t)v[1];
+    out->first_bad = v[0] ? (uint32_t)v[2] : 0xFFFFFFFFu;
+    return SGC_OK;
+}
+
 int sgc_get_stats(sgc_handle* h, sgc_stats* o) {
     if (!h || !o) return fail(SGC_EINVAL, "null argument");
     CK(cudaSetDevice(h->device));

@@ -621,6 +621,12 @@ int sgc_batch_validate(sgc_batch* b, sgc_validation* out) {
     return sgc_validate(b->h, out);
 }
 
+int sgc_batch_check_state(sgc_batch* b, sgc_state_report* out) {
+    if (!b) return fail(SGC_EINVAL, "null batch");
+    if (b->in_tick) return fail(SGC_EINVAL, "a tick is running");
+    return sgc_check_state(b->h, out);
+}
+
 int sgc_batch_stats(sgc_batch* b, sgc_stats* out) {
     if (!b) return fail(SGC_EINVAL, "null batch");
     return sgc_get_stats(b->h, out);

@@ -225,6 +225,18 @@ __device__ __forceinline__ uint64_t live_end(const Dev& g, uint32_t x, uint64_t 
     return cap;
 }
 
+// Row x got an entry in slot q (relative to rp[x]): raise the high-water
+// mark and keep the hole count (free slots inside the mark) exact. A slot
+// below the old mark was a counted hole; a mark raised past free slots makes
+// each of them a hole (a concurrent insert that already took one of them
+// finds the mark above its slot and uncounts it).
+__device__ __forceinline__ void extend_row(const Dev& g, uint32_t x, uint32_t q) {
+    const uint32_t prev_hw = atomicMax(g.hw + x, q + 1);
+    if (!g.holes) return;
+    if (q < prev_hw) atomicSub(g.holes + x, 1u);
+    else if (q > prev_hw) atomicAdd(g.holes + x, q - prev_hw);
+}
+
 __device__ __forceinline__ void flag_asym(const Dev& g, uint32_t x) {
     uint32_t* a = &g.gctl[graph_of(g, x)].asym;
     if (!ld_cg(a)) atomicOr(a, 1u);
@@ -371,8 +383,7 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
         if (lane_id() == 0) {
             old = atomicCAS(g.col + p, INV, nbr);
             if (old == INV) {
-                const uint32_t prev_hw = atomicMax(g.hw + x, (uint32_t)(p - s + 1));
-                if (g.holes && (uint32_t)(p - s) < prev_hw) atomicSub(g.holes + x, 1u);  // filled a hole
+                extend_row(g, x, (uint32_t)(p - s));
                 mark_dirty(g, x);
             }
         }

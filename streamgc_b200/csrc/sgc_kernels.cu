@@ -376,8 +376,7 @@ __device__ __forceinline__ bool warp_drain_insert(const Dev& g, uint32_t x, uint
         if (lane_id() == 0) {
             old = atomicCAS(g.col + p, INV, nbr);
             if (old == INV) {
-                const uint32_t prev_hw = atomicMax(g.hw + x, (uint32_t)(p - s + 1));
-                if (g.holes && (uint32_t)(p - s) < prev_hw) atomicSub(g.holes + x, 1u);
+                extend_row(g, x, (uint32_t)(p - s));
                 mark_dirty(g, x);
             }
         }

@@ -179,5 +179,8 @@ size_t tier2_cub_bytes(uint32_t n, uint32_t rev_cap);
 
 // Validator (sgc_tier2.cu): [violations, uncolored_with_edges, distinct_edges, max_color, out_of_range]
 int run_validate(const Dev& g, cudaStream_t s, uint64_t* out);
+// Layout invariants of every row: out = {rows breaking one, SGC_STATE_* bits
+// seen, lowest such row (~0 if none)}.
+int run_check_state(const Dev& g, cudaStream_t s, uint64_t* out);
 
 }  // namespace sgc

@@ -22,6 +22,7 @@
 
 #include <vector>
 
+#include "../../include/streamgc_b200.h"
 #include "sgc_kernels.cuh"
 
 namespace sgc {
@@ -402,6 +403,77 @@ __global__ void count_unique_kernel(const unsigned long long* keys, uint32_t n, 
 }
 
 }  // namespace
+
+namespace {
+
+// Warp per row: the layout invariants every kernel relies on (see
+// streamgc_b200.h, SGC_STATE_*). Reads stay inside [rp[x], rp[x+1]) whatever
+// the row's other words say.
+__global__ void check_state_kernel(Dev g, unsigned long long* out /* bad rows, flags, first bad */) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = lane_id();
+    for (uint32_t x = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; x < g.n; x += warps) {
+        const uint64_t s = g.rp[x], e = g.rp[x + 1];
+        uint32_t f = 0;
+        if (e < s) f |= SGC_STATE_HW;
+        const uint64_t cap = e >= s ? e - s : 0;
+        const uint64_t hw = g.hw[x];
+        if (hw > cap) f |= SGC_STATE_HW;
+        const uint64_t he = s + (hw < cap ? hw : cap);
+        const uint64_t bl = g.blen ? g.blen[x] : 0;
+        if (bl > he - s) f |= SGC_STATE_RUN;
+        // sorted prefix: the base run (exact selection) or a never-edited row
+        const bool pristine = !(g.edited[x >> 5] & (1u << (x & 31)));
+        const uint64_t se = g.blen ? s + (bl < he - s ? bl : he - s) : (pristine ? he : s);
+        uint32_t holes_in = 0;
+        for (uint64_t i = s + lane; i < e; i += 32) {
+            const uint32_t v = g.col[i];
+            if (i < he) {
+                const bool tomb = g.blen && v != INV && (v & TOMB);
+                const uint32_t id = tomb ? (v & ~TOMB) : v;
+                if (v == INV || tomb) holes_in++;
+                if (v != INV && id >= g.n) f |= SGC_STATE_ID;
+                if (i > s && i < se) {
+                    const uint32_t p = g.col[i - 1];
+                    const uint32_t pid = g.blen ? (p & ~TOMB) : p;
+                    if (v == INV || p == INV || pid >= id) f |= SGC_STATE_RUN;
+                }
+            } else if (v != INV) {
+                f |= SGC_STATE_TAIL;
+            }
+        }
+        f = __reduce_or_sync(FULL, f);
+        holes_in = __reduce_add_sync(FULL, holes_in);
+        if (lane == 0) {
+            if (g.holes && g.holes[x] > he - s) f |= SGC_STATE_HOLES;  // the counter wrapped below zero
+            if (color_of(g.st[x]) > 2048) f |= SGC_STATE_COLOR;
+            if (f) {
+                atomicAdd(out + 0, 1ull);
+                atomicOr(out + 1, (unsigned long long)f);
+                atomicMin(out + 2, (unsigned long long)x);
+            }
+        }
+        (void)holes_in;
+    }
+}
+
+}  // namespace
+
+int run_check_state(const Dev& g, cudaStream_t s, uint64_t* out) {
+    unsigned long long* d = nullptr;
+    if (cudaMallocAsync(&d, 3 * 8, s) != cudaSuccess) return -2;
+    const unsigned long long init[3] = {0, 0, ~0ull};
+    cudaMemcpyAsync(d, init, sizeof(init), cudaMemcpyHostToDevice, s);
+    check_state_kernel<<<148 * 8, 256, 0, s>>>(g, d);
+    unsigned long long h[3];
+    cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(d, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
+    out[0] = h[0];
+    out[1] = h[1];
+    out[2] = h[2];
+    return 0;
+}
 
 int run_validate(const Dev& g, cudaStream_t s, uint64_t* out) {
     // capacity: every live slot

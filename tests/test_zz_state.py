@@ -1,0 +1,61 @@
+"""Row layout invariants on the device (sgc_check_state): after every batch,
+publish and tick the rows of a handle keep their high-water marks inside the
+row capacity, only free slots past the mark, vertex ids in range, a sorted
+base run (exact selection) or sorted never-edited rows, hole counters that
+never wrap, and colors in range; in stream order and in concurrent batches."""
+import numpy as np
+import pytest
+
+import streamgc_b200 as S
+from tests.golden import make_golden as MG
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ["delaunay2k", "rmat11", "overflow512"]
+
+
+def _clean(rep):
+    return rep["bad_rows"] == 0 and rep["flags"] == 0 and rep["first_bad"] == 0xFFFFFFFF
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("exact", [False, True])
+def test_rows_keep_their_invariants(name, exact):
+    c = MG.build_case(name)
+    g = S.Graph(c["rp"], c["col"], c["deg"])
+    ups = np.concatenate([c["init"], c["bench"]])
+    with S.StreamGC(g, epoch_size=c["E"], histogram_threshold=c["thr"], slack_pct=c["slack"],
+                    exact_select=exact) as h:
+        rep = h.check_state()
+        assert rep["rows"] == len(c["rp"]) - 1
+        assert _clean(rep), rep
+        mode = S.MODE_CONCURRENT if exact else S.MODE_DETERMINISTIC
+        B = 2048
+        for i, s in enumerate(range(0, len(ups), B)):
+            h.apply(ups[s:s + B], mode)
+            assert _clean(h.check_state()), (i, h.check_state())
+            if i % 4 == 3:
+                if exact:
+                    assert h.publish()["proper"] == 1
+                else:
+                    h.epoch()
+                assert _clean(h.check_state()), (i, "after epoch", h.check_state())
+
+
+def test_batched_rows_keep_their_invariants():
+    cases = [MG.build_case(n) for n in NAMES]
+    E = 1024
+    b = S.Batch([S.Graph(c["rp"], c["col"], c["deg"]) for c in cases], epoch_sizes=[E] * len(cases),
+                thresholds=[c["thr"] for c in cases])
+    try:
+        assert _clean(b.check_state())
+        scheds = [np.concatenate([c["init"], c["bench"]]) for c in cases]
+        for t in range(12):
+            for k, u in enumerate(scheds):
+                part = u[t * E:(t + 1) * E]
+                if len(part):
+                    b.submit(k, part)
+            assert b.tick()["proper"] == 1
+            assert _clean(b.check_state()), (t, b.check_state())
+    finally:
+        b.close()
