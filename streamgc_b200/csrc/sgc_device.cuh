@@ -216,6 +216,15 @@ __device__ __forceinline__ void mark_dirty(const Dev& g, uint32_t x) {
     if (!(ld_cg(g.edited + (x >> 5)) & (1u << (x & 31)))) atomicOr(g.edited + (x >> 5), 1u << (x & 31));
 }
 __device__ __forceinline__ uint32_t graph_of(const Dev& g, uint32_t x) { return g.gidw ? __ldg(g.gidw + (x >> 5)) : 0u; }
+// Row x's high-water mark, at most the row's capacity. The mark never
+// exceeds it; the clamp keeps every scan and every compaction write inside the
+// row whatever the word holds (sgc_check_state reports such a row).
+__device__ __forceinline__ uint32_t row_len(const Dev& g, uint32_t x) {
+    const uint32_t hw = g.hw[x];
+    const uint64_t cap = g.rp[x + 1] - g.rp[x];
+    return hw <= cap ? hw : (uint32_t)cap;
+}
+
 // End of the slots of row x that scans visit, [s, s + hw), clamped to the
 // row's capacity (a larger mark sets ERR_ROW).
 __device__ __forceinline__ uint64_t live_end(const Dev& g, uint32_t x, uint64_t s) {

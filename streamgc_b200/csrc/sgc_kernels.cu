@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __r
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
         const uint32_t x = list[k];
         const uint64_t s = g.rp[x];
-        const uint32_t hwx = g.hw[x];
+        const uint32_t hwx = row_len(g, x);
         // Lazy mode: a row whose holes fill at most a quarter of its extent stays
         // as it is (every reader skips INV slots and tombstones); it is compacted later.
         if (!force && g.holes && 4u * g.holes[x] <= hwx) {
@@ -457,7 +457,7 @@ __global__ void build_items_kernel(Dev g, SweepBufs b, int list_mode) {
         uint32_t k = 0, x = 0;
         if (t < lim) {
             x = list ? b.wl[t] : t;
-            const uint32_t len = g.hw[x];
+            const uint32_t len = row_len(g, x);
             if (len > SWEEP_TINY) k = (len + tile - 1) / tile;
         }
         uint32_t total = 0;
@@ -497,7 +497,7 @@ __device__ __forceinline__ void item_bounds(const Dev& g, const SweepBufs& b, un
     const uint32_t j = (uint32_t)(it >> 32);
     const uint64_t rs = g.rp[x];
     s = rs + (uint64_t)j * b.tile;
-    const uint64_t re = rs + g.hw[x];
+    const uint64_t re = rs + row_len(g, x);
     e = s + b.tile < re ? s + b.tile : re;
 }
 
@@ -596,7 +596,7 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
             const GraphCtl& gc = g.gctl[graph_of(g, x)];
             with_sym = gc.full && ld_cg(&gc.asym);
         }
-        const uint32_t len = g.hw[x];
+        const uint32_t len = row_len(g, x);
         const uint32_t hd = __ldg(g.hdmap + x);
         const uint32_t w = __ldg(g.st + x);
         const uint16_t myc = color_of(w);
@@ -793,7 +793,7 @@ __global__ void __launch_bounds__(256) indep_decide_kernel(Dev g, SweepBufs b) {
     const uint32_t salt = sweep_salt(ld_cg(&b.rc->it));
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
         const uint32_t x = b.need_v[t];
-        const uint32_t len = g.hw[x];
+        const uint32_t len = row_len(g, x);
         bool blocked = false;
         if (len <= SWEEP_TINY) {
             const uint64_t s = g.rp[x];
@@ -853,7 +853,7 @@ __global__ void sweep_commit_kernel(Dev g, SweepBufs b, int mode) {
         b.needf[x] = 0;
         atomicOr(b.rbits + (x >> 5), 1u << (x & 31));
         if (!incr) atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
-        const uint32_t len = g.hw[x];
+        const uint32_t len = row_len(g, x);
         if (len <= SWEEP_TINY) {
             const uint64_t s = g.rp[x];
             const uint32_t c = color_of(nw);

@@ -32,7 +32,7 @@ size_t tier2_cub_bytes(uint32_t n, uint32_t rev_cap);
 namespace {
 
 __device__ __forceinline__ uint64_t row_s(const Dev& g, uint32_t x) { return g.rp[x]; }
-__device__ __forceinline__ uint64_t row_e(const Dev& g, uint32_t x) { return g.rp[x] + g.hw[x]; }
+__device__ __forceinline__ uint64_t row_e(const Dev& g, uint32_t x) { return g.rp[x] + row_len(g, x); }
 
 // Warp per vertex over the live rows of the vertices in [sp.lo, sp.hi): f(x, y)
 // for every entry y != INV. With sp.masked only rows of graphs whose
