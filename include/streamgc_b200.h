@@ -193,7 +193,10 @@ int sgc_upload(sgc_handle* h, int what, const void* src, uint64_t bytes);   /* S
 /* FindAvailableColor(x) (color_select.cuh:93-115) on the current device state. */
 int sgc_find_color(sgc_handle* h, uint32_t x, uint16_t* color);
 
-int sgc_validate(sgc_handle* h, sgc_validation* out);   /* check_coloring_valid, streamgc.cu:448-556 */
+/* check_coloring_valid, streamgc.cu:448-556. Slabs beyond 2^32 slots are
+ * counted without the distinct-edge sort: each edge at its lower endpoint's
+ * entry (the same counts when every entry has its mirror). */
+int sgc_validate(sgc_handle* h, sgc_validation* out);
 /* Checks every row's layout invariants on the device (a debugging aid with no
  * reference counterpart); call between batches. */
 int sgc_check_state(sgc_handle* h, sgc_state_report* out);

@@ -72,6 +72,54 @@ struct KeySet {
     }
 };
 
+// Whether every row holds strictly ascending neighbor ids.
+bool rows_sorted(const sgc_csr* g) {
+    bool ok = true;
+#pragma omp parallel for reduction(&& : ok) schedule(static)
+    for (int64_t u = 0; u < (int64_t)g->n; u++)
+        for (uint64_t j = g->row_ptr[u] + 1; j < g->row_ptr[u + 1]; j++)
+            if (g->col_idx[j - 1] >= g->col_idx[j]) ok = false;
+    return ok;
+}
+
+// The live edge set of a churn. With sorted rows: the base graph's edges
+// (binary search in the row) plus the changes since (base edges now gone, new
+// edges now live), so it grows with the stream, not with the graph; else
+// every live edge in one KeySet.
+struct LiveEdges {
+    const sgc_csr* g;
+    bool sorted;
+    KeySet full, gone, extra;
+    LiveEdges(const sgc_csr* g_, uint64_t stream)
+        : g(g_), sorted(rows_sorted(g_)), full(sorted ? 1 : g_->nnz / 2 + stream), gone(sorted ? stream : 1),
+          extra(sorted ? stream : 1) {
+        if (!sorted)
+            for (uint32_t u = 0; u < g->n; u++)
+                for (uint64_t j = g->row_ptr[u]; j < g->row_ptr[u + 1]; j++)
+                    if (u < g->col_idx[j]) full.add(key_of(u, g->col_idx[j]));
+    }
+    bool in_base(uint64_t e) const {
+        const uint32_t a = (uint32_t)(e >> 32), b = (uint32_t)e;
+        const uint32_t* lo = g->col_idx + g->row_ptr[a];
+        const uint32_t* hi = g->col_idx + g->row_ptr[a + 1];
+        return std::binary_search(lo, hi, b);
+    }
+    bool has(uint64_t e) const {
+        if (!sorted) return full.has(e);
+        return in_base(e) ? !gone.has(e) : extra.has(e);
+    }
+    void add(uint64_t e) {
+        if (!sorted) full.add(e);
+        else if (in_base(e)) gone.del(e);
+        else extra.add(e);
+    }
+    void del(uint64_t e) {
+        if (!sorted) full.del(e);
+        else if (in_base(e)) gone.add(e);
+        else extra.del(e);
+    }
+};
+
 // Symmetric CSR from normalised (min, max) keys, sorted and unique.
 int csr_from_sorted_keys(uint32_t n, const std::vector<uint64_t>& keys, sgc_csr* out) {
     std::memset(out, 0, sizeof(*out));
@@ -214,15 +262,12 @@ int sgc_gen_churn_stream(const sgc_csr* g, uint64_t size, uint32_t insert_pct, u
                          uint8_t* types) {
     if (!g || g->n == 0) return -1;
     std::mt19937_64 rng(seed);
-    KeySet live(g->nnz / 2 + size);
+    LiveEdges live(g, size);
     std::vector<uint64_t> live_vec;  // (a << 32 | b), a < b, in the order the reference keeps
     live_vec.reserve(g->nnz / 2 + size);
     for (uint32_t u = 0; u < g->n; u++)
         for (uint64_t j = g->row_ptr[u]; j < g->row_ptr[u + 1]; j++)
-            if (u < g->col_idx[j]) {
-                live.add(key_of(u, g->col_idx[j]));
-                live_vec.push_back(key_of(u, g->col_idx[j]));
-            }
+            if (u < g->col_idx[j]) live_vec.push_back(key_of(u, g->col_idx[j]));
     std::vector<uint64_t> pool;  // deleted edges available for re-insertion
     uint64_t k = 0;
     auto emit = [&](uint64_t e, uint8_t t) {
@@ -429,22 +474,66 @@ int sgc_gen_chung_lu(uint32_t n, double exponent, double avg, double maxd, uint6
         scale *= ratio;
         if (std::fabs(ratio - 1.0) < 1e-9) break;
     }
-    std::vector<double> cdf(n);
     double acc = 0;
-    for (uint32_t i = 0; i < n; i++) cdf[i] = (acc += std::min(w[i] * scale, maxd));
+    for (uint32_t i = 0; i < n; i++) acc += (w[i] = std::min(w[i] * scale, maxd));
     const uint64_t m = (uint64_t)std::llround(acc / 2.0);
-    std::mt19937_64 rng(seed);
-    std::uniform_real_distribution<double> U(0.0, acc);
-    auto draw = [&]() -> uint32_t {
-        const double r = U(rng);
-        return (uint32_t)(std::upper_bound(cdf.begin(), cdf.end(), r) - cdf.begin()) % n;
-    };
+    // Endpoints drawn with probability w_i / sum w from an alias table (Vose's
+    // construction of Walker's alias method): one uniform slot and one coin per
+    // draw instead of a binary search.
+    std::vector<float> prob(n);
+    std::vector<uint32_t> alias(n);
+    {
+        std::vector<double> q(n);
+        std::vector<uint32_t> small, large;
+        for (uint32_t i = 0; i < n; i++) {
+            q[i] = w[i] * (double)n / acc;
+            (q[i] < 1.0 ? small : large).push_back(i);
+        }
+        while (!small.empty() && !large.empty()) {
+            const uint32_t l = small.back(), g = large.back();
+            small.pop_back();
+            large.pop_back();
+            prob[l] = (float)q[l];
+            alias[l] = g;
+            q[g] = (q[g] + q[l]) - 1.0;
+            (q[g] < 1.0 ? small : large).push_back(g);
+        }
+        for (uint32_t i : large) prob[i] = 1.0f, alias[i] = i;
+        for (uint32_t i : small) prob[i] = 1.0f, alias[i] = i;  // rounding leftovers
+    }
+    std::vector<double>().swap(w);
+    // Fixed chunks of draws, each from its own generator seeded by (seed,
+    // chunk): the graph does not depend on the number of threads.
+    const uint64_t chunk = 1ull << 22;
+    const uint64_t nchunks = (m + chunk - 1) / chunk;
+    std::vector<std::vector<uint64_t>> parts(nchunks);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t c = 0; c < (int64_t)nchunks; c++) {
+        std::mt19937_64 rng(seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(c + 1)));
+        auto draw = [&]() -> uint32_t {
+            const uint64_t r = rng();
+            const uint32_t i = (uint32_t)(((r >> 32) * (uint64_t)n) >> 32);
+            const double coin = (double)(uint32_t)r * (1.0 / 4294967296.0);  // in [0, 1)
+            return coin < (double)prob[i] ? i : alias[i];
+        };
+        const uint64_t lo = (uint64_t)c * chunk, hi = std::min(m, lo + chunk);
+        std::vector<uint64_t>& out_c = parts[c];
+        out_c.reserve(hi - lo);
+        for (uint64_t k = lo; k < hi; k++) {
+            const uint32_t u = draw(), v = draw();
+            if (u == v) continue;
+            out_c.push_back(key_of(std::min(u, v), std::max(u, v)));
+        }
+    }
     std::vector<uint64_t> keys;
-    keys.reserve(m);
-    for (uint64_t i = 0; i < m; i++) {
-        const uint32_t u = draw(), v = draw();
-        if (u == v) continue;
-        keys.push_back(key_of(std::min(u, v), std::max(u, v)));
+    {
+        uint64_t total = 0;
+        for (auto& p : parts) total += p.size();
+        keys.reserve(total);
+        for (auto& p : parts) {
+            keys.insert(keys.end(), p.begin(), p.end());
+            std::vector<uint64_t>().swap(p);
+        }
     }
     return csr_from_pairs(n, keys, out);
 }

@@ -475,13 +475,66 @@ int run_check_state(const Dev& g, cudaStream_t s, uint64_t* out) {
     return 0;
 }
 
+namespace {
+
+// Validation without the distinct-edge sort, for slabs beyond 2^32 slots: an
+// undirected edge is counted at its lower endpoint's entry (x < y), so the
+// counts equal the distinct ones when every entry has its mirror.
+__global__ void validate_count_kernel(Dev g, unsigned long long* stats /* uncolored, max color, oor, edges, violations */) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t x = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; x < g.n; x += warps) {
+        const uint16_t cx = color_of(g.st[x]);
+        bool eff = false;
+        unsigned long long oor = 0, edges = 0, viol = 0;
+        warp_for_each(g.col, row_s(g, x), row_e(g, x), [&](uint64_t, uint32_t y) {
+            if (y == INV || (g.blen && (y & TOMB))) return;
+            if (y >= g.n) { oor++; return; }
+            eff = true;
+            if (x < y) {
+                edges++;
+                if (cx != 0 && cx == color_of(g.st[y])) viol++;
+            }
+        });
+        eff = __any_sync(FULL, eff);
+        for (int off = 16; off > 0; off >>= 1) {
+            oor += __shfl_xor_sync(FULL, oor, off);
+            edges += __shfl_xor_sync(FULL, edges, off);
+            viol += __shfl_xor_sync(FULL, viol, off);
+        }
+        if (lane_id() == 0) {
+            if (cx == 0 && eff) atomicAdd(stats + 0, 1ull);
+            atomicMax(stats + 1, (unsigned long long)cx);
+            if (oor) atomicAdd(stats + 2, oor);
+            if (edges) atomicAdd(stats + 3, edges);
+            if (viol) atomicAdd(stats + 4, viol);
+        }
+    }
+}
+
+}  // namespace
+
 int run_validate(const Dev& g, cudaStream_t s, uint64_t* out) {
     // capacity: every live slot
     std::vector<uint64_t> rp_last(1);
     cudaMemcpyAsync(rp_last.data(), g.rp + g.n, 8, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     const uint64_t slots = rp_last[0];
-    if (slots > 0xF0000000ull) return -1;  // distinct count needs a 32-bit key count
+    if (slots > 0xF0000000ull) {  // the distinct-edge sort needs 32-bit key counts: count at the lower endpoint
+        unsigned long long* st = nullptr;
+        if (cudaMallocAsync(&st, 5 * 8, s) != cudaSuccess) return -2;
+        cudaMemsetAsync(st, 0, 5 * 8, s);
+        validate_count_kernel<<<148 * 8, 256, 0, s>>>(g, st);
+        unsigned long long hs[5];
+        cudaMemcpyAsync(hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s);
+        cudaFreeAsync(st, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) return -3;
+        out[0] = hs[4];
+        out[1] = hs[0];
+        out[2] = hs[3];
+        out[3] = hs[1];
+        out[4] = hs[2];
+        return 0;
+    }
     const uint32_t ecap = (uint32_t)(slots ? slots : 1);
     const uint32_t vcap = 1u << 22;
     unsigned long long *ekeys = nullptr, *ekeys2 = nullptr, *vkeys = nullptr, *vkeys2 = nullptr, *stats = nullptr;

@@ -61,6 +61,19 @@ def test_streams_match_oracle(name):
     assert np.array_equal(g.churn_stream(size, pct, 42), O.updates_from(pairs, types))
 
 
+@pytest.mark.parametrize("pct", [10, 90])
+def test_stream_with_unsorted_rows_matches_oracle(pct):
+    """Rows given in descending order take the generator's full live-set path;
+    the stream is the same as the oracle's."""
+    c = MG.build_case("rmat11")
+    rp, col = c["rp"], c["col"].copy()
+    for u in range(len(rp) - 1):
+        col[rp[u]:rp[u + 1]] = col[rp[u]:rp[u + 1]][::-1]
+    g = S.Graph(rp, col, c["deg"])
+    pairs, types = O.bench_stream(rp, col, 6000, pct, 7)
+    assert np.array_equal(g.churn_stream(6000, pct, 7), O.updates_from(pairs, types))
+
+
 def test_loader_matches_oracle(tmp_path):
     rp, col, deg = MG.graph_rmat(9, 8, 1)
     g = S.Graph(rp, col, deg)
