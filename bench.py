@@ -220,8 +220,10 @@ def run_ours(a):
     pinned = torch.from_numpy(bench.view(np.uint8)).pin_memory()
     hptr = pinned.data_ptr()
 
-    def step(ptr, b, timed_events=None):
+    def step(ptr, b, mid=None):
         h.apply_ptr(ptr + b * E * 16, E, S.MODE_CONCURRENT)
+        if mid is not None:
+            mid.record(ext)  # end of the apply kernels on the handle's stream
         return h.publish()
 
     b = 0
@@ -242,17 +244,19 @@ def run_ours(a):
             with torch.cuda.stream(ext):
                 flush.add_(1)
             e0 = torch.cuda.Event(enable_timing=True)
+            ea = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(ext)
-            reps.append(step(dptr, b))
+            reps.append(step(dptr, b, ea))
             e1.record(ext)
-            evs.append((e0, e1))
+            evs.append((e0, ea, e1))
             b += 1
         ext.synchronize()
         torch.cuda.synchronize()
         if a.profile_window:
             torch.cuda.profiler.stop()
-        step_ms = [x.elapsed_time(y) for x, y in evs]
+        step_ms = [x.elapsed_time(z) for x, _, z in evs]
+        apply_ms = [x.elapsed_time(y) for x, y, _ in evs]
         st1 = h.stats()
         # e2e: same steps through the C ABI from pinned host memory, wall clock
         h.synchronize()
@@ -280,9 +284,25 @@ def run_ours(a):
         sweeps = st1["sweep_count"] - st0["sweep_count"]
         achieved = (sweep_bytes / (sweep_ms / 1e3) / 1e9) if sweep_ms > 0 else 0.0
         traffic = read_traffic()
+        apply_avg = sum(apply_ms) / len(apply_ms)
+        bpu = cpu.pop("bytes_per_update", None) if cpu else None
         lat = sorted(step_ms)
         p50 = lat[len(lat) // 2]
         p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
+        pk = f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)" if peak_kind == "measured" else "fallback"
+        roof_sweep = {"bound": "hbm", "kernel": "tier-1 sweep (sweep_items + finalize + fac + commit)",
+                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": pk,
+                      "traffic": traffic, "algorithmic_bytes_per_sweep": sweep_bytes / max(1, sweeps),
+                      "sweep_ms_avg": sweep_ms / max(1, sweeps), "sweeps_timed": sweeps}
+        roof_apply = None
+        if bpu:  # the dominant kernel: the oracle's bytes per update (reference algorithm) over the apply time
+            ach = bpu * E / (apply_avg / 1e3) / 1e9
+            roof_apply = {"bound": "hbm", "kernel": "concurrent apply (conc_prep_insert + conc_prep_prev + "
+                          "conc_apply_kernel)", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                          "peak_kind": pk, "traffic": None,
+                          "algorithmic_bytes": "per update, as the sequential oracle reads and writes them "
+                          "(record, slots scanned, state, bitmaps, recolor walk), counted on the CPU sample",
+                          "algorithmic_bytes_per_launch": bpu * E, "apply_ms_avg": apply_avg}
         conf = dict(desc)
         conf.update(mode="concurrent (warp per edge) + repaired publish per epoch, exact color selection",
                     l2="flushed before every timed step (256 MiB write)", parallelism=f"replicas x{world}",
@@ -296,12 +316,10 @@ def run_ours(a):
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": conf,
             "latency_ms": {"update_to_visible_p50": p50, "update_to_visible_p99": p99},
-            "roofline": {"bound": "hbm", "kernel": "tier-1 sweep (sweep_items + finalize + fac + commit)",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)" if peak_kind == "measured"
-                         else "fallback", "traffic": traffic,
-                         "algorithmic_bytes_per_sweep": sweep_bytes / max(1, sweeps),
-                         "sweep_ms_avg": sweep_ms / max(1, sweeps), "sweeps_timed": sweeps},
+            "roofline": roof_apply if roof_apply else roof_sweep,
+            "roofline_sweep": roof_sweep,
+            "apply": {"ms_per_epoch": apply_avg, "share_of_step": apply_avg / (total_ms / a.steps),
+                      "algorithmic_bytes_per_update": bpu},
             "e2e": {"value": world * a.steps * E / e2e_s, "unit": "updates/s",
                     "h2d_bytes_per_step": (d1["h2d_bytes"] - d0["h2d_bytes"]) // a.steps,
                     "d2h_bytes_per_step": (d1["d2h_bytes"] - d0["d2h_bytes"]) // a.steps},
@@ -324,6 +342,7 @@ def cpu_baseline(g, h, bench, first_batch, nb, budget_s):
     o.load_state(h.col(), h.states(), h.bitmaps(), np.zeros(0, dtype=np.uint32))
     # the GPU's last publish was proper on mirror-complete rows: same repair rules from here
     o.set_repair_state(clean=True, asym=False)
+    o.reset_bytes()
     done = 0
     t0 = time.perf_counter()
     for k in range(nb):
@@ -335,10 +354,12 @@ def cpu_baseline(g, h, bench, first_batch, nb, budget_s):
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
+    bytes_update = o.counters()["bytes_update"]
     o.close()
     if not done:
         return None
     return {"value": done * E / dt, "unit": "updates/s", "cores": int(O.lib().og_num_threads()), "kind": "port",
+            "bytes_per_update": bytes_update / (done * E),
             "sample": f"{done} epochs of {E} updates following the GPU-timed ones, same state and rules "
                       f"(exact selection, independent-set repair), updates in stream order + repaired epoch ({dt:.1f}s)"}
 
