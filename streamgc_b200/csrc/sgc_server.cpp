@@ -71,12 +71,14 @@ struct Group {
     uint32_t alive = 0;
     bool has_work = false;
     bool retired = false;            // all tenants removed: freed at the next step
+    sgc_stats last{};                // the batch's counters after its last tick
+    bool last_ok = true;
 };
 
 double pct(std::vector<double> v, double q) {
     if (v.empty()) return 0.0;
-    std::sort(v.begin(), v.end());
     const size_t i = std::min(v.size() - 1, (size_t)(q * (double)(v.size() - 1) + 0.5));
+    std::nth_element(v.begin(), v.begin() + (ptrdiff_t)i, v.end());
     return v[i];
 }
 
@@ -406,10 +408,17 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
         if (rc != SGC_OK && end_rc == SGC_OK) end_rc = rc;
     }
     if (end_rc != SGC_OK) return end_rc;
+    // counters of the ticked groups while their streams are idle (the stats
+    // call reads them without waiting on a running tick)
+    std::vector<sgc_stats> bst(tb.size());
+    std::vector<int> brc(tb.size());
+    for (size_t i = 0; i < tb.size(); i++) brc[i] = sgc_batch_stats(tb[i], &bst[i]);
     std::lock_guard<std::mutex> lk(s->mu);
     const auto now = clk::now();
     for (size_t i = 0; i < ticking.size(); i++) {
         Group& g = s->groups[ticking[i]];
+        g.last = bst[i];
+        g.last_ok = brc[i] == SGC_OK;
         const sgc_batch_tick_report& tr = trs[i];
         r.groups_ticked++;
         r.updates += tr.updates;
@@ -490,11 +499,9 @@ int sgc_server_get_stats(sgc_server* s, sgc_server_stats* o) {
     for (auto& g : s->groups) {
         if (!g.b) continue;
         o->groups++;
-        sgc_stats bs;
-        const int rc = sgc_batch_stats(g.b, &bs);
-        o->overflows += bs.overflow_pending + bs.overflow_lost;
-        o->drain_failed += bs.drain_failed;
-        if (rc != SGC_OK || bs.device_error) o->device_errors++;
+        o->overflows += g.last.overflow_pending + g.last.overflow_lost;
+        o->drain_failed += g.last.drain_failed;
+        if (!g.last_ok || g.last.device_error) o->device_errors++;
     }
     o->resident_bytes = s->resident_bytes;
     o->budget_bytes = s->opt.hbm_budget_bytes;
