@@ -601,7 +601,8 @@ int sgc_batch_rows(sgc_batch* b, uint32_t graph, uint64_t* row_ptr, uint32_t* co
     uint64_t pos = 0;
     row_ptr[0] = 0;
     for (uint32_t x = 0; x < nvx; x++) {
-        for (uint64_t j = rp[x] - s0; j < rp[x] - s0 + hw[x]; j++) {
+        const uint64_t len = std::min<uint64_t>(hw[x], rp[x + 1] - rp[x]);  // a mark never exceeds the row
+        for (uint64_t j = rp[x] - s0; j < rp[x] - s0 + len; j++) {
             const uint32_t y = slots[j];
             if (y >= off && y < off + nvx) {  // live entries only (INV and deleted run entries are >= 2^31)
                 if (col) {
