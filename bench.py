@@ -204,7 +204,7 @@ def run_ours(a):
 
     t = time.time()
     h = S.StreamGC(g, epoch_size=E, histogram_threshold=HIST_THR, slack_pct=300, max_batch=1 << 20,
-                   device=local, profile=True, exact_select=True)
+                   device=local, profile=not a.graph_publish, exact_select=True, graph_publish=a.graph_publish)
     for s in range(0, 0 if init is None else len(init), 1 << 20):
         h.apply(init[s:s + (1 << 20)], S.MODE_CONCURRENT)
     rep = h.publish()
@@ -304,7 +304,8 @@ def run_ours(a):
                           "(record, slots scanned, state, bitmaps, recolor walk), counted on the CPU sample",
                           "algorithmic_bytes_per_launch": bpu * E, "apply_ms_avg": apply_avg}
         conf = dict(desc)
-        conf.update(mode="concurrent (warp per edge) + repaired publish per epoch, exact color selection",
+        conf.update(mode="concurrent (warp per edge) + repaired publish per epoch, exact color selection"
+                    + (", publish as one CUDA graph" if a.graph_publish else ""),
                     l2="flushed before every timed step (256 MiB write)", parallelism=f"replicas x{world}",
                     valid_after_run=val["violations"] == 0 and val["uncolored_with_edges"] == 0,
                     colors_used=int(val["max_color"]), static_greedy_colors=None,
@@ -765,6 +766,9 @@ def main():
     ap.add_argument("--workload", default="skewed", choices=["skewed", "small", "large"],
                     help="plain path: skewed (R-MAT 2^20 x 48, k-core stream), small (Delaunay 2^17 churn), "
                          "large (Chung-Lu 65.6 M vertices, ~1.8 G edges, 10 M churn)")
+    ap.add_argument("--graph-publish", action="store_true",
+                    help="plain path: each publish replays one captured CUDA graph (no per-sweep host sync; "
+                         "sweeps are then not timed one by one)")
     ap.add_argument("--epoch-size", type=int, default=32768,
                     help="plain path: updates per epoch (the large workload's sweep uses 4096, 32768, 262144)")
     ap.add_argument("--cpu-batches", type=int, default=8, help="epochs timed on the CPU baseline (0: skip)")

@@ -43,6 +43,11 @@ typedef struct sgc_handle sgc_handle;
  * never rebuilt and drift, color_select.cuh:120-209). No histogram rows are
  * allocated. Bit-exact parity with the reference needs this flag off. */
 #define SGC_OPT_EXACT_SELECT 2u
+/* With SGC_OPT_EXACT_SELECT, a publish after concurrent batches replays one
+ * captured CUDA graph (compaction, drain, the repair loop as a conditional
+ * while-node, snapshot): one host synchronization per epoch instead of one per
+ * sweep. Sweeps are not timed one by one (sgc_stats.sweep_ms stays 0). */
+#define SGC_OPT_GRAPH_PUBLISH 4u
 
 typedef struct sgc_options {
     uint32_t struct_size;      /* sizeof(sgc_options) */

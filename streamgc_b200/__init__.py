@@ -385,13 +385,13 @@ class StreamGC:
 
     def __init__(self, graph: Graph, epoch_size=32768, histogram_threshold=64, slack_pct=300,
                  max_hist_colors=1024, max_batch=32768, device=0, profile=False, exact_select=False,
-                 full_repair_every=None, repair_tile=None):
+                 full_repair_every=None, repair_tile=None, graph_publish=False):
         L = lib()
         cfg = _Config(1, graph.n, graph.nnz, 1 << 20, epoch_size, 100, histogram_threshold, 0.2)
         opt = _Options()
         L.sgc_default_options(C.byref(opt))
         opt.slack_pct, opt.max_hist_colors, opt.max_batch, opt.device = slack_pct, max_hist_colors, max_batch, device
-        opt.flags = (1 if profile else 0) | (2 if exact_select else 0)
+        opt.flags = (1 if profile else 0) | (2 if exact_select else 0) | (4 if graph_publish else 0)
         if full_repair_every is not None:
             opt.full_repair_every = full_repair_every
         if repair_tile is not None:

@@ -176,15 +176,22 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep, bool force_full) {
         if (!rc->cont) break;
     }
     TRY(check_cuda("repair"));
-    h->tier1_sweeps += rc->it;
-    if (!rc->incr) h->live_entries = rc->live;
-    h->repairs_since_full = rc->incr ? h->repairs_since_full + 1 : 0;
     if (prof) {
         unsigned long long sw[2];
         CK(cudaMemcpyAsync(sw, h->sb.swept, 16, cudaMemcpyDeviceToHost, h->stream));
         TRY(sync(h));
         h->sweep_bytes += 8ull * sw[0] + 28ull * sw[1];
     }
+    return finish_repair(h, rep);
+}
+
+// After the Tier-1 loop (its control block read back into h_rc_out): the
+// counters, and Tier-2 when the loop did not leave a proper coloring.
+int finish_repair(sgc_handle* h, sgc_repair_report* rep) {
+    const RepairCtl* rc = h->h_rc_out;
+    h->tier1_sweeps += rc->it;
+    if (!rc->incr) h->live_entries = rc->live;
+    h->repairs_since_full = rc->incr ? h->repairs_since_full + 1 : 0;
     sgc_repair_report r{};
     r.tier1_iterations = rc->it;
     r.tier1_last_count = rc->need;
@@ -209,6 +216,119 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep, bool force_full) {
         *rep = r;
     }
     return SGC_OK;
+}
+
+// ---- the concurrent configuration's publish as a CUDA graph ----
+//
+// compaction of edited rows, overflow drain, the repair's start, a
+// conditional while-node { sweep, step } and the snapshot into one half of
+// the double buffer, captured once per half; the repair's host fields (mode,
+// sweep cap, full repair) reach the device through the graph's first copy,
+// from pinned memory written before each launch. One host synchronization per
+// epoch instead of one per sweep.
+
+void enqueue_publish_head(sgc_handle* h, cudaStream_t s) {
+    cudaMemsetAsync(&h->ctl->dirty_count, 0, 4, s);
+    launch_dirty_list(h->g, h->dirty_list, &h->ctl->dirty_count, s);
+    launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, false, s);
+    launch_take_overflow(h->g, &h->ctl->drain_n, s);
+    launch_drain(h->g, &h->ctl->drain_n, false, &h->ctl->drain_failed, s);
+    cudaMemcpyAsync(h->sb.rc, h->h_rc_in, 12, cudaMemcpyHostToDevice, s);
+    const size_t mwords = ((h->n + 31) / 32) * 4;
+    cudaMemsetAsync(h->sb.wmark, 0, mwords, s);
+    cudaMemsetAsync(h->sb.rbits, 0, mwords, s);
+    cudaMemsetAsync(h->sb.needf, 0, h->n, s);
+    launch_repair_begin(h->g, h->sb, SWEEP_INDEP, h->num_sms, s);
+}
+
+void drop_publish_graphs(sgc_handle* h) {
+    for (int k = 0; k < 2; k++) {
+        if (h->pub_exec[k]) cudaGraphExecDestroy(h->pub_exec[k]);
+        if (h->pub_graph[k]) cudaGraphDestroy(h->pub_graph[k]);
+        h->pub_exec[k] = nullptr;
+        h->pub_graph[k] = nullptr;
+    }
+}
+
+int capture_publish_impl(sgc_handle* h, int back) {
+    cudaStream_t s = h->stream;
+    cudaGraph_t& graph = h->pub_graph[back];
+    CK(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle cond;
+    CK(cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault));
+    CK(cudaStreamBeginCaptureToGraph(s, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_publish_head(h, s);
+    cudaStreamCaptureStatus st;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    CK(cudaStreamGetCaptureInfo(s, &st, nullptr, nullptr, &deps, &ndeps));
+    std::vector<cudaGraphNode_t> head_tail(deps, deps + ndeps);
+    cudaGraph_t g0 = nullptr;
+    CK(cudaStreamEndCapture(s, &g0));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CK(cudaGraphAddNode(&cnode, graph, head_tail.data(), head_tail.size(), &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    launch_repair_sweep(h->g, h->sb, SWEEP_INDEP, h->num_sms, s);
+    launch_repair_step(h->g, h->sb, h->num_sms, s, &cond);
+    cudaGraph_t g1 = nullptr;
+    CK(cudaStreamEndCapture(s, &g1));
+    CK(cudaStreamBeginCaptureToGraph(s, graph, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
+    launch_snapshot(h->g, h->snap[back], s);
+    cudaMemcpyAsync(h->h_rc_out, h->sb.rc, sizeof(RepairCtl), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h->h_small + 32, h->sb.swept, 16, cudaMemcpyDeviceToHost, s);
+    cudaGraph_t g2 = nullptr;
+    CK(cudaStreamEndCapture(s, &g2));
+    CK(cudaGraphInstantiate(&h->pub_exec[back], graph, 0));
+    return SGC_OK;
+}
+
+int capture_publish(sgc_handle* h, int back) {
+    const int r = capture_publish_impl(h, back);
+    if (r != SGC_OK) {  // leave the stream out of capture mode; the eager publish takes over
+        cudaStreamCaptureStatus st;
+        if (cudaStreamIsCapturing(h->stream, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(h->stream, &g);
+            if (g) cudaGraphDestroy(g);
+        }
+        cudaGetLastError();
+        drop_publish_graphs(h);
+        h->pub_graph_failed = true;
+    }
+    return r;
+}
+
+int publish_graph(sgc_handle* h, sgc_repair_report* rep) {
+    const int back = 1 - h->front;
+    const uint32_t every = h->opt.full_repair_every;
+    RepairCtl* hin = h->h_rc_in;  // read by the graph's first copy
+    hin->mode = (uint32_t)SWEEP_INDEP;
+    hin->max_sweeps = 64u;
+    hin->force_all = (every && h->repairs_since_full + 1 >= every) ? 1u : 0u;
+    CK(cudaGraphLaunch(h->pub_exec[back], h->stream));
+    TRY(sync(h));
+    TRY(check_cuda("publish graph"));
+    const RepairCtl* rc = h->h_rc_out;
+    const unsigned long long* sw = (const unsigned long long*)(h->h_small + 32);
+    h->sweep_bytes += 8ull * sw[0] + 28ull * sw[1];
+    h->launches += (h->g.touched ? 6 : 5) + 10ull * rc->it + 1;
+    h->d2h_bytes += sizeof(RepairCtl) + 16;
+    sgc_repair_report r{};
+    TRY(finish_repair(h, &r));
+    if (r.tier2_ran) {  // Tier-2 changed colors after the graph's snapshot: take it again
+        launch_snapshot(h->g, h->snap[back], h->stream);
+        h->launches += 1;
+    }
+    h->front = back;
+    h->epochs++;
+    if (rep) *rep = r;
+    return check_cuda("publish");
 }
 
 int read_drain(sgc_handle* h, sgc_repair_report* rep, unsigned long long before_failed) {
@@ -247,6 +367,7 @@ int sgc_destroy(sgc_handle* h) {
     if (!h) return SGC_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_publish_graphs(h);
     for (void* p : h->allocs) cudaFree(p);
     if (h->h_stage) cudaFreeHost(h->h_stage);
     if (h->h_small) cudaFreeHost(h->h_small);
@@ -592,6 +713,11 @@ int sgc_repair(sgc_handle* h, sgc_repair_report* rep) {
 int sgc_publish(sgc_handle* h, sgc_repair_report* rep) {
     if (!h) return fail(SGC_EINVAL, "null handle");
     CK(cudaSetDevice(h->device));
+    if ((h->opt.flags & SGC_OPT_GRAPH_PUBLISH) && h->g.exact && h->last_mode == SGC_MODE_CONCURRENT &&
+        !h->pub_graph_failed) {
+        const int back = 1 - h->front;
+        if (h->pub_exec[back] || capture_publish(h, back) == SGC_OK) return publish_graph(h, rep);
+    }
     sgc_repair_report r{};
     TRY(compact_dirty(h, false));
     TRY(drain(h, h->last_mode == SGC_MODE_DETERMINISTIC, &h->ctl->drain_failed));

@@ -80,6 +80,10 @@ struct sgc_handle {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
     double sweep_ms = 0;
     uint64_t sweep_count = 0, sweep_bytes = 0, live_entries = 0;
+    // SGC_OPT_GRAPH_PUBLISH: the publish captured once per snapshot half
+    cudaGraph_t pub_graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t pub_exec[2] = {nullptr, nullptr};
+    bool pub_graph_failed = false;  // capture failed: the eager publish
     uint64_t launches = 0;          // kernels this handle launched
     uint64_t h2d_bytes = 0, d2h_bytes = 0;  // bytes the library moved across PCIe / C2C
 };
@@ -116,6 +120,8 @@ int compact_dirty(sgc_handle* h, bool force);
 int drain(sgc_handle* h, bool ordered, unsigned long long* failed_counter);
 int set_clean(sgc_handle* h, uint32_t v);
 int repair_loop(sgc_handle* h, sgc_repair_report* rep, bool force_full);
+int finish_repair(sgc_handle* h, sgc_repair_report* rep);
+void drop_publish_graphs(sgc_handle* h);
 // Extra layout of a handle that holds several graphs (the batched engine).
 struct CreateExtra {
     const uint32_t* thr_word;  // per 32-vertex word: histogram threshold (null: cfg->histogram_threshold)

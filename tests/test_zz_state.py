@@ -59,3 +59,28 @@ def test_batched_rows_keep_their_invariants():
             assert _clean(b.check_state()), (t, b.check_state())
     finally:
         b.close()
+
+
+@pytest.mark.parametrize("name", ["delaunay2k", "rmat11"])
+def test_graph_publish_is_proper_and_keeps_invariants(name):
+    """The captured-graph publish (SGC_OPT_GRAPH_PUBLISH): every published
+    snapshot proper, the rows' invariants kept, the same counters advancing as
+    with the eager publish."""
+    c = MG.build_case(name)
+    g = S.Graph(c["rp"], c["col"], c["deg"])
+    ups = np.concatenate([c["init"], c["bench"]])
+    with S.StreamGC(g, epoch_size=c["E"], histogram_threshold=c["thr"], slack_pct=c["slack"],
+                    exact_select=True, graph_publish=True) as h:
+        B = 2048
+        for i, s in enumerate(range(0, len(ups), B)):
+            h.apply(ups[s:s + B], S.MODE_CONCURRENT)
+            rep = h.publish()
+            assert rep["proper"] == 1, (i, rep)
+            assert rep["tier1_iterations"] >= 1
+            assert _clean(h.check_state()), (i, h.check_state())
+            snap = h.snapshot()
+            assert np.array_equal(snap, h.colors())  # the published half holds the current colors
+        v = h.validate()
+        assert v["violations"] == 0 and v["uncolored_with_edges"] == 0
+        st = h.stats()
+        assert st["epochs"] >= len(ups) // B and st["tier1_sweeps"] >= st["epochs"]
