@@ -262,8 +262,16 @@ def run_ours(a):
         h.synchronize()
         d0 = h.stats()
         t0 = time.perf_counter()
-        for _ in range(a.steps):
-            step(hptr, b)
+        if a.ingest:  # the next batch's copy staged before this epoch's publish
+            h.stage_ptr(hptr + b * E * 16, E)
+        for k in range(a.steps):
+            if a.ingest:
+                h.apply_staged(S.MODE_CONCURRENT)
+                if k + 1 < a.steps:
+                    h.stage_ptr(hptr + (b + 1) * E * 16, E)
+                h.publish()
+            else:
+                step(hptr, b)
             h.stats()  # the step's result read back to the host
             b += 1
         h.synchronize()
@@ -305,7 +313,8 @@ def run_ours(a):
                           "algorithmic_bytes_per_launch": bpu * E, "apply_ms_avg": apply_avg}
         conf = dict(desc)
         conf.update(mode="concurrent (warp per edge) + repaired publish per epoch, exact color selection"
-                    + (", publish as one CUDA graph" if a.graph_publish else ""),
+                    + (", publish as one CUDA graph" if a.graph_publish else "")
+                    + (", e2e through the ingest slots" if a.ingest else ""),
                     l2="flushed before every timed step (256 MiB write)", parallelism=f"replicas x{world}",
                     valid_after_run=val["violations"] == 0 and val["uncolored_with_edges"] == 0,
                     colors_used=int(val["max_color"]), static_greedy_colors=None,
@@ -766,6 +775,9 @@ def main():
     ap.add_argument("--workload", default="skewed", choices=["skewed", "small", "large"],
                     help="plain path: skewed (R-MAT 2^20 x 48, k-core stream), small (Delaunay 2^17 churn), "
                          "large (Chung-Lu 65.6 M vertices, ~1.8 G edges, 10 M churn)")
+    ap.add_argument("--ingest", action="store_true",
+                    help="plain path, e2e: batches staged through the two ingest slots (copy of the next "
+                         "batch overlapping this epoch's publish)")
     ap.add_argument("--graph-publish", action="store_true",
                     help="plain path: each publish replays one captured CUDA graph (no per-sweep host sync; "
                          "sweeps are then not timed one by one)")

@@ -153,6 +153,17 @@ int sgc_destroy(sgc_handle* h);
  * streamgc.cu:828-856): local_update_kernel semantics per update. `updates`
  * may be host (pageable or pinned) or device memory. No epoch work. */
 int sgc_apply(sgc_handle* h, const EdgeUpdate* updates, uint32_t n, int mode);
+/* Stream ingest (the reference's feeder ring, feeder_thread.cpp:25-92, unused
+ * there): sgc_stage copies a host batch (n <= max_batch) into the next of two
+ * device staging slots on the handle's copy stream and returns without waiting
+ * for the GPU; sgc_apply_staged applies the oldest staged batch on the handle's
+ * stream once its copy is done. Staging batch k+1 before publishing batch k
+ * overlaps the copy with the repair. Pageable input is copied into pinned
+ * memory before sgc_stage returns; pinned or device input is copied as it is
+ * and must not change until the batch is applied. At most two batches are
+ * staged; SGC_EINVAL when both slots are full (stage) or none is (apply). */
+int sgc_stage(sgc_handle* h, const EdgeUpdate* updates, uint32_t n);
+int sgc_apply_staged(sgc_handle* h, int mode);
 
 /* Reference epoch boundary (streamgc.cu:949-1012): publish the snapshot of the
  * current colors, compact edited rows, drain overflow, rebuild bitmaps. */

@@ -164,6 +164,8 @@ SIGNATURES = {
     "sgc_create_ex": (C.c_int, [C.POINTER(_Config), C.POINTER(_Options), _u64p, _u32p, _u32p, C.POINTER(_vp)]),
     "sgc_destroy": (C.c_int, [_vp]),
     "sgc_apply": (C.c_int, [_vp, _vp, C.c_uint32, C.c_int]),
+    "sgc_stage": (C.c_int, [_vp, C.c_void_p, C.c_uint32]),
+    "sgc_apply_staged": (C.c_int, [_vp, C.c_int]),
     "sgc_epoch": (C.c_int, [_vp]),
     "sgc_drain_and_compact": (C.c_int, [_vp, C.POINTER(RepairReport)]),
     "sgc_repair": (C.c_int, [_vp, C.POINTER(RepairReport)]),
@@ -429,6 +431,20 @@ class StreamGC:
         for s in range(0, len(ups), self.max_batch):
             part = ups[s: s + self.max_batch]
             _check(lib().sgc_apply(self.h, part.ctypes.data, len(part), mode), "sgc_apply")
+
+    def stage(self, ups):
+        """Copies a host batch (<= max_batch updates) into the next ingest slot
+        without waiting for the GPU; apply it later with apply_staged()."""
+        ups = np.ascontiguousarray(ups, dtype=EDGE_UPDATE)
+        _check(lib().sgc_stage(self.h, ups.ctypes.data, len(ups)), "sgc_stage")
+
+    def stage_ptr(self, ptr, n):
+        """stage() for updates at a pinned host or device address (unchanged until applied)."""
+        _check(lib().sgc_stage(self.h, C.c_void_p(ptr), n), "sgc_stage")
+
+    def apply_staged(self, mode=MODE_CONCURRENT):
+        """Applies the oldest staged batch once its copy is done."""
+        _check(lib().sgc_apply_staged(self.h, mode), "sgc_apply_staged")
 
     def apply_ptr(self, ptr, n, mode=MODE_CONCURRENT):
         """Updates already in device (or pinned host) memory at address `ptr`."""

@@ -218,6 +218,41 @@ int finish_repair(sgc_handle* h, sgc_repair_report* rep) {
     return SGC_OK;
 }
 
+// ---- applying a batch that is already on the device ----
+
+int apply_device(sgc_handle* h, const EdgeUpdate* src, uint32_t n, int mode) {
+    if (mode == SGC_MODE_DETERMINISTIC) {
+        launch_det_apply(h->g, src, n, h->stream);
+        h->launches += 1;
+    } else {
+        launch_conc_apply(h->g, src, n, h->eo, h->num_sms, h->stream);
+        h->launches += 3;
+    }
+    h->last_mode = mode;
+    h->updates += n;
+    return check_cuda("apply");
+}
+
+// The ingest slots, made on first use: two device batches of max_batch
+// updates, their pinned host images, a copy stream and the events that order
+// a slot's copy before its apply and its apply before its next copy.
+int ensure_ingest(sgc_handle* h) {
+    if (h->copy_stream) return SGC_OK;
+    const size_t bytes = (size_t)h->opt.max_batch * sizeof(EdgeUpdate);
+    for (int k = 0; k < 2; k++) {
+        int r = dalloc(h, &h->slot_dev[k], h->opt.max_batch);
+        if (r) return r;
+        if (cudaHostAlloc(&h->slot_host[k], bytes, cudaHostAllocDefault) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->copy_done[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->slot_free[k], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SGC_ENOMEM, "ingest slot allocation failed");
+        }
+    }
+    CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    return SGC_OK;
+}
+
 // ---- the concurrent configuration's publish as a CUDA graph ----
 //
 // compaction of edited rows, overflow drain, the repair's start, a
@@ -368,6 +403,13 @@ int sgc_destroy(sgc_handle* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_publish_graphs(h);
+    if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+    for (int k = 0; k < 2; k++) {
+        if (h->slot_host[k]) cudaFreeHost(h->slot_host[k]);
+        if (h->copy_done[k]) cudaEventDestroy(h->copy_done[k]);
+        if (h->slot_free[k]) cudaEventDestroy(h->slot_free[k]);
+    }
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     for (void* p : h->allocs) cudaFree(p);
     if (h->h_stage) cudaFreeHost(h->h_stage);
     if (h->h_small) cudaFreeHost(h->h_small);
@@ -659,16 +701,48 @@ int sgc_apply(sgc_handle* h, const EdgeUpdate* ups, uint32_t n, int mode) {
         h->h2d_bytes += (uint64_t)n * sizeof(EdgeUpdate);
         src = h->d_batch;
     }
-    if (mode == SGC_MODE_DETERMINISTIC) {
-        launch_det_apply(h->g, src, n, h->stream);
-        h->launches += 1;
+    return apply_device(h, src, n, mode);
+}
+
+int sgc_stage(sgc_handle* h, const EdgeUpdate* ups, uint32_t n) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    if (n == 0) return SGC_OK;
+    if (!ups) return fail(SGC_EINVAL, "null updates");
+    if (n > h->opt.max_batch) return fail(SGC_EINVAL, "batch %u exceeds max_batch %u", n, h->opt.max_batch);
+    if (h->staged == 2) return fail(SGC_EINVAL, "both staging slots hold a batch");
+    CK(cudaSetDevice(h->device));
+    TRY(ensure_ingest(h));
+    const uint32_t k = h->stage_next;
+    CK(cudaEventSynchronize(h->slot_free[k]));  // the apply that read this slot (and its copy) finished
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, ups) != cudaSuccess) cudaGetLastError();
+    const size_t bytes = (size_t)n * sizeof(EdgeUpdate);
+    if (attr.type == cudaMemoryTypeHost || attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) {
+        // pinned or device memory: copied as it is (it must not change until the copy is done)
+        CK(cudaMemcpyAsync(h->slot_dev[k], ups, bytes, cudaMemcpyDefault, h->copy_stream));
     } else {
-        launch_conc_apply(h->g, src, n, h->eo, h->num_sms, h->stream);
-        h->launches += 3;
+        std::memcpy(h->slot_host[k], ups, bytes);
+        CK(cudaMemcpyAsync(h->slot_dev[k], h->slot_host[k], bytes, cudaMemcpyHostToDevice, h->copy_stream));
     }
-    h->last_mode = mode;
-    h->updates += n;
-    return check_cuda("apply");
+    CK(cudaEventRecord(h->copy_done[k], h->copy_stream));
+    h->h2d_bytes += (uint64_t)n * sizeof(EdgeUpdate);
+    h->slot_n[k] = n;
+    h->stage_next = 1 - k;
+    h->staged++;
+    return SGC_OK;
+}
+
+int sgc_apply_staged(sgc_handle* h, int mode) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    if (h->staged == 0) return fail(SGC_EINVAL, "no staged batch");
+    if (mode != SGC_MODE_DETERMINISTIC && mode != SGC_MODE_CONCURRENT) return fail(SGC_EINVAL, "bad mode %d", mode);
+    CK(cudaSetDevice(h->device));
+    const uint32_t k = h->staged == 2 ? h->stage_next : 1 - h->stage_next;  // the oldest staged slot
+    CK(cudaStreamWaitEvent(h->stream, h->copy_done[k], 0));
+    TRY(apply_device(h, h->slot_dev[k], h->slot_n[k], mode));
+    CK(cudaEventRecord(h->slot_free[k], h->stream));
+    h->staged--;
+    return SGC_OK;
 }
 
 int sgc_epoch(sgc_handle* h) {

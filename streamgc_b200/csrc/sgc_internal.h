@@ -80,6 +80,14 @@ struct sgc_handle {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
     double sweep_ms = 0;
     uint64_t sweep_count = 0, sweep_bytes = 0, live_entries = 0;
+    // stream ingest: two device slots filled on a copy stream (allocated on first use)
+    cudaStream_t copy_stream = nullptr;
+    EdgeUpdate* slot_dev[2] = {nullptr, nullptr};
+    EdgeUpdate* slot_host[2] = {nullptr, nullptr};  // pinned
+    cudaEvent_t copy_done[2] = {nullptr, nullptr};
+    cudaEvent_t slot_free[2] = {nullptr, nullptr};
+    uint32_t slot_n[2] = {0, 0};
+    uint32_t stage_next = 0, staged = 0;  // next slot to fill; slots holding a batch (oldest first from stage_next - staged)
     // SGC_OPT_GRAPH_PUBLISH: the publish captured once per snapshot half
     cudaGraph_t pub_graph[2] = {nullptr, nullptr};
     cudaGraphExec_t pub_exec[2] = {nullptr, nullptr};
@@ -121,6 +129,8 @@ int drain(sgc_handle* h, bool ordered, unsigned long long* failed_counter);
 int set_clean(sgc_handle* h, uint32_t v);
 int repair_loop(sgc_handle* h, sgc_repair_report* rep, bool force_full);
 int finish_repair(sgc_handle* h, sgc_repair_report* rep);
+int apply_device(sgc_handle* h, const EdgeUpdate* src, uint32_t n, int mode);
+int ensure_ingest(sgc_handle* h);
 void drop_publish_graphs(sgc_handle* h);
 // Extra layout of a handle that holds several graphs (the batched engine).
 struct CreateExtra {

@@ -2,7 +2,9 @@
 publish and tick the rows of a handle keep their high-water marks inside the
 row capacity, only free slots past the mark, vertex ids in range, a sorted
 base run (exact selection) or sorted never-edited rows, hole counters that
-never wrap, and colors in range; in stream order and in concurrent batches."""
+never wrap, and colors in range; in stream order and in concurrent batches.
+Then the stream-ingest slots against direct applies, and the captured-graph
+publish."""
 import numpy as np
 import pytest
 
@@ -59,6 +61,34 @@ def test_batched_rows_keep_their_invariants():
             assert _clean(b.check_state()), (t, b.check_state())
     finally:
         b.close()
+
+
+@pytest.mark.parametrize("name", ["delaunay2k", "overflow512"])
+def test_staged_batches_match_direct_applies(name):
+    """Stream ingest (sgc_stage / sgc_apply_staged): in stream order, batches
+    staged ahead (two slots, the next one copied before the current epoch
+    ends) give the same colors and rows as the same batches applied directly."""
+    c = MG.build_case(name)
+    ups = np.concatenate([c["init"], c["bench"]])
+    B = c["batch"]
+    parts = [ups[s:s + B] for s in range(0, len(ups), B)]
+    kw = dict(epoch_size=c["E"], histogram_threshold=c["thr"], slack_pct=c["slack"], max_batch=max(B, 1024))
+    with S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"]), **kw) as a, \
+            S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"]), **kw) as b:
+        b.stage(parts[0])
+        for i, p in enumerate(parts):
+            a.apply(p, S.MODE_DETERMINISTIC)
+            if i + 1 < len(parts):
+                b.stage(parts[i + 1])  # copied while batch i is applied
+            b.apply_staged(S.MODE_DETERMINISTIC)
+            if i % 3 == 2:
+                a.epoch()
+                b.epoch()
+                assert np.array_equal(a.colors(), b.colors()), i
+        assert np.array_equal(a.states(), b.states())
+        assert np.array_equal(a.col(), b.col())
+        with pytest.raises(S.StreamGCError):
+            b.apply_staged(S.MODE_DETERMINISTIC)  # nothing staged
 
 
 @pytest.mark.parametrize("name", ["delaunay2k", "rmat11"])
