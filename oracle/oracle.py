@@ -98,6 +98,7 @@ def lib():
             "og_loaded_copy": (None, [_vp, _u64p, _u32p, _u32p]),
             "og_loaded_free": (None, [_vp]),
             "og_num_threads": (C.c_int, []),
+            "og_set_threads": (None, [C.c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

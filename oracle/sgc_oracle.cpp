@@ -1191,4 +1191,14 @@ int og_num_threads(void) {
 #endif
 }
 
+// Threads of the order-independent passes (compaction, rebuild, repair
+// decisions, validation); updates stay in stream order on one thread.
+void og_set_threads(int t) {
+#ifdef _OPENMP
+    if (t > 0) omp_set_num_threads(t);
+#else
+    (void)t;
+#endif
+}
+
 }  // extern "C"
