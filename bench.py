@@ -672,7 +672,7 @@ def run_served(a):
     log(f"served (rank {rank}): {len(mine)} of {T} tenants generated in {time.time() - t:.1f}s; "
         f"{len(events)} requests over {dur}s")
     srv = S.Server(hbm_budget_bytes=150 << 30, max_tick_updates=1 << 22, max_staleness_us=a.served_staleness_us,
-                   device=local, profile=True)
+                   device=local, profile=True, regrow=a.served_regrow)
     tids = {k: srv.add_tenant(S.Graph(data[k]["row_ptr"], data[k]["col"]), epoch_size=data[k]["spec"]["epoch"])
             for k in mine}
     t = time.time()
@@ -744,7 +744,7 @@ def run_served(a):
            st["ticks"] - st0["ticks"], st["tier2_ticks"] - st0["tier2_ticks"],
            st["tier2_mirror_ticks"] - st0["tier2_mirror_ticks"], st["tier1_sweeps"] - st0["tier1_sweeps"],
            st["tick_device_ms"] - st0["tick_device_ms"], sum(need[k] for k in mine), st["overflows"],
-           st["drain_failed"], st["device_errors"], len(steps), sum(steps)]
+           st["drain_failed"], st["device_errors"], len(steps), sum(steps), st["tenants_regrown"]]
     worst = [t_end, t_sub, late, st["visible_p50_ms"], st["visible_p99_ms"], st["query_p50_ms"], st["query_p99_ms"],
              step_p50, step_p99]
     if dist:  # tenants on every rank: every rank's work, the slowest rank's times and latencies
@@ -757,7 +757,7 @@ def run_served(a):
         if rank != 0:
             return
     (applied, nreq, nq, resident, nv, ne, ticks, t2, t2m, sweeps, tick_ms, offered, ovf, dfail, derr,
-     nsteps, steps_ms) = cnt
+     nsteps, steps_ms, regrown) = cnt
     t_end, t_sub, late, v50, v99, q50, q99, step_p50, step_p99 = worst
     out = {
         "metric": METRIC, "form": "served", "value": applied / t_end, "unit": "updates/s", "n_gpus": world,
@@ -775,7 +775,7 @@ def run_served(a):
                    "tier2_mirror_ticks": int(t2m), "sweeps_per_tick": round(sweeps / max(1, ticks), 2),
                    "tick_device_ms_total": round(tick_ms, 1), "offered_updates": int(offered),
                    "overflows": int(ovf), "drain_failed": int(dfail), "device_errors": int(derr),
-                   "asymmetric_tenants": asym},
+                   "asymmetric_tenants": asym, "regrow": bool(a.served_regrow), "tenants_regrown": int(regrown)},
         "latency_ms": {"update_to_visible_p50": v50, "update_to_visible_p99": v99,
                        "query_p50": q50, "query_p99": q99, "step_p50": step_p50, "step_p99": step_p99},
         "clocks": clk.summary(),
@@ -812,6 +812,8 @@ def main():
     ap.add_argument("--served-seconds", type=float, default=8.0)
     ap.add_argument("--served-staleness-us", type=int, default=2000)
     ap.add_argument("--served-check", action="store_true", help="served: check every tenant's rows for mirrors after the run")
+    ap.add_argument("--served-regrow", action="store_true",
+                    help="served: re-admit tenants whose rows dropped entries, with rebuilt rows")
     a = ap.parse_args()
     global E
     E = a.epoch_size

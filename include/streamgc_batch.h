@@ -113,6 +113,11 @@ int sgc_batch_snapshot(sgc_batch* b, uint32_t graph, uint16_t* out);  /* num_ver
 int sgc_batch_rows(sgc_batch* b, uint32_t graph, uint64_t* row_ptr, uint32_t* col, uint64_t col_cap);
 /* Validator over all graphs (the reference's, streamgc.cu:448-556). */
 int sgc_batch_validate(sgc_batch* b, sgc_validation* out);
+/* out[k] = 1 when graph k has dropped an entry since its creation: an
+ * insert that found its row still full at the drain, or that arrived with the
+ * overflow buffer full (the reference drops such entries too; the mirror
+ * entry in the other row stays). Between ticks. */
+int sgc_batch_dropped(sgc_batch* b, uint8_t* out);
 /* Layout invariants of every graph's rows (sgc_check_state); between ticks. */
 int sgc_batch_check_state(sgc_batch* b, sgc_state_report* out);
 

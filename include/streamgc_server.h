@@ -43,6 +43,9 @@ typedef struct sgc_server_options {
     uint32_t max_staleness_us;   /* 0: epochs close by update count only */
     int32_t  device;
     uint32_t slack_pct;          /* 300 = alpha 4 */
+    uint32_t regrow;             /* 1: a tenant whose rows dropped an entry (a row still full at the
+                                    drain) is re-admitted with rows sized from its current degrees and
+                                    every surviving entry's mirror restored; 0 (default): kept as is */
 } sgc_server_options;
 
 enum { SGC_TENANT_QUEUED = 0, SGC_TENANT_RESIDENT = 1, SGC_TENANT_REMOVED = 2 };
@@ -68,6 +71,7 @@ typedef struct sgc_server_stats {
     double   tick_device_ms;                    /* device time of the ticks (SGC_BATCH_PROFILE groups), else 0 */
     uint64_t overflows, drain_failed;           /* row overflows (pending + lost) and failed drains, all groups */
     uint64_t device_errors;                     /* groups whose device error word is set */
+    uint64_t tenants_regrown;                   /* re-admissions with rebuilt rows (options.regrow) */
 } sgc_server_stats;
 
 int sgc_server_default_options(sgc_server_options* opt);

@@ -133,7 +133,7 @@ BATCH_FEED = C.CFUNCTYPE(C.c_int, _vp, _vp)
 class ServerOptions(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("flags", C.c_uint32), ("hbm_budget_bytes", C.c_uint64),
                 ("max_tick_updates", C.c_uint32), ("max_staleness_us", C.c_uint32), ("device", C.c_int32),
-                ("slack_pct", C.c_uint32)]
+                ("slack_pct", C.c_uint32), ("regrow", C.c_uint32)]
 
 
 class StepReport(C.Structure):
@@ -153,7 +153,7 @@ class ServerStats(C.Structure):
                 ("query_p50_ms", C.c_double), ("query_p99_ms", C.c_double), ("ticks", C.c_uint64),
                 ("tier1_sweeps", C.c_uint64), ("tier2_ticks", C.c_uint64), ("tier2_mirror_ticks", C.c_uint64),
                 ("tick_device_ms", C.c_double), ("overflows", C.c_uint64), ("drain_failed", C.c_uint64),
-                ("device_errors", C.c_uint64)]
+                ("device_errors", C.c_uint64), ("tenants_regrown", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -211,6 +211,7 @@ SIGNATURES = {
     "sgc_batch_rows": (C.c_int, [_vp, C.c_uint32, _u64p, _u32p, C.c_uint64]),
     "sgc_batch_validate": (C.c_int, [_vp, C.POINTER(Validation)]),
     "sgc_batch_check_state": (C.c_int, [_vp, C.POINTER(StateReport)]),
+    "sgc_batch_dropped": (C.c_int, [_vp, _u8p]),
     "sgc_batch_set_thresholds": (C.c_int, [_vp, C.c_uint32]),
     "sgc_batch_get_tuning": (C.c_int, [_vp, C.POINTER(BatchTuning)]),
     "sgc_batch_set_tuning": (C.c_int, [_vp, C.POINTER(BatchTuning)]),
@@ -666,6 +667,12 @@ class Batch:
         _check(lib().sgc_batch_check_state(self.b, C.byref(r)), "sgc_batch_check_state")
         return r.as_dict()
 
+    def dropped(self):
+        """Per graph: 1 when the graph has dropped an entry (full row / full overflow buffer)."""
+        out = np.zeros(len(self.graphs), dtype=np.uint8)
+        _check(lib().sgc_batch_dropped(self.b, _p(out, _u8p)), "sgc_batch_dropped")
+        return out
+
     def set_thresholds(self, thr):
         _check(lib().sgc_batch_set_thresholds(self.b, thr), "sgc_batch_set_thresholds")
 
@@ -705,10 +712,11 @@ class Server:
     submit() and query() may be called from other threads while step() runs."""
 
     def __init__(self, hbm_budget_bytes=150 << 30, max_tick_updates=1 << 20, max_staleness_us=0, device=0,
-                 slack_pct=300, cuda_graph=True, stream_order=False, profile=False):
+                 slack_pct=300, cuda_graph=True, stream_order=False, profile=False, regrow=False):
         L = lib()
         opt = ServerOptions()
         L.sgc_server_default_options(C.byref(opt))
+        opt.regrow = 1 if regrow else 0
         opt.hbm_budget_bytes = hbm_budget_bytes
         opt.max_tick_updates = max_tick_updates
         opt.max_staleness_us = max_staleness_us

@@ -622,6 +622,19 @@ int sgc_batch_validate(sgc_batch* b, sgc_validation* out) {
     return sgc_validate(b->h, out);
 }
 
+int sgc_batch_dropped(sgc_batch* b, uint8_t* out) {
+    if (!b || !out) return fail(SGC_EINVAL, "null argument");
+    if (b->in_tick) return fail(SGC_EINVAL, "a tick is running");
+    sgc_handle* h = b->h;
+    CK(cudaSetDevice(h->device));
+    std::vector<GraphCtl> gc(b->G);
+    CK(cudaMemcpyAsync(gc.data(), h->g.gctl, (size_t)b->G * sizeof(GraphCtl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->d2h_bytes += (uint64_t)b->G * sizeof(GraphCtl);
+    for (uint32_t k = 0; k < b->G; k++) out[k] = gc[k].dropped ? 1 : 0;
+    return SGC_OK;
+}
+
 int sgc_batch_check_state(sgc_batch* b, sgc_state_report* out) {
     if (!b) return fail(SGC_EINVAL, "null batch");
     if (b->in_tick) return fail(SGC_EINVAL, "a tick is running");

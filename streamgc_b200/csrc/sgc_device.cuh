@@ -51,6 +51,7 @@ struct GraphCtl {
     unsigned long long sym;  // mirror checksum of the current repair (full repairs with asym set)
     uint32_t base;    // first vertex of the graph in the handle (ids minus base are the graph's own)
     uint32_t t2;      // the last repair left this graph to Tier-2 (rows missing mirrors, or not converged)
+    uint32_t dropped; // an entry of this graph was dropped (a full row at drain, or the overflow buffer full)
 };
 
 // Device view of one graph's state (handle layout). Row x owns logical slots
@@ -381,6 +382,7 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
                     g.ovf[pos].neighbor_global = nbr;
                 } else {
                     atomicAdd(g.ovf_lost, 1ull);
+                    g.gctl[graph_of(g, x)].dropped = 1u;
                 }
                 flag_asym(g, x);
             }

@@ -398,6 +398,7 @@ __global__ void drain_kernel(Dev g, const uint32_t* __restrict__ drain_n, int or
         if (!ok && lane_id() == 0) {
             if (failed) atomicAdd(failed, 1ull);
             flag_asym(g, oe.local_vertex_idx);
+            g.gctl[graph_of(g, oe.local_vertex_idx)].dropped = 1u;
         }
     }
 }

@@ -62,6 +62,9 @@ struct Tenant {
     uint64_t seen_publishes = 0;
     bool admitting = false;          // its group is being created (its CSR is in use)
     bool remove_pending = false;     // removed while admitting: ends once admission is done
+    bool regrow_wanted = false;      // its rows dropped an entry (options.regrow): re-admit at the next step
+    bool regrowing = false;          // its rows are being rebuilt: requests wait, queries read its old group
+    bool requeued = false;           // ... and it waits in the queue (its old group counts it until it is resident again)
 };
 
 struct Group {
@@ -96,7 +99,7 @@ struct sgc_server {
     std::vector<uint8_t> visible;    // by request id
     std::vector<double> vis_ms, query_ms;
     uint64_t update_requests = 0, updates_applied = 0, queries = 0, query_vertices = 0;
-    uint64_t ticks = 0, tier1_sweeps = 0, tier2_ticks = 0, tier2_mirror_ticks = 0;
+    uint64_t ticks = 0, tier1_sweeps = 0, tier2_ticks = 0, tier2_mirror_ticks = 0, regrown = 0;
     double tick_device_ms = 0;
 };
 
@@ -179,12 +182,13 @@ int sgc_server_remove_tenant(sgc_server* s, uint32_t tenant) {
         t.remove_pending = true;
         return SGC_OK;
     }
-    if (t.state == SGC_TENANT_QUEUED) {
+    if (t.state == SGC_TENANT_QUEUED || t.requeued)
         s->queue.erase(std::remove(s->queue.begin(), s->queue.end(), tenant), s->queue.end());
-    } else {
+    if (t.state == SGC_TENANT_RESIDENT) {  // a requeued tenant still counts in its old group
         Group& g = s->groups[t.group];
         if (--g.alive == 0) g.retired = true;  // its memory goes back to the budget at the next step
     }
+    t.regrowing = t.requeued = false;
     t.state = SGC_TENANT_REMOVED;
     std::vector<uint64_t>().swap(t.rp);
     std::vector<uint32_t>().swap(t.col);
@@ -241,6 +245,82 @@ int sgc_server_query(sgc_server* s, uint32_t tenant, const uint32_t* v, uint16_t
 
 namespace {
 
+// Tenants whose rows dropped entries (options.regrow): their live rows are
+// read back, every entry's mirror restored (an edge is kept when either
+// direction survived), and the tenant is queued again at the front with rows
+// sized from its new degrees. Until its new group is resident, queries read
+// its old group (which keeps counting it) and its requests wait; the updates
+// already forwarded are in the rows read, so they become visible at the new
+// group's first publish.
+int regrow_tenants(sgc_server* s) {
+    struct Job {
+        uint32_t tid;
+        sgc_batch* b;
+        uint32_t local, n;
+    };
+    std::vector<Job> jobs;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (uint32_t tid = 0; tid < (uint32_t)s->tenants.size(); tid++) {
+            Tenant& t = s->tenants[tid];
+            if (!t.regrow_wanted) continue;
+            t.regrow_wanted = false;
+            if (t.state != SGC_TENANT_RESIDENT || t.regrowing || t.admitting || !s->groups[t.group].b) continue;
+            t.regrowing = true;  // from here its requests are held
+            jobs.push_back({tid, s->groups[t.group].b, t.local, t.n});
+        }
+    }
+    for (const Job& j : jobs) {
+        // the live rows (the groups' ticks are done: the step is single-threaded)
+        std::vector<uint64_t> rp((size_t)j.n + 1);
+        int rc = sgc_batch_rows(j.b, j.local, rp.data(), nullptr, 0);
+        std::vector<uint32_t> col(std::max<uint64_t>(rp[j.n], 1));
+        if (rc == SGC_OK) rc = sgc_batch_rows(j.b, j.local, rp.data(), col.data(), col.size());
+        // undirected edges from either direction, then both directions, rows ascending
+        std::vector<uint64_t> keys;
+        std::vector<uint64_t> nrp((size_t)j.n + 1, 0);
+        std::vector<uint32_t> ncol, ndeg(j.n, 0);
+        if (rc == SGC_OK) {
+            keys.reserve(rp[j.n]);
+            for (uint32_t x = 0; x < j.n; x++)
+                for (uint64_t e = rp[x]; e < rp[x + 1]; e++) {
+                    const uint32_t y = col[e];
+                    if (y == x || y >= j.n) continue;
+                    keys.push_back(x < y ? ((uint64_t)x << 32 | y) : ((uint64_t)y << 32 | x));
+                }
+            std::sort(keys.begin(), keys.end());
+            keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+            for (uint64_t k : keys) {
+                ndeg[k >> 32]++;
+                ndeg[(uint32_t)k]++;
+            }
+            for (uint32_t v = 0; v < j.n; v++) nrp[v + 1] = nrp[v] + ndeg[v];
+            ncol.resize(nrp[j.n]);
+            std::vector<uint64_t> fill(nrp.begin(), nrp.end() - 1);
+            for (uint64_t k : keys) {  // keys ascend by (a, b): every row comes out ascending
+                const uint32_t a = (uint32_t)(k >> 32), c = (uint32_t)k;
+                ncol[fill[a]++] = c;
+                ncol[fill[c]++] = a;
+            }
+        }
+        std::lock_guard<std::mutex> lk(s->mu);
+        Tenant& t = s->tenants[j.tid];
+        if (t.state != SGC_TENANT_RESIDENT || rc != SGC_OK) {  // removed meanwhile (it left its group then)
+            t.regrowing = false;
+            if (rc != SGC_OK) return rc;
+            continue;
+        }
+        t.rp.swap(nrp);
+        t.col.swap(ncol);
+        t.deg.swap(ndeg);
+        t.footprint = sgc_tenant_footprint(t.n, t.rp[t.n], s->opt.slack_pct);
+        t.requeued = true;
+        s->queue.push_front(j.tid);
+        s->regrown++;
+    }
+    return SGC_OK;
+}
+
 // One tenant's requests moved out of its held buffer by a step.
 struct Forward {
     sgc_batch* b;
@@ -269,6 +349,10 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
     }
     sgc_server_step_report r{};
     r.proper = 1;
+    if (s->opt.regrow) {
+        const int rc = regrow_tenants(s);
+        if (rc != SGC_OK) return rc;
+    }
     // 1. admission: first come first served against the budget
     std::vector<uint32_t> admit;
     uint64_t add_bytes = (uint64_t)s->opt.max_tick_updates * kBytesPerTickUpdate;
@@ -306,6 +390,11 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
                 Tenant& t = s->tenants[*it];
                 t.admitting = false;
                 if (t.remove_pending) {
+                    if (t.requeued) {  // it still counted in its old group
+                        Group& og = s->groups[t.group];
+                        if (--og.alive == 0) og.retired = true;
+                    }
+                    t.regrowing = t.requeued = false;
                     t.state = SGC_TENANT_REMOVED;
                     continue;
                 }
@@ -321,8 +410,14 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
         for (size_t i = 0; i < admit.size(); i++) {
             Tenant& t = s->tenants[admit[i]];
             t.admitting = false;
+            if (t.requeued) {  // re-admitted with rebuilt rows: it leaves its old group now
+                Group& og = s->groups[t.group];
+                if (--og.alive == 0) og.retired = true;
+            }
+            t.regrowing = t.requeued = false;
             t.group = gi;
             t.local = (uint32_t)i;
+            t.seen_publishes = 0;  // the new group's publish count starts at 0
             std::vector<uint64_t>().swap(t.rp);  // the CSR lives on the device now
             std::vector<uint32_t>().swap(t.col);
             std::vector<uint32_t>().swap(t.deg);
@@ -353,7 +448,7 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
             if (s->groups[gi].b) room[gi] = s->opt.max_tick_updates - sgc_batch_pending(s->groups[gi].b);
         const auto now = clk::now();
         for (auto& t : s->tenants) {
-            if (t.state != SGC_TENANT_RESIDENT) continue;
+            if (t.state != SGC_TENANT_RESIDENT || t.regrowing) continue;  // a regrowing tenant's requests wait
             Group& g = s->groups[t.group];
             if (!t.held_reqs.empty()) {
                 uint64_t take = 0;
@@ -412,7 +507,14 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
     // call reads them without waiting on a running tick)
     std::vector<sgc_stats> bst(tb.size());
     std::vector<int> brc(tb.size());
-    for (size_t i = 0; i < tb.size(); i++) brc[i] = sgc_batch_stats(tb[i], &bst[i]);
+    std::vector<std::vector<uint8_t>> dropped(tb.size());
+    for (size_t i = 0; i < tb.size(); i++) {
+        brc[i] = sgc_batch_stats(tb[i], &bst[i]);
+        if (s->opt.regrow && bst[i].drain_failed + bst[i].overflow_lost > 0) {  // which graphs dropped entries
+            dropped[i].resize(sgc_batch_num_graphs(tb[i]));
+            if (sgc_batch_dropped(tb[i], dropped[i].data()) != SGC_OK) dropped[i].clear();
+        }
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     const auto now = clk::now();
     for (size_t i = 0; i < ticking.size(); i++) {
@@ -431,7 +533,8 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
         if (!tr.proper) r.proper = 0;
         for (uint32_t tid : g.tenants) {
             Tenant& t = s->tenants[tid];
-            if (t.state != SGC_TENANT_RESIDENT) continue;
+            if (t.state != SGC_TENANT_RESIDENT || t.group != ticking[i]) continue;  // moved tenants left this group
+            if (!dropped[i].empty() && dropped[i][t.local] && !t.regrowing) t.regrow_wanted = true;
             const uint64_t p = sgc_batch_publish_count(g.b, t.local);
             if (p != t.seen_publishes) {  // everything forwarded so far is in this snapshot
                 t.seen_publishes = p;
@@ -519,6 +622,7 @@ int sgc_server_get_stats(sgc_server* s, sgc_server_stats* o) {
     o->tier2_ticks = s->tier2_ticks;
     o->tier2_mirror_ticks = s->tier2_mirror_ticks;
     o->tick_device_ms = s->tick_device_ms;
+    o->tenants_regrown = s->regrown;
     return SGC_OK;
 }
 
