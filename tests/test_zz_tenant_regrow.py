@@ -3,6 +3,8 @@ no longer fit its rows loses entries at the drain, as the reference does; the
 server then reads its live rows back, restores each surviving entry's mirror
 and admits it again with rows sized from its current degrees. Afterwards its
 rows hold every edge in both directions and its snapshot is proper."""
+import time
+
 import numpy as np
 import pytest
 
@@ -25,16 +27,18 @@ def test_tenant_with_full_rows(regrow):
     nbr0 = set(g.col_idx[g.row_ptr[0]:g.row_ptr[1]].tolist())
     star = [v for v in range(1, 2000) if v not in nbr0][:300]  # new edges at vertex 0: its row overflows
     ups = S.updates_from([[0, v] for v in star], [S.ADD] * len(star))
-    with S.Server(max_tick_updates=1 << 16, slack_pct=0, regrow=regrow) as srv:
+    with S.Server(max_tick_updates=1 << 16, slack_pct=0, regrow=regrow, max_staleness_us=1000) as srv:
         t = srv.add_tenant(g, epoch_size=64)
         assert srv.step()["admitted"] == 1
         for s0 in range(0, len(ups), 50):
             srv.submit(t, ups[s0:s0 + 50])
             for _ in range(3):
                 assert srv.step()["proper"] == 1
-        for _ in range(12):
+        for _ in range(12):  # the staleness deadline publishes the last epoch's updates
+            time.sleep(0.002)
             assert srv.step()["proper"] == 1
         st = srv.stats()
+        assert st["requests_visible"] == st["update_requests"]
         assert st["drain_failed"] > 0 or st["tenants_regrown"] > 0
         rp, col = srv.rows(t)
         snap = srv.snapshot(t)
