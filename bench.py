@@ -204,7 +204,8 @@ def run_ours(a):
 
     t = time.time()
     h = S.StreamGC(g, epoch_size=E, histogram_threshold=HIST_THR, slack_pct=300, max_batch=1 << 20,
-                   device=local, profile=not a.graph_publish, exact_select=True, graph_publish=a.graph_publish)
+                   device=local, profile=not a.graph_publish, exact_select=True, graph_publish=a.graph_publish,
+                   sorted_rows=a.sorted_rows)
     for s in range(0, 0 if init is None else len(init), 1 << 20):
         h.apply(init[s:s + (1 << 20)], S.MODE_CONCURRENT)
     rep = h.publish()
@@ -314,7 +315,8 @@ def run_ours(a):
         conf = dict(desc)
         conf.update(mode="concurrent (warp per edge) + repaired publish per epoch, exact color selection"
                     + (", publish as one CUDA graph" if a.graph_publish else "")
-                    + (", e2e through the ingest slots" if a.ingest else ""),
+                    + (", e2e through the ingest slots" if a.ingest else "")
+                    + (", rows kept as one sorted run" if a.sorted_rows else ""),
                     l2="flushed before every timed step (256 MiB write)", parallelism=f"replicas x{world}",
                     valid_after_run=val["violations"] == 0 and val["uncolored_with_edges"] == 0,
                     colors_used=int(val["max_color"]), static_greedy_colors=None,
@@ -507,7 +509,8 @@ def run_batched(a):
     # ---- arm 2: the batched engine ----
     t = time.time()
     cap = max(sum(epochs), 1 << 20)
-    b = S.Batch(graphs, epoch_sizes=epochs, max_tick_updates=cap, device=local, profile=True)
+    b = S.Batch(graphs, epoch_sizes=epochs, max_tick_updates=cap, device=local, profile=True,
+                sorted_rows=a.sorted_rows)
     # the rows hold every edge from creation; the first tick colors all graphs
     # from scratch and publishes them (as the served form admits tenants)
     b.close_epochs()
@@ -672,7 +675,7 @@ def run_served(a):
     log(f"served (rank {rank}): {len(mine)} of {T} tenants generated in {time.time() - t:.1f}s; "
         f"{len(events)} requests over {dur}s")
     srv = S.Server(hbm_budget_bytes=150 << 30, max_tick_updates=1 << 22, max_staleness_us=a.served_staleness_us,
-                   device=local, profile=True, regrow=a.served_regrow)
+                   device=local, profile=True, regrow=a.served_regrow, sorted_rows=a.sorted_rows)
     tids = {k: srv.add_tenant(S.Graph(data[k]["row_ptr"], data[k]["col"]), epoch_size=data[k]["spec"]["epoch"])
             for k in mine}
     t = time.time()
@@ -792,6 +795,8 @@ def main():
     ap.add_argument("--workload", default="skewed", choices=["skewed", "small", "large"],
                     help="plain path: skewed (R-MAT 2^20 x 48, k-core stream), small (Delaunay 2^17 churn), "
                          "large (Chung-Lu 65.6 M vertices, ~1.8 G edges, 10 M churn)")
+    ap.add_argument("--sorted-rows", action="store_true",
+                    help="compaction keeps rows of up to 1024 live entries as one sorted run (SGC_OPT_SORTED_ROWS)")
     ap.add_argument("--ingest", action="store_true",
                     help="plain path, e2e: batches staged through the two ingest slots (copy of the next "
                          "batch overlapping this epoch's publish)")

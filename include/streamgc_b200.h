@@ -48,6 +48,12 @@ typedef struct sgc_handle sgc_handle;
  * while-node, snapshot): one host synchronization per epoch instead of one per
  * sweep. Sweeps are not timed one by one (sgc_stats.sweep_ms stays 0). */
 #define SGC_OPT_GRAPH_PUBLISH 4u
+/* With SGC_OPT_EXACT_SELECT, compaction also sorts every row of at most 1024
+ * live entries into one base run, and compacts a row whose unsorted tail (the
+ * entries inserted since its last compaction) outgrows an eighth of it even
+ * with few holes: searches stay 32-ary over long runs. Colors do not depend on
+ * it. */
+#define SGC_OPT_SORTED_ROWS 8u
 
 typedef struct sgc_options {
     uint32_t struct_size;      /* sizeof(sgc_options) */

@@ -49,6 +49,7 @@ typedef struct sgc_batch_graph {
 #define SGC_BATCH_STREAM_ORDER 2u  /* each graph's updates in submission order (one warp per graph):
                                       a graph's colors do not depend on the other graphs */
 #define SGC_BATCH_PROFILE      4u  /* time every tick with CUDA events */
+#define SGC_BATCH_SORTED_ROWS  8u  /* compaction keeps rows as one sorted run (SGC_OPT_SORTED_ROWS) */
 
 typedef struct sgc_batch_options {
     uint32_t struct_size;          /* sizeof(sgc_batch_options) */

@@ -388,13 +388,14 @@ class StreamGC:
 
     def __init__(self, graph: Graph, epoch_size=32768, histogram_threshold=64, slack_pct=300,
                  max_hist_colors=1024, max_batch=32768, device=0, profile=False, exact_select=False,
-                 full_repair_every=None, repair_tile=None, graph_publish=False):
+                 full_repair_every=None, repair_tile=None, graph_publish=False, sorted_rows=False):
         L = lib()
         cfg = _Config(1, graph.n, graph.nnz, 1 << 20, epoch_size, 100, histogram_threshold, 0.2)
         opt = _Options()
         L.sgc_default_options(C.byref(opt))
         opt.slack_pct, opt.max_hist_colors, opt.max_batch, opt.device = slack_pct, max_hist_colors, max_batch, device
-        opt.flags = (1 if profile else 0) | (2 if exact_select else 0) | (4 if graph_publish else 0)
+        opt.flags = (1 if profile else 0) | (2 if exact_select else 0) | (4 if graph_publish else 0) | \
+            (8 if sorted_rows else 0)
         if full_repair_every is not None:
             opt.full_repair_every = full_repair_every
         if repair_tile is not None:
@@ -571,6 +572,7 @@ def version():
 BATCH_CUDA_GRAPH = 1
 BATCH_STREAM_ORDER = 2
 BATCH_PROFILE = 4
+BATCH_SORTED_ROWS = 8
 
 
 class Batch:
@@ -580,7 +582,8 @@ class Batch:
     epoch closed."""
 
     def __init__(self, graphs, epoch_sizes=None, thresholds=None, max_tick_updates=1 << 20, slack_pct=300,
-                 device=0, cuda_graph=True, stream_order=False, profile=False, repair_tile=0, apply_blocks_per_sm=0):
+                 device=0, cuda_graph=True, stream_order=False, profile=False, repair_tile=0, apply_blocks_per_sm=0,
+                 sorted_rows=False):
         L = lib()
         self.graphs = list(graphs)
         G = len(self.graphs)
@@ -596,7 +599,7 @@ class Batch:
         L.sgc_batch_default_options(C.byref(opt))
         opt.slack_pct, opt.max_tick_updates, opt.device = slack_pct, max_tick_updates, device
         opt.flags = (BATCH_CUDA_GRAPH if cuda_graph else 0) | (BATCH_STREAM_ORDER if stream_order else 0) | \
-            (BATCH_PROFILE if profile else 0)
+            (BATCH_PROFILE if profile else 0) | (BATCH_SORTED_ROWS if sorted_rows else 0)
         opt.repair_tile, opt.apply_blocks_per_sm = repair_tile, apply_blocks_per_sm
         self.b = _vp()
         _check(L.sgc_batch_create(arr, G, C.byref(opt), C.byref(self.b)), "sgc_batch_create")
@@ -712,7 +715,7 @@ class Server:
     submit() and query() may be called from other threads while step() runs."""
 
     def __init__(self, hbm_budget_bytes=150 << 30, max_tick_updates=1 << 20, max_staleness_us=0, device=0,
-                 slack_pct=300, cuda_graph=True, stream_order=False, profile=False, regrow=False):
+                 slack_pct=300, cuda_graph=True, stream_order=False, profile=False, regrow=False, sorted_rows=False):
         L = lib()
         opt = ServerOptions()
         L.sgc_server_default_options(C.byref(opt))
@@ -722,7 +725,7 @@ class Server:
         opt.max_staleness_us = max_staleness_us
         opt.device, opt.slack_pct = device, slack_pct
         opt.flags = (BATCH_CUDA_GRAPH if cuda_graph else 0) | (BATCH_STREAM_ORDER if stream_order else 0) | \
-            (BATCH_PROFILE if profile else 0)
+            (BATCH_PROFILE if profile else 0) | (BATCH_SORTED_ROWS if sorted_rows else 0)
         self.s = _vp()
         _check(L.sgc_server_create(C.byref(opt), C.byref(self.s)), "sgc_server_create")
         self.n = {}

@@ -90,7 +90,8 @@ int sync(sgc_handle* h) {
 int compact_dirty(sgc_handle* h, bool force) {
     CK(cudaMemsetAsync(&h->ctl->dirty_count, 0, 4, h->stream));
     launch_dirty_list(h->g, h->dirty_list, &h->ctl->dirty_count, h->stream);
-    launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, force, h->stream);
+    launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, force, h->stream,
+                   (h->opt.flags & SGC_OPT_SORTED_ROWS) != 0);
     h->launches += 2;
     return check_cuda("compact");
 }
@@ -265,7 +266,7 @@ int ensure_ingest(sgc_handle* h) {
 void enqueue_publish_head(sgc_handle* h, cudaStream_t s) {
     cudaMemsetAsync(&h->ctl->dirty_count, 0, 4, s);
     launch_dirty_list(h->g, h->dirty_list, &h->ctl->dirty_count, s);
-    launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, false, s);
+    launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, false, s, (h->opt.flags & SGC_OPT_SORTED_ROWS) != 0);
     launch_take_overflow(h->g, &h->ctl->drain_n, s);
     launch_drain(h->g, &h->ctl->drain_n, false, &h->ctl->drain_failed, s);
     cudaMemcpyAsync(h->sb.rc, h->h_rc_in, 12, cudaMemcpyHostToDevice, s);

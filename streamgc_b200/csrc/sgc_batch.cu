@@ -124,7 +124,7 @@ void enqueue_head(sgc_batch* b, cudaStream_t s) {
         launch_conc_apply_dyn(h->g, h->d_batch, b->d_dyn, h->eo, h->num_sms, (int)b->bps, s);
     cudaMemsetAsync(&h->ctl->dirty_count, 0, 4, s);
     launch_dirty_list(h->g, h->dirty_list, &h->ctl->dirty_count, s);
-    launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, false, s);
+    launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, false, s, (h->opt.flags & SGC_OPT_SORTED_ROWS) != 0);
     launch_take_overflow(h->g, &h->ctl->drain_n, s);
     launch_drain(h->g, &h->ctl->drain_n, (b->flags & SGC_BATCH_STREAM_ORDER) != 0, &h->ctl->drain_failed, s);
     const size_t mwords = ((h->n + 31) / 32) * 4;
@@ -309,7 +309,7 @@ int sgc_batch_create(const sgc_batch_graph* graphs, uint32_t count, const sgc_ba
     hopt.slack_pct = opt.slack_pct;
     hopt.max_batch = opt.max_tick_updates;
     hopt.device = opt.device;
-    hopt.flags = SGC_OPT_EXACT_SELECT;
+    hopt.flags = SGC_OPT_EXACT_SELECT | ((opt.flags & SGC_BATCH_SORTED_ROWS) ? SGC_OPT_SORTED_ROWS : 0u);
     hopt.full_repair_every = 0;  // a graph is repaired in full only when it needs it
     hopt.repair_tile = opt.repair_tile ? opt.repair_tile : SWEEP_CH;
     CreateExtra ex{thr_word.data(), gidw.data(), count, voff.data()};

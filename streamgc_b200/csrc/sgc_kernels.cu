@@ -280,19 +280,48 @@ void launch_dirty_list(const Dev& g, uint32_t* list, uint32_t* count, cudaStream
 // hw = live count.
 // Under exact selection a tombstone (id | TOMB) is a hole too, and the live
 // entries of the base run, which stay in front and in order, form the new run.
+// With `merge` (exact selection), a compacted row of at most kMergeMax live
+// entries is also sorted into one base run (warp-wide bitonic sort in shared
+// memory), so its later searches stay 32-ary instead of scanning a growing
+// unsorted tail; and a row whose tail outgrows an eighth of it is compacted
+// even with few holes.
+constexpr uint32_t kMergeMax = 1024;
+
+__device__ __forceinline__ void warp_sort_row(uint32_t* buf, uint32_t lane) {
+    for (uint32_t k = 2; k <= kMergeMax; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = lane; i < kMergeMax; i += 32) {
+                const uint32_t p = i ^ j;
+                if (p > i) {
+                    const uint32_t a = buf[i], b = buf[p];
+                    if ((a > b) == ((i & k) == 0)) {
+                        buf[i] = b;
+                        buf[p] = a;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+}
+
 __global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __restrict__ list,
-                                                      const uint32_t* __restrict__ count, int force) {
+                                                      const uint32_t* __restrict__ count, int force, int merge) {
+    extern __shared__ uint32_t sort_buf[];  // kMergeMax words per warp, only with `merge`
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
     const uint32_t cnt = *count;
+    merge = merge && g.blen;
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
         const uint32_t x = list[k];
         const uint64_t s = g.rp[x];
         const uint32_t hwx = row_len(g, x);
         // Lazy mode: a row whose holes fill at most a quarter of its extent stays
         // as it is (every reader skips INV slots and tombstones); it is compacted later.
-        if (!force && g.holes && 4u * g.holes[x] <= hwx) {
-            if (g.holes[x] && lane == 0) atomicOr(g.dirty + (x >> 5), 1u << (x & 31));  // still a candidate
+        const uint32_t run = merge ? min(g.blen[x], hwx) : 0u;
+        const bool long_tail = merge && hwx - run > max(32u, hwx >> 3);
+        if (!force && g.holes && 4u * g.holes[x] <= hwx && !long_tail) {
+            if ((g.holes[x] || (merge && run < hwx)) && lane == 0)  // still a candidate (holes, or a tail to merge)
+                atomicOr(g.dirty + (x >> 5), 1u << (x & 31));
             continue;
         }
         const uint64_t e = s + hwx;
@@ -327,8 +356,18 @@ __global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __r
             __syncwarp();
         }
         for (uint64_t j = w + lane; j < e; j += 32) g.col[j] = INV;
+        const uint32_t live = (uint32_t)(w - s);
+        if (merge && live > run_live && live <= kMergeMax) {  // tail entries behind the run: one sorted run
+            __syncwarp();
+            uint32_t* buf = sort_buf + ((threadIdx.x >> 5) & 7) * kMergeMax;
+            for (uint32_t i = lane; i < kMergeMax; i += 32) buf[i] = i < live ? g.col[s + i] : INV;
+            __syncwarp();
+            warp_sort_row(buf, lane);
+            for (uint32_t i = lane; i < live; i += 32) g.col[s + i] = buf[i];
+            run_live = live;
+        }
         if (lane == 0) {
-            g.hw[x] = (uint32_t)(w - s);
+            g.hw[x] = live;
             if (g.holes) g.holes[x] = 0;
             if (g.blen) g.blen[x] = (uint32_t)run_live;
         }
@@ -337,11 +376,12 @@ __global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __r
 }
 
 void launch_compact(const Dev& g, const uint32_t* list, const uint32_t* count, uint32_t max_rows, bool force,
-                    cudaStream_t s) {
+                    cudaStream_t s, bool merge) {
     if (!max_rows) return;
     uint32_t blocks = (max_rows + 7) / 8;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    compact_kernel<<<blocks, 256, 0, s>>>(g, list, count, force ? 1 : 0);
+    const size_t smem = merge && g.blen ? 8 * kMergeMax * sizeof(uint32_t) : 0;  // 32 KiB: under the 48 KiB default
+    compact_kernel<<<blocks, 256, smem, s>>>(g, list, count, force ? 1 : 0, (merge && g.blen) ? 1 : 0);
 }
 
 // ---------------------------------------------------------------------------

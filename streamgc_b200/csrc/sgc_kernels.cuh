@@ -114,7 +114,7 @@ void launch_dirty_list(const Dev& g, uint32_t* list, uint32_t* count, cudaStream
 // force: compact every listed row (else rows whose holes fill at most a quarter
 // of their extent wait, under exact selection).
 void launch_compact(const Dev& g, const uint32_t* list, const uint32_t* count, uint32_t max_rows, bool force,
-                    cudaStream_t s);
+                    cudaStream_t s, bool merge = false);
 void launch_take_overflow(const Dev& g, uint32_t* drain_n, cudaStream_t s);
 void launch_drain(const Dev& g, const uint32_t* drain_n, bool ordered, unsigned long long* failed, cudaStream_t s);
 void launch_snapshot(const Dev& g, uint16_t* snap, cudaStream_t s);
