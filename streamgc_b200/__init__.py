@@ -185,6 +185,7 @@ SIGNATURES = {
     "sgc_version": (C.c_char_p, []),
     "sgc_load_mtx": (C.c_int, [C.c_char_p, C.POINTER(_CSR)]),
     "sgc_csr_from_edges": (C.c_int, [C.c_uint32, _u32p, C.c_uint64, C.POINTER(_CSR)]),
+    "sgc_csr_symmetrize": (C.c_int, [C.c_uint32, _u64p, _u32p, C.POINTER(_CSR)]),
     "sgc_csr_free": (None, [C.POINTER(_CSR)]),
     "sgc_write_mtx": (C.c_int, [C.c_char_p, C.POINTER(_CSR)]),
     "sgc_gen_init_stream": (C.c_uint64, [C.POINTER(_CSR), _u32p]),
@@ -316,6 +317,16 @@ class Graph:
         pairs = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1, 2)
         c = _CSR()
         _check(lib().sgc_csr_from_edges(n, _p(pairs, _u32p), len(pairs), C.byref(c)), "csr_from_edges")
+        return Graph._take(c)
+
+    @staticmethod
+    def symmetrized(row_ptr, col):
+        """The graph of rows that may miss mirror entries: an edge is kept when
+        either direction is present."""
+        rp = np.ascontiguousarray(row_ptr, dtype=np.uint64)
+        cl = np.ascontiguousarray(col, dtype=np.uint32)
+        c = _CSR()
+        _check(lib().sgc_csr_symmetrize(len(rp) - 1, _p(rp, _u64p), _p(cl, _u32p), C.byref(c)), "csr_symmetrize")
         return Graph._take(c)
 
     @staticmethod

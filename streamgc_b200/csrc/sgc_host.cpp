@@ -178,6 +178,19 @@ int sgc_csr_from_edges(uint32_t n, const uint32_t* pairs, uint64_t m, sgc_csr* o
     return csr_from_pairs(n, keys, out);
 }
 
+int sgc_csr_symmetrize(uint32_t n, const uint64_t* row_ptr, const uint32_t* col_idx, sgc_csr* out) {
+    if (!out || !row_ptr || (row_ptr[n] && !col_idx)) return -1;
+    std::vector<uint64_t> keys;
+    keys.reserve(row_ptr[n]);
+    for (uint32_t x = 0; x < n; x++)
+        for (uint64_t e = row_ptr[x]; e < row_ptr[x + 1]; e++) {
+            const uint32_t y = col_idx[e];
+            if (y == x || y >= n) continue;
+            keys.push_back(x < y ? key_of(x, y) : key_of(y, x));
+        }
+    return csr_from_pairs(n, keys, out);
+}
+
 int sgc_load_mtx(const char* path, sgc_csr* out) {
     if (!path || !out) return -1;
     FILE* f = fopen(path, "r");

@@ -28,6 +28,10 @@ typedef struct sgc_csr {
 int sgc_load_mtx(const char* path, sgc_csr* out);
 /* Same construction from an in-memory 0-based edge list (pairs[2*i], pairs[2*i+1]). */
 int sgc_csr_from_edges(uint32_t n, const uint32_t* pairs, uint64_t m, sgc_csr* out);
+/* The symmetric closure of rows that may miss mirror entries: an edge is kept
+ * when either direction is present (self loops and ids >= n dropped); rows
+ * ascending, degrees from the result. */
+int sgc_csr_symmetrize(uint32_t n, const uint64_t* row_ptr, const uint32_t* col_idx, sgc_csr* out);
 void sgc_csr_free(sgc_csr* g);
 /* Writes an undirected .mtx (pattern, one line per edge u > v, 1-based). */
 int sgc_write_mtx(const char* path, const sgc_csr* g);

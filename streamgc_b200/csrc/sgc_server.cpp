@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/streamgc_server.h"
+#include "sgc_host.h"
 
 namespace sgci {
 int fail(int code, const char* fmt, ...);  // sgc_api.cu: sets the message sgc_last_error() returns
@@ -277,31 +278,18 @@ int regrow_tenants(sgc_server* s) {
         std::vector<uint32_t> col(std::max<uint64_t>(rp[j.n], 1));
         if (rc == SGC_OK) rc = sgc_batch_rows(j.b, j.local, rp.data(), col.data(), col.size());
         // undirected edges from either direction, then both directions, rows ascending
-        std::vector<uint64_t> keys;
-        std::vector<uint64_t> nrp((size_t)j.n + 1, 0);
-        std::vector<uint32_t> ncol, ndeg(j.n, 0);
+        std::vector<uint64_t> nrp;
+        std::vector<uint32_t> ncol, ndeg;
         if (rc == SGC_OK) {
-            keys.reserve(rp[j.n]);
-            for (uint32_t x = 0; x < j.n; x++)
-                for (uint64_t e = rp[x]; e < rp[x + 1]; e++) {
-                    const uint32_t y = col[e];
-                    if (y == x || y >= j.n) continue;
-                    keys.push_back(x < y ? ((uint64_t)x << 32 | y) : ((uint64_t)y << 32 | x));
-                }
-            std::sort(keys.begin(), keys.end());
-            keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
-            for (uint64_t k : keys) {
-                ndeg[k >> 32]++;
-                ndeg[(uint32_t)k]++;
+            sgc_csr sym{};
+            if (sgc_csr_symmetrize(j.n, rp.data(), col.data(), &sym) != 0) {
+                rc = SGC_ENOMEM;
+            } else {
+                nrp.assign(sym.row_ptr, sym.row_ptr + (size_t)j.n + 1);
+                ncol.assign(sym.col_idx, sym.col_idx + sym.nnz);
+                ndeg.assign(sym.degree, sym.degree + j.n);
             }
-            for (uint32_t v = 0; v < j.n; v++) nrp[v + 1] = nrp[v] + ndeg[v];
-            ncol.resize(nrp[j.n]);
-            std::vector<uint64_t> fill(nrp.begin(), nrp.end() - 1);
-            for (uint64_t k : keys) {  // keys ascend by (a, b): every row comes out ascending
-                const uint32_t a = (uint32_t)(k >> 32), c = (uint32_t)k;
-                ncol[fill[a]++] = c;
-                ncol[fill[c]++] = a;
-            }
+            sgc_csr_free(&sym);
         }
         std::lock_guard<std::mutex> lk(s->mu);
         Tenant& t = s->tenants[j.tid];

@@ -149,3 +149,29 @@ def test_write_coloring_format(tmp_path):
     S.write_coloring(p, colors)
     assert open(p, "rb").read() == colors.astype("<u2").tobytes()
     assert open(p + ".txt").read() == "# vertices: 4\n# colors: 7\n# algorithm: streamgc\n0 1\n1 2\n2 0\n3 7\n"
+
+
+def test_symmetrize_restores_mirrors():
+    """sgc_csr_symmetrize: rows that lost one direction of some edges (and hold
+    a self loop and an out-of-range id) become the symmetric closure."""
+    g = S.Graph.delaunay(500, seed=9)
+    rp, col = g.row_ptr.astype(np.uint64), g.col_idx.copy()
+    rng = np.random.default_rng(2)
+    keep = rng.random(len(col)) > 0.2  # drop 20% of the directed entries
+    rows = [col[rp[u]:rp[u + 1]][keep[rp[u]:rp[u + 1]]].tolist() for u in range(g.n)]
+    rows[0] = rows[0] + [0, 10 ** 6]
+    lrp = np.zeros(g.n + 1, dtype=np.uint64)
+    lrp[1:] = np.cumsum([len(r) for r in rows])
+    lcol = np.array([v for r in rows for v in r], dtype=np.uint32)
+    h = S.Graph.symmetrized(lrp, lcol)
+    want = set()
+    for u, r in enumerate(rows):
+        for v in r:
+            if v != u and v < g.n:
+                want.add((min(u, v), max(u, v)))
+    got = {(u, int(v)) for u in range(h.n) for v in h.col_idx[h.row_ptr[u]:h.row_ptr[u + 1]] if u < v}
+    assert got == want
+    for u in range(h.n):
+        row = h.col_idx[h.row_ptr[u]:h.row_ptr[u + 1]].astype(np.int64)
+        assert np.all(np.diff(row) > 0)
+        assert h.degree[u] == len(row)
