@@ -164,13 +164,23 @@ def sum_over_ranks(dist, values, device):
     return [float(x) for x in t]
 
 
+def dist_backend():
+    """NCCL between GPU ranks; SGC_DIST_BACKEND=gloo runs the host-side
+    reductions of the sharded forms on CPU ranks (tests)."""
+    return os.environ.get("SGC_DIST_BACKEND", "nccl")
+
+
+def reduce_device(local):
+    return "cpu" if dist_backend() == "gloo" else f"cuda:{local}"
+
+
 def init_dist(world):
-    """The process group of a multi-rank run (NCCL, short timeout), else None."""
+    """The process group of a multi-rank run (short timeout), else None."""
     if world <= 1:
         return None
     import datetime
     import torch.distributed as dist
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dist.init_process_group(dist_backend(), timeout=datetime.timedelta(seconds=600))
     return dist
 
 
@@ -448,7 +458,7 @@ def run_batched(a):
 
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    dev = f"cuda:{local}"
+    dev = reduce_device(local)
     dist = init_dist(world)
     ticks = a.warmup + a.steps
     specs_all = W.batch_specs(a.batch_graphs, seed=42)
@@ -627,7 +637,7 @@ def run_served(a):
 
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    dev = f"cuda:{local}"
+    dev = reduce_device(local)
     dist = init_dist(world)
     rate, dur = a.served_rate, a.served_seconds
     specs = W.batch_specs(63, seed=43)
