@@ -202,11 +202,7 @@ def run_ours(a):
 
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dist = init_dist(world)
     nbatch = a.warmup + 2 * a.steps + a.cpu_batches
     base_len = {"skewed": 2_000_000, "small": 1_000_000, "large": 10_000_000}[a.workload]
     stream_len = max(base_len, nbatch * E)
@@ -290,7 +286,7 @@ def run_ours(a):
         d1 = h.stats()
     total_ms = sum(step_ms)
     if dist:
-        total_ms, e2e_s = max_over_ranks(dist, [total_ms, e2e_s], f"cuda:{local}")
+        total_ms, e2e_s = max_over_ranks(dist, [total_ms, e2e_s], reduce_device(local))
     val = h.validate()
     cpu = None
     if rank == 0 and world == 1 and a.cpu_batches > 0:

@@ -1,7 +1,7 @@
-"""The sharded forms of the bench on two gloo ranks (CPU): graphs (batched) and
-tenants (served) placed on the ranks by resident bytes, each rank running its
-share, rank 0 alone printing one line with every rank's work over the slowest
-rank's time. The engines are replaced by stand-ins that count what they are
+"""The multi-rank forms of the bench on two gloo ranks (CPU): replicas of the
+plain path, and graphs (batched) and tenants (served) placed on the ranks by
+resident bytes, each rank running its share; rank 0 alone prints one line
+with every rank's work over the slowest rank's time. The engines are replaced by stand-ins that count what they are
 given; what runs for real is the bench's placement, generation, client loop
 and the host-side reductions."""
 import io
@@ -103,6 +103,75 @@ class _Server:
         pass
 
 
+class _PlainHandle:
+    def __init__(self, g, **k):
+        self.n = g.n
+        self.k = 0
+
+    def apply(self, ups, mode=0):
+        pass
+
+    def apply_ptr(self, ptr, n, mode=0):
+        pass
+
+    def publish(self):
+        return dict(tier1_iterations=1, tier1_last_count=0, tier2_ran=0, tier2_fixed=0, tier2_gave_up=0,
+                    drained=0, drain_failed=0, proper=1, incremental=1)
+
+    def synchronize(self):
+        pass
+
+    def cuda_stream(self):
+        return 0
+
+    def stats(self):
+        self.k += 1
+        return dict(sweep_ms=1.0 * self.k, sweep_bytes=10 ** 9 * self.k, sweep_count=3 * self.k,
+                    kernel_launches=100 * self.k, h2d_bytes=0, d2h_bytes=0)
+
+    def validate(self):
+        return dict(violations=0, uncolored_with_edges=0, max_color=12, edges=1, out_of_range=0)
+
+    def close(self):
+        pass
+
+
+class _Event:
+    n = 0
+
+    def __init__(self, enable_timing=True):
+        _Event.n += 1
+        self.t = _Event.n
+
+    def record(self, s=None):
+        pass
+
+    def elapsed_time(self, o):
+        return 0.25 * (o.t - self.t)
+
+
+class _Tensor:
+    def to(self, *a, **k):
+        return self
+
+    def data_ptr(self):
+        return 0
+
+    def pin_memory(self):
+        return self
+
+    def add_(self, x):
+        return self
+
+
+class _Stream:
+    def __init__(self, *a, **k):
+        pass
+
+    def synchronize(self):
+        pass
+
+
 def _small_specs(count, seed=42, **k):
     rng = np.random.default_rng(seed)
     fams = ("delaunay", "rmat", "chung_lu")
@@ -121,19 +190,27 @@ def _rank(rank, world, port, form, q):
     import bench
     import streamgc_b200 as S
     from streamgc_b200 import workloads as W
-    S.StreamGC, S.Batch, S.Server = _Handle, _Batch, _Server
+    S.StreamGC, S.Batch, S.Server = (_PlainHandle if form == "plain" else _Handle), _Batch, _Server
+    if form == "plain":
+        import contextlib
+        torch.cuda.ExternalStream = _Stream
+        torch.cuda.Event = _Event
+        torch.cuda.stream = lambda st: contextlib.nullcontext()
+        torch.from_numpy = lambda arr: _Tensor()
+        torch.empty = lambda *a, **k: _Tensor()
     W.batch_specs = _small_specs
     real_rmat = S.Graph.rmat
     S.Graph.rmat = staticmethod(lambda scale, ef, a=0.57, b=0.19, c=0.19, seed=42:
                                 real_rmat(min(scale, 10), min(ef, 8), a, b, c, seed))
     args = types.SimpleNamespace(gpus=world, steps=2, warmup=3, batch_graphs=6, autotune=False, served_rate=2e5,
                                  served_seconds=0.3, served_staleness_us=2000, served_check=False,
-                                 served_regrow=False, sorted_rows=False)
+                                 served_regrow=False, sorted_rows=False, workload="small", cpu_batches=0,
+                                 cpu_seconds=1.0, profile_window=False, graph_publish=False, ingest=False)
     out, err = io.StringIO(), None
     old = sys.stdout
     sys.stdout = out
     try:
-        (bench.run_batched if form == "batched" else bench.run_served)(args)
+        {"plain": bench.run_ours, "batched": bench.run_batched, "served": bench.run_served}[form](args)
     except Exception as e:  # reported to the parent
         err = repr(e)
     finally:
@@ -142,7 +219,7 @@ def _rank(rank, world, port, form, q):
 
 
 @pytest.mark.timeout(600)
-@pytest.mark.parametrize("form", ["batched", "served"])
+@pytest.mark.parametrize("form", ["plain", "batched", "served"])
 def test_two_ranks_share_the_work(form):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -161,7 +238,12 @@ def test_two_ranks_share_the_work(form):
     lines = [json.loads(l) for l in got[0][0].splitlines() if l.startswith("{")]
     assert len(lines) == 1 and not [l for l in got[1][0].splitlines() if l.startswith("{")]
     line = lines[0]
-    assert line["n_gpus"] == 2 and line["form"] == form and line["value"] > 0
+    assert line["n_gpus"] == 2 and line["value"] > 0
+    if form == "plain":  # replicas: twice one replica's epochs over the slowest replica's time
+        assert line["config"]["parallelism"] == "replicas x2"
+        assert line["value"] == pytest.approx(2 * 2 * 32768 / (line["ms_per_step"] * 2 / 1e3))
+        return
+    assert line["form"] == form
     assert line["config"]["placement"].startswith("2 ranks")
     specs = _small_specs(6 if form == "batched" else 63, seed=42 if form == "batched" else 43)
     if form == "batched":
