@@ -144,8 +144,10 @@ __global__ void conc_prep_prev(uint32_t n_arg, EdgeOrder eo, const uint32_t* dyn
 // stream order; the later ones are skipped at their own tickets. So the
 // updates of one edge never run concurrently and no warp waits for another.
 // The batch and the ordering words were written by the copy and the prep
-// kernels before this launch: L2-coherent loads.
-__global__ void __launch_bounds__(256) conc_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg,
+// kernels before this launch: L2-coherent loads. Three blocks per SM: 80
+// registers with little spilling (the budget the one-warp-per-update version
+// ran fastest with; 64 registers spill the update path).
+__global__ void __launch_bounds__(256, 3) conc_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg,
                                                             EdgeOrder eo, const uint32_t* dyn) {
     const uint32_t n = batch_n(n_arg, dyn);
     for (;;) {
