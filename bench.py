@@ -443,9 +443,9 @@ def run_batched(a):
     8,192, 32,768}), each with its own churn stream (16x its edge count, the
     first ticks' worth generated). A tick submits one epoch of every graph. The
     same graphs and updates run twice: per-graph plain launches (one handle per
-    graph, colored by its init stream: apply + publish per epoch) and the
-    batched engine (colored from scratch by its first tick; then one tick = one
-    CUDA-graph launch). Both arms are wall-clock timed from host memory."""
+    graph: apply + publish per epoch) and the batched engine (one tick = one
+    CUDA-graph launch). Both arms start from a full repair of the loaded rows
+    and are wall-clock timed from host memory."""
     import torch
     import streamgc_b200 as S
     from streamgc_b200 import workloads as W
@@ -479,12 +479,9 @@ def run_batched(a):
     hs = [S.StreamGC(gr, epoch_size=epochs[k], histogram_threshold=HIST_THR, slack_pct=300,
                      max_batch=max(epochs[k], 1 << 16), device=local, exact_select=True, full_repair_every=0)
           for k, gr in enumerate(graphs)]
-    for k, h in enumerate(hs):
-        init = W.init_stream(data[k])
-        for s in range(0, len(init), 1 << 16):
-            h.apply(init[s:s + (1 << 16)], S.MODE_CONCURRENT)
-        h.publish()
-        del init
+    for h in hs:  # colored from its loaded rows by one full repair, as the batched arm's first tick does
+        if not h.publish()["proper"]:
+            raise SystemExit("plain arm init not proper")
     torch.cuda.synchronize()
     log(f"plain arm: {len(hs)} handles created and colored in {time.time() - t:.1f}s")
     plain_ticks, plain_updates, plain_ok = [], 0, True
