@@ -10,6 +10,9 @@
 //   --stream-kcore <pct>   dense stream over the k-core at that core-number
 //                          percentile (2 inserts per delete) instead of churn
 //   --slack-pct <p> --max-hist-colors <c>   the reference's compile-time knobs
+//   --exact-select         concurrent configuration: exact color selection and
+//                          independent-set repair (SGC_OPT_EXACT_SELECT)
+//   --graph-publish --sorted-rows            SGC_OPT_GRAPH_PUBLISH, SGC_OPT_SORTED_ROWS
 //
 // Output names follow the code (streamgc.cu:1479-1481):
 //   <dir>/streamgc_<G>gpu_stream<N>_<pct>pct.coloring (+ .txt, + .meta)
@@ -101,6 +104,9 @@ int main(int argc, char** argv) {
         else if (is("--stream-kcore")) kcore_pct = atof(argv[++i]);
         else if (is("--slack-pct")) opt.slack_pct = (uint32_t)atoi(argv[++i]);
         else if (is("--max-hist-colors")) opt.max_hist_colors = (uint32_t)atoi(argv[++i]);
+        else if (strcmp(argv[i], "--exact-select") == 0) opt.flags |= SGC_OPT_EXACT_SELECT;
+        else if (strcmp(argv[i], "--graph-publish") == 0) opt.flags |= SGC_OPT_GRAPH_PUBLISH;
+        else if (strcmp(argv[i], "--sorted-rows") == 0) opt.flags |= SGC_OPT_SORTED_ROWS;
     }
     if (!graph_file) {
         fprintf(stderr, "Usage: %s --graph <path.mtx> [options]\n", argv[0]);
