@@ -113,7 +113,7 @@ int main(int argc, char** argv) {
         return 1;
     }
     if (num_gpus != 1) {
-        fprintf(stderr, "[StreamGC] --num-gpus %u: this build runs the single-GPU path only\n", num_gpus);
+        fprintf(stderr, "[StreamGC] --num-gpus %u: this program runs the single-GPU path only\n", num_gpus);
         return 1;
     }
     std::string hw;

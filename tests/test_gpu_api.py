@@ -153,7 +153,8 @@ def test_reference_integration_test_runs_on_dropin_kernels():
     """The reference's test_single_gpu.cu, linked unchanged against the drop-in,
     gives the same per-test outcome as when it is built with the reference's
     own kernels. On B200 both fail cycle_graph_100: from a long run of equal
-    colors the reference's Tier-1 rule needs about n/2 sweeps,
+    colors the reference's Tier-1 rule needs about n/2 sweeps (each sweep
+    settles only the vertices whose higher-priority neighbors already differ),
     more than the test's 20."""
     def outcome(exe):
         r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
