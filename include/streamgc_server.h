@@ -64,8 +64,8 @@ typedef struct sgc_server_stats {
     uint64_t tenants_resident, tenants_queued, groups;
     uint64_t resident_bytes, budget_bytes;
     uint64_t update_requests, updates_applied, requests_visible, queries, query_vertices;
-    double   visible_p50_ms, visible_p99_ms;  /* update-to-visible */
-    double   query_p50_ms, query_p99_ms;
+    double   visible_p50_ms, visible_p99_ms;  /* update-to-visible, over the last 2^20 requests */
+    double   query_p50_ms, query_p99_ms;      /* over the last 2^20 queries */
     uint64_t ticks, tier1_sweeps, tier2_ticks;  /* group ticks, their repair sweeps, ticks that needed Tier-2 */
     uint64_t tier2_mirror_ticks;                /* ... of which because some tenant's rows may miss mirror entries */
     double   tick_device_ms;                    /* device time of the ticks (SGC_BATCH_PROFILE groups), else 0 */

@@ -79,6 +79,24 @@ struct Group {
     bool last_ok = true;
 };
 
+// The most recent latency samples of one kind (a bounded ring): a long-running
+// server reports percentiles over its last kMax requests.
+struct LatencyWindow {
+    static constexpr size_t kMax = size_t(1) << 20;
+    std::vector<double> v;
+    size_t next = 0;
+    uint64_t total = 0;
+    void add(double ms) {
+        if (v.size() < kMax) {
+            v.push_back(ms);
+        } else {
+            v[next] = ms;
+            next = (next + 1) % kMax;
+        }
+        total++;
+    }
+};
+
 double pct(std::vector<double> v, double q) {
     if (v.empty()) return 0.0;
     const size_t i = std::min(v.size() - 1, (size_t)(q * (double)(v.size() - 1) + 0.5));
@@ -98,7 +116,7 @@ struct sgc_server {
     uint64_t resident_bytes = 0;
     uint64_t next_request = 1;
     std::vector<uint8_t> visible;    // by request id
-    std::vector<double> vis_ms, query_ms;
+    LatencyWindow vis_ms, query_ms;
     uint64_t update_requests = 0, updates_applied = 0, queries = 0, query_vertices = 0;
     uint64_t ticks = 0, tier1_sweeps = 0, tier2_ticks = 0, tier2_mirror_ticks = 0, regrown = 0;
     double tick_device_ms = 0;
@@ -240,7 +258,7 @@ int sgc_server_query(sgc_server* s, uint32_t tenant, const uint32_t* v, uint16_t
     std::lock_guard<std::mutex> lk(s->mu);
     s->queries++;
     s->query_vertices += k;
-    s->query_ms.push_back(ms);
+    s->query_ms.add(ms);
     return rc;
 }
 
@@ -528,7 +546,7 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
                 t.seen_publishes = p;
                 for (auto& q : t.waiting) {
                     s->visible[q.id] = 1;
-                    s->vis_ms.push_back(ms_since(q.arrival, now));
+                    s->vis_ms.add(ms_since(q.arrival, now));
                     r.requests_visible++;
                 }
                 t.waiting.clear();
@@ -598,13 +616,13 @@ int sgc_server_get_stats(sgc_server* s, sgc_server_stats* o) {
     o->budget_bytes = s->opt.hbm_budget_bytes;
     o->update_requests = s->update_requests;
     o->updates_applied = s->updates_applied;
-    o->requests_visible = s->vis_ms.size();
+    o->requests_visible = s->vis_ms.total;
     o->queries = s->queries;
     o->query_vertices = s->query_vertices;
-    o->visible_p50_ms = pct(s->vis_ms, 0.50);
-    o->visible_p99_ms = pct(s->vis_ms, 0.99);
-    o->query_p50_ms = pct(s->query_ms, 0.50);
-    o->query_p99_ms = pct(s->query_ms, 0.99);
+    o->visible_p50_ms = pct(s->vis_ms.v, 0.50);
+    o->visible_p99_ms = pct(s->vis_ms.v, 0.99);
+    o->query_p50_ms = pct(s->query_ms.v, 0.50);
+    o->query_p99_ms = pct(s->query_ms.v, 0.99);
     o->ticks = s->ticks;
     o->tier1_sweeps = s->tier1_sweeps;
     o->tier2_ticks = s->tier2_ticks;

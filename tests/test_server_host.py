@@ -35,3 +35,22 @@ def test_tenants_queue_until_a_step_and_can_leave():
         assert st["tenants_queued"] == 1 and st["tenants_resident"] == 0 and st["update_requests"] == 1
     finally:
         srv.close()
+
+
+def test_queries_before_admission_answer_zero_and_are_counted():
+    """A tenant that is not resident yet answers 0 for every vertex; each query
+    is counted and timed (p50/p99 over the most recent queries)."""
+    c = MG.build_case("delaunay2k")
+    g = S.Graph(c["rp"], c["col"], c["deg"])
+    srv = S.Server(hbm_budget_bytes=1 << 30, max_tick_updates=1 << 12)
+    try:
+        t = srv.add_tenant(g, epoch_size=1024)
+        for k in range(25):
+            out = srv.query(t, [0, 1, 2, k])
+            assert out.tolist() == [0, 0, 0, 0]
+        st = srv.stats()
+        assert st["queries"] == 25 and st["query_vertices"] == 100
+        assert 0.0 <= st["query_p50_ms"] <= st["query_p99_ms"]
+        assert st["requests_visible"] == 0 and st["tenants_regrown"] == 0
+    finally:
+        srv.close()
