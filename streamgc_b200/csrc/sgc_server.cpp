@@ -16,6 +16,7 @@
 #include <deque>
 #include <mutex>
 #include <shared_mutex>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/streamgc_server.h"
@@ -115,12 +116,24 @@ struct sgc_server {
     std::deque<uint32_t> queue;      // tenants waiting for admission, in arrival order
     uint64_t resident_bytes = 0;
     uint64_t next_request = 1;
-    std::vector<uint8_t> visible;    // by request id
+    // Request states from the oldest one not yet resolved (0 pending, 1 visible,
+    // 2 dropped with its tenant); older ids are visible unless in `dropped`.
+    std::deque<uint8_t> req_state;
+    uint64_t req_base = 1;
+    std::unordered_set<uint64_t> dropped;
     LatencyWindow vis_ms, query_ms;
     uint64_t update_requests = 0, updates_applied = 0, queries = 0, query_vertices = 0;
     uint64_t ticks = 0, tier1_sweeps = 0, tier2_ticks = 0, tier2_mirror_ticks = 0, regrown = 0;
     double tick_device_ms = 0;
 };
+
+// Drops the resolved requests at the front of the state window (under mu).
+void trim_requests(sgc_server* s) {
+    while (!s->req_state.empty() && s->req_state.front() != 0) {
+        s->req_state.pop_front();
+        s->req_base++;
+    }
+}
 
 namespace {
 
@@ -152,7 +165,6 @@ int sgc_server_create(const sgc_server_options* opt, sgc_server** out) {
     sgc_server* s = new sgc_server();
     sgc_server_default_options(&s->opt);
     if (opt) s->opt = *opt;
-    s->visible.push_back(0);
     *out = s;
     return SGC_OK;
 }
@@ -209,6 +221,12 @@ int sgc_server_remove_tenant(sgc_server* s, uint32_t tenant) {
     }
     t.regrowing = t.requeued = false;
     t.state = SGC_TENANT_REMOVED;
+    for (const auto* reqs : {&t.held_reqs, &t.waiting})  // never visible now
+        for (const Request& q : *reqs) {
+            s->req_state[q.id - s->req_base] = 2;
+            s->dropped.insert(q.id);
+        }
+    trim_requests(s);
     std::vector<uint64_t>().swap(t.rp);
     std::vector<uint32_t>().swap(t.col);
     std::vector<uint32_t>().swap(t.deg);
@@ -226,7 +244,7 @@ int sgc_server_submit(sgc_server* s, uint32_t tenant, const EdgeUpdate* ups, uin
     if (t.state == SGC_TENANT_REMOVED) return bad("tenant was removed");
     if (n > s->opt.max_tick_updates) return bad("request larger than max_tick_updates");
     Request r{s->next_request++, clk::now(), n};
-    s->visible.push_back(0);
+    s->req_state.push_back(0);
     s->update_requests++;
     // held on the host until the next step forwards it (a step may be running)
     t.held.insert(t.held.end(), ups, ups + n);
@@ -545,7 +563,7 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
             if (p != t.seen_publishes) {  // everything forwarded so far is in this snapshot
                 t.seen_publishes = p;
                 for (auto& q : t.waiting) {
-                    s->visible[q.id] = 1;
+                    s->req_state[q.id - s->req_base] = 1;
                     s->vis_ms.add(ms_since(q.arrival, now));
                     r.requests_visible++;
                 }
@@ -555,6 +573,7 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
             if ((!t.waiting.empty() && s->opt.max_staleness_us) || !t.held_reqs.empty()) g.has_work = true;
         }
     }
+    trim_requests(s);
     r.step_ms = ms_since(t0, clk::now());
     if (rep) *rep = r;
     return SGC_OK;
@@ -563,7 +582,9 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
 int sgc_server_request_visible(sgc_server* s, uint64_t request) {
     if (!s) return SGC_EINVAL;
     std::lock_guard<std::mutex> lk(s->mu);
-    return request < s->visible.size() ? s->visible[request] : 0;
+    if (request == 0 || request >= s->next_request) return 0;
+    if (request < s->req_base) return s->dropped.count(request) ? 0 : 1;
+    return s->req_state[request - s->req_base] == 1 ? 1 : 0;
 }
 
 int sgc_server_snapshot(sgc_server* s, uint32_t tenant, uint16_t* out) {

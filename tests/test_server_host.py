@@ -54,3 +54,18 @@ def test_queries_before_admission_answer_zero_and_are_counted():
         assert st["requests_visible"] == 0 and st["tenants_regrown"] == 0
     finally:
         srv.close()
+
+
+def test_requests_of_a_removed_tenant_are_never_visible():
+    c = MG.build_case("delaunay2k")
+    g = S.Graph(c["rp"], c["col"], c["deg"])
+    srv = S.Server(hbm_budget_bytes=1 << 30, max_tick_updates=1 << 12)
+    try:
+        t = srv.add_tenant(g, epoch_size=1024)
+        ids = [srv.submit(t, c["bench"][k:k + 4]) for k in range(0, 40, 4)]
+        assert ids == sorted(ids) and len(set(ids)) == len(ids)
+        srv.remove_tenant(t)
+        assert not any(srv.visible(i) for i in ids)
+        assert not srv.visible(0) and not srv.visible(ids[-1] + 1)
+    finally:
+        srv.close()
