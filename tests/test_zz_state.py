@@ -91,6 +91,28 @@ def test_staged_batches_match_direct_applies(name):
             b.apply_staged(S.MODE_DETERMINISTIC)  # nothing staged
 
 
+def test_sorted_rows_keep_one_run():
+    """SGC_OPT_SORTED_ROWS: after a forced compaction every row of at most 1024
+    live entries is one strictly ascending run; publishes stay proper and the
+    rows keep their invariants."""
+    c = MG.build_case("rmat11")
+    g = S.Graph(c["rp"], c["col"], c["deg"])
+    ups = np.concatenate([c["init"], c["bench"]])
+    with S.StreamGC(g, epoch_size=c["E"], histogram_threshold=c["thr"], slack_pct=c["slack"],
+                    exact_select=True, sorted_rows=True) as h:
+        for s in range(0, len(ups), 2048):
+            h.apply(ups[s:s + 2048], S.MODE_CONCURRENT)
+            assert h.publish()["proper"] == 1
+            assert _clean(h.check_state())
+        h.drain_and_compact()
+        assert _clean(h.check_state())
+        rp, hw, col = h.row_ptr(), h.highwater(), h.col()
+        for x in range(len(hw)):
+            if hw[x] <= 1024:
+                run = col[rp[x]:rp[x] + hw[x]].astype(np.int64)
+                assert np.all(np.diff(run) > 0), x
+
+
 @pytest.mark.parametrize("name", ["delaunay2k", "rmat11"])
 def test_graph_publish_is_proper_and_keeps_invariants(name):
     """The captured-graph publish (SGC_OPT_GRAPH_PUBLISH): every published
@@ -114,25 +136,3 @@ def test_graph_publish_is_proper_and_keeps_invariants(name):
         assert v["violations"] == 0 and v["uncolored_with_edges"] == 0
         st = h.stats()
         assert st["epochs"] >= len(ups) // B and st["tier1_sweeps"] >= st["epochs"]
-
-
-def test_sorted_rows_keep_one_run():
-    """SGC_OPT_SORTED_ROWS: after a forced compaction every row of at most 1024
-    live entries is one strictly ascending run; publishes stay proper and the
-    rows keep their invariants."""
-    c = MG.build_case("rmat11")
-    g = S.Graph(c["rp"], c["col"], c["deg"])
-    ups = np.concatenate([c["init"], c["bench"]])
-    with S.StreamGC(g, epoch_size=c["E"], histogram_threshold=c["thr"], slack_pct=c["slack"],
-                    exact_select=True, sorted_rows=True) as h:
-        for s in range(0, len(ups), 2048):
-            h.apply(ups[s:s + 2048], S.MODE_CONCURRENT)
-            assert h.publish()["proper"] == 1
-            assert _clean(h.check_state())
-        h.drain_and_compact()
-        assert _clean(h.check_state())
-        rp, hw, col = h.row_ptr(), h.highwater(), h.col()
-        for x in range(len(hw)):
-            if hw[x] <= 1024:
-                run = col[rp[x]:rp[x] + hw[x]].astype(np.int64)
-                assert np.all(np.diff(run) > 0), x
