@@ -1,23 +1,31 @@
 #!/usr/bin/env python
 """Throughput of the streaming graph-coloring path on B200.
 
-Workload (default, `--workload skewed`): R-MAT graph with 2^20 vertices and
-edge factor 48 (a,b,c,d = .57,.19,.19,.05; symmetrised, de-duplicated, self
-loops dropped; ~44.4M undirected edges), colored by its degree-sorted init
-stream, then a dense stream of 2,000,000 updates over the k-core at the 90th
-percentile of core numbers (two inserts of non-adjacent core pairs per delete
-of a live core edge), epoch E = 32,768, histogram threshold 64, alpha = 4.
-`--workload small`: Delaunay triangulation of 131,072 uniform points (seed 42)
-with the reference's 50/50 churn stream of 1,000,000 updates.
+Workload (default, `--workload large`): Chung-Lu graph with 65,608,366
+vertices, expected degrees from a power law with exponent 2.1 scaled to an
+average of 55 and capped at 100,000 (seed 42; ~1.8 G undirected edges, a
+slack CSR of ~14.3 G slots with 64-bit row offsets), colored by one full
+repair of its loaded rows, then the reference's 50/50 churn stream of
+10,000,000 updates (seed 42), epoch E = 32,768 (`--epoch-size` 4,096 and
+262,144 give the epoch sweep), histogram threshold 64, alpha = 4.
+`--workload skewed`: R-MAT graph with 2^20 vertices and edge factor 48
+(a,b,c,d = .57,.19,.19,.05; ~44.4M undirected edges), colored by its
+degree-sorted init stream, then a dense stream of 2,000,000 updates over the
+k-core at the 90th percentile of core numbers (two inserts of non-adjacent
+core pairs per delete). `--workload small`: Delaunay triangulation of 131,072
+uniform points (seed 42) with the reference's 50/50 churn of 1,000,000 updates.
 
 One step = one epoch: E updates applied concurrently (one warp per update)
 followed by the repaired publish (compaction of edited rows, overflow drain,
 fused rebuild + Tier-1 sweeps, Tier-2 when needed, double-buffered snapshot).
 `value` times steps on the device with CUDA events on the library's stream,
 inputs resident in HBM, L2 flushed (256 MiB write) before every timed step;
-`e2e` times the same steps through the C ABI from pinned host memory with the
+every published snapshot is validated between the timed steps. `e2e` times
+the same steps through the C ABI from pinned host memory with the
 host->device copy of each batch and the read-back of the step's counters
-inside the timed region.
+inside the timed region. Update-to-visible latency is the time from a batch's
+submission through the C ABI (host memory) to the return of the publish that
+makes it visible, over `--latency-epochs` further epochs.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -135,17 +143,25 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def read_traffic():
-    """DRAM bytes per launch of the sweep's main kernel, from the committed ncu
-    summary (its `sweep_dram_bytes_per_launch` row), if present."""
-    p = os.path.join(ROOT, "profiles", "sweep_items_skewed_rmat20.md")
+def read_traffic(profile, row):
+    """A per-launch DRAM byte count from a committed ncu summary under
+    profiles/ (its `| row | value |` line), if present."""
+    p = os.path.join(ROOT, "profiles", profile)
     try:
         for line in open(p):
-            if line.startswith("| sweep_dram_bytes_per_launch |"):
-                return int(line.split("|")[2])
+            if line.startswith(f"| {row} |"):
+                return int(float(line.split("|")[2]))
     except (OSError, ValueError):
         pass
     return None
+
+
+# The ncu summaries each workload's roofline traffic comes from.
+PROFILES = {
+    "skewed": ("apply_skewed_rmat20.md", "sweep_items_skewed_rmat20.md"),
+    "large": ("apply_large_chunglu.md", "sweep_items_large_chunglu.md"),
+    "small": (None, None),
+}
 
 
 def max_over_ranks(dist, values, device):
@@ -203,7 +219,7 @@ def run_ours(a):
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
     dist = init_dist(world)
-    nbatch = a.warmup + 2 * a.steps + a.cpu_batches
+    nbatch = a.warmup + 2 * a.steps + a.cpu_batches + a.latency_epochs
     base_len = {"skewed": 2_000_000, "small": 1_000_000, "large": 10_000_000}[a.workload]
     stream_len = max(base_len, nbatch * E)
     g, init, bench, desc = build_workload(a.workload, stream_len)
@@ -241,6 +257,7 @@ def run_ours(a):
     st0 = h.stats()
     evs = []
     reps = []
+    checks = []  # validator on each published snapshot, between the timed steps
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -258,6 +275,9 @@ def run_ours(a):
             e1.record(ext)
             evs.append((e0, ea, e1))
             b += 1
+            if a.validate_steps:
+                ext.synchronize()
+                checks.append(h.validate())  # live colors = the snapshot just published
         ext.synchronize()
         torch.cuda.synchronize()
         if a.profile_window:
@@ -284,6 +304,16 @@ def run_ours(a):
         h.synchronize()
         e2e_s = time.perf_counter() - t0
         d1 = h.stats()
+    # update-to-visible: a batch submitted from pinned host memory through the
+    # C ABI until the publish that contains it has returned
+    vis_ms = []
+    for _ in range(a.latency_epochs):
+        t0 = time.perf_counter()
+        h.apply_ptr(hptr + b * E * 16, E, S.MODE_CONCURRENT)
+        h.publish()
+        h.synchronize()
+        vis_ms.append(1e3 * (time.perf_counter() - t0))
+        b += 1
     total_ms = sum(step_ms)
     if dist:
         total_ms, e2e_s = max_over_ranks(dist, [total_ms, e2e_s], reduce_device(local))
@@ -298,25 +328,30 @@ def run_ours(a):
         sweep_bytes = st1["sweep_bytes"] - st0["sweep_bytes"]
         sweeps = st1["sweep_count"] - st0["sweep_count"]
         achieved = (sweep_bytes / (sweep_ms / 1e3) / 1e9) if sweep_ms > 0 else 0.0
-        traffic = read_traffic()
+        apply_prof, sweep_prof = PROFILES[a.workload] if E == 32768 else (None, None)
+        traffic = read_traffic(sweep_prof, "sweep_dram_bytes_per_launch") if sweep_prof else None
+        apply_traffic = read_traffic(apply_prof, "apply_dram_bytes_per_launch") if apply_prof else None
         apply_avg = sum(apply_ms) / len(apply_ms)
         bpu = cpu.pop("bytes_per_update", None) if cpu else None
-        lat = sorted(step_ms)
-        p50 = lat[len(lat) // 2]
-        p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
+
+        def pctl(v, q):
+            v = sorted(v)
+            return v[min(len(v) - 1, int(round(q * (len(v) - 1))))] if v else None
         pk = f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)" if peak_kind == "measured" else "fallback"
         roof_sweep = {"bound": "hbm", "kernel": "tier-1 sweep (sweep_items + finalize + fac + commit)",
                       "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": pk,
                       "traffic": traffic, "algorithmic_bytes_per_sweep": sweep_bytes / max(1, sweeps),
                       "sweep_ms_avg": sweep_ms / max(1, sweeps), "sweeps_timed": sweeps}
         roof_apply = None
-        if bpu:  # the dominant kernel: the oracle's bytes per update (reference algorithm) over the apply time
+        if bpu:  # the dominant kernel: algorithmic bytes per update under its own rules over the apply time
             ach = bpu * E / (apply_avg / 1e3) / 1e9
             roof_apply = {"bound": "hbm", "kernel": "concurrent apply (conc_prep_insert + conc_prep_prev + "
                           "conc_apply_kernel)", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                          "peak_kind": pk, "traffic": None,
-                          "algorithmic_bytes": "per update, as the sequential oracle reads and writes them "
-                          "(record, slots scanned, state, bitmaps, recolor walk), counted on the CPU sample",
+                          "peak_kind": pk, "traffic": apply_traffic,
+                          "algorithmic_bytes": "per update, the array elements the concurrent apply's rules read "
+                          "and write (record; 32-ary base-run search and tail scan up to the high-water mark; "
+                          "state, bitmap and degree words; recolor walk and early-exit reduce over the live "
+                          "extent), counted by the oracle run under those rules on the CPU sample",
                           "algorithmic_bytes_per_launch": bpu * E, "apply_ms_avg": apply_avg}
         conf = dict(desc)
         conf.update(mode="concurrent (warp per edge) + repaired publish per epoch, exact color selection"
@@ -328,12 +363,19 @@ def run_ours(a):
                     colors_used=int(val["max_color"]), static_greedy_colors=None,
                     tier1_sweeps_per_step=round(sweeps / max(1, a.steps), 2),
                     tier2_runs_in_timed=sum(r["tier2_ran"] for r in reps),
-                    all_published_proper=all(r["proper"] for r in reps))
+                    all_published_proper=all(r["proper"] for r in reps),
+                    snapshots_validated=len(checks),
+                    snapshot_violations=sum(int(c["violations"]) + int(c["uncolored_with_edges"]) for c in checks),
+                    max_colors_in_timed=max((int(c["max_color"]) for c in checks), default=None),
+                    reference_gpu=REFERENCE_GPU[a.workload])
         out = {
             "metric": METRIC, "value": job_rate(a.steps * E, world, total_ms / 1e3), "unit": "updates/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": conf,
-            "latency_ms": {"update_to_visible_p50": p50, "update_to_visible_p99": p99},
+            "latency_ms": {"update_to_visible_p50": pctl(vis_ms, 0.50), "update_to_visible_p99": pctl(vis_ms, 0.99),
+                           "samples": len(vis_ms), "epoch_device_ms_p50": pctl(step_ms, 0.50),
+                           "what": "per epoch of E updates: submit from pinned host memory through the C ABI to "
+                                   "the return of the publish that makes it visible (wall clock)"},
             "roofline": roof_apply if roof_apply else roof_sweep,
             "roofline_sweep": roof_sweep,
             "apply": {"ms_per_epoch": apply_avg, "share_of_step": apply_avg / (total_ms / a.steps),
@@ -353,13 +395,21 @@ def run_ours(a):
 
 
 def cpu_baseline(g, h, bench, first_batch, nb, budget_s):
-    """The oracle (CPU restatement, OpenMP where order-independent) timed on the
-    same state and the next batches of the same stream."""
+    """The oracle (CPU restatement, OpenMP where order-independent) run under
+    the concurrent configuration's rules, timed on the GPU's current state and
+    the next batches of the same stream. The slot slab is downloaded straight
+    into the oracle's own (one host copy of it, whatever the graph's size)."""
     from oracle import oracle as O
-    o = O.Oracle(g.row_ptr, g.col_idx, g.degree, hist_threshold=HIST_THR, exact=True)
-    o.load_state(h.col(), h.states(), h.bitmaps(), np.zeros(0, dtype=np.uint32))
+    import resource
+    t = time.perf_counter()
+    o = O.Oracle(g.row_ptr, g.col_idx, g.degree, hist_threshold=HIST_THR, exact=True, conc=True)
+    ptr, nbytes = o.col_data()
+    h.download_into("col", ptr, nbytes)
+    o.load_state_inplace(g.row_ptr, g.col_idx, h.states(), h.bitmaps())
+    o.load_rows_model(h.highwater(), h.base_runs(), h.holes())
     # the GPU's last publish was proper on mirror-complete rows: same repair rules from here
     o.set_repair_state(clean=True, asym=False)
+    load_s = time.perf_counter() - t
     o.reset_bytes()
     done = 0
     t0 = time.perf_counter()
@@ -391,31 +441,74 @@ def cpu_baseline(g, h, bench, first_batch, nb, budget_s):
     o.close()
     if not done:
         return None
+    rss_gb = resource.getrusage(resource.RUSAGE_SELF).ru_maxrss / 2**20
     return {"value": done * E / dt, "unit": "updates/s", "cores": cores, "kind": "port",
             "bytes_per_update": bytes_update / (done * E),
             "single_core": ({"value": done1 * E / dt1, "cores": 1, "sample": f"{done1} further epochs of {E} updates"}
                             if done1 else None),
-            "sample": f"{done} epochs of {E} updates following the GPU-timed ones, same state and rules "
-                      f"(exact selection, independent-set repair), updates in stream order + repaired epoch ({dt:.1f}s)"}
+            "sample": f"{done} epochs of {E} updates following the GPU-timed ones, from the GPU's state, under the "
+                      f"concurrent configuration's rules (updates in stream order + repaired epoch, {dt:.1f}s)",
+            "host": host_facts(), "state_load_s": round(load_s, 1), "peak_rss_gb": round(rss_gb, 1)}
+
+
+def host_facts():
+    """CPU model, thread count and C++ runtime of this host (the stream
+    generators call libstdc++'s distributions)."""
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    libstdcxx = None
+    for d in ("/usr/lib/x86_64-linux-gnu", "/usr/lib64", "/usr/lib"):
+        try:
+            names = sorted(f for f in os.listdir(d) if f.startswith("libstdc++.so.6."))
+        except OSError:
+            continue
+        if names:
+            libstdcxx = names[-1]
+            break
+    return {"cpu_model": model, "threads": os.cpu_count(), "libstdcxx": libstdcxx}
+
+
+# The reference's own kernels on the GPU (built for sm_100a from its sources):
+# measured on the small and skewed workloads only (profiles/reference_kernels_sm100a.md).
+REFERENCE_GPU = {
+    "large": {"unavailable": "the reference's row offsets are 32-bit (include/streamgc.cuh:56-58): its slack CSR "
+                             "cannot address this graph's ~14.3 G slots"},
+    "skewed": {"see": "profiles/reference_kernels_sm100a.md"},
+    "small": {"see": "profiles/reference_kernels_sm100a.md"},
+}
 
 
 def run_reference(a):
-    """The reference path's CPU restatement (oracle port): it has no CPU
-    implementation of its own, so the oracle stands for it."""
+    """The path's CPU restatement (the oracle: the reference has no CPU
+    implementation of its own) on the same workload, under the same rules as
+    the GPU arm (exact selection, independent-set repair, the concurrent
+    apply's row layout), all host threads, one epoch of E updates plus its
+    repaired publish per step. The large graph starts from a first-fit
+    coloring of its rows (its init stream is 1.8 G updates); the others from
+    their init streams."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return
-    if a.workload == "large":
-        print(json.dumps({"impl": "reference", "unavailable": "the oracle's state for the 1.8 G-edge Chung-Lu "
-                          "graph does not fit a bounded CPU run; the small and skewed workloads have one"}), flush=True)
-        return
     from oracle import oracle as O
-    stream_len = max(2_000_000 if a.workload == "skewed" else 1_000_000, (a.warmup + a.steps) * E)
+    stream_len = max({"skewed": 2_000_000, "small": 1_000_000, "large": 10_000_000}[a.workload],
+                     (a.warmup + a.steps) * E)
     g, init, bench, desc = build_workload(a.workload, stream_len)
     t = time.time()
-    o = O.Oracle(g.row_ptr, g.col_idx, g.degree, hist_threshold=HIST_THR)
-    o.process_stream_repaired(init, len(init), len(init))
-    log(f"oracle init {time.time() - t:.1f}s")
+    o = O.Oracle(g.row_ptr, g.col_idx, g.degree, hist_threshold=HIST_THR, exact=True, conc=True)
+    if init is None:
+        colors = o.color_greedy()
+        how = f"first-fit coloring of the loaded rows in id order ({colors} colors)"
+    else:
+        o.process_stream_repaired(init, len(init), len(init))
+        how = "init stream (every edge as an ADD) + repaired publish"
+    del g
+    log(f"oracle initial coloring {time.time() - t:.1f}s: {how}")
     for k in range(a.warmup):
         o.process_stream_repaired(bench[k * E:(k + 1) * E], E, E)
     times = []
@@ -426,14 +519,20 @@ def run_reference(a):
     total = sum(times)
     v = a.steps * E / total
     cores = int(O.lib().og_num_threads())
+    colors = int(o.colors().max())
+    o.close()
     conf = dict(desc)
-    conf.update(mode="CPU oracle: updates in stream order + repaired epoch", parallelism="1 process")
+    conf.update(init=how, mode="CPU oracle under the concurrent configuration's rules (exact selection, "
+                "independent-set repair, base runs with tombstones): updates in stream order + repaired epoch",
+                parallelism="1 process", colors_after=colors)
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "updates/s", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total / a.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": conf,
            "cpu_baseline": {"value": v, "unit": "updates/s", "cores": cores, "kind": "port",
-                            "sample": f"{a.steps} epochs of {E} updates after {a.warmup} warm-up epochs"},
-           "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                            "sample": f"{a.steps} epochs of {E} updates after {a.warmup} warm-up epochs",
+                            "host": host_facts()},
+           "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "workload_generation": "the library's host-side generators (C++; no GPU is used by this arm)"}
     print(json.dumps(out), flush=True)
 
 
@@ -795,7 +894,7 @@ def main():
     ap.add_argument("--steps", type=int, default=24)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="skewed", choices=["skewed", "small", "large"],
+    ap.add_argument("--workload", default="large", choices=["skewed", "small", "large"],
                     help="plain path: skewed (R-MAT 2^20 x 48, k-core stream), small (Delaunay 2^17 churn), "
                          "large (Chung-Lu 65.6 M vertices, ~1.8 G edges, 10 M churn)")
     ap.add_argument("--sorted-rows", action="store_true",
@@ -809,6 +908,10 @@ def main():
     ap.add_argument("--epoch-size", type=int, default=32768,
                     help="plain path: updates per epoch (the large workload's sweep uses 4096, 32768, 262144)")
     ap.add_argument("--cpu-batches", type=int, default=8, help="epochs timed on the CPU baseline (0: skip)")
+    ap.add_argument("--latency-epochs", type=int, default=128,
+                    help="plain path: epochs timed one by one from submission to visibility after the e2e steps")
+    ap.add_argument("--no-validate-steps", dest="validate_steps", action="store_false",
+                    help="plain path: skip the validator on each published snapshot between timed steps")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--profile-window", action="store_true",
                     help="bracket the device-timed steps with cudaProfilerStart/Stop (for ncu)")
@@ -825,8 +928,8 @@ def main():
     a = ap.parse_args()
     global E
     E = a.epoch_size
-    if a.workload == "large" and "--cpu-batches" not in sys.argv:
-        a.cpu_batches = 0  # the oracle's state for 1.8 G edges does not fit a bounded CPU sample
+    if a.workload == "large" and "--cpu-seconds" not in sys.argv:
+        a.cpu_seconds = 30.0
     if a.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
     if a.impl == "reference":

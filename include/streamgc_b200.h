@@ -139,6 +139,8 @@ typedef struct sgc_state_report {
 #define SGC_DL_HIGHWATER 7   /* uint32[n] per-row high-water mark */
 #define SGC_DL_HDMAP     8   /* uint32[n] histogram row or 0xFFFFFFFF */
 #define SGC_DL_OVERFLOW  9   /* OverflowEdge[min(overflow_pending, 262144)] */
+#define SGC_DL_BASE_RUN 10   /* uint32[n] length of each row's sorted base run (exact selection), else zeros */
+#define SGC_DL_HOLES    11   /* uint32[n] free slots below each row's mark (exact selection), else zeros */
 
 /* Fills defaults: slack 300, 1024 histogram colors, batch 32768, device 0. */
 int sgc_default_options(sgc_options* opt);

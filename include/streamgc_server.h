@@ -44,8 +44,11 @@ typedef struct sgc_server_options {
     int32_t  device;
     uint32_t slack_pct;          /* 300 = alpha 4 */
     uint32_t regrow;             /* 1: a tenant whose rows dropped an entry (a row still full at the
-                                    drain) is re-admitted with rows sized from its current degrees and
-                                    every surviving entry's mirror restored; 0 (default): kept as is */
+                                    drain) is re-admitted with rows sized from its current degrees: every
+                                    surviving entry's mirror is restored, and every edge whose last
+                                    forwarded update since its last admission was an insert is put back
+                                    (the server keeps those edges per tenant while this is on);
+                                    0 (default): kept as is */
 } sgc_server_options;
 
 enum { SGC_TENANT_QUEUED = 0, SGC_TENANT_RESIDENT = 1, SGC_TENANT_REMOVED = 2 };
@@ -72,6 +75,8 @@ typedef struct sgc_server_stats {
     uint64_t overflows, drain_failed;           /* row overflows (pending + lost) and failed drains, all groups */
     uint64_t device_errors;                     /* groups whose device error word is set */
     uint64_t tenants_regrown;                   /* re-admissions with rebuilt rows (options.regrow) */
+    uint64_t requests_tracked;                  /* request states kept: from the oldest unresolved request on */
+    uint64_t requests_dropped;                  /* requests dropped with removed tenants, all time */
 } sgc_server_stats;
 
 int sgc_server_default_options(sgc_server_options* opt);
@@ -93,7 +98,10 @@ int sgc_server_query(sgc_server* s, uint32_t tenant, const uint32_t* v, uint16_t
 /* One scheduling round: admit, tick every group with work, publish, record
  * latencies. Steps must not overlap each other (one stepping thread). */
 int sgc_server_step(sgc_server* s, sgc_server_step_report* rep);
-/* 1 once the request's updates are in a published snapshot. */
+/* 1 once the request's updates are in a published snapshot; 0 while pending
+ * or when it was dropped with its removed tenant. The server remembers the
+ * ids of the last 2^20 dropped requests: for an older resolved request that
+ * may have been among earlier drops the answer is SGC_EINVAL (unknown). */
 int sgc_server_request_visible(sgc_server* s, uint64_t request);
 int sgc_server_snapshot(sgc_server* s, uint32_t tenant, uint16_t* out);
 /* A resident tenant's live rows in its own ids (as sgc_batch_rows); call

@@ -68,6 +68,10 @@ def lib():
             "og_process_stream_repaired": (C.c_uint32, [_vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32]),
             "og_phase_end": (C.c_uint32, [_vp, C.POINTER(C.c_int), _u32p]),
             "og_load_state": (None, [_vp, _u32p, _u32p, _u64p, _u32p]),
+            "og_col_data": (C.c_void_p, [_vp]),
+            "og_load_rows_model": (None, [_vp, _u32p, _u32p, _u32p]),
+            "og_color_greedy": (C.c_uint16, [_vp]),
+            "og_load_state_inplace": (None, [_vp, _u64p, _u32p, _u32p, _u64p, _u32p]),
             "og_publish_repair": (None, [_vp, C.c_int, _u32p]),
             "og_set_full_repair_every": (None, [_vp, C.c_uint32]),
             "og_set_repair_state": (None, [_vp, C.c_int, C.c_int]),
@@ -123,16 +127,21 @@ class Oracle:
     """Single-GPU StreamGC state restated on the CPU (sequential, stream order)."""
 
     def __init__(self, row_ptr, col, degree, hist_threshold=64, slack_pct=300, max_hist_colors=1024,
-                 exact=False):
+                 exact=False, conc=False):
         """exact: exact color selection above the threshold and the independent-set
-        Tier-1 (the concurrent configuration's rules); default: the reference's."""
+        Tier-1 (the concurrent configuration's rules); default: the reference's.
+        conc (with exact): also the concurrent apply's row layout and update
+        rules (sorted base runs with tombstones, tail inserts, scans bounded by
+        the high-water mark, lazy compaction, early-exit color reduction), so
+        that the byte counters count what those rules read and write."""
         self.L = lib()
         rp = np.ascontiguousarray(row_ptr, dtype=np.uint64)
         col = np.ascontiguousarray(col, dtype=np.uint32)
         deg = np.ascontiguousarray(degree, dtype=np.uint32)
         self.n = len(rp) - 1
         self.h = self.L.og_create(self.n, _p(rp, _u64p), _p(col, _u32p), _p(deg, _u32p),
-                                  hist_threshold, slack_pct, max_hist_colors, 1 if exact else 0)
+                                  hist_threshold, slack_pct, max_hist_colors,
+                                  (1 if exact else 0) | (2 if exact and conc else 0))
 
     def close(self):
         if self.h:
@@ -201,6 +210,33 @@ class Oracle:
         bitmaps = np.ascontiguousarray(bitmaps, dtype=np.uint64)
         hist = np.ascontiguousarray(hist, dtype=np.uint32)
         self.L.og_load_state(self.h, _p(col, _u32p), _p(states, _u32p), _p(bitmaps, _u64p), _p(hist, _u32p))
+
+    def col_data(self):
+        """Address and byte size of the oracle's slot slab (filled in place by
+        load_state_inplace's caller)."""
+        return int(self.L.og_col_data(self.h)), int(self.L.og_total_slots(self.h)) * 4
+
+    def load_state_inplace(self, row_ptr, col_idx, states, bitmaps, hist=None):
+        """After the slab was written through col_data(): rows that differ from
+        their base rows are marked edited; states, bitmaps (and histograms)
+        are copied in."""
+        rp = np.ascontiguousarray(row_ptr, dtype=np.uint64)
+        col = np.ascontiguousarray(col_idx, dtype=np.uint32)
+        states = np.ascontiguousarray(states, dtype=np.uint32)
+        bitmaps = np.ascontiguousarray(bitmaps, dtype=np.uint64)
+        hp = None if hist is None else _p(np.ascontiguousarray(hist, dtype=np.uint32), _u32p)
+        self.L.og_load_state_inplace(self.h, _p(rp, _u64p), _p(col, _u32p), _p(states, _u32p), _p(bitmaps, _u64p),
+                                     hp)
+
+    def load_rows_model(self, highwater, base_runs, holes):
+        """Concurrent rules: each row's high-water mark, base-run length and
+        hole count (the library's, after load_state)."""
+        a = [np.ascontiguousarray(x, dtype=np.uint32) for x in (highwater, base_runs, holes)]
+        self.L.og_load_rows_model(self.h, *[_p(x, _u32p) for x in a])
+
+    def color_greedy(self):
+        """First-fit coloring of the live rows in id order; returns the largest color."""
+        return int(self.L.og_color_greedy(self.h))
 
     def set_states(self, a):
         a = np.ascontiguousarray(a, dtype=np.uint32)

@@ -9,6 +9,17 @@
 //                  stream order (the deterministic reference run the golden
 //                  fixtures come from)
 //   --launch ref   the reference's own launch shape (streamgc.cu:847-853), timed
+//   --repair       after each phase's drain_and_compact, the reference's phase-end
+//                  repair: the Tier-1 loop of conflict_repair_kernel launches
+//                  (streamgc.cu:1317-1393) and Tier-2 (streamgc.cu:1057-1240, run
+//                  by the oracle's restatement of it, which writes back states
+//                  only, as the reference does); a "final" record then holds the
+//                  color count and the violations of the final coloring
+//   --no-dump      no per-epoch state records (timing runs on large graphs)
+//
+// Timing follows the reference's process_stream: wall clock around the whole
+// stream (batch copy, launch, synchronize, epoch steps), plus CUDA-event time
+// of the local_update_kernel launches and of the epoch steps' kernels.
 //
 // The partition is built the way allocate_gpu_partition does it for one GPU
 // (streamgc.cu:144-444): identity hash map, max_owned = n + n/4, per-row
@@ -37,6 +48,17 @@ __global__ void epoch_snapshot_kernel(GPUPartition* partition, uint32_t num_vert
 __global__ void compact_csr_kernel(GPUPartition* partition);
 __global__ void drain_overflow_local_kernel(GPUPartition* partition, uint32_t overflow_count, uint32_t* num_failed);
 __global__ void rebuild_bitmaps_kernel(GPUPartition* partition);
+__global__ void conflict_repair_kernel(GPUPartition* partition, uint32_t histogram_threshold, uint32_t* num_conflicts);
+
+// The oracle's C interface (oracle/sgc_oracle.cpp), for Tier-2.
+extern "C" {
+void* og_create(uint32_t n, const uint64_t* row_ptr, const uint32_t* col_idx, const uint32_t* degree,
+                uint32_t hist_thr, uint32_t slack_pct, uint32_t max_hist_colors, uint32_t flags);
+void og_destroy(void* h);
+void og_load_state(void* h, const uint32_t* col, const uint32_t* states, const uint64_t* bitmaps, const uint32_t* hist);
+uint32_t og_tier2(void* h);
+void og_get_states(void* h, uint32_t* out);
+}
 
 static FILE* g_out = nullptr;
 
@@ -158,11 +180,13 @@ static void dump(const Built& b, uint32_t n, const char* tag) {
 int main(int argc, char** argv) {
     const char* in = nullptr;
     const char* out = nullptr;
-    bool det = true;
+    bool det = true, repair = false, dumps = true;
     for (int i = 1; i < argc; i++) {
         if (!strcmp(argv[i], "--in") && i + 1 < argc) in = argv[++i];
         else if (!strcmp(argv[i], "--out") && i + 1 < argc) out = argv[++i];
         else if (!strcmp(argv[i], "--launch") && i + 1 < argc) det = strcmp(argv[++i], "ref") != 0;
+        else if (!strcmp(argv[i], "--repair")) repair = true;
+        else if (!strcmp(argv[i], "--no-dump")) dumps = false;
     }
     if (!in || !out) {
         fprintf(stderr, "usage: %s --in <case.bin> --out <dump.bin> [--launch det|ref]\n", argv[0]);
@@ -205,8 +229,18 @@ int main(int argc, char** argv) {
             CUDA_CHECK(cudaDeviceSynchronize());
         }
     };
+    cudaEvent_t ev0, ev1;
+    CUDA_CHECK(cudaEventCreate(&ev0));
+    CUDA_CHECK(cudaEventCreate(&ev1));
+    double ev_apply_ms = 0, ev_epoch_ms = 0, wall_epoch_ms = 0;
+    auto event_ms = [&]() {
+        float ms = 0;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, ev0, ev1));
+        return (double)ms;
+    };
     auto epoch = [&]() {
         const int blk = (n + 255) / 256;
+        CUDA_CHECK(cudaEventRecord(ev0));
         epoch_snapshot_kernel<<<blk, 256>>>(b.d, n);
         compact_csr_kernel<<<blk, 256>>>(b.d);
         CUDA_CHECK(cudaDeviceSynchronize());
@@ -217,14 +251,18 @@ int main(int argc, char** argv) {
         }
         CUDA_CHECK(cudaDeviceSynchronize());
         rebuild_bitmaps_kernel<<<blk, 256>>>(b.d);
+        CUDA_CHECK(cudaEventRecord(ev1));
         CUDA_CHECK(cudaDeviceSynchronize());
     };
+    int bench_epochs = 0;
     auto process = [&](const std::vector<EdgeUpdate>& ups, const char* phase) -> double {
         uint64_t processed = 0, since = 0;
+        const bool timed = !strcmp(phase, "bench");
         auto t0 = std::chrono::high_resolution_clock::now();
         while (processed < ups.size()) {
             const uint32_t c = (uint32_t)std::min<uint64_t>(batch, ups.size() - processed);
             CUDA_CHECK(cudaMemcpy(d_up, ups.data() + processed, (size_t)c * 16, cudaMemcpyHostToDevice));
+            CUDA_CHECK(cudaEventRecord(ev0));
             if (det) {
                 local_update_kernel<<<1, 32>>>(d_up, c, b.d, thr);
             } else {
@@ -232,13 +270,22 @@ int main(int argc, char** argv) {
                 const int blocks = std::max<int>((c * 32 + threads - 1) / threads, 1);
                 local_update_kernel<<<blocks, threads>>>(d_up, c, b.d, thr);
             }
+            CUDA_CHECK(cudaEventRecord(ev1));
             CUDA_CHECK(cudaDeviceSynchronize());
+            if (timed) ev_apply_ms += event_ms();
             processed += c;
             since += c;
             if (since >= E) {
+                auto te = std::chrono::high_resolution_clock::now();
                 epoch();
+                if (timed) {
+                    ev_epoch_ms += event_ms();
+                    wall_epoch_ms += std::chrono::duration<double, std::milli>(
+                        std::chrono::high_resolution_clock::now() - te).count();
+                    bench_epochs++;
+                }
                 since = 0;
-                if (det) {
+                if (det && dumps) {
                     char t[32];
                     snprintf(t, sizeof(t), "%s_e%d", phase, epoch_no);
                     dump(b, n, t);
@@ -260,18 +307,96 @@ int main(int argc, char** argv) {
         CUDA_CHECK(cudaDeviceSynchronize());
         rebuild_bitmaps_kernel<<<blk, 256>>>(b.d);
         CUDA_CHECK(cudaDeviceSynchronize());
-        dump(b, n, tag);
+        if (dumps) dump(b, n, tag);
+    };
+    // Phase-end repair: Tier-1 loop (streamgc.cu:1317-1393), then Tier-2.
+    uint32_t* d_nconf = nullptr;
+    CUDA_CHECK(cudaMallocManaged(&d_nconf, 4));
+    std::vector<uint64_t> rp64(rp.begin(), rp.end());
+    double t1_iters[2] = {0, 0}, t2_fixed[2] = {0, 0}, rep_ms[2] = {0, 0};
+    auto phase_repair = [&](int ph) {
+        auto t0 = std::chrono::high_resolution_clock::now();
+        const int blk = (n + 255) / 256;
+        uint32_t prev = UINT32_MAX;
+        int plateau = 0, it = 0;
+        for (; it < 20; it++) {
+            rebuild_bitmaps_kernel<<<blk, 256>>>(b.d);
+            CUDA_CHECK(cudaDeviceSynchronize());
+            *d_nconf = 0;
+            conflict_repair_kernel<<<blk, 256>>>(b.d, thr, d_nconf);
+            CUDA_CHECK(cudaDeviceSynchronize());
+            const uint32_t c = *d_nconf;
+            if (c == 0) { it++; break; }
+            if (c == prev) {
+                if (++plateau >= 3) { it++; break; }
+            } else {
+                plateau = 0;
+            }
+            prev = c;
+        }
+        t1_iters[ph] = it;
+        // Tier-2 on the pulled state; states written back
+        auto st = d2h(reinterpret_cast<const uint32_t*>(b.h.owned), n);
+        auto bm = d2h(b.h.neighbor_bitmap, n);
+        auto cl = d2h(b.h.col_idx, b.total);
+        auto hs = d2h(b.h.freq_histogram, (size_t)b.h.num_high_degree * MAX_HISTOGRAM_COLORS);
+        void* o = og_create(n, rp64.data(), col.data(), deg.data(), thr, slack, MAX_HISTOGRAM_COLORS, 0);
+        og_load_state(o, cl.data(), st.data(), bm.data(), hs.data());
+        const uint32_t fixed = og_tier2(o);
+        if (fixed) {
+            og_get_states(o, st.data());
+            CUDA_CHECK(cudaMemcpy(b.h.owned, st.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
+        }
+        og_destroy(o);
+        t2_fixed[ph] = fixed;
+        rep_ms[ph] = std::chrono::duration<double, std::milli>(std::chrono::high_resolution_clock::now() - t0).count();
+    };
+    // Color count and properness of the final coloring on the live CSR
+    // (check_coloring_valid, streamgc.cu:448-556, counted per entry x < y).
+    auto final_record = [&]() {
+        auto st = d2h(reinterpret_cast<const uint32_t*>(b.h.owned), n);
+        auto cl = d2h(b.h.col_idx, b.total);
+        std::vector<uint32_t> lrp(n + 1);
+        CUDA_CHECK(cudaMemcpy(lrp.data(), b.h.row_ptr, (n + 1) * 4, cudaMemcpyDeviceToHost));
+        uint64_t viol = 0, edges = 0, unc = 0, maxc = 0;
+        for (uint32_t x = 0; x < n; x++) {
+            const uint32_t cx = st[x] & 0xFFFFu;
+            bool eff = false;
+            for (uint32_t j = lrp[x]; j < lrp[x + 1]; j++) {
+                const uint32_t y = cl[j];
+                if (y == CSR_INVALID || y >= n) continue;
+                eff = true;
+                if (x < y) {
+                    edges++;
+                    if (cx && cx == (st[y] & 0xFFFFu)) viol++;
+                }
+            }
+            if (!cx && eff) unc++;
+            if (cx > maxc) maxc = cx;
+        }
+        const double fin[4] = {(double)maxc, (double)viol, (double)unc, (double)edges};
+        rec("final", nullptr, 0);
+        rec("values", fin, sizeof(fin));
+        printf("ref_driver: final colors %llu, violations %llu, uncolored with edges %llu, edges %llu\n",
+               (unsigned long long)maxc, (unsigned long long)viol, (unsigned long long)unc, (unsigned long long)edges);
     };
     const double init_ms = process(init, "init");
     drain_and_compact("init_dc");
+    if (repair) phase_repair(0);
     const double bench_ms = process(bench, "bench");
     drain_and_compact("bench_dc");
+    if (repair) phase_repair(1);
+    final_record();
     double mups = bench_ms > 0 ? nb / bench_ms / 1000.0 : 0.0;
     rec("timing", nullptr, 0);
-    double tm[3] = {init_ms, bench_ms, mups};
+    double tm[12] = {init_ms,      bench_ms,     mups,       ev_apply_ms, ev_epoch_ms, wall_epoch_ms,
+                     (double)bench_epochs, t1_iters[0], t1_iters[1], t2_fixed[0], t2_fixed[1], rep_ms[1]};
     rec("ms", tm, sizeof(tm));
     fclose(g_out);
-    printf("ref_driver: n=%u init %.2f ms, bench %.2f ms (%.3f M updates/s), launch=%s, epochs=%d\n", n, init_ms,
-           bench_ms, mups, det ? "det" : "ref", epoch_no);
+    printf("ref_driver: n=%u init %.2f ms, bench %.2f ms (%.3f M updates/s), launch=%s, epochs=%d, "
+           "bench kernels: apply %.2f ms, epoch steps %.2f ms over %d epochs; repair: tier1 %g/%g iters, "
+           "tier2 fixed %g/%g, bench repair %.1f ms\n",
+           n, init_ms, bench_ms, mups, det ? "det" : "ref", epoch_no, ev_apply_ms, ev_epoch_ms, bench_epochs,
+           t1_iters[0], t1_iters[1], t2_fixed[0], t2_fixed[1], rep_ms[1]);
     return 0;
 }

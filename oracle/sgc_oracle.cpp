@@ -53,6 +53,7 @@ namespace {
 constexpr uint32_t INV = SGC_CSR_INVALID;
 constexpr uint32_t EMPTY = SGC_HASH_EMPTY;
 constexpr uint32_t OVF_CAP = SGC_OVERFLOW_CAPACITY;
+constexpr uint32_t TOMB = 0x80000000u;  // tombstone bit (concurrent-rules layout)
 
 struct Bytes {
     uint64_t update = 0;   // local update path
@@ -66,6 +67,20 @@ struct Oracle {
     uint32_t hist_thr = 64;
     uint32_t maxc = 1024;          // MAX_HISTOGRAM_COLORS
     bool exact = false;            // exact selection above the threshold + independent-set Tier-1
+    // Concurrent rules (with exact): the row layout and update rules the
+    // library's concurrent apply runs by, applied here in stream order. Rows
+    // keep a sorted base run [rp, rp+mbl) searched 32-ary (a delete there
+    // leaves id | TOMB, a re-insert of the id revives it); other inserts go to
+    // the tail at the first free slot after the run; every reader stops at the
+    // high-water mark rp+mhw; compaction is lazy (rows whose holes exceed a
+    // quarter of the mark); a delete's color reduction on a row above the
+    // threshold moves to the freed color only when no live neighbor holds it
+    // (an early-exit scan). Colors and edge sets follow the same rules as the
+    // library's concurrent configuration; byte counters count what those rules
+    // read and write.
+    bool conc = false;
+    std::vector<uint32_t> mhw, mbl, mholes;
+    std::vector<uint8_t> mdirty;
     std::vector<uint64_t> rp;      // logical row starts, rp[n] = total slots
     std::vector<uint32_t> col;     // slack CSR slots
     std::vector<uint32_t> st;      // packed (color | version << 16)
@@ -97,6 +112,9 @@ struct Oracle {
 
     // -------- state helpers (vertex_state.cuh:17-27, priority.cuh:8-10) --------
     inline uint16_t color(uint32_t x) const { return (uint16_t)(st[x] & 0xFFFFu); }
+    // end of the slots readers visit; a slot that holds no entry
+    inline uint64_t re(uint32_t x) const { return conc ? rp[x] + mhw[x] : rp[x + 1]; }
+    inline bool hole(uint32_t v) const { return v == INV || (conc && (v & TOMB)); }
     inline uint16_t ver(uint32_t x) const { return (uint16_t)(st[x] >> 16); }
     inline uint64_t prio(uint32_t x) const { return ((uint64_t)deg[x] << 32) | x; }
     inline uint32_t* hrow(uint32_t x) {
@@ -113,7 +131,7 @@ struct Oracle {
         if (~bmv != 0) return (uint16_t)(__builtin_ctzll(~bmv) + 1);
         bool used[256];
         std::memset(used, 0, sizeof(used));
-        for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+        for (uint64_t j = rp[x]; j < re(x); j++) {
             uint32_t ng = col[j];
             b += 4;
             if (ng == INV) continue;
@@ -142,7 +160,7 @@ struct Oracle {
     // Exact selection: the first color (1..2047) no live neighbor holds, else 2048.
     uint16_t fac_exact(uint32_t x, const std::vector<uint32_t>& cols, uint64_t& b) const {
         std::vector<uint8_t> used(2048, 0);
-        for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+        for (uint64_t j = rp[x]; j < re(x); j++) {
             uint32_t ng = col[j];
             b += 4;
             if (ng == INV || ng >= n) continue;
@@ -201,9 +219,119 @@ struct Oracle {
         return ~0ull;
     }
 
+    // -------- concurrent-rules row edits (the library's warp_add_slot /
+    // warp_remove_slot with a base run) --------
+    // Slot of id `key` (live or tombstone) in the run, or ~0; counts one
+    // 32-slot probe round per level of the 32-ary search.
+    uint64_t run_find(uint32_t x, uint32_t key, uint64_t& b) const {
+        uint64_t lo = rp[x], hi = rp[x] + mbl[x];
+        if (lo == hi) return ~0ull;
+        uint64_t len = hi - lo;
+        for (; len > 32; len = len - 31 * (len / 32)) b += 128;  // 32 probes per round
+        b += 4 * len;                                           // the last bucket, one slot per lane
+        while (lo < hi) {
+            const uint64_t m = lo + (hi - lo) / 2;
+            if ((col[m] & ~TOMB) < key) lo = m + 1;
+            else hi = m;
+        }
+        if (lo < rp[x] + mbl[x] && (col[lo] & ~TOMB) == key) return lo;
+        return ~0ull;
+    }
+    void extend_row(uint32_t x, uint32_t q) {
+        if (q < mhw[x]) mholes[x]--;
+        else if (q > mhw[x]) mholes[x] += q - mhw[x];
+        if (q + 1 > mhw[x]) mhw[x] = q + 1;
+        mdirty[x] = 1;
+    }
+    int add_slot_conc(uint32_t x, uint32_t nbr, uint64_t& b) {
+        b += 4;  // run length
+        const uint64_t p = run_find(x, nbr, b);
+        if (p != ~0ull) {
+            if (col[p] == nbr) return 1;
+            col[p] = nbr;  // revive the tombstone
+            b += 8;
+            mholes[x]--;
+            mdirty[x] = 1;
+            return 0;
+        }
+        for (uint64_t j = rp[x] + mbl[x]; j < rp[x + 1]; j++) {
+            const uint32_t s = col[j];
+            b += 4;
+            if (s == INV) {
+                col[j] = nbr;
+                b += 12;  // slot, high-water mark, hole count
+                extend_row(x, (uint32_t)(j - rp[x]));
+                return 0;
+            }
+            if (s == nbr) return 1;
+        }
+        uint32_t pos = ovf_count++;
+        if (pos < OVF_CAP) { ovf[pos].local_vertex_idx = x; ovf[pos].neighbor_global = nbr; b += 8; }
+        else ovf_lost++;
+        asym = true;
+        return 2;
+    }
+    bool remove_slot_conc(uint32_t x, uint32_t nbr, uint64_t& b) {
+        b += 8;  // run length, high-water mark
+        const uint64_t p = run_find(x, nbr, b);
+        if (p != ~0ull && col[p] == nbr) {
+            col[p] = nbr | TOMB;
+            b += 8;
+            mholes[x]++;
+            mdirty[x] = 1;
+            return true;
+        }
+        for (uint64_t j = rp[x] + mbl[x]; j < re(x); j++) {
+            b += 4;
+            if (col[j] == nbr) {
+                col[j] = INV;
+                b += 8;
+                mholes[x]++;
+                mdirty[x] = 1;
+                return true;
+            }
+        }
+        return false;
+    }
+    // Lazy compaction of the rows edited since their last compaction: a row
+    // whose holes fill more than a quarter of its mark (every row with
+    // `force`) keeps its live run entries in front and in order, then its live
+    // tail; the rest stay candidates while they hold holes.
+    void compact_conc(bool force) {
+        uint64_t b = 0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : b)
+        for (int64_t xi = 0; xi < (int64_t)n; xi++) {
+            const uint32_t x = (uint32_t)xi;
+            if (!mdirty[x]) continue;
+            b += 8;
+            if (!force && 4ull * mholes[x] <= mhw[x]) {
+                if (!mholes[x]) mdirty[x] = 0;
+                continue;
+            }
+            const uint64_t s = rp[x], e = s + mhw[x], run_end = s + mbl[x];
+            uint64_t w = s, run_live = 0;
+            for (uint64_t j = s; j < e; j++) {
+                const uint32_t v = col[j];
+                b += 4;
+                if (hole(v)) continue;
+                if (j < run_end) run_live++;
+                if (w != j) { col[w] = v; b += 4; }
+                w++;
+            }
+            for (uint64_t j = w; j < e; j++) { col[j] = INV; b += 4; }
+            mhw[x] = (uint32_t)(w - s);
+            mbl[x] = (uint32_t)run_live;
+            mholes[x] = 0;
+            mdirty[x] = 0;
+            b += 12;
+        }
+        bytes.epoch += b;
+    }
+
     // -------- slack CSR row edits (local_update.cu:12-56) --------
     // Returns 0 inserted, 1 already present, 2 overflowed.
     int add_slot(uint32_t x, uint32_t nbr, uint64_t& b) {
+        if (conc) return add_slot_conc(x, nbr, b);
         uint64_t from = rp[x];
         if (!edited[x]) {
             if (pristine_find(x, nbr, b) != ~0ull) return 1;
@@ -223,6 +351,7 @@ struct Oracle {
     }
     // Returns whether an entry was removed.
     bool remove_slot(uint32_t x, uint32_t nbr, uint64_t& b) {
+        if (conc) return remove_slot_conc(x, nbr, b);
         if (!edited[x]) {
             const uint64_t p = pristine_find(x, nbr, b);
             if (p != ~0ull) { col[p] = INV; b += 4; edited[x] = 1; return true; }
@@ -246,7 +375,7 @@ struct Oracle {
         b += 4;
         recolors++;
         // update_incremental_state: every live row entry, duplicates included.
-        for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+        for (uint64_t j = rp[x]; j < re(x); j++) {
             uint32_t ng = col[j];
             b += 4;
             if (ng == INV || ng >= n) continue;
@@ -258,6 +387,19 @@ struct Oracle {
         b += 4;
         if (cur == 0) return;
         if (freed >= cur) return;
+        if (conc && hdmap[x] != EMPTY) {  // early-exit scan for a neighbor still holding `freed`
+            b += 4;
+            if (freed == 0) return;
+            for (uint64_t j = rp[x]; j < re(x); j++) {
+                const uint32_t ng = col[j];
+                b += 4;
+                if (ng >= n) continue;
+                b += 4;
+                if (color(ng) == freed) return;
+            }
+            recolor(x, b, freed);
+            return;
+        }
         uint16_t best = fac(x, st, b);
         if (best < cur) recolor(x, b, best);
     }
@@ -312,6 +454,7 @@ struct Oracle {
         bytes.epoch += (uint64_t)n * 6;
     }
     void compact_all() {
+        if (conc) { compact_conc(false); return; }
         uint64_t b = 0;
 #pragma omp parallel for schedule(dynamic, 1024) reduction(+ : b)
         for (int64_t xi = 0; xi < (int64_t)n; xi++) {
@@ -334,6 +477,15 @@ struct Oracle {
         for (uint32_t i = 0; i < cnt; i++) {
             uint32_t x = ovf[i].local_vertex_idx, nb = ovf[i].neighbor_global;
             bool done = false;
+            if (conc) {  // run revival, else the first free tail slot (the library's drain insert)
+                uint64_t b = 0;
+                const uint32_t keep = ovf_count;
+                done = add_slot_conc(x, nb, b) != 2;
+                if (!done) ovf_count = keep;  // a failed drain does not overflow again
+                bytes.epoch += b;
+                if (!done) { failed++; asym = true; }
+                continue;
+            }
             for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
                 bytes.epoch += 4;
                 uint32_t s = col[j];
@@ -347,7 +499,7 @@ struct Oracle {
     }
     uint64_t rebuild_one(uint32_t x, const std::vector<uint32_t>& cols, uint64_t& b) {
         uint64_t m = 0;
-        for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+        for (uint64_t j = rp[x]; j < re(x); j++) {
             uint32_t ng = col[j];
             b += 4;
             if (ng == INV || ng >= n) continue;
@@ -385,7 +537,8 @@ struct Oracle {
     }
     // drain_and_compact (streamgc.cu:1243-1314).
     uint64_t drain_and_compact() {
-        compact_all();
+        if (conc) compact_conc(true);
+        else compact_all();
         uint64_t f = drain_pending();
         rebuild_all(bytes.epoch);
         return f;
@@ -469,10 +622,10 @@ struct Oracle {
             uint32_t x = (uint32_t)xi;
             uint16_t my = (uint16_t)(old[x] & 0xFFFFu);
             bool has = false, conf = false;
-            for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+            for (uint64_t j = rp[x]; j < re(x); j++) {
                 uint32_t ng = col[j];
                 b += 4;
-                if (ng == INV) continue;
+                if (hole(ng)) continue;
                 has = true;
                 if (my == 0 || ng >= n) continue;
                 b += 4;
@@ -490,7 +643,7 @@ struct Oracle {
             uint32_t x = (uint32_t)xi;
             if (!need[x]) continue;
             bool blocked = false;
-            for (uint64_t j = rp[x]; j < rp[x + 1] && !blocked; j++) {
+            for (uint64_t j = rp[x]; j < re(x) && !blocked; j++) {
                 uint32_t y = col[j];
                 b += 4;
                 if (y == INV || y >= n || y == x) continue;
@@ -550,7 +703,7 @@ struct Oracle {
 #pragma omp parallel for schedule(dynamic, 1024) reduction(+ : sum)
         for (int64_t xi = 0; xi < (int64_t)n; xi++) {
             const uint32_t x = (uint32_t)xi;
-            for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+            for (uint64_t j = rp[x]; j < re(x); j++) {
                 const uint32_t y = col[j];
                 if (y >= n || y == x) continue;
                 sum += pair_hash(x, y) - pair_hash(y, x);
@@ -562,9 +715,9 @@ struct Oracle {
     // entry is uncolored.
     bool is_proper() const {
         for (uint32_t x = 0; x < n; x++)
-            for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+            for (uint64_t j = rp[x]; j < re(x); j++) {
                 const uint32_t y = col[j];
-                if (y == INV) continue;
+                if (hole(y)) continue;
                 if (color(x) == 0) return false;
                 if (y < n && y != x && color(y) == color(x)) return false;
             }
@@ -591,9 +744,9 @@ struct Oracle {
                 const uint16_t my = (uint16_t)(old[x] & 0xFFFFu);
                 uint64_t bits = 0;
                 bool has = false, conf = false;
-                for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                for (uint64_t j = rp[x]; j < re(x); j++) {
                     const uint32_t ng = col[j];
-                    if (ng == INV) continue;
+                    if (hole(ng)) continue;
                     has = true;
                     if (ng >= n) continue;
                     const uint16_t c = (uint16_t)(old[ng] & 0xFFFFu);
@@ -616,7 +769,7 @@ struct Oracle {
             uint64_t b = 0;
             for (uint32_t x : need) {
                 bool blocked = false;
-                for (uint64_t j = rp[x]; j < rp[x + 1] && !blocked; j++) {
+                for (uint64_t j = rp[x]; j < re(x) && !blocked; j++) {
                     const uint32_t y = col[j];
                     if (y >= n || y == x) continue;
                     if (needf[y] && sel_rank(x, salt) < sel_rank(y, salt)) blocked = true;
@@ -631,7 +784,7 @@ struct Oracle {
                 needf[x] = 0;
                 const uint16_t c = color(x);
                 if (c == 0 || c > 64) continue;
-                for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                for (uint64_t j = rp[x]; j < re(x); j++) {
                     const uint32_t y = col[j];
                     if (y < n) bm[y] |= 1ull << (c - 1);
                 }
@@ -696,13 +849,13 @@ struct Oracle {
         {
             std::vector<uint32_t> d(n, 0);
             for (uint32_t x = 0; x < n; x++)
-                for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                for (uint64_t j = rp[x]; j < re(x); j++) {
                     uint32_t y = col[j];
                     if (y != INV && y < n && y != x) { d[x]++; d[y]++; }
                 }
             for (uint32_t x = 0; x < n; x++) if (d[x]) adj[x].reserve(d[x]);
             for (uint32_t x = 0; x < n; x++)
-                for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
+                for (uint64_t j = rp[x]; j < re(x); j++) {
                     uint32_t y = col[j];
                     bytes.tier2 += 4;
                     if (y == INV || y >= n || y == x) continue;
@@ -775,6 +928,7 @@ void* og_create(uint32_t n, const uint64_t* row_ptr, const uint32_t* col_idx, co
                 uint32_t hist_thr, uint32_t slack_pct, uint32_t max_hist_colors, uint32_t flags) {
     Oracle* g = new Oracle();
     g->exact = (flags & 1u) != 0;
+    g->conc = g->exact && (flags & 2u) != 0;
     g->n = n;
     g->hist_thr = hist_thr;
     g->maxc = max_hist_colors ? max_hist_colors : SGC_MAX_HISTOGRAM_COLORS_DEFAULT;
@@ -807,7 +961,32 @@ void* og_create(uint32_t n, const uint64_t* row_ptr, const uint32_t* col_idx, co
     g->snap.assign(n, 0);
     g->ovf.resize(OVF_CAP);
     g->touched.assign(n, 0);
+    if (g->conc) {  // marks at the base counts; sorted base rows are runs
+        g->mhw.resize(n);
+        g->mbl.resize(n);
+        g->mholes.assign(n, 0);
+        g->mdirty.assign(n, 0);
+        for (uint32_t x = 0; x < n; x++) {
+            g->mhw[x] = g->base_len[x];
+            g->mbl[x] = g->edited[x] ? 0u : g->base_len[x];
+        }
+    }
     return g;
+}
+
+// Concurrent rules: per-row high-water marks, base-run lengths and hole
+// counts taken from elsewhere (the library's state after load_state); rows
+// with holes are compaction candidates.
+void og_load_rows_model(void* h, const uint32_t* hw, const uint32_t* blen, const uint32_t* holes) {
+    Oracle* g = (Oracle*)h;
+    if (!g->conc) return;
+    for (uint32_t x = 0; x < g->n; x++) {
+        const uint32_t cap = (uint32_t)(g->rp[x + 1] - g->rp[x]);
+        g->mhw[x] = hw[x] < cap ? hw[x] : cap;
+        g->mbl[x] = blen[x] < g->mhw[x] ? blen[x] : g->mhw[x];
+        g->mholes[x] = holes[x];
+        g->mdirty[x] = holes[x] ? 1 : 0;
+    }
 }
 
 void og_destroy(void* h) { delete (Oracle*)h; }
@@ -942,6 +1121,30 @@ void og_load_state(void* h, const uint32_t* col, const uint32_t* states, const u
     g->asym = true;
 }
 
+// The same for a state too large to hold twice in host memory: the caller
+// first writes the slots straight into the oracle's slab (og_col_data, same
+// row layout), then this marks as edited every row whose slots differ from
+// its base row (row_ptr/col_idx, INV after it) and copies the rest.
+uint32_t* og_col_data(void* h) { return ((Oracle*)h)->col.data(); }
+void og_load_state_inplace(void* h, const uint64_t* row_ptr, const uint32_t* col_idx, const uint32_t* states,
+                           const uint64_t* bitmaps, const uint32_t* hist) {
+    Oracle* g = (Oracle*)h;
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t xi = 0; xi < (int64_t)g->n; xi++) {
+        const uint32_t x = (uint32_t)xi;
+        const uint64_t cnt = row_ptr[x + 1] - row_ptr[x], cap = g->rp[x + 1] - g->rp[x];
+        const uint32_t* row = &g->col[g->rp[x]];
+        bool same = std::memcmp(row, col_idx + row_ptr[x], cnt * 4) == 0;
+        for (uint64_t j = cnt; same && j < cap; j++) same = row[j] == INV;
+        if (!same) g->edited[x] = 1;
+    }
+    std::memcpy(g->st.data(), states, g->n * 4ull);
+    std::memcpy(g->bm.data(), bitmaps, g->n * 8ull);
+    if (hist) std::memcpy(g->hist.data(), hist, g->hist.size() * 4ull);
+    g->clean = false;
+    g->asym = true;
+}
+
 // ---------------- state access ----------------
 void og_get_states(void* h, uint32_t* out) { Oracle* g = (Oracle*)h; std::memcpy(out, g->st.data(), g->n * 4ull); }
 void og_set_states(void* h, const uint32_t* in) {
@@ -1001,7 +1204,7 @@ void og_validate(void* h, uint64_t* out) {
     for (uint32_t x = 0; x < g->n; x++)
         for (uint64_t j = g->rp[x]; j < g->rp[x + 1]; j++) {
             uint32_t y = g->col[j];
-            if (y == INV) continue;
+            if (g->hole(y)) continue;
             if (y >= g->n) { oor++; continue; }
             eff[x]++;
             uint32_t lo = std::min(x, y), hi = std::max(x, y);
@@ -1037,6 +1240,38 @@ void og_validate_colors(uint32_t n, const uint64_t* rp, const uint32_t* col, con
         mx = std::max(mx, colors[x]);
     }
     out[0] = viol; out[1] = unc; out[2] = mx;
+}
+
+// First-fit coloring of the live rows in id order (the static greedy of
+// streamgc.cu:559-592 applied to the current rows), each color with version 1,
+// then the bitmaps of the bitmap-mode rows rebuilt. The result is proper on
+// mirror-complete rows, so the next repair may start from touched vertices.
+// Returns the largest color.
+uint16_t og_color_greedy(void* h) {
+    Oracle* g = (Oracle*)h;
+    const uint32_t n = g->n;
+    std::vector<uint32_t> used(4096, 0);
+    uint32_t stamp = 0;
+    uint16_t mx = 0;
+    for (uint32_t v = 0; v < n; v++) {
+        stamp++;
+        for (uint64_t j = g->rp[v]; j < g->re(v); j++) {
+            const uint32_t y = g->col[j];
+            if (y >= n) continue;
+            const uint16_t c = g->color(y);
+            if (c && c < used.size()) used[c] = stamp;
+        }
+        uint16_t k = 1;
+        while (k < used.size() && used[k] == stamp) k++;
+        g->st[v] = sgc_pack_state(k, 1);
+        if (k > mx) mx = k;
+    }
+    uint64_t b = 0;
+    g->rebuild_all(b);
+    std::fill(g->touched.begin(), g->touched.end(), (uint8_t)0);
+    g->clean = true;
+    g->asym = false;
+    return mx;
 }
 
 // ---------------- static greedy (streamgc.cu:559-592) ----------------

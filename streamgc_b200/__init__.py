@@ -31,7 +31,8 @@ ADD, DEL = 0, 1
 EDGE_UPDATE = np.dtype([("u", "<u4"), ("v", "<u4"), ("type", "u1"), ("_pad", "u1", (7,))], align=True)
 assert EDGE_UPDATE.itemsize == 16
 
-DL = dict(states=0, colors=1, bitmaps=2, hist=3, row_ptr=4, col=5, snapshot=6, highwater=7, hdmap=8, overflow=9)
+DL = dict(states=0, colors=1, bitmaps=2, hist=3, row_ptr=4, col=5, snapshot=6, highwater=7, hdmap=8, overflow=9,
+          base_run=10, holes=11)
 
 
 class StreamGCError(RuntimeError):
@@ -153,7 +154,8 @@ class ServerStats(C.Structure):
                 ("query_p50_ms", C.c_double), ("query_p99_ms", C.c_double), ("ticks", C.c_uint64),
                 ("tier1_sweeps", C.c_uint64), ("tier2_ticks", C.c_uint64), ("tier2_mirror_ticks", C.c_uint64),
                 ("tick_device_ms", C.c_double), ("overflows", C.c_uint64), ("drain_failed", C.c_uint64),
-                ("device_errors", C.c_uint64), ("tenants_regrown", C.c_uint64)]
+                ("device_errors", C.c_uint64), ("tenants_regrown", C.c_uint64), ("requests_tracked", C.c_uint64),
+                ("requests_dropped", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -521,6 +523,16 @@ class StreamGC:
         out = np.zeros(count, dtype=dtype)
         _check(lib().sgc_download(self.h, DL[what], out.ctypes.data, out.nbytes), f"download {what}")
         return out
+
+    def download_into(self, what, ptr, nbytes):
+        """Copies a device array (see DL) into caller memory at address `ptr`."""
+        _check(lib().sgc_download(self.h, DL[what], ptr, nbytes), f"download {what}")
+
+    def base_runs(self):
+        return self._dl("base_run", np.uint32, self.n)
+
+    def holes(self):
+        return self._dl("holes", np.uint32, self.n)
 
     def states(self):
         return self._dl("states", np.uint32, self.n)

@@ -893,8 +893,7 @@ int sgc_query_noalloc(sgc_handle* h, const uint32_t* v, uint16_t* out, uint32_t 
     uint32_t* dv = base;
     uint16_t* dout = reinterpret_cast<uint16_t*>(base + QUERY_NOALLOC_MAX);
     CK(cudaMemcpyAsync(dv, v, (size_t)k * 4, cudaMemcpyHostToDevice, h->stream));
-    launch_query(h->snap[h->front], h->n, dv, dout, k, h->stream);
-    h->launches += 1;
+    launch_query(h->snap[h->front], h->n, dv, dout, k, h->stream);  // not counted in launches, as in sgc_query
     CK(cudaMemcpyAsync(out, dout, (size_t)k * 2, cudaMemcpyDeviceToHost, h->stream));
     return sync(h);
 }
@@ -914,6 +913,18 @@ int sgc_download(sgc_handle* h, int what, void* dst, uint64_t bytes) {
         case SGC_DL_SNAPSHOT: src = h->snap[h->front]; need = h->n * 2ull; break;
         case SGC_DL_HIGHWATER: src = h->g.hw; need = h->n * 4ull; break;
         case SGC_DL_HDMAP: src = h->g.hdmap; need = h->n * 4ull; break;
+        case SGC_DL_BASE_RUN:
+        case SGC_DL_HOLES: {
+            uint32_t* a = what == SGC_DL_BASE_RUN ? h->g.blen : h->g.holes;
+            need = h->n * 4ull;
+            if (bytes < need) return fail(SGC_EINVAL, "download target %d needs %llu bytes", what, (unsigned long long)need);
+            if (!a) {
+                std::memset(dst, 0, need);
+                return SGC_OK;
+            }
+            src = a;
+            break;
+        }
         case SGC_DL_COLORS: {
             CK(cudaMallocAsync(&tmp, h->n * 2ull, h->stream));
             launch_colors(h->g, tmp, h->stream);

@@ -67,6 +67,11 @@ struct Tenant {
     bool regrow_wanted = false;      // its rows dropped an entry (options.regrow): re-admit at the next step
     bool regrowing = false;          // its rows are being rebuilt: requests wait, queries read its old group
     bool requeued = false;           // ... and it waits in the queue (its old group counts it until it is resident again)
+    // options.regrow: edges whose last forwarded update since the tenant's
+    // last admission was an insert, as (min << 32 | max). An insert whose two
+    // directions were both dropped on full rows is in no row; re-admission
+    // merges these edges back into the rows it reads.
+    std::unordered_set<uint64_t> inserted;
 };
 
 struct Group {
@@ -120,7 +125,14 @@ struct sgc_server {
     // 2 dropped with its tenant); older ids are visible unless in `dropped`.
     std::deque<uint8_t> req_state;
     uint64_t req_base = 1;
+    // Ids of the most recent kMaxDropped requests dropped with their tenants
+    // (in the order they were dropped); an id at or below `forgotten` that is
+    // not among them may have been dropped earlier and is reported unknown.
+    static constexpr size_t kMaxDropped = size_t(1) << 20;
     std::unordered_set<uint64_t> dropped;
+    std::deque<uint64_t> dropped_order;
+    uint64_t forgotten = 0;
+    uint64_t dropped_total = 0;
     LatencyWindow vis_ms, query_ms;
     uint64_t update_requests = 0, updates_applied = 0, queries = 0, query_vertices = 0;
     uint64_t ticks = 0, tier1_sweeps = 0, tier2_ticks = 0, tier2_mirror_ticks = 0, regrown = 0;
@@ -133,6 +145,36 @@ void trim_requests(sgc_server* s) {
         s->req_state.pop_front();
         s->req_base++;
     }
+}
+
+// A tenant leaves for good (under mu): its held and forwarded requests will
+// never be visible. They are resolved as dropped, so the state window can
+// move past them, and the tenant's host buffers are released.
+void end_tenant(sgc_server* s, Tenant& t) {
+    t.state = SGC_TENANT_REMOVED;
+    t.regrowing = t.requeued = false;
+    for (const auto* reqs : {&t.held_reqs, &t.waiting})
+        for (const Request& q : *reqs) {
+            s->req_state[q.id - s->req_base] = 2;
+            if (s->dropped.insert(q.id).second) {
+                s->dropped_order.push_back(q.id);
+                s->dropped_total++;
+            }
+        }
+    while (s->dropped_order.size() > sgc_server::kMaxDropped) {
+        const uint64_t id = s->dropped_order.front();
+        s->dropped_order.pop_front();
+        s->dropped.erase(id);
+        if (id > s->forgotten) s->forgotten = id;
+    }
+    trim_requests(s);
+    std::vector<uint64_t>().swap(t.rp);
+    std::vector<uint32_t>().swap(t.col);
+    std::vector<uint32_t>().swap(t.deg);
+    std::vector<EdgeUpdate>().swap(t.held);
+    t.held_reqs.clear();
+    t.waiting.clear();
+    std::unordered_set<uint64_t>().swap(t.inserted);
 }
 
 namespace {
@@ -219,20 +261,7 @@ int sgc_server_remove_tenant(sgc_server* s, uint32_t tenant) {
         Group& g = s->groups[t.group];
         if (--g.alive == 0) g.retired = true;  // its memory goes back to the budget at the next step
     }
-    t.regrowing = t.requeued = false;
-    t.state = SGC_TENANT_REMOVED;
-    for (const auto* reqs : {&t.held_reqs, &t.waiting})  // never visible now
-        for (const Request& q : *reqs) {
-            s->req_state[q.id - s->req_base] = 2;
-            s->dropped.insert(q.id);
-        }
-    trim_requests(s);
-    std::vector<uint64_t>().swap(t.rp);
-    std::vector<uint32_t>().swap(t.col);
-    std::vector<uint32_t>().swap(t.deg);
-    t.held.clear();
-    t.held_reqs.clear();
-    t.waiting.clear();
+    end_tenant(s, t);
     return SGC_OK;
 }
 
@@ -313,6 +342,34 @@ int regrow_tenants(sgc_server* s) {
         int rc = sgc_batch_rows(j.b, j.local, rp.data(), nullptr, 0);
         std::vector<uint32_t> col(std::max<uint64_t>(rp[j.n], 1));
         if (rc == SGC_OK) rc = sgc_batch_rows(j.b, j.local, rp.data(), col.data(), col.size());
+        // inserts that are in no row (both directions dropped): appended to
+        // their lower endpoint's row before the mirrors are restored
+        if (rc == SGC_OK) {
+            std::vector<uint64_t> extra;
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                const Tenant& t = s->tenants[j.tid];
+                extra.assign(t.inserted.begin(), t.inserted.end());
+            }
+            if (!extra.empty()) {
+                std::sort(extra.begin(), extra.end());
+                std::vector<uint64_t> add((size_t)j.n + 1, 0);
+                for (uint64_t e : extra) add[(e >> 32) + 1]++;
+                for (uint32_t x = 0; x < j.n; x++) add[x + 1] += add[x];
+                std::vector<uint64_t> rp2((size_t)j.n + 1, 0);
+                std::vector<uint32_t> col2(std::max<uint64_t>(rp[j.n] + extra.size(), 1));
+                size_t k = 0;
+                for (uint32_t x = 0; x < j.n; x++) {
+                    uint64_t w = rp[x] + add[x];
+                    rp2[x] = w;
+                    for (uint64_t i = rp[x]; i < rp[x + 1]; i++) col2[w++] = col[i];
+                    for (; k < extra.size() && (extra[k] >> 32) == x; k++) col2[w++] = (uint32_t)extra[k];
+                }
+                rp2[j.n] = rp[j.n] + extra.size();
+                rp.swap(rp2);
+                col.swap(col2);
+            }
+        }
         // undirected edges from either direction, then both directions, rows ascending
         std::vector<uint64_t> nrp;
         std::vector<uint32_t> ncol, ndeg;
@@ -418,8 +475,7 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
                         Group& og = s->groups[t.group];
                         if (--og.alive == 0) og.retired = true;
                     }
-                    t.regrowing = t.requeued = false;
-                    t.state = SGC_TENANT_REMOVED;
+                    end_tenant(s, t);
                     continue;
                 }
                 s->queue.push_front(*it);
@@ -445,10 +501,9 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
             std::vector<uint64_t>().swap(t.rp);  // the CSR lives on the device now
             std::vector<uint32_t>().swap(t.col);
             std::vector<uint32_t>().swap(t.deg);
+            std::unordered_set<uint64_t>().swap(t.inserted);  // the rows just admitted hold them
             if (t.remove_pending) {
-                t.state = SGC_TENANT_REMOVED;
-                t.held.clear();
-                t.held_reqs.clear();
+                end_tenant(s, t);
             } else {
                 t.state = SGC_TENANT_RESIDENT;
                 g.alive++;
@@ -488,6 +543,13 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
                     }
                     room[t.group] -= take;
                     s->updates_applied += take;
+                    if (s->opt.regrow)
+                        for (const EdgeUpdate& e : f.ups) {
+                            if (e.u == e.v || e.u >= t.n || e.v >= t.n) continue;  // skipped on the device too
+                            const uint64_t key = e.u < e.v ? ((uint64_t)e.u << 32) | e.v : ((uint64_t)e.v << 32) | e.u;
+                            if (e.type == SGC_UPDATE_ADD) t.inserted.insert(key);
+                            else t.inserted.erase(key);
+                        }
                     for (size_t i = 0; i < k; i++) t.waiting.push_back(t.held_reqs[i]);
                     t.held_reqs.erase(t.held_reqs.begin(), t.held_reqs.begin() + (ptrdiff_t)k);
                     g.has_work = true;
@@ -583,7 +645,13 @@ int sgc_server_request_visible(sgc_server* s, uint64_t request) {
     if (!s) return SGC_EINVAL;
     std::lock_guard<std::mutex> lk(s->mu);
     if (request == 0 || request >= s->next_request) return 0;
-    if (request < s->req_base) return s->dropped.count(request) ? 0 : 1;
+    if (request < s->req_base) {
+        if (s->dropped.count(request)) return 0;
+        if (request <= s->forgotten)
+            return sgci::fail(SGC_EINVAL, "request %llu is older than the dropped requests the server remembers",
+                              (unsigned long long)request);
+        return 1;
+    }
     return s->req_state[request - s->req_base] == 1 ? 1 : 0;
 }
 
@@ -650,6 +718,8 @@ int sgc_server_get_stats(sgc_server* s, sgc_server_stats* o) {
     o->tier2_mirror_ticks = s->tier2_mirror_ticks;
     o->tick_device_ms = s->tick_device_ms;
     o->tenants_regrown = s->regrown;
+    o->requests_tracked = s->req_state.size();
+    o->requests_dropped = s->dropped_total;
     return SGC_OK;
 }
 

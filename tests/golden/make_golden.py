@@ -7,11 +7,16 @@ kernels on them through oracle/_ref/ref_driver (one warp, stream order), and
 records a SHA-256 of every state array at every epoch boundary and after each
 drain_and_compact into tests/golden/ref_epochs.json.
 
-    python tests/golden/make_golden.py --run OUT_DIR   # on a GPU box
-    python tests/golden/make_golden.py --list          # case summary
+    python tests/golden/make_golden.py --run OUT_DIR         # on a GPU box
+    python tests/golden/make_golden.py --run-scale OUT_DIR   # the full-size case, on a GPU box
+    python tests/golden/make_golden.py --list                # case summary
 
-The JSON is committed; tests rebuild the same cases and compare the oracle's
-and the CUDA path's states against it.
+The JSONs are committed; tests rebuild the same cases and compare the oracle's
+and the CUDA path's states against them. The full-size case (SCALE_CASES) is
+the plain small workload at its real size: Delaunay of 131,072 points (seed
+42), the reference's 50/50 churn stream of 1,000,000 updates (seed 42),
+epochs of 32,768, threshold 64, alpha 4 -- 30 bench epochs and 12 init
+epochs, each pinned to the reference's kernels (tests/golden/ref_epochs_c1.json).
 """
 from __future__ import annotations
 
@@ -30,6 +35,7 @@ sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 
 GOLDEN_JSON = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_epochs.json")
+GOLDEN_SCALE_JSON = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_epochs_c1.json")
 ARRAYS = ("states", "bitmaps", "col", "snapshot", "hist", "ovf_count")
 
 
@@ -87,9 +93,14 @@ CASES = {
 }
 
 
+SCALE_CASES = {
+    "delaunay17_c1": (lambda: graph_delaunay(131072, 42), 1_000_000, 50, 64, 32768, 32768, 300),
+}
+
+
 def build_case(name):
     """Returns dict(rp, col, deg, init, bench, thr, E, batch, slack)."""
-    gb, size, pct, thr, E, batch, slack = CASES[name]
+    gb, size, pct, thr, E, batch, slack = CASES[name] if name in CASES else SCALE_CASES[name]
     rp, col, deg = gb()
     init = O.updates_from(O.init_stream(rp, col, deg))
     pairs, types = O.bench_stream(rp, col, size, pct, 42)
@@ -145,11 +156,11 @@ def epoch_tags(c):
     return tags
 
 
-def run(out_dir):
+def run(out_dir, cases=CASES, out_name="ref_epochs.json"):
     driver = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
     os.makedirs(out_dir, exist_ok=True)
     result = {}
-    for name in CASES:
+    for name in cases:
         c = build_case(name)
         cin = os.path.join(out_dir, f"{name}.bin")
         cout = os.path.join(out_dir, f"{name}.dump")
@@ -159,23 +170,27 @@ def run(out_dir):
         recs = parse_dump(cout)
         entry = {"input_sha256": hashlib.sha256(case_bytes(c)).hexdigest(), "epochs": {}}
         for tag, arrays in recs:
-            if tag == "timing":
+            if tag in ("timing", "final"):
                 continue
             entry["epochs"][tag] = {k: hashlib.sha256(v).hexdigest() for k, v in arrays.items()}
             entry["epochs"][tag]["ovf_count_value"] = struct.unpack("<I", arrays["ovf_count"])[0]
         result[name] = entry
-    with open(os.path.join(out_dir, "ref_epochs.json"), "w") as f:
+        os.remove(cout)  # the full-size dump is about 0.8 GB
+    with open(os.path.join(out_dir, out_name), "w") as f:
         json.dump(result, f, indent=1, sort_keys=True)
-    print("wrote", os.path.join(out_dir, "ref_epochs.json"))
+    print("wrote", os.path.join(out_dir, out_name))
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--run", metavar="OUT_DIR")
+    ap.add_argument("--run-scale", metavar="OUT_DIR")
     ap.add_argument("--list", action="store_true")
     a = ap.parse_args()
     if a.run:
         run(a.run)
+    elif a.run_scale:
+        run(a.run_scale, SCALE_CASES, "ref_epochs_c1.json")
     else:
         for name in CASES:
             c = build_case(name)

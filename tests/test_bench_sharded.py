@@ -205,7 +205,8 @@ def _rank(rank, world, port, form, q):
     args = types.SimpleNamespace(gpus=world, steps=2, warmup=3, batch_graphs=6, autotune=False, served_rate=2e5,
                                  served_seconds=0.3, served_staleness_us=2000, served_check=False,
                                  served_regrow=False, sorted_rows=False, workload="small", cpu_batches=0,
-                                 cpu_seconds=1.0, profile_window=False, graph_publish=False, ingest=False)
+                                 cpu_seconds=1.0, profile_window=False, graph_publish=False, ingest=False,
+                                 latency_epochs=4, validate_steps=True)
     out, err = io.StringIO(), None
     old = sys.stdout
     sys.stdout = out
@@ -242,6 +243,8 @@ def test_two_ranks_share_the_work(form):
     if form == "plain":  # replicas: twice one replica's epochs over the slowest replica's time
         assert line["config"]["parallelism"] == "replicas x2"
         assert line["value"] == pytest.approx(2 * 2 * 32768 / (line["ms_per_step"] * 2 / 1e3))
+        assert line["config"]["snapshots_validated"] == 2 and line["config"]["snapshot_violations"] == 0
+        assert line["latency_ms"]["samples"] == 4
         return
     assert line["form"] == form
     assert line["config"]["placement"].startswith("2 ranks")

@@ -147,6 +147,45 @@ def test_stream_gc_program(tmp_path):
     assert np.array_equal(colors, o.colors())
 
 
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "streaming_gc")),
+                    reason="the reference program was not built (no reference tree at build time)")
+def test_outputs_match_the_reference_program(tmp_path):
+    """The reference's own program (built from its sources for sm_100a) and
+    stream_gc on the same graph and flags: the same output file names, the
+    same .coloring.meta keys in the same order with the same non-timing
+    values, and the same .coloring.txt header and line format."""
+    import json
+    g = S.Graph.delaunay(3000, seed=3)
+    mtx = str(tmp_path / "del3k.mtx")
+    g.write_mtx(mtx)
+    flags = ["--graph", mtx, "--stream", "20000", "--insert-pct", "50", "--epoch-size", "4096", "--seed", "42",
+             "--hw-tag", "B200_test"]
+    outs = {}
+    for name, exe in (("ref", os.path.join(ROOT, "oracle", "_ref", "streaming_gc")),
+                      ("ours", os.path.join(ROOT, "streamgc_b200", "lib", "stream_gc"))):
+        d = tmp_path / name
+        d.mkdir()
+        r = subprocess.run([exe] + flags + ["--output-dir", str(d), "--log-dir", str(d)], capture_output=True,
+                           text=True, timeout=300)
+        assert r.returncode == 0, name + ": " + r.stdout[-2000:] + r.stderr[-2000:]
+        outs[name] = d
+    files = {name: sorted(p.name for p in d.iterdir() if ".coloring" in p.name) for name, d in outs.items()}
+    assert files["ours"] == files["ref"] == ["streamgc_1gpu_stream20000_50pct.coloring",
+                                             "streamgc_1gpu_stream20000_50pct.coloring.meta",
+                                             "streamgc_1gpu_stream20000_50pct.coloring.txt"]
+    metas = {name: json.loads((d / files[name][1]).read_text()) for name, d in outs.items()}
+    assert list(metas["ours"]) == list(metas["ref"])
+    for k in ("algorithm", "graph", "num_vertices", "num_edges", "static_greedy_colors", "partition_info",
+              "stream_size", "insert_pct", "seed", "num_gpus", "hw_tag", "query_count"):
+        assert metas["ours"][k] == metas["ref"][k], k
+    for name, d in outs.items():
+        colors = np.fromfile(str(d / files[name][0]), dtype="<u2")
+        assert len(colors) == 3000 and metas[name]["num_colors_used"] == int(colors.max())
+        lines = (d / files[name][2]).read_text().splitlines()
+        assert lines[:3] == [f"# vertices: 3000", f"# colors: {int(colors.max())}", "# algorithm: streamgc"]
+        assert lines[3:] == [f"{i} {c}" for i, c in enumerate(colors.tolist())]
+
+
 @pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "test_single_gpu_dropin")),
                     reason="drop-in link check binary not built (no reference tree at build time)")
 def test_reference_integration_test_runs_on_dropin_kernels():

@@ -41,6 +41,21 @@ def test_deterministic_mode_matches_reference_kernels(name):
     assert n == len(gold["epochs"])
 
 
+@pytest.mark.skipif(not os.path.exists(MG.GOLDEN_SCALE_JSON), reason="full-size epoch fixtures not generated yet")
+@pytest.mark.parametrize("name", list(MG.SCALE_CASES))
+def test_deterministic_mode_matches_reference_kernels_full_size(name):
+    """Delaunay 2^17 with the 1 M-update churn stream, E = 32,768: every state
+    array equals the reference's kernels' at all 43 epoch boundaries."""
+    gold = json.load(open(MG.GOLDEN_SCALE_JSON))[name]
+    c = MG.build_case(name)
+    n = 0
+    for tag, arrays in _util.gpu_epochs(c, S.MODE_DETERMINISTIC):
+        for k in _util.ARRAY_NAMES:
+            assert _util.sha(arrays[k]) == gold["epochs"][tag][k], f"{name} {tag} {k}"
+        n += 1
+    assert n == len(gold["epochs"]) == 43
+
+
 def _both(name):
     c = MG.build_case(name)
     g = O.Oracle(c["rp"], c["col"], c["deg"], hist_threshold=c["thr"], slack_pct=c["slack"])

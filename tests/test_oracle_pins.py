@@ -76,3 +76,20 @@ def test_oracle_matches_reference_epochs(name):
             assert _util.sha(arrays[k]) == g[k], f"{name} {tag} {k}"
         seen += 1
     assert seen == len(gold["epochs"])
+
+
+@pytest.mark.skipif(not os.path.exists(MG.GOLDEN_SCALE_JSON), reason="full-size epoch fixtures not generated yet")
+@pytest.mark.parametrize("name", list(MG.SCALE_CASES))
+def test_oracle_matches_reference_epochs_full_size(name):
+    """The plain small workload at full size (Delaunay 2^17, 1 M churn, 43
+    epoch boundaries): the oracle equals the reference's kernels at every one."""
+    gold = json.load(open(MG.GOLDEN_SCALE_JSON))[name]
+    c = MG.build_case(name)
+    assert _util.sha(np.frombuffer(MG.case_bytes(c), dtype=np.uint8)) == gold["input_sha256"], "case input drifted"
+    seen = 0
+    for tag, arrays in _util.oracle_epochs(c):
+        g = gold["epochs"][tag]
+        for k in _util.ARRAY_NAMES:
+            assert _util.sha(arrays[k]) == g[k], f"{name} {tag} {k}"
+        seen += 1
+    assert seen == len(gold["epochs"]) == 43

@@ -69,3 +69,27 @@ def test_requests_of_a_removed_tenant_are_never_visible():
         assert not srv.visible(0) and not srv.visible(ids[-1] + 1)
     finally:
         srv.close()
+
+
+def test_removed_tenant_requests_leave_the_state_window():
+    """Requests of a removed tenant are resolved as dropped on every removal
+    path, so the window of request states moves past them; the count of
+    dropped requests is kept."""
+    c = MG.build_case("delaunay2k")
+    g = S.Graph(c["rp"], c["col"], c["deg"])
+    srv = S.Server(hbm_budget_bytes=1 << 30, max_tick_updates=1 << 12)
+    try:
+        t0 = srv.add_tenant(g, epoch_size=1024)
+        t1 = srv.add_tenant(g, epoch_size=1024)
+        a = [srv.submit(t0, c["bench"][k:k + 4]) for k in range(0, 40, 4)]
+        b = [srv.submit(t1, c["bench"][k:k + 4]) for k in range(0, 40, 4)]
+        assert srv.stats()["requests_tracked"] == 20
+        srv.remove_tenant(t1)  # its requests sit behind t0's unresolved ones
+        st = srv.stats()
+        assert st["requests_tracked"] == 20 and st["requests_dropped"] == 10
+        srv.remove_tenant(t0)
+        st = srv.stats()
+        assert st["requests_tracked"] == 0 and st["requests_dropped"] == 20
+        assert not any(srv.visible(i) for i in a + b)
+    finally:
+        srv.close()
