@@ -48,6 +48,7 @@ sys.path.insert(0, ROOT)
 METRIC = "updates/sec on 1 B200 (plain vs batched/served); p50/p99 update-to-visible ms"
 E = 32768
 HIST_THR = 64
+CORE_MIN_DEGREE = 256  # a graph loaded without its init stream: vertices colored one by one before the repair
 
 
 def log(*a):
@@ -62,7 +63,7 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def build_workload(kind, stream_len):
+def build_workload(kind, stream_len, large_div=1):
     import streamgc_b200 as S
     t = time.time()
     if kind == "skewed":
@@ -72,11 +73,12 @@ def build_workload(kind, stream_len):
                     vertices=g.n, undirected_edges=g.nnz // 2, stream=f"k-core dense, {stream_len} updates, 2 inserts per delete, seed 42",
                     core_k=k, core_vertices=csize)
     elif kind == "large":
-        g = S.Graph.chung_lu(65_608_366, 2.1, 55.0, 100_000.0, 42)
+        nv = 65_608_366 // large_div  # large_div > 1: the same family scaled down (profiling captures)
+        g = S.Graph.chung_lu(nv, 2.1, 55.0, 100_000.0, 42)
         bench = g.churn_stream(stream_len, 50, 42)
-        desc = dict(workload="chunglu65m_churn", graph="Chung-Lu, 65,608,366 vertices, exponent 2.1, avg degree 55, "
-                    "cap 100,000, seed 42", vertices=g.n, undirected_edges=g.nnz // 2,
-                    stream=f"churn 50% insert, {stream_len} updates, seed 42")
+        desc = dict(workload="chunglu65m_churn" if large_div == 1 else f"chunglu65m_div{large_div}_churn",
+                    graph=f"Chung-Lu, {nv:,} vertices, exponent 2.1, avg degree 55, cap 100,000, seed 42",
+                    vertices=g.n, undirected_edges=g.nnz // 2, stream=f"churn 50% insert, {stream_len} updates, seed 42")
     else:
         g = S.Graph.delaunay(131072, seed=42)
         bench = g.churn_stream(stream_len, 50, 42)
@@ -86,7 +88,8 @@ def build_workload(kind, stream_len):
     # init stream (every edge, sorted by endpoint degrees) is 1.8 G updates
     init = None if kind == "large" else g.init_stream()
     desc.update(epoch_size=E, histogram_threshold=HIST_THR, alpha=4,
-                init="full repair of the loaded rows" if init is None else "init stream (every edge as an ADD)")
+                init=(f"core of degree >= {CORE_MIN_DEGREE} colored one by one in descending degree order, then one "
+                      "full repair of the loaded rows") if init is None else "init stream (every edge as an ADD)")
     log(f"workload {desc['workload']}: n={g.n} m={g.nnz // 2} init={0 if init is None else len(init)} "
         f"stream={len(bench)} ({time.time() - t:.1f}s)")
     return g, init, bench, desc
@@ -222,7 +225,7 @@ def run_ours(a):
     nbatch = a.warmup + 2 * a.steps + a.cpu_batches + a.latency_epochs
     base_len = {"skewed": 2_000_000, "small": 1_000_000, "large": 10_000_000}[a.workload]
     stream_len = max(base_len, nbatch * E)
-    g, init, bench, desc = build_workload(a.workload, stream_len)
+    g, init, bench, desc = build_workload(a.workload, stream_len, a.large_div)
 
     t = time.time()
     h = S.StreamGC(g, epoch_size=E, histogram_threshold=HIST_THR, slack_pct=300, max_batch=1 << 20,
@@ -230,9 +233,13 @@ def run_ours(a):
                    sorted_rows=a.sorted_rows)
     for s in range(0, 0 if init is None else len(init), 1 << 20):
         h.apply(init[s:s + (1 << 20)], S.MODE_CONCURRENT)
+    t1 = time.time()
+    core = h.color_core(CORE_MIN_DEGREE) if init is None else 0  # no init stream: the dense core first
+    t2 = time.time()
     rep = h.publish()
     h.synchronize()
-    log(f"init colored on GPU in {time.time() - t:.1f}s: {rep}")
+    log(f"init colored on GPU in {time.time() - t:.1f}s (handle {t1 - t:.1f}s, core of {core} vertices "
+        f"{t2 - t1:.1f}s, full repair {time.time() - t2:.1f}s): {rep}")
     if not rep["proper"]:
         raise SystemExit("init coloring not proper")
 
@@ -498,7 +505,7 @@ def run_reference(a):
     from oracle import oracle as O
     stream_len = max({"skewed": 2_000_000, "small": 1_000_000, "large": 10_000_000}[a.workload],
                      (a.warmup + a.steps) * E)
-    g, init, bench, desc = build_workload(a.workload, stream_len)
+    g, init, bench, desc = build_workload(a.workload, stream_len, a.large_div)
     t = time.time()
     o = O.Oracle(g.row_ptr, g.col_idx, g.degree, hist_threshold=HIST_THR, exact=True, conc=True)
     if init is None:
@@ -543,8 +550,9 @@ def run_batched(a):
     first ticks' worth generated). A tick submits one epoch of every graph. The
     same graphs and updates run twice: per-graph plain launches (one handle per
     graph: apply + publish per epoch) and the batched engine (one tick = one
-    CUDA-graph launch). Both arms start from a full repair of the loaded rows
-    and are wall-clock timed from host memory."""
+    CUDA-graph launch). Both arms start from the same coloring of the loaded
+    rows (each graph's core of degree >= CORE_MIN_DEGREE one vertex at a time,
+    then a full repair) and are wall-clock timed from host memory."""
     import torch
     import streamgc_b200 as S
     from streamgc_b200 import workloads as W
@@ -578,9 +586,11 @@ def run_batched(a):
     hs = [S.StreamGC(gr, epoch_size=epochs[k], histogram_threshold=HIST_THR, slack_pct=300,
                      max_batch=max(epochs[k], 1 << 16), device=local, exact_select=True, full_repair_every=0)
           for k, gr in enumerate(graphs)]
-    for h in hs:  # colored from its loaded rows by one full repair, as the batched arm's first tick does
+    for h in hs:  # colored from its loaded rows (core first, then a full repair), as the batched arm is
+        h.color_core(CORE_MIN_DEGREE)
         if not h.publish()["proper"]:
             raise SystemExit("plain arm init not proper")
+        h.synchronize()
     torch.cuda.synchronize()
     log(f"plain arm: {len(hs)} handles created and colored in {time.time() - t:.1f}s")
     plain_ticks, plain_updates, plain_ok = [], 0, True
@@ -616,6 +626,7 @@ def run_batched(a):
     # the rows hold every edge from creation; the first tick colors all graphs
     # from scratch and publishes them (as the served form admits tenants)
     b.close_epochs()
+    b.color_core(CORE_MIN_DEGREE)  # every graph's dense core first; the first tick repairs the rest
     if not b.tick()["proper"]:
         raise SystemExit("batched init not proper")
     log(f"batched arm: created and colored in {time.time() - t:.1f}s")
@@ -908,6 +919,8 @@ def main():
     ap.add_argument("--epoch-size", type=int, default=32768,
                     help="plain path: updates per epoch (the large workload's sweep uses 4096, 32768, 262144)")
     ap.add_argument("--cpu-batches", type=int, default=8, help="epochs timed on the CPU baseline (0: skip)")
+    ap.add_argument("--large-div", type=int, default=1,
+                    help="large workload scaled down by this factor (same family; for profiling captures)")
     ap.add_argument("--latency-epochs", type=int, default=128,
                     help="plain path: epochs timed one by one from submission to visibility after the e2e steps")
     ap.add_argument("--no-validate-steps", dest="validate_steps", action="store_false",

@@ -214,6 +214,14 @@ int sgc_query_noalloc(sgc_handle* h, const uint32_t* vertices, uint16_t* colors,
 
 int sgc_download(sgc_handle* h, int what, void* dst, uint64_t bytes);
 int sgc_upload(sgc_handle* h, int what, const void* src, uint64_t bytes);   /* STATES, BITMAPS, HIST */
+/* Colors the uncolored vertices of initial degree >= min_degree one at a time,
+ * in descending degree order (ties by id), each with the first color in
+ * 1..2047 that none of its live neighbors holds (version 1). For a large graph
+ * loaded without an init stream: its dense high-degree core then needs no
+ * long chain of independent-set sweeps; the next repair (sgc_publish) visits
+ * every vertex and colors the rest. No reference counterpart (the reference
+ * colors its graph with the init stream, streamgc.cu:1395-1408). */
+int sgc_color_core(sgc_handle* h, uint32_t min_degree, uint32_t* colored);
 /* FindAvailableColor(x) (color_select.cuh:93-115) on the current device state. */
 int sgc_find_color(sgc_handle* h, uint32_t x, uint16_t* color);
 

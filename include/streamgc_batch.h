@@ -114,6 +114,10 @@ int sgc_batch_snapshot(sgc_batch* b, uint32_t graph, uint16_t* out);  /* num_ver
 int sgc_batch_rows(sgc_batch* b, uint32_t graph, uint64_t* row_ptr, uint32_t* col, uint64_t col_cap);
 /* Validator over all graphs (the reference's, streamgc.cu:448-556). */
 int sgc_batch_validate(sgc_batch* b, sgc_validation* out);
+/* sgc_color_core over every graph of the batch (graphs are disjoint, so each
+ * one's colors are the same as alone); call before the first tick, which then
+ * repairs every graph in full. */
+int sgc_batch_color_core(sgc_batch* b, uint32_t min_degree, uint32_t* colored);
 /* out[k] = 1 when graph k has dropped an entry since its creation: an
  * insert that found its row still full at the drain, or that arrived with the
  * overflow buffer full (the reference drops such entries too; the mirror

@@ -71,6 +71,7 @@ def lib():
             "og_col_data": (C.c_void_p, [_vp]),
             "og_load_rows_model": (None, [_vp, _u32p, _u32p, _u32p]),
             "og_color_greedy": (C.c_uint16, [_vp]),
+            "og_color_core": (C.c_uint32, [_vp, C.c_uint32]),
             "og_load_state_inplace": (None, [_vp, _u64p, _u32p, _u32p, _u64p, _u32p]),
             "og_publish_repair": (None, [_vp, C.c_int, _u32p]),
             "og_set_full_repair_every": (None, [_vp, C.c_uint32]),
@@ -233,6 +234,10 @@ class Oracle:
         hole count (the library's, after load_state)."""
         a = [np.ascontiguousarray(x, dtype=np.uint32) for x in (highwater, base_runs, holes)]
         self.L.og_load_rows_model(self.h, *[_p(x, _u32p) for x in a])
+
+    def color_core(self, min_degree):
+        """The library's sgc_color_core restated; returns how many were colored."""
+        return int(self.L.og_color_core(self.h, min_degree))
 
     def color_greedy(self):
         """First-fit coloring of the live rows in id order; returns the largest color."""

@@ -1274,6 +1274,38 @@ uint16_t og_color_greedy(void* h) {
     return mx;
 }
 
+// The library's sgc_color_core: the uncolored vertices of initial degree >=
+// min_degree one at a time in descending degree order (ties by id), each with
+// the first color in 1..2047 none of its live neighbors holds (2048 when all
+// do), version 1. Returns how many were colored.
+uint32_t og_color_core(void* h, uint32_t min_degree) {
+    Oracle* g = (Oracle*)h;
+    std::vector<uint32_t> list;
+    for (uint32_t x = 0; x < g->n; x++)
+        if (g->deg[x] >= min_degree && g->deg[x] > 0) list.push_back(x);
+    std::sort(list.begin(), list.end(), [&](uint32_t a, uint32_t b) {
+        return g->deg[a] != g->deg[b] ? g->deg[a] > g->deg[b] : a < b;
+    });
+    uint32_t done = 0;
+    std::vector<uint8_t> used(2048);
+    for (uint32_t v : list) {
+        if (g->color(v) != 0) continue;
+        std::fill(used.begin(), used.end(), (uint8_t)0);
+        for (uint64_t j = g->rp[v]; j < g->re(v); j++) {
+            const uint32_t y = g->col[j];
+            if (y >= g->n) continue;
+            const uint16_t c = g->color(y);
+            if (c != 0 && c < 2048) used[c] = 1;
+        }
+        uint16_t c = 1;
+        while (c < 2048 && used[c]) c++;
+        g->st[v] = sgc_pack_state(c, 1);
+        done++;
+    }
+    g->clean = false;
+    return done;
+}
+
 // ---------------- static greedy (streamgc.cu:559-592) ----------------
 uint16_t og_static_greedy(uint32_t n, const uint64_t* rp, const uint32_t* col) {
     std::vector<uint16_t> c(n, 0);

@@ -177,6 +177,7 @@ SIGNATURES = {
     "sgc_query_noalloc": (C.c_int, [_vp, _u32p, _u16p, C.c_uint32]),
     "sgc_download": (C.c_int, [_vp, C.c_int, _vp, C.c_uint64]),
     "sgc_upload": (C.c_int, [_vp, C.c_int, _vp, C.c_uint64]),
+    "sgc_color_core": (C.c_int, [_vp, C.c_uint32, _u32p]),
     "sgc_find_color": (C.c_int, [_vp, C.c_uint32, _u16p]),
     "sgc_validate": (C.c_int, [_vp, C.POINTER(Validation)]),
     "sgc_check_state": (C.c_int, [_vp, C.POINTER(StateReport)]),
@@ -212,6 +213,7 @@ SIGNATURES = {
     "sgc_batch_query": (C.c_int, [_vp, C.c_uint32, _u32p, _u16p, C.c_uint32]),
     "sgc_batch_snapshot": (C.c_int, [_vp, C.c_uint32, _u16p]),
     "sgc_batch_rows": (C.c_int, [_vp, C.c_uint32, _u64p, _u32p, C.c_uint64]),
+    "sgc_batch_color_core": (C.c_int, [_vp, C.c_uint32, _u32p]),
     "sgc_batch_validate": (C.c_int, [_vp, C.POINTER(Validation)]),
     "sgc_batch_check_state": (C.c_int, [_vp, C.POINTER(StateReport)]),
     "sgc_batch_dropped": (C.c_int, [_vp, _u8p]),
@@ -571,6 +573,13 @@ class StreamGC:
         arr = np.ascontiguousarray(arr)
         _check(lib().sgc_upload(self.h, DL[what], arr.ctypes.data, arr.nbytes), f"upload {what}")
 
+    def color_core(self, min_degree):
+        """Colors the uncolored vertices of degree >= min_degree one at a time in
+        descending degree order (first free color); returns how many."""
+        out = np.zeros(1, dtype=np.uint32)
+        _check(lib().sgc_color_core(self.h, min_degree, _p(out, _u32p)), "color_core")
+        return int(out[0])
+
     def find_color(self, x):
         c = np.zeros(1, dtype=np.uint16)
         _check(lib().sgc_find_color(self.h, x, _p(c, _u16p)), "sgc_find_color")
@@ -682,6 +691,12 @@ class Batch:
         col = np.zeros(max(int(rp[-1]), 1), dtype=np.uint32)
         _check(lib().sgc_batch_rows(self.b, k, _p(rp, _u64p), _p(col, _u32p), len(col)), "sgc_batch_rows")
         return rp, col[: int(rp[-1])]
+
+    def color_core(self, min_degree):
+        """sgc_color_core over every graph (before the first tick); returns how many were colored."""
+        out = np.zeros(1, dtype=np.uint32)
+        _check(lib().sgc_batch_color_core(self.b, min_degree, _p(out, _u32p)), "sgc_batch_color_core")
+        return int(out[0])
 
     def validate(self):
         v = Validation()

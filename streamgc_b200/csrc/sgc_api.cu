@@ -968,6 +968,35 @@ int sgc_upload(sgc_handle* h, int what, const void* src, uint64_t bytes) {
     return sync(h);
 }
 
+int sgc_color_core(sgc_handle* h, uint32_t min_degree, uint32_t* colored) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    CK(cudaSetDevice(h->device));
+    std::vector<uint32_t> deg(h->n);
+    CK(cudaMemcpyAsync(deg.data(), h->g.deg, (size_t)h->n * 4, cudaMemcpyDeviceToHost, h->stream));
+    TRY(sync(h));
+    std::vector<uint32_t> list;
+    for (uint32_t x = 0; x < h->n; x++)
+        if (deg[x] >= min_degree && deg[x] > 0) list.push_back(x);
+    std::sort(list.begin(), list.end(), [&](uint32_t a, uint32_t b) { return deg[a] != deg[b] ? deg[a] > deg[b] : a < b; });
+    uint32_t done = 0;
+    if (!list.empty()) {
+        uint32_t* d = nullptr;
+        CK(cudaMallocAsync(&d, (list.size() + 1) * 4, h->stream));
+        CK(cudaMemcpyAsync(d, list.data(), list.size() * 4, cudaMemcpyHostToDevice, h->stream));
+        launch_color_list(h->g, d, (uint32_t)list.size(), d + list.size(), h->stream);
+        h->launches += 1;
+        CK(cudaMemcpyAsync(h->h_small, d + list.size(), 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaFreeAsync(d, h->stream));
+        for (uint32_t k = 0; k < std::max<uint32_t>(h->sb.G, 1u); k++)  // every graph's next repair is full
+            CK(cudaMemsetAsync(&h->g.gctl[k].clean, 0, 4, h->stream));
+        TRY(sync(h));
+        TRY(check_cuda("color_core"));
+        done = h->h_small[0];
+    }
+    if (colored) *colored = done;
+    return SGC_OK;
+}
+
 int sgc_find_color(sgc_handle* h, uint32_t x, uint16_t* color) {
     if (!h || !color) return fail(SGC_EINVAL, "null argument");
     if (x >= h->n) return fail(SGC_EINVAL, "vertex %u out of range", x);

@@ -617,6 +617,11 @@ int sgc_batch_rows(sgc_batch* b, uint32_t graph, uint64_t* row_ptr, uint32_t* co
     return SGC_OK;
 }
 
+int sgc_batch_color_core(sgc_batch* b, uint32_t min_degree, uint32_t* colored) {
+    if (!b) return fail(SGC_EINVAL, "null batch");
+    return sgc_color_core(b->h, min_degree, colored);
+}
+
 int sgc_batch_validate(sgc_batch* b, sgc_validation* out) {
     if (!b) return fail(SGC_EINVAL, "null batch");
     return sgc_validate(b->h, out);

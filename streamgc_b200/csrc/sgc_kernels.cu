@@ -462,6 +462,53 @@ void launch_snapshot(const Dev& g, uint16_t* snap, cudaStream_t s) {
 }
 void launch_colors(const Dev& g, uint16_t* out, cudaStream_t s) { launch_snapshot(g, out, s); }
 
+// First-fit coloring of a vertex list in list order: one block walks the
+// list, all its threads on the current vertex's row, which gathers the colors
+// its live neighbors hold (colors given earlier in the walk included); the
+// vertex takes the first color in 1..2047 none of them holds (2048 when all
+// do), version 1. Vertices already colored are skipped.
+__global__ void __launch_bounds__(1024) color_list_kernel(Dev g, const uint32_t* __restrict__ list, uint32_t m,
+                                                          uint32_t* colored) {
+    __shared__ uint32_t used[64];
+    const uint32_t tid = threadIdx.x;
+    uint32_t done = 0;
+    for (uint32_t k = 0; k < m; k++) {
+        const uint32_t v = list[k];
+        if (color_of(ld_cg(g.st + v)) != 0) continue;  // the same word for every thread
+        if (tid < 64) used[tid] = 0;
+        __syncthreads();
+        const uint64_t s = g.rp[v], e = s + row_len(g, v);
+        for (uint64_t j = s + tid; j < e; j += blockDim.x) {
+            const uint32_t y = g.col[j];
+            if (y < g.n) {
+                const uint32_t c = color_of(ld_cg(g.st + y));
+                if (c != 0 && c < 2048) atomicOr(&used[c >> 5], 1u << (c & 31));
+            }
+        }
+        __syncthreads();
+        if (tid < 32) {
+            uint32_t f0 = ~used[2 * tid], f1 = ~used[2 * tid + 1];
+            if (tid == 0) f0 &= ~1u;  // color 0 is not a candidate
+            const uint32_t any = __ballot_sync(FULL, (f0 | f1) != 0);
+            uint32_t c = 2048;
+            if (any) {
+                const uint32_t src = __ffs(any) - 1;
+                const uint32_t mine = f0 ? 64 * tid + __ffs(f0) - 1 : 64 * tid + 32 + __ffs(f1) - 1;
+                c = __shfl_sync(FULL, (f0 | f1) ? mine : 0u, src);
+            }
+            if (tid == 0) {
+                g.st[v] = pack((uint16_t)c, 1);
+                done++;
+            }
+        }
+        __syncthreads();  // the new color is visible to the next vertex's gathers
+    }
+    if (tid == 0) *colored = done;
+}
+void launch_color_list(const Dev& g, const uint32_t* list, uint32_t m, uint32_t* colored, cudaStream_t s) {
+    color_list_kernel<<<1, 1024, 0, s>>>(g, list, m, colored);
+}
+
 __global__ void query_kernel(const uint16_t* __restrict__ snap, uint32_t n, const uint32_t* __restrict__ v,
                              uint16_t* __restrict__ out, uint32_t k) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -139,6 +139,7 @@ void launch_repair_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int n
 void launch_repair_step(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s,
                         const cudaGraphConditionalHandle* cond);
 void launch_query(const uint16_t* snap, uint32_t n, const uint32_t* v, uint16_t* out, uint32_t k, cudaStream_t s);
+void launch_color_list(const Dev& g, const uint32_t* list, uint32_t m, uint32_t* colored, cudaStream_t s);
 void launch_colors(const Dev& g, uint16_t* out, cudaStream_t s);
 
 // Tier-2 (sgc_tier2.cu)

@@ -25,6 +25,12 @@ class _Handle:
     def __init__(self, g, **k):
         self.n = g.n
 
+    def color_core(self, min_degree):
+        return 0
+
+    def synchronize(self):
+        pass
+
     def apply(self, ups, mode=0):
         pass
 
@@ -41,6 +47,9 @@ class _Handle:
 class _Batch:
     def __init__(self, graphs, **k):
         self.k = 0
+
+    def color_core(self, min_degree):
+        return 0
 
     def submit(self, k, part):
         pass
@@ -107,6 +116,9 @@ class _PlainHandle:
     def __init__(self, g, **k):
         self.n = g.n
         self.k = 0
+
+    def color_core(self, min_degree):
+        return 0
 
     def apply(self, ups, mode=0):
         pass
@@ -206,7 +218,7 @@ def _rank(rank, world, port, form, q):
                                  served_seconds=0.3, served_staleness_us=2000, served_check=False,
                                  served_regrow=False, sorted_rows=False, workload="small", cpu_batches=0,
                                  cpu_seconds=1.0, profile_window=False, graph_publish=False, ingest=False,
-                                 latency_epochs=4, validate_steps=True)
+                                 latency_epochs=4, validate_steps=True, large_div=1)
     out, err = io.StringIO(), None
     old = sys.stdout
     sys.stdout = out

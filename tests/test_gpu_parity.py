@@ -243,3 +243,27 @@ def test_validator_matches_oracle_on_improper_state():
     finally:
         h.close()
         g.close()
+
+
+def test_core_coloring_then_full_repair_matches_oracle():
+    """A loaded power-law graph colored without an init stream: the high-degree
+    core one vertex at a time (sgc_color_core), then one full repair. States
+    equal the oracle's after each step; the result is proper."""
+    g = S.Graph.chung_lu(30000, 2.1, 17.0, 3000.0, 11)
+    o = O.Oracle(g.row_ptr, g.col_idx, g.degree, hist_threshold=64, exact=True)
+    h = S.StreamGC(g, histogram_threshold=64, exact_select=True)
+    try:
+        k = h.color_core(96)
+        assert k == o.color_core(96) > 0
+        assert np.array_equal(h.states(), o.states())
+        rep = h.publish()
+        ref = o.publish_repair()
+        assert rep["proper"] == 1 == ref["proper"]
+        assert rep["tier1_iterations"] == ref["tier1_iterations"]
+        assert np.array_equal(h.states(), o.states())
+        v = h.validate()
+        assert v["violations"] == 0 and v["uncolored_with_edges"] == 0
+        assert h.color_core(96) == 0  # nothing left uncolored
+    finally:
+        h.close()
+        o.close()
