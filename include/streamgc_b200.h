@@ -54,6 +54,20 @@ typedef struct sgc_handle sgc_handle;
  * with few holes: searches stay 32-ary over long runs. Colors do not depend on
  * it. */
 #define SGC_OPT_SORTED_ROWS 8u
+/* The reference's ablation builds (Makefile abl-* targets), as options of the
+ * reference rules (not with SGC_OPT_EXACT_SELECT):
+ *   FORCE_BITMAP  every vertex picks its color from its neighbor bitmap
+ *                 (STREAMGC_ABLATION_FORCE_BITMAP, color_select.cuh:98-100);
+ *   NO_OVERFLOW   an insert into a full row is dropped, not buffered
+ *                 (STREAMGC_ABLATION_NO_OVERFLOW, local_update.cu:28-38);
+ *   LIVE_DEG      Tier-1 ranks a vertex by its live degree against its
+ *                 neighbors' frozen priorities (STREAMGC_ABLATION_LIVE_DEG_PRIORITY,
+ *                 conflict_repair.cu:46-57).
+ * The reference's abl-force-histogram build compiles the same dispatch as its
+ * default (color_select.cuh:101-107), so it has no option here. */
+#define SGC_OPT_ABL_FORCE_BITMAP 16u
+#define SGC_OPT_ABL_NO_OVERFLOW  32u
+#define SGC_OPT_ABL_LIVE_DEG     64u
 
 typedef struct sgc_options {
     uint32_t struct_size;      /* sizeof(sgc_options) */

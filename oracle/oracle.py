@@ -113,6 +113,9 @@ def lib():
     return _lib
 
 
+ABLATIONS = {"force_bitmap": 4, "no_overflow": 8, "live_deg": 16}
+
+
 def updates_from(pairs, types=None):
     """Pack (k,2) uint32 pairs and uint8 types (0=ADD,1=DEL) into EdgeUpdate records."""
     pairs = np.asarray(pairs, dtype=np.uint32).reshape(-1, 2)
@@ -128,13 +131,15 @@ class Oracle:
     """Single-GPU StreamGC state restated on the CPU (sequential, stream order)."""
 
     def __init__(self, row_ptr, col, degree, hist_threshold=64, slack_pct=300, max_hist_colors=1024,
-                 exact=False, conc=False):
+                 exact=False, conc=False, ablations=()):
         """exact: exact color selection above the threshold and the independent-set
         Tier-1 (the concurrent configuration's rules); default: the reference's.
         conc (with exact): also the concurrent apply's row layout and update
         rules (sorted base runs with tombstones, tail inserts, scans bounded by
         the high-water mark, lazy compaction, early-exit color reduction), so
-        that the byte counters count what those rules read and write."""
+        that the byte counters count what those rules read and write.
+        ablations: names among "force_bitmap", "no_overflow", "live_deg" (the
+        reference's ablation builds; reference rules only)."""
         self.L = lib()
         rp = np.ascontiguousarray(row_ptr, dtype=np.uint64)
         col = np.ascontiguousarray(col, dtype=np.uint32)
@@ -142,7 +147,8 @@ class Oracle:
         self.n = len(rp) - 1
         self.h = self.L.og_create(self.n, _p(rp, _u64p), _p(col, _u32p), _p(deg, _u32p),
                                   hist_threshold, slack_pct, max_hist_colors,
-                                  (1 if exact else 0) | (2 if exact and conc else 0))
+                                  (1 if exact else 0) | (2 if exact and conc else 0) |
+                                  sum(ABLATIONS[a] for a in ablations))
 
     def close(self):
         if self.h:

@@ -79,6 +79,11 @@ struct Oracle {
     // library's concurrent configuration; byte counters count what those rules
     // read and write.
     bool conc = false;
+    // The reference's ablation builds (reference rules only): every color
+    // choice from the bitmap (color_select.cuh:98-100); a full row drops the
+    // insert (local_update.cu:28-38); Tier-1 ranks a vertex by its live degree
+    // against its neighbors' frozen priorities (conflict_repair.cu:46-57).
+    bool abl_force_bitmap = false, abl_no_overflow = false, abl_live_deg = false;
     std::vector<uint32_t> mhw, mbl, mholes;
     std::vector<uint8_t> mdirty;
     std::vector<uint64_t> rp;      // logical row starts, rp[n] = total slots
@@ -174,7 +179,7 @@ struct Oracle {
     }
     uint16_t fac(uint32_t x, const std::vector<uint32_t>& cols, uint64_t& b) const {
         b += 4;  // high_degree_map read
-        if (hdmap[x] != EMPTY) return exact ? fac_exact(x, cols, b) : fac_hist(x, b);
+        if (hdmap[x] != EMPTY && !abl_force_bitmap) return exact ? fac_exact(x, cols, b) : fac_hist(x, b);
         return fac_bitmap(x, cols, b);
     }
 
@@ -343,10 +348,11 @@ struct Oracle {
             if (s == INV) { col[j] = nbr; b += 4; edited[x] = 1; return 0; }
             if (s == nbr) return 1;
         }
+        asym = true;
+        if (abl_no_overflow) return 2;  // dropped, nothing buffered
         uint32_t pos = ovf_count++;
         if (pos < OVF_CAP) { ovf[pos].local_vertex_idx = x; ovf[pos].neighbor_global = nbr; b += 8; }
         else ovf_lost++;
-        asym = true;
         return 2;
     }
     // Returns whether an entry was removed.
@@ -570,6 +576,11 @@ struct Oracle {
                 continue;
             }
             uint64_t myp = prio(x);
+            if (abl_live_deg) {  // live entries of the (compact) row
+                uint32_t live = 0;
+                for (uint64_t j = rp[x]; j < rp[x + 1]; j++) live += col[j] != INV;
+                myp = ((uint64_t)live << 32) | x;
+            }
             b += 4;
             bool need = false;
             for (uint64_t j = rp[x]; j < rp[x + 1]; j++) {
@@ -929,6 +940,9 @@ void* og_create(uint32_t n, const uint64_t* row_ptr, const uint32_t* col_idx, co
     Oracle* g = new Oracle();
     g->exact = (flags & 1u) != 0;
     g->conc = g->exact && (flags & 2u) != 0;
+    g->abl_force_bitmap = (flags & 4u) != 0;
+    g->abl_no_overflow = (flags & 8u) != 0;
+    g->abl_live_deg = (flags & 16u) != 0;
     g->n = n;
     g->hist_thr = hist_thr;
     g->maxc = max_hist_colors ? max_hist_colors : SGC_MAX_HISTOGRAM_COLORS_DEFAULT;

@@ -35,6 +35,9 @@ DL = dict(states=0, colors=1, bitmaps=2, hist=3, row_ptr=4, col=5, snapshot=6, h
           base_run=10, holes=11)
 
 
+ABLATIONS = {"force_bitmap": 16, "no_overflow": 32, "live_deg": 64}  # SGC_OPT_ABL_*
+
+
 class StreamGCError(RuntimeError):
     pass
 
@@ -403,14 +406,16 @@ class StreamGC:
 
     def __init__(self, graph: Graph, epoch_size=32768, histogram_threshold=64, slack_pct=300,
                  max_hist_colors=1024, max_batch=32768, device=0, profile=False, exact_select=False,
-                 full_repair_every=None, repair_tile=None, graph_publish=False, sorted_rows=False):
+                 full_repair_every=None, repair_tile=None, graph_publish=False, sorted_rows=False, ablations=()):
+        """ablations: names among "force_bitmap", "no_overflow", "live_deg" -- the
+        reference's ablation builds, with its rules (not with exact_select)."""
         L = lib()
         cfg = _Config(1, graph.n, graph.nnz, 1 << 20, epoch_size, 100, histogram_threshold, 0.2)
         opt = _Options()
         L.sgc_default_options(C.byref(opt))
         opt.slack_pct, opt.max_hist_colors, opt.max_batch, opt.device = slack_pct, max_hist_colors, max_batch, device
         opt.flags = (1 if profile else 0) | (2 if exact_select else 0) | (4 if graph_publish else 0) | \
-            (8 if sorted_rows else 0)
+            (8 if sorted_rows else 0) | sum(ABLATIONS[a] for a in ablations)
         if full_repair_every is not None:
             opt.full_repair_every = full_repair_every
         if repair_tile is not None:

@@ -469,6 +469,8 @@ int sgci::create_internal(const StreamGCConfig* cfg, const sgc_options* opt_in, 
         if (degree[x] > thr) hdmap[x] = num_hd++;
     }
     const bool exact_sel = (opt.flags & SGC_OPT_EXACT_SELECT) != 0;
+    if (exact_sel && (opt.flags & (SGC_OPT_ABL_FORCE_BITMAP | SGC_OPT_ABL_NO_OVERFLOW | SGC_OPT_ABL_LIVE_DEG)))
+        return fail(SGC_EINVAL, "the ablation options apply to the reference rules, not to SGC_OPT_EXACT_SELECT");
     for (uint64_t j = 0; j < nnz; j++) {
         if (col_idx[j] == INV) return fail(SGC_EINVAL, "col_idx holds the INVALID sentinel at %llu", (unsigned long long)j);
         if (exact_sel && (col_idx[j] & TOMB))  // the top bit marks deleted entries under exact selection
@@ -501,6 +503,9 @@ int sgci::create_internal(const StreamGCConfig* cfg, const sgc_options* opt_in, 
     g.n = n;
     g.maxc = h->maxc;
     g.exact = (opt.flags & SGC_OPT_EXACT_SELECT) ? 1u : 0u;
+    g.abl = ((opt.flags & SGC_OPT_ABL_FORCE_BITMAP) ? ABL_FORCE_BITMAP : 0u) |
+            ((opt.flags & SGC_OPT_ABL_NO_OVERFLOW) ? ABL_NO_OVERFLOW : 0u) |
+            ((opt.flags & SGC_OPT_ABL_LIVE_DEG) ? ABL_LIVE_DEG : 0u);
     const uint32_t hist_rows = g.exact ? 0u : num_hd;  // exact selection keeps no histogram rows
     uint64_t* d_rp; A(&d_rp, (size_t)n + 1);
     const uint64_t padded = ((h->total_slots + 3) & ~3ull) + 8;  // 16-byte loads stay inside

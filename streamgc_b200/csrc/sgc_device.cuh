@@ -40,6 +40,13 @@ enum : uint32_t {
     ERR_ROW = 1u << 5,            // a row's high-water mark lay past its capacity (scans clamped)
 };
 
+// Ablations of the reference rules (Dev::abl), as its abl-* builds.
+enum : uint32_t {
+    ABL_FORCE_BITMAP = 1u << 0,  // every color choice from the bitmap (color_select.cuh:98-100)
+    ABL_NO_OVERFLOW = 1u << 1,   // a full row drops the insert (local_update.cu:28-38)
+    ABL_LIVE_DEG = 1u << 2,      // Tier-1: own live degree vs neighbors' frozen priority (conflict_repair.cu:46-57)
+};
+
 // Repair flags of one graph of a handle.
 struct GraphCtl {
     uint32_t clean;   // the last repair ended proper and only updates changed colors since
@@ -63,6 +70,7 @@ struct Dev {
     uint32_t maxc;                 // histogram colors per row (multiple of 4)
     uint32_t exact;                // 1: colors above the threshold are chosen from the live
                                    // neighbors (no global histogram rows are kept)
+    uint32_t abl;                  // ablations of the reference rules (ABL_* bits)
     const uint64_t* rp;            // n+1 row starts (64-bit: slabs beyond 2^32 slots)
     uint32_t* col;                 // slots, padded so 16-byte loads never leave the allocation
     uint32_t* st;                  // packed (color | version << 16)
@@ -375,7 +383,10 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
         uint32_t v = 0;
         const bool hit = warp_find(g.col, from, e, [nbr](uint32_t t) { return t == INV || t == nbr; }, p, v);
         if (!hit) {
-            if (lane_id() == 0) {
+            if (lane_id() == 0 && (g.abl & ABL_NO_OVERFLOW)) {  // the ablation drops the edge
+                g.gctl[graph_of(g, x)].dropped = 1u;
+                flag_asym(g, x);
+            } else if (lane_id() == 0) {
                 const uint32_t pos = atomicAdd(g.ovf_count, 1u);
                 if (pos < OVF_CAP) {
                     g.ovf[pos].local_vertex_idx = x;
@@ -564,7 +575,8 @@ __device__ __forceinline__ uint16_t warp_fac_exact(const Dev& g, uint32_t x, con
 // FindAvailableColor: histogram row when the vertex has one, else bitmap.
 __device__ __forceinline__ uint16_t warp_fac(const Dev& g, uint32_t x, const uint32_t* cols) {
     const uint32_t hd = __ldg(g.hdmap + x);
-    if (hd != EMPTY) return g.exact ? warp_fac_exact(g, x, cols) : warp_fac_hist(g.hist + (uint64_t)hd * g.maxc, g.maxc);
+    if (hd != EMPTY && !(g.abl & ABL_FORCE_BITMAP))
+        return g.exact ? warp_fac_exact(g, x, cols) : warp_fac_hist(g.hist + (uint64_t)hd * g.maxc, g.maxc);
     const uint64_t bmv = ld_cg(g.bm + x);
     if (~bmv) return (uint16_t)__ffsll((long long)~bmv);
     return warp_fac_scan(g, x, cols);

@@ -609,7 +609,7 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
         GraphCtl* gc = SYM ? &g.gctl[graph_of(g, x)] : nullptr;
         const bool symx = SYM && gc->full && ld_cg(&gc->asym);
         const uint32_t myc = color_of(__ldg(g.st + x));
-        const uint32_t mydeg = __ldg(g.deg + x);
+        const uint32_t mydeg = (g.abl & ABL_LIVE_DEG) ? row_len(g, x) : __ldg(g.deg + x);
         uint32_t lo = 0, hi = 0;
         unsigned long long sym = 0;
         bool conf = false;
@@ -695,7 +695,7 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
         live = len;
         if (len <= SWEEP_TINY) {
             const uint64_t s = g.rp[x];
-            const uint32_t mydeg = __ldg(g.deg + x);
+            const uint32_t mydeg = (g.abl & ABL_LIVE_DEG) ? len : __ldg(g.deg + x);
             uint32_t lo = 0, hi = 0;
             for (uint32_t j = 0; j < len; j++) {
                 const uint32_t ng = __ldg(g.col + s + j);

@@ -13,6 +13,8 @@
 //   --exact-select         concurrent configuration: exact color selection and
 //                          independent-set repair (SGC_OPT_EXACT_SELECT)
 //   --graph-publish --sorted-rows            SGC_OPT_GRAPH_PUBLISH, SGC_OPT_SORTED_ROWS
+//   --ablation force-bitmap|no-overflow|live-deg   the reference's abl-* builds
+//                          (SGC_OPT_ABL_*), with its rules
 //
 // Output names follow the code (streamgc.cu:1479-1481):
 //   <dir>/streamgc_<G>gpu_stream<N>_<pct>pct.coloring (+ .txt, + .meta)
@@ -107,6 +109,16 @@ int main(int argc, char** argv) {
         else if (strcmp(argv[i], "--exact-select") == 0) opt.flags |= SGC_OPT_EXACT_SELECT;
         else if (strcmp(argv[i], "--graph-publish") == 0) opt.flags |= SGC_OPT_GRAPH_PUBLISH;
         else if (strcmp(argv[i], "--sorted-rows") == 0) opt.flags |= SGC_OPT_SORTED_ROWS;
+        else if (is("--ablation")) {  // the reference's abl-* builds (Makefile:55-78)
+            const char* a = argv[++i];
+            if (!strcmp(a, "force-bitmap")) opt.flags |= SGC_OPT_ABL_FORCE_BITMAP;
+            else if (!strcmp(a, "no-overflow")) opt.flags |= SGC_OPT_ABL_NO_OVERFLOW;
+            else if (!strcmp(a, "live-deg")) opt.flags |= SGC_OPT_ABL_LIVE_DEG;
+            else {
+                fprintf(stderr, "[StreamGC] unknown ablation %s (force-bitmap, no-overflow, live-deg)\n", a);
+                return 1;
+            }
+        }
     }
     if (!graph_file) {
         fprintf(stderr, "Usage: %s --graph <path.mtx> [options]\n", argv[0]);

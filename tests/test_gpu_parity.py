@@ -267,3 +267,36 @@ def test_core_coloring_then_full_repair_matches_oracle():
     finally:
         h.close()
         o.close()
+
+
+@pytest.mark.parametrize("name, ablation", [("overflow512", "no_overflow"), ("rmat11", "force_bitmap"),
+                                            ("rmat11", "live_deg"), ("rmat11_thr16_a2", "live_deg")])
+def test_ablation_builds_match_oracle(name, ablation):
+    """The reference's abl-* builds as handle options: deterministic epochs and
+    phase-end repairs bit-exact with the oracle under the same ablation."""
+    c = MG.build_case(name)
+    g = O.Oracle(c["rp"], c["col"], c["deg"], hist_threshold=c["thr"], slack_pct=c["slack"], ablations=(ablation,))
+    h = S.StreamGC(S.Graph(c["rp"], c["col"], c["deg"]), epoch_size=c["E"], histogram_threshold=c["thr"],
+                   slack_pct=c["slack"], max_batch=c["batch"], ablations=(ablation,))
+    try:
+        for ups in (c["init"], c["bench"]):
+            since = 0
+            for s in range(0, len(ups), c["batch"]):
+                part = ups[s:s + c["batch"]]
+                h.apply(part, S.MODE_DETERMINISTIC)
+                g.apply(part)
+                since += len(part)
+                if since >= c["E"]:
+                    h.epoch()
+                    g.epoch()
+                    since = 0
+            rep = h.repair()
+            it, last, fixed = g.phase_end()
+            assert (rep["tier1_iterations"], rep["tier1_last_count"], rep["tier2_fixed"]) == (it, last, fixed)
+            for k, a, b in (("states", h.states(), g.states()), ("bitmaps", h.bitmaps(), g.bitmaps()),
+                            ("col", h.col(), g.col()), ("hist", h.hist(), g.hist())):
+                assert np.array_equal(a, b), f"{name} {ablation} {k}"
+            assert h.stats()["overflow_pending"] == g.overflow_count()
+    finally:
+        h.close()
+        g.close()
