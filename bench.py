@@ -228,9 +228,10 @@ def run_ours(a):
     g, init, bench, desc = build_workload(a.workload, stream_len, a.large_div)
 
     t = time.time()
+    # no periodic full repair: every published snapshot is checked by the validator instead
     h = S.StreamGC(g, epoch_size=E, histogram_threshold=HIST_THR, slack_pct=300, max_batch=1 << 20,
                    device=local, profile=not a.graph_publish, exact_select=True, graph_publish=a.graph_publish,
-                   sorted_rows=a.sorted_rows)
+                   sorted_rows=a.sorted_rows, full_repair_every=a.full_repair_every)
     for s in range(0, 0 if init is None else len(init), 1 << 20):
         h.apply(init[s:s + (1 << 20)], S.MODE_CONCURRENT)
     t1 = time.time()
@@ -371,6 +372,7 @@ def run_ours(a):
                     tier1_sweeps_per_step=round(sweeps / max(1, a.steps), 2),
                     tier2_runs_in_timed=sum(r["tier2_ran"] for r in reps),
                     all_published_proper=all(r["proper"] for r in reps),
+                    full_repair_every=a.full_repair_every,
                     snapshots_validated=len(checks),
                     snapshot_violations=sum(int(c["violations"]) + int(c["uncolored_with_edges"]) for c in checks),
                     max_colors_in_timed=max((int(c["max_color"]) for c in checks), default=None),
@@ -919,6 +921,9 @@ def main():
     ap.add_argument("--epoch-size", type=int, default=32768,
                     help="plain path: updates per epoch (the large workload's sweep uses 4096, 32768, 262144)")
     ap.add_argument("--cpu-batches", type=int, default=8, help="epochs timed on the CPU baseline (0: skip)")
+    ap.add_argument("--full-repair-every", type=int, default=0,
+                    help="plain path: every k-th publish repairs every vertex (0: only when the incremental rule "
+                         "cannot be used); every published snapshot is validated either way")
     ap.add_argument("--large-div", type=int, default=1,
                     help="large workload scaled down by this factor (same family; for profiling captures)")
     ap.add_argument("--latency-epochs", type=int, default=128,

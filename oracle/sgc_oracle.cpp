@@ -380,6 +380,7 @@ struct Oracle {
         st[x] = sgc_pack_state(newc, nv);
         b += 4;
         recolors++;
+        if (exact) touched[x] = 1;  // a color change: the next repair starts from x
         // update_incremental_state: every live row entry, duplicates included.
         for (uint64_t j = rp[x]; j < re(x); j++) {
             uint32_t ng = col[j];
@@ -417,7 +418,12 @@ struct Oracle {
         uint32_t u = e.u, v = e.v;
         if (u >= n || v >= n) { skipped_updates++; return; }  // hash miss -> continue
         updates_applied++;
-        if (exact && (e.type == SGC_UPDATE_ADD || e.type == SGC_UPDATE_DEL)) touched[u] = touched[v] = 1;
+        if (exact && (e.type == SGC_UPDATE_ADD || e.type == SGC_UPDATE_DEL)) {
+            // bitmap-class rows are revisited (bitmaps rebuilt); histogram-class
+            // rows only when their color changes or an ADD leaves a conflict
+            if (hdmap[u] == EMPTY) touched[u] = 1;
+            if (hdmap[v] == EMPTY) touched[v] = 1;
+        }
         if (e.type == SGC_UPDATE_ADD) {
             if (add_slot(u, v, b) != add_slot(v, u, b)) asym = true;
             b += 4;
@@ -425,6 +431,7 @@ struct Oracle {
                 uint16_t c = fac(u, st, b);
                 st[u] = sgc_pack_state(c, 1);
                 b += 4;
+                if (exact) touched[u] = 1;
             }
             b += 4;
             if (color(v) == 0) {
@@ -432,6 +439,7 @@ struct Oracle {
                 uint16_t c = fac(v, st, b);
                 st[v] = sgc_pack_state(c, 1);
                 b += 4;
+                if (exact) touched[v] = 1;
             }
             new_nbr(u, color(v), b);
             new_nbr(v, color(u), b);
@@ -451,6 +459,18 @@ struct Oracle {
             removed_nbr(v, fv, b);
             try_reduce(u, fu, b);
             try_reduce(v, fv, b);
+        }
+    }
+
+    // End of a batch (exact selection): both endpoints of every ADD whose
+    // colors are equal are marked for the next repair (the library's
+    // add_check_kernel after each apply).
+    void batch_end(const EdgeUpdate* ups, uint64_t cnt) {
+        if (!exact) return;
+        for (uint64_t i = 0; i < cnt; i++) {
+            const EdgeUpdate& e = ups[i];
+            if (e.type != SGC_UPDATE_ADD || e.u >= n || e.v >= n || e.u == e.v) continue;
+            if (color(e.u) == color(e.v) && color(e.u) != 0) touched[e.u] = touched[e.v] = 1;
         }
     }
 
@@ -1015,6 +1035,7 @@ uint32_t og_max_hist_colors(void* h) { return ((Oracle*)h)->maxc; }
 void og_apply(void* h, const EdgeUpdate* ups, uint64_t n) {
     Oracle* g = (Oracle*)h;
     for (uint64_t i = 0; i < n; i++) g->apply_one(ups[i]);
+    g->batch_end(ups, n);
 }
 void og_epoch(void* h) { ((Oracle*)h)->epoch(); }
 uint64_t og_drain_and_compact(void* h) { return ((Oracle*)h)->drain_and_compact(); }
@@ -1039,6 +1060,7 @@ uint32_t og_process_stream(void* h, const EdgeUpdate* ups, uint64_t n, uint32_t 
     while (processed < n) {
         uint64_t b = std::min<uint64_t>(batch, n - processed);
         for (uint64_t i = 0; i < b; i++) g->apply_one(ups[processed + i]);
+        g->batch_end(ups + processed, b);
         processed += b;
         since += b;
         if (since >= epoch_size) { g->epoch(); since = 0; epochs++; }
@@ -1097,6 +1119,7 @@ uint32_t og_process_stream_repaired(void* h, const EdgeUpdate* ups, uint64_t n, 
     while (processed < n) {
         uint64_t b = std::min<uint64_t>(step, n - processed);
         for (uint64_t i = 0; i < b; i++) g->apply_one(ups[processed + i]);
+        g->batch_end(ups + processed, b);
         processed += b;
         since += b;
         if (since >= epoch_size) {

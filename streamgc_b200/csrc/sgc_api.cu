@@ -229,6 +229,10 @@ int apply_device(sgc_handle* h, const EdgeUpdate* src, uint32_t n, int mode) {
         launch_conc_apply(h->g, src, n, h->eo, h->num_sms, h->stream);
         h->launches += 3;
     }
+    if (h->g.touched) {
+        launch_add_check(h->g, src, n, nullptr, h->num_sms, h->stream);
+        h->launches += 1;
+    }
     h->last_mode = mode;
     h->updates += n;
     return check_cuda("apply");

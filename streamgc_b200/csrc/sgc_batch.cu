@@ -122,6 +122,7 @@ void enqueue_head(sgc_batch* b, cudaStream_t s) {
         launch_seg_apply(h->g, h->d_batch, b->d_segs, b->d_dyn, b->G, h->num_sms, s);
     else
         launch_conc_apply_dyn(h->g, h->d_batch, b->d_dyn, h->eo, h->num_sms, (int)b->bps, s);
+    launch_add_check(h->g, h->d_batch, 0, b->d_dyn, h->num_sms, s);
     cudaMemsetAsync(&h->ctl->dirty_count, 0, 4, s);
     launch_dirty_list(h->g, h->dirty_list, &h->ctl->dirty_count, s);
     launch_compact(h->g, h->dirty_list, &h->ctl->dirty_count, h->n, false, s, (h->opt.flags & SGC_OPT_SORTED_ROWS) != 0);

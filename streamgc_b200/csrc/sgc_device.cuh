@@ -90,8 +90,10 @@ struct Dev {
     uint32_t* err;
     uint32_t* blen;                // exact selection: per row, length of the base run [rp, rp+blen):
                                    // ids strictly ascending, deleted ones kept as id | TOMB (null otherwise)
-    uint32_t* touched;             // exact selection: bitmask of update endpoints since the last repair
-                                   // (null otherwise)
+    uint32_t* touched;             // exact selection: bitmask of the vertices the next incremental repair
+                                   // starts from (null otherwise): every vertex whose color changed, every
+                                   // bitmap-class endpoint of an update (its bitmap is rebuilt), and both
+                                   // endpoints of an ADD whose colors are equal at the end of its batch
     GraphCtl* gctl;                // per graph: repair flags (one entry for a single-graph handle)
     const uint32_t* gidw;          // graph of each 32-vertex word (graphs start at multiples of 32);
                                    // null: one graph
@@ -189,18 +191,19 @@ __device__ __forceinline__ void warp_for_each(const uint32_t* col, uint64_t s, u
 }
 
 // Warp-collective visit of every slot of [s, e) holding a vertex id y < n,
-// with arr[y] (a coherent load): a lane issues the loads of its 16 slots and
-// their 16 gathers before it uses any of them. f(y, arr[y]) runs once per slot.
-// With STOP, the scan ends after the first round in which f returned true on
-// any lane (warp vote); the return value says whether that happened.
-template <bool STOP, class F>
+// with arr[y] (a coherent load): a lane issues the loads of its 4K slots and
+// their 4K gathers before it uses any of them (K 16-byte loads per lane per
+// round). f(y, arr[y]) runs once per slot. With STOP, the scan ends after the
+// first round in which f returned true on any lane (warp vote); the return
+// value says whether that happened.
+template <bool STOP, int K = 4, class F>
 __device__ __forceinline__ bool warp_gather_each(const uint32_t* col, uint64_t s, uint64_t e, uint32_t n,
                                                  const uint32_t* arr, F f) {
     const uint32_t lane = lane_id();
-    for (uint64_t c = s & ~3ull; c < e; c += 512) {
-        uint32_t y[16], w[16];
+    for (uint64_t c = s & ~3ull; c < e; c += 128 * K) {
+        uint32_t y[4 * K], w[4 * K];
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < K; k++) {
             const uint64_t i = c + 128ull * k + 4ull * lane;
             uint4 q = make_uint4(INV, INV, INV, INV);
             if (i < e) q = ld_cg4(col + i);
@@ -210,10 +213,10 @@ __device__ __forceinline__ bool warp_gather_each(const uint32_t* col, uint64_t s
             y[4 * k + 3] = (i + 3 >= s && i + 3 < e) ? q.w : INV;
         }
 #pragma unroll
-        for (int t = 0; t < 16; t++) w[t] = y[t] < n ? ld_cg(arr + y[t]) : 0u;
+        for (int t = 0; t < 4 * K; t++) w[t] = y[t] < n ? ld_cg(arr + y[t]) : 0u;
         bool hit = false;
 #pragma unroll
-        for (int t = 0; t < 16; t++)
+        for (int t = 0; t < 4 * K; t++)
             if (y[t] < n) hit |= f(y[t], w[t]);
         if (STOP && __any_sync(FULL, hit)) return true;
     }
@@ -253,6 +256,10 @@ __device__ __forceinline__ void extend_row(const Dev& g, uint32_t x, uint32_t q)
     if (!g.holes) return;
     if (q < prev_hw) atomicSub(g.holes + x, 1u);
     else if (q > prev_hw) atomicAdd(g.holes + x, q - prev_hw);
+}
+
+__device__ __forceinline__ void mark_touched(const Dev& g, uint32_t x) {
+    if (g.touched && !(ld_cg(g.touched + (x >> 5)) & (1u << (x & 31)))) atomicOr(g.touched + (x >> 5), 1u << (x & 31));
 }
 
 __device__ __forceinline__ void flag_asym(const Dev& g, uint32_t x) {
@@ -378,10 +385,22 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
         // one would have marked the row edited.
         from = s + len;
     }
+    // The first free slot at or after `from` lies at or below the high-water
+    // mark, so the first scan stops one slot past it (not at the end of the
+    // row's slack); if a concurrent insert took those slots meanwhile, the
+    // scan goes on to the end of the row.
+    uint64_t lim = s + ld_cg(g.hw + x) + 1;
+    if (lim > e) lim = e;
     for (;;) {
         uint64_t p = 0;
         uint32_t v = 0;
-        const bool hit = warp_find(g.col, from, e, [nbr](uint32_t t) { return t == INV || t == nbr; }, p, v);
+        const bool hit =
+            from < lim && warp_find(g.col, from, lim, [nbr](uint32_t t) { return t == INV || t == nbr; }, p, v);
+        if (!hit && lim < e) {
+            if (lim > from) from = lim;
+            lim = e;
+            continue;
+        }
         if (!hit) {
             if (lane_id() == 0 && (g.abl & ABL_NO_OVERFLOW)) {  // the ablation drops the edge
                 g.gctl[graph_of(g, x)].dropped = 1u;
@@ -584,9 +603,16 @@ __device__ __forceinline__ uint16_t warp_fac(const Dev& g, uint32_t x, const uin
 
 // ---------------- incremental bitmap / histogram (color_select.cuh:120-209) ----------------
 
+// Sets color c's bit (1..64) of x's bitmap; a bit already set is left alone
+// (bits are only cleared by rebuilds, which never overlap an apply).
+__device__ __forceinline__ void set_bm_bit(const Dev& g, uint32_t x, uint16_t c) {
+    const unsigned long long bit = 1ull << (c - 1);
+    if (!(ld_cg(g.bm + x) & bit)) atomicOr((unsigned long long*)(g.bm + x), bit);
+}
+
 __device__ __forceinline__ void nbr_color_change(const Dev& g, uint32_t x, uint16_t oldc, uint16_t newc) {
     if (oldc == newc) return;
-    if (newc != 0 && newc <= 64) atomicOr((unsigned long long*)(g.bm + x), 1ull << (newc - 1));
+    if (newc != 0 && newc <= 64) set_bm_bit(g, x, newc);
     const uint32_t hd = __ldg(g.hdmap + x);
     if (hd != EMPTY && !g.exact) {
         uint32_t* h = g.hist + (uint64_t)hd * g.maxc;
@@ -596,7 +622,7 @@ __device__ __forceinline__ void nbr_color_change(const Dev& g, uint32_t x, uint1
 }
 __device__ __forceinline__ void new_nbr(const Dev& g, uint32_t x, uint16_t c) {
     if (c == 0) return;
-    if (c <= 64) atomicOr((unsigned long long*)(g.bm + x), 1ull << (c - 1));
+    if (c <= 64) set_bm_bit(g, x, c);
     const uint32_t hd = __ldg(g.hdmap + x);
     if (hd != EMPTY && !g.exact && c <= g.maxc) atomicAdd(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
 }
@@ -637,6 +663,7 @@ __device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x, uint16_t 
         newc = warp_fac(g, x, g.st);
         if (newc == color_of(cur)) return;
     }
+    if (lane_id() == 0) mark_touched(g, x);
     const uint16_t oldc = color_of(cur);
     const uint64_t s = g.rp[x], e = live_end(g, x, s);
     warp_for_each(g.col, s, e, [&](uint64_t, uint32_t ng) {
@@ -650,7 +677,8 @@ __device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x, uint16_t 
 // first round that finds one.
 __device__ __forceinline__ bool warp_color_held(const Dev& g, uint32_t x, uint16_t c) {
     const uint64_t s = g.rp[x], e = live_end(g, x, s);
-    return warp_gather_each<true>(g.col, s, e, g.n, g.st, [c](uint32_t, uint32_t w) { return color_of(w) == c; });
+    // rounds of 128 slots: a holder is usually among the first neighbors
+    return warp_gather_each<true, 1>(g.col, s, e, g.n, g.st, [c](uint32_t, uint32_t w) { return color_of(w) == c; });
 }
 
 // try_color_reduction: after a delete freed `freed`, move to a lower color if one is open.
@@ -676,7 +704,7 @@ __device__ __forceinline__ void warp_color_if_uncolored(const Dev& g, uint32_t x
     const uint32_t cur = warp_load_state(g, x);
     if (color_of(cur) != 0) return;
     const uint16_t c = warp_fac(g, x, g.st);
-    if (lane_id() == 0) atomicCAS(g.st + x, cur, pack(c, 1));
+    if (lane_id() == 0 && atomicCAS(g.st + x, cur, pack(c, 1)) == cur) mark_touched(g, x);
     __syncwarp();
 }
 
@@ -687,8 +715,11 @@ __device__ __forceinline__ void warp_color_if_uncolored(const Dev& g, uint32_t x
 // to the linear scan whenever the search does not find the key.
 __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v, uint8_t type, bool exact) {
     if (g.touched && lane_id() == 0 && (type == SGC_UPDATE_ADD || type == SGC_UPDATE_DEL)) {
-        atomicOr(g.touched + (u >> 5), 1u << (u & 31));
-        atomicOr(g.touched + (v >> 5), 1u << (v & 31));
+        // bitmap-class rows are revisited (their bitmaps rebuilt); a row with a
+        // histogram class takes exact colors from its live neighbors instead,
+        // and is revisited only when its color changes or an ADD leaves a conflict
+        if (__ldg(g.hdmap + u) == EMPTY) mark_touched(g, u);
+        if (__ldg(g.hdmap + v) == EMPTY) mark_touched(g, v);
     }
     if (type == SGC_UPDATE_ADD) {
         const int ru = warp_add_slot(g, u, v, exact);

@@ -184,6 +184,30 @@ __global__ void __launch_bounds__(256, 3) conc_apply_kernel(Dev g, const EdgeUpd
     }
 }
 
+// After a batch (exact selection): both endpoints of every ADD whose colors
+// are equal are marked for the next repair. Together with the marks of every
+// color change, this makes every conflict of the rows have a marked endpoint
+// once the last repair ended proper.
+__global__ void add_check_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n, const uint32_t* dyn) {
+    const uint32_t cnt = dyn ? ld_cg(dyn) : n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
+        if ((r.z & 0xFFu) != SGC_UPDATE_ADD || r.x >= g.n || r.y >= g.n || r.x == r.y) continue;
+        const uint16_t a = color_of(ld_cg(g.st + r.x)), b = color_of(ld_cg(g.st + r.y));
+        if (a == b && a != 0) {
+            mark_touched(g, r.x);
+            mark_touched(g, r.y);
+        }
+    }
+}
+void launch_add_check(const Dev& g, const EdgeUpdate* ups, uint32_t n, const uint32_t* dyn, int num_sms,
+                      cudaStream_t s) {
+    if (!g.touched || (!dyn && !n)) return;
+    uint32_t blk = dyn ? (uint32_t)num_sms * 4 : (n + 255) / 256;
+    if (blk > (uint32_t)num_sms * 4) blk = num_sms * 4;
+    add_check_kernel<<<blk, 256, 0, s>>>(g, ups, n, dyn);
+}
+
 void launch_det_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, cudaStream_t s) {
     if (n) det_apply_kernel<<<1, 32, 0, s>>>(g, ups, n);
 }

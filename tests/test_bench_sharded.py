@@ -218,7 +218,8 @@ def _rank(rank, world, port, form, q):
                                  served_seconds=0.3, served_staleness_us=2000, served_check=False,
                                  served_regrow=False, sorted_rows=False, workload="small", cpu_batches=0,
                                  cpu_seconds=1.0, profile_window=False, graph_publish=False, ingest=False,
-                                 latency_epochs=4, validate_steps=True, large_div=1)
+                                 latency_epochs=4, validate_steps=True, large_div=1,
+                                 full_repair_every=0)
     out, err = io.StringIO(), None
     old = sys.stdout
     sys.stdout = out
