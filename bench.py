@@ -322,6 +322,11 @@ def run_ours(a):
         h.synchronize()
         vis_ms.append(1e3 * (time.perf_counter() - t0))
         b += 1
+    # one full repair after the run (every vertex swept; not in any timed figure): the
+    # sweep kernels' bandwidth over the whole graph, and a last properness check
+    fs0 = h.stats()
+    full_rep = h.repair() if a.profile_full_sweep else None
+    fs1 = h.stats()
     total_ms = sum(step_ms)
     if dist:
         total_ms, e2e_s = max_over_ranks(dist, [total_ms, e2e_s], reduce_device(local))
@@ -376,7 +381,7 @@ def run_ours(a):
                     snapshots_validated=len(checks),
                     snapshot_violations=sum(int(c["violations"]) + int(c["uncolored_with_edges"]) for c in checks),
                     max_colors_in_timed=max((int(c["max_color"]) for c in checks), default=None),
-                    reference_gpu=REFERENCE_GPU[a.workload])
+                    reference_gpu=reference_gpu(a.workload))
         out = {
             "metric": METRIC, "value": job_rate(a.steps * E, world, total_ms / 1e3), "unit": "updates/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
@@ -387,6 +392,7 @@ def run_ours(a):
                                    "the return of the publish that makes it visible (wall clock)"},
             "roofline": roof_apply if roof_apply else roof_sweep,
             "roofline_sweep": roof_sweep,
+            "roofline_full_sweep": full_sweep_roofline(fs0, fs1, full_rep, peak, pk),
             "apply": {"ms_per_epoch": apply_avg, "share_of_step": apply_avg / (total_ms / a.steps),
                       "algorithmic_bytes_per_update": bpu},
             "e2e": {"value": world * a.steps * E / e2e_s, "unit": "updates/s",
@@ -401,6 +407,23 @@ def run_ours(a):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def full_sweep_roofline(s0, s1, rep, peak, peak_kind):
+    """The sweep kernels over every vertex (the full repair run after the
+    timed steps): algorithmic bytes (8 per live entry + 28 per vertex) over
+    their CUDA-event time."""
+    if rep is None:
+        return None
+    ms = s1["sweep_ms"] - s0["sweep_ms"]
+    by = s1["sweep_bytes"] - s0["sweep_bytes"]
+    n = s1["sweep_count"] - s0["sweep_count"]
+    if ms <= 0 or n <= 0:
+        return None
+    ach = by / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": "tier-1 sweep over every vertex (sweep_items + finalize + fac + commit)",
+            "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
+            "algorithmic_bytes": by, "sweeps": n, "ms": ms, "proper": rep["proper"]}
 
 
 def cpu_baseline(g, h, bench, first_batch, nb, budget_s):
@@ -483,14 +506,22 @@ def host_facts():
     return {"cpu_model": model, "threads": os.cpu_count(), "libstdcxx": libstdcxx}
 
 
-# The reference's own kernels on the GPU (built for sm_100a from its sources):
-# measured on the small and skewed workloads only (profiles/reference_kernels_sm100a.md).
-REFERENCE_GPU = {
-    "large": {"unavailable": "the reference's row offsets are 32-bit (include/streamgc.cuh:56-58): its slack CSR "
-                             "cannot address this graph's ~14.3 G slots"},
-    "skewed": {"see": "profiles/reference_kernels_sm100a.md"},
-    "small": {"see": "profiles/reference_kernels_sm100a.md"},
-}
+def reference_gpu(workload):
+    """The reference's own kernels (built for sm_100a from its sources) on the
+    same graph and stream: measured by oracle/ref_gpu_runs.py on a B200 and
+    kept in tests/golden/ref_gpu_runs.json (profiles/reference_kernels_sm100a.md)."""
+    if workload == "large":
+        return {"unavailable": "the reference's row offsets are 32-bit (include/streamgc.cuh:56-58): its slack CSR "
+                               "cannot address this graph's ~14.3 G slots"}
+    name = {"small": "delaunay17_churn", "skewed": "rmat20_ef48_kcore90_dense"}[workload]
+    try:
+        r = json.load(open(os.path.join(ROOT, "tests", "golden", "ref_gpu_runs.json")))[name]
+    except (OSError, KeyError, ValueError):
+        return None
+    return {"source": "tests/golden/ref_gpu_runs.json (oracle/ref_gpu_runs.py, one B200)",
+            "bench_updates_per_s_wall": r["bench_updates_per_s"],
+            "kernels_ms_per_epoch": r["apply_plus_epoch_ms_per_epoch"],
+            "final_colors": r["final_colors"], "snapshots": "unrepaired at epochs; repaired at phase end"}
 
 
 def run_reference(a):
@@ -921,6 +952,8 @@ def main():
     ap.add_argument("--epoch-size", type=int, default=32768,
                     help="plain path: updates per epoch (the large workload's sweep uses 4096, 32768, 262144)")
     ap.add_argument("--cpu-batches", type=int, default=8, help="epochs timed on the CPU baseline (0: skip)")
+    ap.add_argument("--no-full-sweep", dest="profile_full_sweep", action="store_false",
+                    help="plain path: skip the full repair after the run (its sweep bandwidth is reported)")
     ap.add_argument("--full-repair-every", type=int, default=0,
                     help="plain path: every k-th publish repairs every vertex (0: only when the incremental rule "
                          "cannot be used); every published snapshot is validated either way")

@@ -42,6 +42,9 @@ double ms_since(clk::time_point t0, clk::time_point t1) {
 constexpr uint64_t kBytesPerVertex = 176;
 constexpr uint64_t kBytesPerSlot = 4;
 constexpr uint64_t kBytesPerTickUpdate = 64;
+// Vertices of at least this degree in a newly admitted group are colored one
+// at a time (descending degree) before its first repair (sgc_color_core).
+constexpr uint32_t kCoreMinDegree = 256;
 
 struct Request {
     uint64_t id;
@@ -463,7 +466,14 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
         bo.device = s->opt.device;
         bo.flags = s->opt.flags;
         Group g;
-        const int rc = sgc_batch_create(gs.data(), (uint32_t)gs.size(), &bo, &g.b);
+        int rc = sgc_batch_create(gs.data(), (uint32_t)gs.size(), &bo, &g.b);
+        // the first tick colors the new tenants' graphs and publishes them; their
+        // dense cores (degree >= kCoreMinDegree) are colored one vertex at a time
+        // first (outside the table lock)
+        if (rc == SGC_OK && (rc = sgc_batch_color_core(g.b, kCoreMinDegree, nullptr)) != SGC_OK) {
+            sgc_batch_destroy(g.b);
+            g.b = nullptr;
+        }
         std::lock_guard<std::mutex> lk(s->mu);
         if (rc != SGC_OK) {  // back to the head of the queue
             s->resident_bytes -= add_bytes;
@@ -482,7 +492,7 @@ int sgc_server_step(sgc_server* s, sgc_server_step_report* rep) {
             }
             return rc;
         }
-        sgc_batch_close_epochs(g.b);  // the first tick colors the new tenants' graphs and publishes them
+        sgc_batch_close_epochs(g.b);
         g.tenants = admit;
         g.bytes = add_bytes;
         g.has_work = true;

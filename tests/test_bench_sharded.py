@@ -130,6 +130,9 @@ class _PlainHandle:
         return dict(tier1_iterations=1, tier1_last_count=0, tier2_ran=0, tier2_fixed=0, tier2_gave_up=0,
                     drained=0, drain_failed=0, proper=1, incremental=1)
 
+    def repair(self):
+        return dict(self.publish(), incremental=0)
+
     def synchronize(self):
         pass
 
@@ -219,7 +222,7 @@ def _rank(rank, world, port, form, q):
                                  served_regrow=False, sorted_rows=False, workload="small", cpu_batches=0,
                                  cpu_seconds=1.0, profile_window=False, graph_publish=False, ingest=False,
                                  latency_epochs=4, validate_steps=True, large_div=1,
-                                 full_repair_every=0)
+                                 full_repair_every=0, profile_full_sweep=True)
     out, err = io.StringIO(), None
     old = sys.stdout
     sys.stdout = out
