@@ -187,6 +187,20 @@ int sgc_apply(sgc_handle* h, const EdgeUpdate* updates, uint32_t n, int mode);
 int sgc_stage(sgc_handle* h, const EdgeUpdate* updates, uint32_t n);
 int sgc_apply_staged(sgc_handle* h, int mode);
 
+/* Ingest ring: the role of the reference's feeder thread and pinned ring,
+ * which it declares but never calls (feeder_thread.cpp:25-92, streamgc.cu:285-292).
+ * A pinned, device-mapped ring of 2^log2_slots update slots; one producer
+ * thread appends with sgc_ring_push (no CUDA call: a copy into the ring and a
+ * release of the new tail; *accepted may be below n when the ring is full),
+ * and the stepping thread drains it with sgc_ring_apply: one kernel copies up
+ * to max_updates published slots straight from host memory into the batch
+ * buffer, then the batch is applied (no cudaMemcpy per batch). Slots return
+ * to the producer once the GPU has read them (checked at the next
+ * sgc_ring_apply). */
+int sgc_ring_create(sgc_handle* h, uint32_t log2_slots);
+int sgc_ring_push(sgc_handle* h, const EdgeUpdate* updates, uint32_t n, uint32_t* accepted);
+int sgc_ring_apply(sgc_handle* h, uint32_t max_updates, int mode, uint32_t* applied);
+
 /* Reference epoch boundary (streamgc.cu:949-1012): publish the snapshot of the
  * current colors, compact edited rows, drain overflow, rebuild bitmaps. */
 int sgc_epoch(sgc_handle* h);

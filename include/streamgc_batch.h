@@ -87,7 +87,10 @@ uint32_t sgc_batch_epoch_size(const sgc_batch* b, uint32_t graph);
 
 /* Stages updates of one graph for the next tick (host memory; ids local to the
  * graph; an id outside the graph makes the update a no-op, counted as skipped).
- * SGC_EINVAL when the tick buffer is full. */
+ * SGC_EINVAL when the tick buffer is full. Allowed while a tick runs (between
+ * sgc_batch_tick_begin and _end): the staging buffer has two halves, so the
+ * next tick's updates are staged while the current ones are applied. Calls
+ * come from one thread (the one that ticks). */
 int sgc_batch_submit(sgc_batch* b, uint32_t graph, const EdgeUpdate* ups, uint32_t n);
 /* Updates staged and not yet applied, over all graphs. */
 uint64_t sgc_batch_pending(const sgc_batch* b);
@@ -95,7 +98,7 @@ uint64_t sgc_batch_pending(const sgc_batch* b);
 int sgc_batch_tick(sgc_batch* b, sgc_batch_tick_report* rep);
 /* The same in two halves: begin launches the tick on the batch's stream and
  * returns; end waits for it (ticks of several batches then overlap on the
- * device). No submit between them. */
+ * device, and the next tick's submits overlap this one). */
 int sgc_batch_tick_begin(sgc_batch* b);
 int sgc_batch_tick_end(sgc_batch* b, sgc_batch_tick_report* rep);
 /* Publishes every graph's current colors (closes all epochs) on the next tick. */

@@ -181,6 +181,9 @@ SIGNATURES = {
     "sgc_download": (C.c_int, [_vp, C.c_int, _vp, C.c_uint64]),
     "sgc_upload": (C.c_int, [_vp, C.c_int, _vp, C.c_uint64]),
     "sgc_color_core": (C.c_int, [_vp, C.c_uint32, _u32p]),
+    "sgc_ring_create": (C.c_int, [_vp, C.c_uint32]),
+    "sgc_ring_push": (C.c_int, [_vp, _vp, C.c_uint32, _u32p]),
+    "sgc_ring_apply": (C.c_int, [_vp, C.c_uint32, C.c_int, _u32p]),
     "sgc_find_color": (C.c_int, [_vp, C.c_uint32, _u16p]),
     "sgc_validate": (C.c_int, [_vp, C.POINTER(Validation)]),
     "sgc_check_state": (C.c_int, [_vp, C.POINTER(StateReport)]),
@@ -468,6 +471,30 @@ class StreamGC:
         """Applies the oldest staged batch once its copy is done."""
         _check(lib().sgc_apply_staged(self.h, mode), "sgc_apply_staged")
 
+    def ring_create(self, log2_slots):
+        """A pinned, device-mapped ingest ring of 2**log2_slots update slots."""
+        _check(lib().sgc_ring_create(self.h, log2_slots), "ring_create")
+
+    def ring_push(self, ups, offset=0):
+        """Appends ups[offset:] to the ring (any one producer thread; no CUDA
+        call); returns how many fit."""
+        out = np.zeros(1, dtype=np.uint32)
+        _check(lib().sgc_ring_push(self.h, ups.ctypes.data + 16 * offset, len(ups) - offset, _p(out, _u32p)),
+               "ring_push")
+        return int(out[0])
+
+    def ring_push_ptr(self, ptr, n):
+        out = np.zeros(1, dtype=np.uint32)
+        _check(lib().sgc_ring_push(self.h, ptr, n, _p(out, _u32p)), "ring_push")
+        return int(out[0])
+
+    def ring_apply(self, max_updates, mode=MODE_CONCURRENT):
+        """The GPU copies up to max_updates published slots from the ring and
+        applies them; returns how many."""
+        out = np.zeros(1, dtype=np.uint32)
+        _check(lib().sgc_ring_apply(self.h, max_updates, mode, _p(out, _u32p)), "ring_apply")
+        return int(out[0])
+
     def apply_ptr(self, ptr, n, mode=MODE_CONCURRENT):
         """Updates already in device (or pinned host) memory at address `ptr`."""
         _check(lib().sgc_apply(self.h, C.c_void_p(ptr), n, mode), "sgc_apply")
@@ -672,6 +699,15 @@ class Batch:
     def tick(self):
         r = TickReport()
         _check(lib().sgc_batch_tick(self.b, C.byref(r)), "sgc_batch_tick")
+        return r.as_dict()
+
+    def tick_begin(self):
+        """Launches the tick and returns; submits for the next tick may follow."""
+        _check(lib().sgc_batch_tick_begin(self.b), "sgc_batch_tick_begin")
+
+    def tick_end(self):
+        r = TickReport()
+        _check(lib().sgc_batch_tick_end(self.b, C.byref(r)), "sgc_batch_tick_end")
         return r.as_dict()
 
     def close_epochs(self):

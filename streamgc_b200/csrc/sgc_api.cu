@@ -415,6 +415,8 @@ int sgc_destroy(sgc_handle* h) {
         if (h->slot_free[k]) cudaEventDestroy(h->slot_free[k]);
     }
     if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+    if (h->ring_host) cudaFreeHost(h->ring_host);
+    if (h->ring_done) cudaEventDestroy(h->ring_done);
     for (void* p : h->allocs) cudaFree(p);
     if (h->h_stage) cudaFreeHost(h->h_stage);
     if (h->h_small) cudaFreeHost(h->h_small);
@@ -753,6 +755,71 @@ int sgc_apply_staged(sgc_handle* h, int mode) {
     CK(cudaEventRecord(h->slot_free[k], h->stream));
     h->staged--;
     return SGC_OK;
+}
+
+int sgc_ring_create(sgc_handle* h, uint32_t log2_slots) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    if (h->ring_host) return fail(SGC_EINVAL, "the handle already has a ring");
+    if (log2_slots < 10 || log2_slots > 28) return fail(SGC_EINVAL, "log2_slots must be in [10, 28]");
+    CK(cudaSetDevice(h->device));
+    const uint64_t slots = 1ull << log2_slots;
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, slots * sizeof(EdgeUpdate), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SGC_ENOMEM, "pinned mapped ring of %llu slots", (unsigned long long)slots);
+    }
+    void* d = nullptr;
+    if (cudaHostGetDevicePointer(&d, p, 0) != cudaSuccess || cudaEventCreateWithFlags(&h->ring_done, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeHost(p);
+        return fail(SGC_ECUDA, "ring mapping failed");
+    }
+    h->ring_host = static_cast<EdgeUpdate*>(p);
+    h->ring_dev = static_cast<EdgeUpdate*>(d);
+    h->ring_mask = slots - 1;
+    return SGC_OK;
+}
+
+int sgc_ring_push(sgc_handle* h, const EdgeUpdate* ups, uint32_t n, uint32_t* accepted) {
+    if (!h || (n && !ups)) return fail(SGC_EINVAL, "null argument");
+    if (!h->ring_host) return fail(SGC_EINVAL, "no ring (sgc_ring_create)");
+    const uint64_t tail = h->ring_tail.load(std::memory_order_relaxed);
+    const uint64_t free_slots = h->ring_mask + 1 - (tail - h->ring_released.load(std::memory_order_acquire));
+    const uint32_t k = (uint32_t)std::min<uint64_t>(n, free_slots);
+    for (uint32_t i = 0; i < k;) {  // at most two runs of consecutive slots
+        const uint64_t pos = (tail + i) & h->ring_mask;
+        const uint32_t run = (uint32_t)std::min<uint64_t>(k - i, h->ring_mask + 1 - pos);
+        std::memcpy(h->ring_host + pos, ups + i, (size_t)run * sizeof(EdgeUpdate));
+        i += run;
+    }
+    h->ring_tail.store(tail + k, std::memory_order_release);  // the slots are written before they are published
+    if (accepted) *accepted = k;
+    return SGC_OK;
+}
+
+int sgc_ring_apply(sgc_handle* h, uint32_t max_updates, int mode, uint32_t* applied) {
+    if (!h) return fail(SGC_EINVAL, "null handle");
+    if (!h->ring_host) return fail(SGC_EINVAL, "no ring (sgc_ring_create)");
+    if (mode != SGC_MODE_DETERMINISTIC && mode != SGC_MODE_CONCURRENT) return fail(SGC_EINVAL, "bad mode %d", mode);
+    CK(cudaSetDevice(h->device));
+    // slots of the previous gather go back to the producer once it has finished
+    if (h->ring_inflight > h->ring_released.load(std::memory_order_relaxed)) {
+        const cudaError_t q = cudaEventQuery(h->ring_done);
+        if (q == cudaSuccess) h->ring_released.store(h->ring_inflight, std::memory_order_release);
+        else if (q != cudaErrorNotReady) return fail(SGC_ECUDA, "ring: %s", cudaGetErrorString(q));
+    }
+    const uint64_t tail = h->ring_tail.load(std::memory_order_acquire);
+    const uint32_t k = (uint32_t)std::min<uint64_t>({tail - h->ring_head, (uint64_t)max_updates,
+                                                    (uint64_t)h->opt.max_batch});
+    if (applied) *applied = k;
+    if (!k) return SGC_OK;
+    launch_ring_gather(h->ring_dev, h->ring_mask, h->ring_head, k, h->d_batch, h->num_sms, h->stream);
+    h->launches += 1;
+    h->h2d_bytes += (uint64_t)k * sizeof(EdgeUpdate);
+    h->ring_head += k;
+    h->ring_inflight = h->ring_head;
+    CK(cudaEventRecord(h->ring_done, h->stream));
+    return apply_device(h, h->d_batch, k, mode);
 }
 
 int sgc_epoch(sgc_handle* h) {

@@ -65,7 +65,9 @@ struct sgc_batch {
     uint32_t cap = 0;
     // staging
     std::vector<std::vector<EdgeUpdate>> per_graph;  // stream-order mode: grouped by graph
-    EdgeUpdate* h_stage = nullptr;                   // pinned, cap entries
+    EdgeUpdate* h_stage = nullptr;                   // pinned, cap entries: the half being filled
+    EdgeUpdate* h_stage_buf[2] = {nullptr, nullptr}; // two halves: the next tick's updates are staged
+    uint32_t fill = 0;                               // while the current tick's are copied and applied
     uint32_t staged = 0;
     bool close_all = false;
     // per-tick control (device + pinned mirrors)
@@ -228,7 +230,8 @@ int sgc_batch_destroy(sgc_batch* b) {
     if (!b) return SGC_OK;
     if (b->h) cudaSetDevice(b->h->device);
     drop_graph(b);
-    if (b->h_stage) cudaFreeHost(b->h_stage);
+    for (EdgeUpdate* p : b->h_stage_buf)
+        if (p) cudaFreeHost(p);
     if (b->h_dyn) cudaFreeHost(b->h_dyn);
     if (b->h_segs) cudaFreeHost(b->h_segs);
     if (b->h_target) cudaFreeHost(b->h_target);
@@ -350,13 +353,15 @@ int sgc_batch_create(const sgc_batch_graph* graphs, uint32_t count, const sgc_ba
         cudaGetLastError();
         return bail(fail(SGC_ENOMEM, "batch control allocation failed"));
     }
-    if (cudaHostAlloc(&b->h_stage, (size_t)b->cap * sizeof(EdgeUpdate), cudaHostAllocDefault) ||
+    if (cudaHostAlloc(&b->h_stage_buf[0], (size_t)b->cap * sizeof(EdgeUpdate), cudaHostAllocDefault) ||
+        cudaHostAlloc(&b->h_stage_buf[1], (size_t)b->cap * sizeof(EdgeUpdate), cudaHostAllocDefault) ||
         cudaHostAlloc(&b->h_dyn, 16, cudaHostAllocDefault) ||
         cudaHostAlloc(&b->h_segs, ((size_t)count + 1) * 4, cudaHostAllocDefault) ||
         cudaHostAlloc(&b->h_target, count, cudaHostAllocDefault)) {
         cudaGetLastError();
         return bail(fail(SGC_ENOMEM, "batch staging allocation failed"));
     }
+    b->h_stage = b->h_stage_buf[0];
     CK(cudaMemcpyAsync(b->d_hdidx, h->g.hdmap, (size_t)n * 4, cudaMemcpyDeviceToDevice, h->stream));
     CK(cudaMemcpyAsync(b->d_thr, b->thr.data(), (size_t)count * 4, cudaMemcpyHostToDevice, h->stream));
     rethreshold_kernel<<<h->num_sms * 8, 256, 0, h->stream>>>(h->g, const_cast<uint32_t*>(h->g.hdmap), b->d_hdidx,
@@ -386,7 +391,6 @@ uint64_t sgc_batch_pending(const sgc_batch* b) { return b ? b->staged : 0; }
 int sgc_batch_submit(sgc_batch* b, uint32_t graph, const EdgeUpdate* ups, uint32_t n) {
     if (!b || (n && !ups)) return fail(SGC_EINVAL, "null argument");
     if (graph >= b->G) return fail(SGC_EINVAL, "graph %u out of range", graph);
-    if (b->in_tick) return fail(SGC_EINVAL, "submit while a tick runs: end it first");
     if ((uint64_t)b->staged + n > b->cap) return fail(SGC_EINVAL, "tick buffer full (%u updates)", b->cap);
     const uint32_t off = b->voff[graph], lim = b->nv[graph];
     auto translate = [&](const EdgeUpdate& e) {
@@ -466,6 +470,12 @@ int sgc_batch_tick_begin(sgc_batch* b) {
     CK(cudaMemcpyAsync(b->d_dyn, b->h_dyn, 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(b->d_dyn + 2, b->h_dyn + 2, 4, cudaMemcpyHostToDevice, h->stream));
     if (nup) CK(cudaMemcpyAsync(h->d_batch, b->h_stage, (size_t)nup * sizeof(EdgeUpdate), cudaMemcpyHostToDevice, h->stream));
+    // the staged updates are consumed: the next tick's go to the other half (its
+    // copy belonged to the previous tick, which has ended)
+    for (uint32_t k = 0; k < G; k++) b->pending[k] = 0;
+    b->staged = 0;
+    b->fill ^= 1u;
+    b->h_stage = b->h_stage_buf[b->fill];
     CK(cudaMemcpyAsync(b->d_target, b->h_target, G, cudaMemcpyHostToDevice, h->stream));
     h->h2d_bytes += (uint64_t)nup * sizeof(EdgeUpdate) + G + 8;
     const bool prof = (b->flags & SGC_BATCH_PROFILE) != 0;
@@ -526,8 +536,6 @@ int sgc_batch_tick_end(sgc_batch* b, sgc_batch_tick_report* rep) {
                 b->publishes[k]++;
             }
     }
-    for (uint32_t k = 0; k < G; k++) b->pending[k] = 0;
-    b->staged = 0;
     h->updates += nup;
     h->tier1_sweeps += rc.it;
     h->epochs += published;

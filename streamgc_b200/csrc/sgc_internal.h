@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <utility>
+#include <atomic>
 #include <vector>
 
 #include "../../include/streamgc_b200.h"
@@ -88,6 +89,16 @@ struct sgc_handle {
     cudaEvent_t slot_free[2] = {nullptr, nullptr};
     uint32_t slot_n[2] = {0, 0};
     uint32_t stage_next = 0, staged = 0;  // next slot to fill; slots holding a batch (oldest first from stage_next - staged)
+    // ingest ring (sgc_ring_*): pinned, device-mapped slots the GPU copies from itself.
+    // Positions count updates since creation; slot = position & ring_mask.
+    EdgeUpdate* ring_host = nullptr;     // 2^k slots, written by the producer
+    EdgeUpdate* ring_dev = nullptr;      // the same memory as the GPU addresses it
+    uint64_t ring_mask = 0;
+    std::atomic<uint64_t> ring_tail{0};      // producer: positions published (slots written)
+    std::atomic<uint64_t> ring_released{0};  // consumer: positions whose gather has finished
+    uint64_t ring_head = 0;              // consumer: positions gathered (launched)
+    uint64_t ring_inflight = 0;          // consumer: end of the last launched gather
+    cudaEvent_t ring_done = nullptr;     // recorded after the last gather
     // SGC_OPT_GRAPH_PUBLISH: the publish captured once per snapshot half
     cudaGraph_t pub_graph[2] = {nullptr, nullptr};
     cudaGraphExec_t pub_exec[2] = {nullptr, nullptr};

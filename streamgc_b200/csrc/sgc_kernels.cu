@@ -212,6 +212,23 @@ void launch_det_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, cudaStrea
     if (n) det_apply_kernel<<<1, 32, 0, s>>>(g, ups, n);
 }
 
+// The ingest ring's drain: positions [head, head + n) of a host ring of
+// mask + 1 slots, read straight from pinned, device-mapped host memory (16
+// bytes per thread, consecutive slots) into the batch buffer.
+__global__ void ring_gather_kernel(const uint4* __restrict__ ring, unsigned long long mask, unsigned long long head,
+                                   uint32_t n, uint4* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = ring[(head + i) & mask];
+}
+void launch_ring_gather(const EdgeUpdate* ring, uint64_t mask, uint64_t head, uint32_t n, EdgeUpdate* out,
+                        int num_sms, cudaStream_t s) {
+    if (!n) return;
+    uint32_t blk = (n + 255) / 256;
+    if (blk > (uint32_t)num_sms * 4) blk = num_sms * 4;
+    ring_gather_kernel<<<blk, 256, 0, s>>>(reinterpret_cast<const uint4*>(ring), mask, head, n,
+                                           reinterpret_cast<uint4*>(out));
+}
+
 int conc_apply_occupancy() {
     static int occ = 0;
     if (!occ) {

@@ -99,6 +99,8 @@ enum SweepMode : int { SWEEP_REBUILD = 0, SWEEP_TIER1 = 1, SWEEP_INDEP = 2 };
 
 // ---- launchers (sgc_kernels.cu) ----
 void launch_det_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, cudaStream_t s);
+void launch_ring_gather(const EdgeUpdate* ring, uint64_t mask, uint64_t head, uint32_t n, EdgeUpdate* out,
+                        int num_sms, cudaStream_t s);
 void launch_add_check(const Dev& g, const EdgeUpdate* ups, uint32_t n, const uint32_t* dyn, int num_sms,
                       cudaStream_t s);
 void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const EdgeOrder& eo, int num_sms,

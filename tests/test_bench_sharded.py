@@ -60,6 +60,12 @@ class _Batch:
     def tick(self):
         return dict(proper=1, device_ms=0.3)
 
+    def tick_begin(self):
+        pass
+
+    def tick_end(self):
+        return self.tick()
+
     def tuning(self):
         return {"tile": 512}
 

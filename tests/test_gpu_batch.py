@@ -170,3 +170,37 @@ def test_query_reads_the_published_snapshot():
         assert bad[0] == 0
     finally:
         b.close()
+
+
+def test_submits_during_a_tick_stage_the_next_one():
+    """With the tick split (begin / end), the next tick's updates are submitted
+    while the current tick runs; in stream order the snapshots equal those of
+    submit-then-tick."""
+    cases = _cases()
+    T = 8
+    sched = [_ticks(c, T) for c in cases]
+    thr = [c["thr"] for c in cases]
+    a = S.Batch([_graph(c) for c in cases], epoch_sizes=[E] * len(cases), thresholds=thr, stream_order=True)
+    b = S.Batch([_graph(c) for c in cases], epoch_sizes=[E] * len(cases), thresholds=thr, stream_order=True)
+
+    def submit(batch, t):
+        for k in range(len(cases)):
+            part = sched[k][t] if t < len(sched[k]) else None
+            if part is not None and len(part):
+                batch.submit(k, part)
+
+    try:
+        submit(b, 0)
+        for t in range(T):
+            submit(a, t)
+            ra = a.tick()
+            b.tick_begin()
+            if t + 1 < T:
+                submit(b, t + 1)  # staged while tick t runs
+            rb = b.tick_end()
+            assert ra["proper"] == rb["proper"] == 1 and ra["updates"] == rb["updates"]
+            for k in range(len(cases)):
+                assert np.array_equal(a.snapshot(k), b.snapshot(k)), (NAMES[k], t)
+    finally:
+        a.close()
+        b.close()

@@ -5,6 +5,8 @@ base run (exact selection) or sorted never-edited rows, hole counters that
 never wrap, and colors in range; in stream order and in concurrent batches.
 Then the stream-ingest slots against direct applies, and the captured-graph
 publish."""
+import time
+
 import numpy as np
 import pytest
 
@@ -136,3 +138,52 @@ def test_graph_publish_is_proper_and_keeps_invariants(name):
         assert v["violations"] == 0 and v["uncolored_with_edges"] == 0
         st = h.stats()
         assert st["epochs"] >= len(ups) // B and st["tier1_sweeps"] >= st["epochs"]
+
+
+def test_ingest_ring_matches_direct_applies():
+    """A producer thread feeds the stream into a ring smaller than the stream
+    (it wraps around many times; pushes that do not fit are retried); the
+    stepping thread lets the GPU drain it one host batch at a time, in stream
+    order. States, bitmaps and rows equal direct applies of the same batches."""
+    import threading
+    c = MG.build_case("rmat11")
+    ups = np.concatenate([c["init"], c["bench"]])
+    batch = 2048
+    g = S.Graph(c["rp"], c["col"], c["deg"])
+    with S.StreamGC(g, epoch_size=c["E"], histogram_threshold=c["thr"], max_batch=batch) as a, \
+            S.StreamGC(g, epoch_size=c["E"], histogram_threshold=c["thr"], max_batch=batch) as b:
+        b.ring_create(12)  # 4,096 slots
+        done = threading.Event()
+
+        def produce():
+            pos = 0
+            while pos < len(ups):
+                k = b.ring_push(ups[pos:pos + 3000])
+                pos += k
+                if k == 0:
+                    time.sleep(0.0002)
+            done.set()
+
+        th = threading.Thread(target=produce)
+        th.start()
+        applied = 0
+        for s0 in range(0, len(ups), batch):
+            part = ups[s0:s0 + batch]
+            a.apply(part, S.MODE_DETERMINISTIC)
+            got = 0
+            while got < len(part):
+                k = b.ring_apply(len(part) - got, S.MODE_DETERMINISTIC)
+                if k == 0:
+                    time.sleep(0.0002)
+                got += k
+            assert got == len(part)
+            applied += got
+            if (s0 // batch) % 4 == 3:
+                a.epoch()
+                b.epoch()
+        th.join(30)
+        assert done.is_set() and applied == len(ups)
+        assert b.ring_apply(batch, S.MODE_DETERMINISTIC) == 0
+        for name in ("states", "bitmaps", "col", "hist"):
+            assert np.array_equal(getattr(a, name)(), getattr(b, name)()), name
+        assert b.stats()["h2d_bytes"] >= 16 * len(ups)
