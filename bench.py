@@ -63,6 +63,32 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def shared_workload(dist, rank, kind, stream_len, large_div):
+    """Replicas on one node: rank 0 generates the workload and writes its
+    arrays to /dev/shm; the other ranks map them read-only after a barrier.
+    Returns the workload and the files to remove once every rank built its
+    handle."""
+    import streamgc_b200 as S
+    tag = f"/dev/shm/sgc_{kind}_{large_div}_{os.environ.get('MASTER_PORT', '0')}"
+    names = ["row_ptr", "col_idx", "degree", "stream"]
+    if rank == 0:
+        g, init, bench, desc = build_workload(kind, stream_len, large_div)
+        for nm, arr in zip(names, [g.row_ptr, g.col_idx, g.degree, bench]):
+            arr.tofile(f"{tag}_{nm}")
+        with open(f"{tag}_desc.json", "w") as f:
+            json.dump(desc, f)
+    dist.barrier()
+    if rank != 0:
+        rp = np.memmap(f"{tag}_row_ptr", dtype=np.uint64, mode="r")
+        col = np.memmap(f"{tag}_col_idx", dtype=np.uint32, mode="r")
+        deg = np.memmap(f"{tag}_degree", dtype=np.uint32, mode="r")
+        g = S.Graph(rp, col, deg)
+        bench = np.fromfile(f"{tag}_stream", dtype=S.EDGE_UPDATE)
+        desc = json.load(open(f"{tag}_desc.json"))
+        init = None
+    return g, init, bench, desc, [f"{tag}_{nm}" for nm in names] + [f"{tag}_desc.json"]
+
+
 def build_workload(kind, stream_len, large_div=1):
     import streamgc_b200 as S
     t = time.time()
@@ -225,7 +251,11 @@ def run_ours(a):
     nbatch = a.warmup + 2 * a.steps + a.cpu_batches + a.latency_epochs
     base_len = {"skewed": 2_000_000, "small": 1_000_000, "large": 10_000_000}[a.workload]
     stream_len = max(base_len, nbatch * E)
-    g, init, bench, desc = build_workload(a.workload, stream_len, a.large_div)
+    if dist and a.workload == "large":  # one copy of the 1.8 G-edge graph in host memory for all ranks
+        g, init, bench, desc, shm = shared_workload(dist, rank, a.workload, stream_len, a.large_div)
+    else:
+        g, init, bench, desc = build_workload(a.workload, stream_len, a.large_div)
+        shm = []
 
     t = time.time()
     # no periodic full repair: every published snapshot is checked by the validator instead.
@@ -241,6 +271,11 @@ def run_ours(a):
     t2 = time.time()
     rep = h.publish()
     h.synchronize()
+    if shm:  # every rank's handle holds its own copy now
+        dist.barrier()
+        if rank == 0:
+            for f in shm:
+                os.remove(f)
     log(f"init colored on GPU in {time.time() - t:.1f}s (handle {t1 - t:.1f}s, core of {core} vertices "
         f"{t2 - t1:.1f}s, full repair {time.time() - t2:.1f}s): {rep}")
     if not rep["proper"]:

@@ -200,7 +200,7 @@ def _small_specs(count, seed=42, **k):
             for i in range(count)]
 
 
-def _rank(rank, world, port, form, q):
+def _rank(rank, world, port, form, q, workload="small", large_div=1):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
                       LOCAL_RANK="0", SGC_DIST_BACKEND="gloo")
     import types
@@ -225,9 +225,9 @@ def _rank(rank, world, port, form, q):
                                 real_rmat(min(scale, 10), min(ef, 8), a, b, c, seed))
     args = types.SimpleNamespace(gpus=world, steps=2, warmup=3, batch_graphs=6, autotune=False, served_rate=2e5,
                                  served_seconds=0.3, served_staleness_us=2000, served_check=False,
-                                 served_regrow=False, sorted_rows=False, workload="small", cpu_batches=0,
+                                 served_regrow=False, sorted_rows=False, workload=workload, cpu_batches=0,
                                  cpu_seconds=1.0, profile_window=False, graph_publish=False, ingest=False,
-                                 latency_epochs=4, validate_steps=True, large_div=1,
+                                 latency_epochs=4, validate_steps=True, large_div=large_div,
                                  full_repair_every=0, profile_full_sweep=True)
     out, err = io.StringIO(), None
     old = sys.stdout
@@ -275,3 +275,28 @@ def test_two_ranks_share_the_work(form):
         assert line["config"]["vertices"] == sum(s["n"] for s in specs)
     else:
         assert line["config"]["vertices"] == sum(s["n"] for s in specs) + (1 << 22)  # the R-MAT 2^22 tenant's spec
+
+
+@pytest.mark.timeout(600)
+def test_replicas_share_one_host_copy_of_the_large_graph():
+    """Replicas of the large workload (here scaled down): rank 0 generates it
+    and shares the arrays through /dev/shm, the other rank maps them; the
+    files are gone once both handles exist."""
+    import glob
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, "plain", q, "large", 8192)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = {}
+    for _ in procs:
+        r, text, err = q.get(timeout=540)
+        got[r] = (text, err)
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    assert got[0][1] is None and got[1][1] is None, (got[0][1], got[1][1])
+    line = [json.loads(l) for l in got[0][0].splitlines() if l.startswith("{")][0]
+    assert line["config"]["workload"] == "chunglu65m_div8192_churn" and line["n_gpus"] == 2
+    assert not glob.glob(f"/dev/shm/sgc_large_8192_{port}_*")
