@@ -120,10 +120,20 @@ int set_clean(sgc_handle* h, uint32_t v) {
     return SGC_OK;
 }
 
+// Writes the back half of the snapshot and makes it the front. With
+// incremental snapshots only the colors changed in the last two epochs are
+// copied (plus a full copy while snap_full says so).
 void publish_snapshot(sgc_handle* h) {
     const int back = 1 - h->front;
-    launch_snapshot(h->g, h->snap[back], h->stream);
-    h->launches += 1;
+    if (h->g.chg) {
+        launch_snapshot_changes(h->g, h->chg_prev, h->snap[back], h->stream);
+        h->launches += 1;
+    }
+    if (!h->g.chg || h->snap_full > 0) {
+        launch_snapshot(h->g, h->snap[back], h->stream);
+        h->launches += 1;
+        if (h->snap_full > 0) h->snap_full--;
+    }
     h->front = back;
 }
 
@@ -319,7 +329,8 @@ int capture_publish_impl(sgc_handle* h, int back) {
     cudaGraph_t g1 = nullptr;
     CK(cudaStreamEndCapture(s, &g1));
     CK(cudaStreamBeginCaptureToGraph(s, graph, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
-    launch_snapshot(h->g, h->snap[back], s);
+    if (h->g.chg) launch_snapshot_changes(h->g, h->chg_prev, h->snap[back], s);
+    else launch_snapshot(h->g, h->snap[back], s);
     cudaMemcpyAsync(h->h_rc_out, h->sb.rc, sizeof(RepairCtl), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(h->h_small + 32, h->sb.swept, 16, cudaMemcpyDeviceToHost, s);
     cudaGraph_t g2 = nullptr;
@@ -361,9 +372,10 @@ int publish_graph(sgc_handle* h, sgc_repair_report* rep) {
     h->d2h_bytes += sizeof(RepairCtl) + 16;
     sgc_repair_report r{};
     TRY(finish_repair(h, &r));
-    if (r.tier2_ran) {  // Tier-2 changed colors after the graph's snapshot: take it again
-        launch_snapshot(h->g, h->snap[back], h->stream);
+    if (r.tier2_ran || (h->g.chg && h->snap_full > 0)) {  // Tier-2 changed colors after the graph's
+        launch_snapshot(h->g, h->snap[back], h->stream);      // snapshot, or a full one is due: take it again
         h->launches += 1;
+        if (h->snap_full > 0) h->snap_full--;
     }
     h->front = back;
     h->epochs++;
@@ -631,6 +643,12 @@ int sgci::create_internal(const StreamGCConfig* cfg, const sgc_options* opt_in, 
     sb.G = G;
     if (g.exact) A(&g.touched, (n + 31) / 32 + 1, 0);
     else g.touched = nullptr;
+    if (g.exact && G == 1) {  // incremental snapshots (a batched handle publishes per graph)
+        A(&g.chg, (n + 31) / 32 + 1, 0);
+        A(&h->chg_prev, (n + 31) / 32 + 1, 0);
+    } else {
+        g.chg = nullptr;
+    }
     if (g.exact) {  // base runs: rows whose base entries are strictly ascending
         std::vector<uint32_t> bl(n);
         for (uint32_t x = 0; x < n; x++) bl[x] = (edited[x >> 5] >> (x & 31)) & 1u ? 0u : hw[x];
@@ -1033,7 +1051,7 @@ int sgc_upload(sgc_handle* h, int what, const void* src, uint64_t bytes) {
     void* dst = nullptr;
     uint64_t need = 0;
     switch (what) {
-        case SGC_DL_STATES: dst = h->g.st; need = h->n * 4ull; break;
+        case SGC_DL_STATES: dst = h->g.st; need = h->n * 4ull; h->snap_full = 2; break;
         case SGC_DL_BITMAPS: dst = h->g.bm; need = h->n * 8ull; break;
         case SGC_DL_HIST: dst = h->g.hist; need = (uint64_t)h->hist_rows * h->maxc * 4; break;
         default: return fail(SGC_EINVAL, "upload target %d not writable", what);

@@ -94,6 +94,8 @@ struct Dev {
                                    // starts from (null otherwise): every vertex whose color changed, every
                                    // bitmap-class endpoint of an update (its bitmap is rebuilt), and both
                                    // endpoints of an ADD whose colors are equal at the end of its batch
+    uint32_t* chg;                 // single-graph handles under exact selection: bitmask of the vertices
+                                   // whose color changed since the last snapshot (null otherwise)
     GraphCtl* gctl;                // per graph: repair flags (one entry for a single-graph handle)
     const uint32_t* gidw;          // graph of each 32-vertex word (graphs start at multiples of 32);
                                    // null: one graph
@@ -223,9 +225,11 @@ __device__ __forceinline__ bool warp_gather_each(const uint32_t* col, uint64_t s
     return false;
 }
 
+// Marks are fire-and-forget reductions (their results unused): the warp does
+// not wait for them on the update path.
 __device__ __forceinline__ void mark_dirty(const Dev& g, uint32_t x) {
     atomicOr(g.dirty + (x >> 5), 1u << (x & 31));
-    if (!(ld_cg(g.edited + (x >> 5)) & (1u << (x & 31)))) atomicOr(g.edited + (x >> 5), 1u << (x & 31));
+    atomicOr(g.edited + (x >> 5), 1u << (x & 31));
 }
 __device__ __forceinline__ uint32_t graph_of(const Dev& g, uint32_t x) { return g.gidw ? __ldg(g.gidw + (x >> 5)) : 0u; }
 // Row x's high-water mark, at most the row's capacity. The mark never
@@ -259,7 +263,11 @@ __device__ __forceinline__ void extend_row(const Dev& g, uint32_t x, uint32_t q)
 }
 
 __device__ __forceinline__ void mark_touched(const Dev& g, uint32_t x) {
-    if (g.touched && !(ld_cg(g.touched + (x >> 5)) & (1u << (x & 31)))) atomicOr(g.touched + (x >> 5), 1u << (x & 31));
+    if (g.touched) atomicOr(g.touched + (x >> 5), 1u << (x & 31));
+}
+// Every write of a state word notes the vertex for the next incremental snapshot.
+__device__ __forceinline__ void note_color(const Dev& g, uint32_t x) {
+    if (g.chg) atomicOr(g.chg + (x >> 5), 1u << (x & 31));
 }
 
 __device__ __forceinline__ void flag_asym(const Dev& g, uint32_t x) {
@@ -603,16 +611,20 @@ __device__ __forceinline__ uint16_t warp_fac(const Dev& g, uint32_t x, const uin
 
 // ---------------- incremental bitmap / histogram (color_select.cuh:120-209) ----------------
 
-// Sets color c's bit (1..64) of x's bitmap; a bit already set is left alone
-// (bits are only cleared by rebuilds, which never overlap an apply).
+// Sets color c's bit (1..64) of x's bitmap. With READ_FIRST a bit already set
+// is left alone (bits are only cleared by rebuilds, which never overlap an
+// apply): the recolor walk sets one bit in every neighbor's bitmap, most of
+// them already set. Otherwise a fire-and-forget reduction: one vertex on the
+// update path, where the warp should not wait.
+template <bool READ_FIRST>
 __device__ __forceinline__ void set_bm_bit(const Dev& g, uint32_t x, uint16_t c) {
     const unsigned long long bit = 1ull << (c - 1);
-    if (!(ld_cg(g.bm + x) & bit)) atomicOr((unsigned long long*)(g.bm + x), bit);
+    if (!READ_FIRST || !(ld_cg(g.bm + x) & bit)) atomicOr((unsigned long long*)(g.bm + x), bit);
 }
 
 __device__ __forceinline__ void nbr_color_change(const Dev& g, uint32_t x, uint16_t oldc, uint16_t newc) {
     if (oldc == newc) return;
-    if (newc != 0 && newc <= 64) set_bm_bit(g, x, newc);
+    if (newc != 0 && newc <= 64) set_bm_bit<true>(g, x, newc);
     const uint32_t hd = __ldg(g.hdmap + x);
     if (hd != EMPTY && !g.exact) {
         uint32_t* h = g.hist + (uint64_t)hd * g.maxc;
@@ -622,7 +634,7 @@ __device__ __forceinline__ void nbr_color_change(const Dev& g, uint32_t x, uint1
 }
 __device__ __forceinline__ void new_nbr(const Dev& g, uint32_t x, uint16_t c) {
     if (c == 0) return;
-    if (c <= 64) set_bm_bit(g, x, c);
+    if (c <= 64) set_bm_bit<false>(g, x, c);
     const uint32_t hd = __ldg(g.hdmap + x);
     if (hd != EMPTY && !g.exact && c <= g.maxc) atomicAdd(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
 }
@@ -663,7 +675,10 @@ __device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x, uint16_t 
         newc = warp_fac(g, x, g.st);
         if (newc == color_of(cur)) return;
     }
-    if (lane_id() == 0) mark_touched(g, x);
+    if (lane_id() == 0) {
+        mark_touched(g, x);
+        note_color(g, x);
+    }
     const uint16_t oldc = color_of(cur);
     const uint64_t s = g.rp[x], e = live_end(g, x, s);
     warp_for_each(g.col, s, e, [&](uint64_t, uint32_t ng) {
@@ -681,13 +696,25 @@ __device__ __forceinline__ bool warp_color_held(const Dev& g, uint32_t x, uint16
     return warp_gather_each<true, 1>(g.col, s, e, g.n, g.st, [c](uint32_t, uint32_t w) { return color_of(w) == c; });
 }
 
+// Both endpoints' state words in one round trip (lanes 0 and 1).
+__device__ __forceinline__ void warp_load_states2(const Dev& g, uint32_t u, uint32_t v, uint32_t& su, uint32_t& sv) {
+    const uint32_t lane = lane_id();
+    uint32_t w = 0;
+    if (lane < 2) w = ld_cg(g.st + (lane ? v : u));
+    su = __shfl_sync(FULL, w, 0);
+    sv = __shfl_sync(FULL, w, 1);
+}
+
 // try_color_reduction: after a delete freed `freed`, move to a lower color if one is open.
 // `stream_order` false (a concurrent batch) with exact selection on a row above
 // the threshold: instead of the full first-free scan, x moves to `freed` when no
 // live neighbor holds it any more (an early-exit scan; the full scan of a
 // high-degree row would almost always confirm the current color).
-__device__ __forceinline__ void warp_try_reduce(const Dev& g, uint32_t x, uint16_t freed, bool stream_order) {
-    const uint16_t cur = color_of(warp_load_state(g, x));
+// `state` is x's state word as the caller last read it (in stream order
+// nothing else changes it before this call; concurrently, a recolor re-reads it).
+__device__ __forceinline__ void warp_try_reduce(const Dev& g, uint32_t x, uint16_t freed, bool stream_order,
+                                                uint32_t state) {
+    const uint16_t cur = color_of(state);
     if (cur == 0) return;
     if (freed >= cur) return;
     if (!stream_order && g.exact && __ldg(g.hdmap + x) != EMPTY) {
@@ -698,14 +725,24 @@ __device__ __forceinline__ void warp_try_reduce(const Dev& g, uint32_t x, uint16
     if (best < cur) warp_recolor(g, x, best);
 }
 
-// Colors x with FAC when it is still uncolored; version becomes 1
-// (local_update.cu:90-101). Returns the color x holds afterwards.
-__device__ __forceinline__ void warp_color_if_uncolored(const Dev& g, uint32_t x) {
-    const uint32_t cur = warp_load_state(g, x);
-    if (color_of(cur) != 0) return;
+// Colors x, read uncolored as state word `cur`, with FAC; version becomes 1
+// (local_update.cu:90-101). Returns x's state word afterwards (another warp's
+// color if it got there first).
+__device__ __forceinline__ uint32_t warp_color_uncolored(const Dev& g, uint32_t x, uint32_t cur) {
     const uint16_t c = warp_fac(g, x, g.st);
-    if (lane_id() == 0 && atomicCAS(g.st + x, cur, pack(c, 1)) == cur) mark_touched(g, x);
-    __syncwarp();
+    uint32_t got = 0;
+    if (lane_id() == 0) {
+        const uint32_t want = pack(c, 1);
+        const uint32_t old = atomicCAS(g.st + x, cur, want);
+        if (old == cur) {
+            mark_touched(g, x);
+            note_color(g, x);
+            got = want;
+        } else {
+            got = old;
+        }
+    }
+    return __shfl_sync(FULL, got, 0);
 }
 
 // ---------------- one update (local_update.cu:61-147) ----------------
@@ -721,30 +758,39 @@ __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v,
         if (__ldg(g.hdmap + u) == EMPTY) mark_touched(g, u);
         if (__ldg(g.hdmap + v) == EMPTY) mark_touched(g, v);
     }
+    // The state words are read once, after the row edits, and kept: in stream
+    // order only this warp changes them, so the reference's re-reads give the
+    // same values; in a concurrent batch a later change by another warp is a
+    // color change (marked) or leaves this ADD's endpoints equal (caught by
+    // the check after the batch).
     if (type == SGC_UPDATE_ADD) {
         const int ru = warp_add_slot(g, u, v, exact);
         const int rv = warp_add_slot(g, v, u, exact);
         if (ru != rv && lane_id() == 0) flag_asym(g, u);
-        warp_color_if_uncolored(g, u);
-        if (color_of(warp_load_state(g, v)) == 0) {
-            if (lane_id() == 0) new_nbr(g, v, color_of(ld_cg(g.st + u)));
+        uint32_t su, sv;
+        warp_load_states2(g, u, v, su, sv);
+        if (color_of(su) == 0) {
+            su = warp_color_uncolored(g, u, su);
+            if (v == u) sv = su;
+        }
+        if (color_of(sv) == 0) {
+            if (lane_id() == 0) new_nbr(g, v, color_of(su));
             __syncwarp();
-            warp_color_if_uncolored(g, v);
+            sv = warp_color_uncolored(g, v, sv);
         }
-        if (lane_id() == 0) {
-            new_nbr(g, u, color_of(ld_cg(g.st + v)));
-            new_nbr(g, v, color_of(ld_cg(g.st + u)));
-        }
+        if (lane_id() == 0) new_nbr(g, u, color_of(sv));
+        else if (lane_id() == 1) new_nbr(g, v, color_of(su));
         __syncwarp();
-        const uint16_t cu = color_of(warp_load_state(g, u));
-        const uint16_t cv = color_of(warp_load_state(g, v));
+        const uint16_t cu = color_of(su), cv = color_of(sv);
         if (cu == cv && cu != 0) {
             const uint32_t loser = prio_less(__ldg(g.deg + u), u, __ldg(g.deg + v), v) ? u : v;
             warp_recolor(g, loser);
         }
     } else if (type == SGC_UPDATE_DEL) {
-        const uint16_t fu = color_of(warp_load_state(g, v));
-        const uint16_t fv = color_of(warp_load_state(g, u));
+        uint32_t su, sv;
+        warp_load_states2(g, u, v, su, sv);
+        const uint16_t fu = color_of(sv);
+        const uint16_t fv = color_of(su);
         const bool du = warp_remove_slot(g, u, v, exact);
         const bool dv = warp_remove_slot(g, v, u, exact);
         if (lane_id() == 0) {
@@ -753,8 +799,9 @@ __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v,
             removed_nbr(g, v, fv);
         }
         __syncwarp();
-        warp_try_reduce(g, u, fu, exact);
-        warp_try_reduce(g, v, fv, exact);
+        warp_try_reduce(g, u, fu, exact, su);
+        if (v == u) sv = warp_load_state(g, v);
+        warp_try_reduce(g, v, fv, exact, sv);
     }
 }
 

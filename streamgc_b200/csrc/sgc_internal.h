@@ -62,6 +62,11 @@ struct sgc_handle {
     sgci::Ctl* ctl = nullptr;
     uint16_t* snap[2] = {nullptr, nullptr};
     int front = 0;
+    // incremental snapshots (g.chg set): the marks of the epoch before, and how
+    // many more snapshots must be written in full (both halves once at first,
+    // again after states were uploaded)
+    uint32_t* chg_prev = nullptr;
+    int snap_full = 2;
     EdgeUpdate* d_batch = nullptr;
     EdgeUpdate* h_stage = nullptr;  // pinned staging for pageable inputs
     cudaEvent_t stage_free = nullptr;

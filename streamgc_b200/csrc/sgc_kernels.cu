@@ -498,6 +498,33 @@ __global__ void snapshot_kernel(Dev g, uint16_t* snap) {
     for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < g.n; x += gridDim.x * blockDim.x)
         snap[x] = color_of(g.st[x]);
 }
+// Incremental snapshot into the back half, which was last written two
+// snapshots ago: the colors of the vertices noted since then (`chg`, this
+// epoch's, and `prev`, the epoch before) are copied from the state words;
+// then this epoch's marks become `prev` and `chg` starts empty.
+__global__ void snapshot_changes_kernel(Dev g, uint32_t* __restrict__ prev, uint16_t* __restrict__ snap) {
+    const uint32_t nw = (g.n + 31) / 32;
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += gridDim.x * blockDim.x) {
+        const uint32_t cur = g.chg[w], old = prev[w];
+        if (cur | old) {
+            prev[w] = cur;
+            if (cur) g.chg[w] = 0;
+        }
+        uint32_t bits = cur | old;
+        while (bits) {
+            const uint32_t x = w * 32 + (__ffs(bits) - 1);
+            bits &= bits - 1;
+            snap[x] = color_of(g.st[x]);
+        }
+    }
+}
+void launch_snapshot_changes(const Dev& g, uint32_t* prev, uint16_t* snap, cudaStream_t s) {
+    const uint32_t nw = (g.n + 31) / 32;
+    uint32_t blk = (nw + 255) / 256;
+    if (blk > 148 * 8) blk = 148 * 8;
+    snapshot_changes_kernel<<<blk, 256, 0, s>>>(g, prev, snap);
+}
+
 void launch_snapshot(const Dev& g, uint16_t* snap, cudaStream_t s) {
     snapshot_kernel<<<(g.n + 255) / 256 < 148 * 16 ? (g.n + 255) / 256 : 148 * 16, 256, 0, s>>>(g, snap);
 }
@@ -539,6 +566,7 @@ __global__ void __launch_bounds__(1024) color_list_kernel(Dev g, const uint32_t*
             }
             if (tid == 0) {
                 g.st[v] = pack((uint16_t)c, 1);
+                note_color(g, v);
                 done++;
             }
         }
@@ -717,6 +745,31 @@ __global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b, in
 // One vertex of the finalize pass (warp-collective: every lane calls it; `valid`
 // lanes own a vertex). Short rows are swept here directly; long rows read the
 // accumulators. REBUILD writes bitmaps; TIER1 and INDEP also decide.
+// The vertex ids of a row of at most SWEEP_TINY live slots starting at slot s
+// (any alignment), INV where no vertex: the covering 16-byte chunks are loaded
+// in one round (aligned, inside the slab: chunks past the live slots are not
+// loaded), then the row's neighbor states in a second round, instead of one
+// dependent load-then-gather per slot.
+constexpr int kTinyChunks = (SWEEP_TINY + 3) / 4 + 1;
+__device__ __forceinline__ void tiny_row(const Dev& g, uint64_t s, uint32_t len, uint32_t (&y)[4 * kTinyChunks],
+                                         uint32_t (&w)[4 * kTinyChunks]) {
+    const uint64_t e = s + len, base = s & ~3ull;
+#pragma unroll
+    for (int c = 0; c < kTinyChunks; c++) {
+        const uint64_t i = base + 4ull * c;
+        uint4 q = make_uint4(INV, INV, INV, INV);
+        if (i < e) q = __ldg(reinterpret_cast<const uint4*>(g.col + i));
+        const uint32_t v[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const uint64_t p = i + t;
+            y[4 * c + t] = (p >= s && p < e && v[t] < g.n) ? v[t] : INV;
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < 4 * kTinyChunks; t++) w[t] = y[t] != INV ? __ldg(g.st + y[t]) : 0u;
+}
+
 __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, int mode, bool valid, uint32_t x,
                                              bool with_sym, bool push) {
     bool fac_needed = false, pend = false, need = false;
@@ -735,14 +788,16 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
         bool conf = false;
         live = len;
         if (len <= SWEEP_TINY) {
-            const uint64_t s = g.rp[x];
             const uint32_t mydeg = (g.abl & ABL_LIVE_DEG) ? len : __ldg(g.deg + x);
             uint32_t lo = 0, hi = 0;
-            for (uint32_t j = 0; j < len; j++) {
-                const uint32_t ng = __ldg(g.col + s + j);
-                if (ng >= g.n) continue;
+            uint32_t y[4 * kTinyChunks], sw[4 * kTinyChunks];
+            tiny_row(g, g.rp[x], len, y, sw);
+#pragma unroll
+            for (int t = 0; t < 4 * kTinyChunks; t++) {
+                const uint32_t ng = y[t];
+                if (ng == INV) continue;
                 if (with_sym && ng != x) sym += sym_term(x, ng);
-                const uint32_t nc = color_of(__ldg(g.st + ng));
+                const uint32_t nc = color_of(sw[t]);
                 add_color_bit(nc, lo, hi);
                 if (nc == myc && nc != 0) {
                     if (prio_less(mydeg, x, __ldg(g.deg + ng), ng)) conf = true;
@@ -981,6 +1036,7 @@ __global__ void sweep_commit_kernel(Dev g, SweepBufs b, int mode) {
         const uint32_t x = b.pend_v[k];
         const uint32_t nw = b.pend_w[k];
         g.st[x] = nw;
+        note_color(g, x);
         b.needf[x] = 0;
         atomicOr(b.rbits + (x >> 5), 1u << (x & 31));
         if (!incr) atomicOr(b.wmark + (x >> 5), 1u << (x & 31));

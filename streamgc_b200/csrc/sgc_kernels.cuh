@@ -144,6 +144,7 @@ void launch_repair_step(const Dev& g, const SweepBufs& b, int num_sms, cudaStrea
                         const cudaGraphConditionalHandle* cond);
 void launch_query(const uint16_t* snap, uint32_t n, const uint32_t* v, uint16_t* out, uint32_t k, cudaStream_t s);
 void launch_color_list(const Dev& g, const uint32_t* list, uint32_t m, uint32_t* colored, cudaStream_t s);
+void launch_snapshot_changes(const Dev& g, uint32_t* prev, uint16_t* snap, cudaStream_t s);
 void launch_colors(const Dev& g, uint16_t* out, cudaStream_t s);
 
 // Tier-2 (sgc_tier2.cu)

@@ -133,6 +133,7 @@ __device__ __forceinline__ void greedy_color(const Dev& g, uint32_t v, const uns
         const uint32_t w = ld_cg(g.st + v);
         if (c != 0 && c != color_of(w)) {
             g.st[v] = pack((uint16_t)c, (uint16_t)(version_of(w) + 1));
+            note_color(g, v);
             atomicAdd(fixed, 1u);
         }
     }

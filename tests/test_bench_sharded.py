@@ -153,6 +153,12 @@ class _PlainHandle:
     def validate(self):
         return dict(violations=0, uncolored_with_edges=0, max_color=12, edges=1, out_of_range=0)
 
+    def snapshot(self):
+        return np.zeros(self.n, np.uint16)
+
+    def colors(self):
+        return np.zeros(self.n, np.uint16)
+
     def close(self):
         pass
 

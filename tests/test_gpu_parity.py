@@ -205,6 +205,7 @@ def test_concurrent_mode_publishes_proper_snapshots(name, exact):
                 rep = h.publish()
                 assert rep["proper"] == 1
                 snap = h.snapshot()
+                assert np.array_equal(snap, h.colors())  # the published half holds the current colors
                 v = O.validate_colors(h.row_ptr(), h.col(), snap)
                 assert v["violations"] == 0 and v["uncolored_with_edges"] == 0
         g.process_stream_repaired(c["bench"], c["E"], c["batch"])
