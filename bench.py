@@ -364,7 +364,13 @@ def run_ours(a):
     # one full repair after the run (every vertex swept; not in any timed figure): the
     # sweep kernels' bandwidth over the whole graph, and a last properness check
     fs0 = h.stats()
+    if a.profile_full_sweep and a.profile_full_sweep_window:
+        h.synchronize()
+        torch.cuda.profiler.start()
     full_rep = h.repair() if a.profile_full_sweep else None
+    if a.profile_full_sweep and a.profile_full_sweep_window:
+        h.synchronize()
+        torch.cuda.profiler.stop()
     fs1 = h.stats()
     total_ms = sum(step_ms)
     if dist:
@@ -1036,6 +1042,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--profile-window", action="store_true",
                     help="bracket the device-timed steps with cudaProfilerStart/Stop (for ncu)")
+    ap.add_argument("--profile-full-sweep-window", action="store_true",
+                    help="bracket the full repair after the run with cudaProfilerStart/Stop instead (for ncu)")
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "served"],
                     help="plain: one graph (the headline); batched: many graphs per tick; served: request loop")
     ap.add_argument("--batch-graphs", type=int, default=256)

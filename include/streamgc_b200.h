@@ -117,6 +117,9 @@ typedef struct sgc_stats {
     uint64_t kernel_launches;    /* kernels launched by this handle */
     uint64_t h2d_bytes;          /* update bytes copied host -> device by sgc_apply */
     uint64_t d2h_bytes;          /* bytes the library read back (repair counters, stats) */
+    uint64_t hub_deferred;       /* row-scale operations of concurrent batches (color reductions and
+                                    recolors of rows longer than 512 live entries) finished by the
+                                    block-wide pass after the batch (cumulative) */
 } sgc_stats;
 
 typedef struct sgc_validation {
@@ -132,7 +135,7 @@ typedef struct sgc_validation {
 #define SGC_STATE_TAIL   0x2u   /* a slot at or past the high-water mark that is not free */
 #define SGC_STATE_ID     0x4u   /* an entry naming a vertex >= n */
 #define SGC_STATE_RUN    0x8u   /* sorted prefix (base run / never-edited row) not strictly ascending */
-#define SGC_STATE_HOLES  0x10u  /* hole counter above the row's extent (wrapped below zero) */
+#define SGC_STATE_HOLES  0x10u  /* live-entry count differs from the row's live slots */
 #define SGC_STATE_COLOR  0x20u  /* a color above 2048 */
 
 typedef struct sgc_state_report {
@@ -154,7 +157,7 @@ typedef struct sgc_state_report {
 #define SGC_DL_HDMAP     8   /* uint32[n] histogram row or 0xFFFFFFFF */
 #define SGC_DL_OVERFLOW  9   /* OverflowEdge[min(overflow_pending, 262144)] */
 #define SGC_DL_BASE_RUN 10   /* uint32[n] length of each row's sorted base run (exact selection), else zeros */
-#define SGC_DL_HOLES    11   /* uint32[n] free slots below each row's mark (exact selection), else zeros */
+#define SGC_DL_HOLES    11   /* uint32[n] free slots and tombstones below each row's mark (exact selection), else zeros */
 
 /* Fills defaults: slack 300, 1024 histogram colors, batch 32768, device 0. */
 int sgc_default_options(sgc_options* opt);

@@ -535,8 +535,8 @@ int sgci::create_internal(const StreamGCConfig* cfg, const sgc_options* opt_in, 
     h->hist_rows = hist_rows;
     uint32_t* d_deg; A(&d_deg, n);
     A(&g.hw, n);
-    if (g.exact) A(&g.holes, n, 0);  // lazy compaction goes with the concurrent configuration
-    else g.holes = nullptr;
+    if (g.exact) A(&g.live, n);  // lazy compaction goes with the concurrent configuration
+    else g.live = nullptr;
     A(&g.dirty, (n + 31) / 32 + 1, 0);
     A(&g.edited, (n + 31) / 32 + 1, 0);
     A(&g.ovf, OVF_CAP);
@@ -577,6 +577,7 @@ int sgci::create_internal(const StreamGCConfig* cfg, const sgc_options* opt_in, 
         cudaMemcpyAsync(d_hdmap, hdmap.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) ||
         cudaMemcpyAsync(d_deg, degree, (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) ||
         cudaMemcpyAsync(g.hw, hw.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h->stream) ||
+        (g.live && cudaMemcpyAsync(g.live, hw.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h->stream)) ||
         cudaMemcpyAsync(g.edited, edited.data(), edited.size() * 4, cudaMemcpyHostToDevice, h->stream))
         return bail(fail(SGC_ECUDA, "upload failed"));
     // base entries: staged through a temporary device copy of the base CSR
@@ -615,6 +616,12 @@ int sgci::create_internal(const StreamGCConfig* cfg, const sgc_options* opt_in, 
     A(&eo.tsucc, mb);
     eo.ticket = &h->ctl->ticket;
     eo.tmask = tsize - 1;
+    if (g.exact) {  // row-scale operations of concurrent batches: the pass after the batch
+        A(&g.hub_ops, 2ull * mb);
+        g.hub_count = &h->ctl->hub_count;
+        g.hub_cap = 2 * mb;
+        g.hub_total = &h->ctl->hub_total;
+    }
     // sweep buffers
     SweepBufs& sb = h->sb;
     const uint64_t icap = h->total_slots / SWEEP_CH_MIN + (uint64_t)n + 1;
@@ -1007,17 +1014,30 @@ int sgc_download(sgc_handle* h, int what, void* dst, uint64_t bytes) {
         case SGC_DL_SNAPSHOT: src = h->snap[h->front]; need = h->n * 2ull; break;
         case SGC_DL_HIGHWATER: src = h->g.hw; need = h->n * 4ull; break;
         case SGC_DL_HDMAP: src = h->g.hdmap; need = h->n * 4ull; break;
-        case SGC_DL_BASE_RUN:
-        case SGC_DL_HOLES: {
-            uint32_t* a = what == SGC_DL_BASE_RUN ? h->g.blen : h->g.holes;
+        case SGC_DL_BASE_RUN: {
             need = h->n * 4ull;
             if (bytes < need) return fail(SGC_EINVAL, "download target %d needs %llu bytes", what, (unsigned long long)need);
-            if (!a) {
+            if (!h->g.blen) {
                 std::memset(dst, 0, need);
                 return SGC_OK;
             }
-            src = a;
+            src = h->g.blen;
             break;
+        }
+        case SGC_DL_HOLES: {  // each row's mark minus its live count
+            need = h->n * 4ull;
+            if (bytes < need) return fail(SGC_EINVAL, "download target %d needs %llu bytes", what, (unsigned long long)need);
+            if (!h->g.live) {
+                std::memset(dst, 0, need);
+                return SGC_OK;
+            }
+            std::vector<uint32_t> lv(h->n);
+            uint32_t* out = static_cast<uint32_t*>(dst);
+            CK(cudaMemcpyAsync(out, h->g.hw, need, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(lv.data(), h->g.live, need, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            for (uint32_t x = 0; x < h->n; x++) out[x] = out[x] > lv[x] ? out[x] - lv[x] : 0u;
+            return SGC_OK;
         }
         case SGC_DL_COLORS: {
             CK(cudaMallocAsync(&tmp, h->n * 2ull, h->stream));
@@ -1159,6 +1179,7 @@ int sgc_get_stats(sgc_handle* h, sgc_stats* o) {
     o->kernel_launches = h->launches;
     o->h2d_bytes = h->h2d_bytes;
     o->d2h_bytes = h->d2h_bytes;
+    o->hub_deferred = c.hub_total;
     return c.err ? fail(SGC_EDEVICE, "device error word 0x%x", c.err) : SGC_OK;
 }
 

@@ -61,6 +61,18 @@ struct GraphCtl {
     uint32_t dropped; // an entry of this graph was dropped (a full row at drain, or the overflow buffer full)
 };
 
+// A row-scale operation of a concurrent batch left to the pass after it
+// (exact selection): HUB_REDUCE moves x to color `freed` when that is below
+// x's color and no live neighbor of x holds it; HUB_RECOLOR moves x to its
+// first free color. The pass re-reads x's state word.
+enum : uint32_t { HUB_REDUCE = 1u, HUB_RECOLOR = 2u };
+struct HubOp {
+    uint32_t x;
+    uint32_t op;  // kind << 16 | freed
+};
+// Live slots a warp scans itself before it leaves the rest of a row to the pass.
+constexpr uint32_t kHubScan = 512;
+
 // Device view of one graph's state (handle layout). Row x owns logical slots
 // [rp[x], rp[x+1]); hw[x] bounds the slots ever written since the row was last
 // compacted (every slot at or past rp[x]+hw[x] holds INV), so after compaction
@@ -79,7 +91,8 @@ struct Dev {
     uint32_t* hist;                // num_hd * maxc counters
     const uint32_t* deg;           // frozen initial degree: priority = (deg << 32) | id
     uint32_t* hw;                  // per-row high-water mark (slots, relative to rp[x])
-    uint32_t* holes;               // lazy compaction (exact mode): INV slots inside [rp, rp+hw); else null
+    uint32_t* live;                // lazy compaction (exact mode): live entries inside [rp, rp+hw) (the row's
+                                   // holes, free slots and tombstones, are hw minus this count); else null
     uint32_t* dirty;               // bitmask of rows edited since their last compaction
     uint32_t* edited;              // bitmask of rows edited since creation (clear = pristine:
                                    // base entries sorted ascending in [rp, rp+hw), INV after)
@@ -96,6 +109,10 @@ struct Dev {
                                    // endpoints of an ADD whose colors are equal at the end of its batch
     uint32_t* chg;                 // single-graph handles under exact selection: bitmask of the vertices
                                    // whose color changed since the last snapshot (null otherwise)
+    HubOp* hub_ops;                // concurrent batches under exact selection: row-scale operations left
+    uint32_t* hub_count;           // to the pass after the batch (null: none are deferred); the count
+    uint32_t hub_cap;              // runs past hub_cap when the list is full (those are done in place)
+    unsigned long long* hub_total; // cumulative count of the operations the pass took
     GraphCtl* gctl;                // per graph: repair flags (one entry for a single-graph handle)
     const uint32_t* gidw;          // graph of each 32-vertex word (graphs start at multiples of 32);
                                    // null: one graph
@@ -131,39 +148,66 @@ __device__ __forceinline__ uint32_t mask4(const uint4& q, uint64_t i, uint64_t s
     return m;
 }
 
-// Warp-collective: first slot index p in [s, e) whose value satisfies pred,
+// A lane group: the whole warp (W = 32) or one half of it (W = 16, lanes
+// [base, base + 16)). Votes and shuffles stay inside the group, so the two
+// halves of a warp can edit two different rows at once; every branch the
+// group takes depends only on the group's own votes and shuffles.
+template <int W>
+struct Lanes {
+    static_assert(W == 32 || W == 16, "a warp or half a warp");
+    uint32_t base, lane, mask;
+    __device__ __forceinline__ Lanes() {
+        const uint32_t l = lane_id();
+        base = W == 32 ? 0u : (l & 16u);
+        lane = l - base;
+        mask = W == 32 ? FULL : (0xFFFFu << base);
+    }
+    __device__ __forceinline__ bool leader() const { return lane == 0; }
+    // bit k: the group's lane k
+    __device__ __forceinline__ uint32_t ballot(bool p) const { return __ballot_sync(mask, p) >> base; }
+    template <class T>
+    __device__ __forceinline__ T shfl(T v, int src) const { return __shfl_sync(mask, v, src, W); }
+    __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+};
+
+// Group-collective: first slot index p in [s, e) whose value satisfies pred,
 // scanning in slot order exactly like the reference's serial loop. Loads are
 // 16-byte aligned (col must be 16-byte aligned and padded past the last row
 // to a multiple of 4 slots). Returns false when no slot matches.
-template <class P>
-__device__ __forceinline__ bool warp_find(const uint32_t* col, uint64_t s, uint64_t e, P pred,
-                                          uint64_t& pos, uint32_t& val) {
-    const uint32_t lane = lane_id();
-    for (uint64_t c = s & ~3ull; c < e; c += 512) {  // four 16-byte loads per lane in flight
+template <int W, class P>
+__device__ __forceinline__ bool grp_find(const Lanes<W>& L, const uint32_t* col, uint64_t s, uint64_t e, P pred,
+                                         uint64_t& pos, uint32_t& val) {
+    constexpr uint64_t R = 4ull * W;  // slots per group-wide 16-byte load
+    for (uint64_t c = s & ~3ull; c < e; c += 4 * R) {  // four 16-byte loads per lane in flight
         uint4 q[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            const uint64_t i = c + 128ull * k + 4ull * lane;
+            const uint64_t i = c + R * k + 4ull * L.lane;
             q[k] = make_uint4(INV, INV, INV, INV);
             if (i < e) q[k] = ld_cg4(col + i);
         }
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            const uint64_t i = c + 128ull * k + 4ull * lane;
+            const uint64_t i = c + R * k + 4ull * L.lane;
             const uint32_t m = mask4(q[k], i, s, e, pred);
-            const uint32_t b = __ballot_sync(FULL, m != 0);
+            const uint32_t b = L.ballot(m != 0);
             if (b) {
                 const int src = __ffs(b) - 1;
                 const int kk = __ffs(m) - 1;
                 const uint32_t v = m ? pick4(q[k], kk) : 0u;
-                const int ks = __shfl_sync(FULL, kk, src);
-                val = __shfl_sync(FULL, v, src);
-                pos = c + 128ull * k + 4ull * src + ks;
+                const int ks = L.shfl(kk, src);
+                val = L.shfl(v, src);
+                pos = c + R * k + 4ull * src + ks;
                 return true;
             }
         }
     }
     return false;
+}
+template <class P>
+__device__ __forceinline__ bool warp_find(const uint32_t* col, uint64_t s, uint64_t e, P pred,
+                                          uint64_t& pos, uint32_t& val) {
+    return grp_find(Lanes<32>(), col, s, e, pred, pos, val);
 }
 
 // Warp-collective visit of every slot in [s, e): f(slot_index, value) runs on
@@ -246,20 +290,23 @@ __device__ __forceinline__ uint32_t row_len(const Dev& g, uint32_t x) {
 __device__ __forceinline__ uint64_t live_end(const Dev& g, uint32_t x, uint64_t s) {
     const uint64_t e = s + ld_cg(g.hw + x), cap = g.rp[x + 1];
     if (e <= cap) return e;
-    if (lane_id() == 0) atomicOr(g.err, ERR_ROW);
+    if ((lane_id() & 15u) == 0) atomicOr(g.err, ERR_ROW);  // the first lane of each half-warp group
     return cap;
 }
 
 // Row x got an entry in slot q (relative to rp[x]): raise the high-water
-// mark and keep the hole count (free slots inside the mark) exact. A slot
-// below the old mark was a counted hole; a mark raised past free slots makes
-// each of them a hole (a concurrent insert that already took one of them
-// finds the mark above its slot and uncounts it).
+// mark and count the entry live. Both are reductions the warp does not wait
+// for, and they commute with every other row edit of the batch, so once the
+// batch's edits have landed the mark minus the live count is exactly the
+// row's free slots and tombstones inside the mark.
 __device__ __forceinline__ void extend_row(const Dev& g, uint32_t x, uint32_t q) {
-    const uint32_t prev_hw = atomicMax(g.hw + x, q + 1);
-    if (!g.holes) return;
-    if (q < prev_hw) atomicSub(g.holes + x, 1u);
-    else if (q > prev_hw) atomicAdd(g.holes + x, q - prev_hw);
+    atomicMax(g.hw + x, q + 1);
+    if (g.live) atomicAdd(g.live + x, 1u);
+}
+// Holes of row x (free slots and tombstones inside the mark `hw`).
+__device__ __forceinline__ uint32_t row_holes(const Dev& g, uint32_t x, uint32_t hw) {
+    const uint32_t lv = g.live[x];
+    return hw > lv ? hw - lv : 0u;
 }
 
 __device__ __forceinline__ void mark_touched(const Dev& g, uint32_t x) {
@@ -278,50 +325,51 @@ __device__ __forceinline__ bool pristine(const Dev& g, uint32_t x) {
     return !(ld_cg(g.edited + (x >> 5)) & (1u << (x & 31)));
 }
 
-// Warp-collective 32-ary search for `key` in the ascending run col[s, e):
-// each round probes 32 evenly spaced slots and keeps the bucket holding the
+// Group-collective W-ary search for `key` in the ascending run col[s, e):
+// each round probes W evenly spaced slots and keeps the bucket holding the
 // last probe <= key. Returns the slot index, or ~0 when key is absent.
-__device__ __forceinline__ uint64_t warp_bsearch(const uint32_t* col, uint64_t s, uint64_t e, uint32_t key) {
-    const uint32_t lane = lane_id();
+template <int W>
+__device__ __forceinline__ uint64_t grp_bsearch(const Lanes<W>& L, const uint32_t* col, uint64_t s, uint64_t e,
+                                                uint32_t key) {
     uint64_t lo = s, hi = e;
-    while (hi - lo > 32) {
-        const uint64_t step = (hi - lo) / 32;
-        const uint32_t v = ld_cg(col + lo + lane * step);
-        const uint32_t b = __ballot_sync(FULL, v <= key);
+    while (hi - lo > W) {
+        const uint64_t step = (hi - lo) / W;
+        const uint32_t v = ld_cg(col + lo + L.lane * step);
+        const uint32_t b = L.ballot(v <= key);
         if (!b) return ~0ull;
-        const uint32_t L = 31 - __clz(b);
-        const uint64_t nlo = lo + L * step;
-        hi = (L == 31) ? hi : nlo + step;
+        const uint32_t top = 31 - __clz(b);
+        const uint64_t nlo = lo + top * step;
+        hi = (top == W - 1) ? hi : nlo + step;
         lo = nlo;
     }
-    const uint64_t i = lo + lane;
+    const uint64_t i = lo + L.lane;
     const bool hit = i < hi && ld_cg(col + i) == key;
-    const uint32_t b = __ballot_sync(FULL, hit);
+    const uint32_t b = L.ballot(hit);
     return b ? lo + (__ffs(b) - 1) : ~0ull;
 }
 
-// 32-ary search by id in a base run (ascending ids, tombstones keep their id
+// W-ary search by id in a base run (ascending ids, tombstones keep their id
 // under TOMB). Returns the slot index, or ~0 when the id is absent; `val` gets
 // the slot's value (the id, or id | TOMB).
-__device__ __forceinline__ uint64_t warp_bsearch_key(const uint32_t* col, uint64_t s, uint64_t e, uint32_t key,
-                                                     uint32_t& val) {
-    const uint32_t lane = lane_id();
+template <int W>
+__device__ __forceinline__ uint64_t grp_bsearch_key(const Lanes<W>& L, const uint32_t* col, uint64_t s, uint64_t e,
+                                                    uint32_t key, uint32_t& val) {
     uint64_t lo = s, hi = e;
-    while (hi - lo > 32) {
-        const uint64_t step = (hi - lo) / 32;
-        const uint32_t v = ld_cg(col + lo + lane * step) & ~TOMB;
-        const uint32_t b = __ballot_sync(FULL, v <= key);
+    while (hi - lo > W) {
+        const uint64_t step = (hi - lo) / W;
+        const uint32_t v = ld_cg(col + lo + L.lane * step) & ~TOMB;
+        const uint32_t b = L.ballot(v <= key);
         if (!b) return ~0ull;
-        const uint32_t L = 31 - __clz(b);
-        const uint64_t nlo = lo + L * step;
-        hi = (L == 31) ? hi : nlo + step;
+        const uint32_t top = 31 - __clz(b);
+        const uint64_t nlo = lo + top * step;
+        hi = (top == W - 1) ? hi : nlo + step;
         lo = nlo;
     }
-    const uint64_t i = lo + lane;
+    const uint64_t i = lo + L.lane;
     const uint32_t v = i < hi ? ld_cg(col + i) : INV;
-    const uint32_t b = __ballot_sync(FULL, i < hi && (v & ~TOMB) == key);
+    const uint32_t b = L.ballot(i < hi && (v & ~TOMB) == key);
     if (!b) return ~0ull;
-    val = __shfl_sync(FULL, v, __ffs(b) - 1);
+    val = L.shfl(v, __ffs(b) - 1);
     return lo + (__ffs(b) - 1);
 }
 
@@ -331,54 +379,65 @@ enum { ADD_INSERTED = 0, ADD_PRESENT = 1, ADD_OVERFLOW = 2 };
 
 // Concurrent batches under exact selection: rows keep their base run sorted
 // (a delete there leaves a tombstone, a re-insert of the same id revives it),
-// so an update finds a base entry by a 32-ary search; only entries inserted
+// so an update finds a base entry by a W-ary search; only entries inserted
 // since the row's last compaction (its tail) are scanned. The updates of one
 // edge are ordered, so no other warp touches the slot of `nbr` meanwhile.
 // Add: returns ADD_PRESENT / ADD_INSERTED when the run holds nbr (live or
 // tombstone), -1 when it does not.
-__device__ __forceinline__ int warp_run_add(const Dev& g, uint32_t x, uint32_t nbr, uint64_t s, uint32_t bl) {
+template <int W>
+__device__ __forceinline__ int grp_run_add(const Lanes<W>& L, const Dev& g, uint32_t x, uint32_t nbr, uint64_t s,
+                                           uint32_t bl) {
     uint32_t val = 0;
-    const uint64_t p = warp_bsearch_key(g.col, s, s + bl, nbr, val);
+    const uint64_t p = grp_bsearch_key(L, g.col, s, s + bl, nbr, val);
     if (p == ~0ull) return -1;
     if (val == nbr) return ADD_PRESENT;
     uint32_t old = 0;
-    if (lane_id() == 0) {
+    if (L.leader()) {
         old = atomicCAS(g.col + p, nbr | TOMB, nbr);
         if (old == (nbr | TOMB)) {
-            atomicSub(g.holes + x, 1u);
+            atomicAdd(g.live + x, 1u);
             mark_dirty(g, x);
         }
     }
-    old = __shfl_sync(FULL, old, 0);
+    old = L.shfl(old, 0);
     return old == nbr ? ADD_PRESENT : ADD_INSERTED;
 }
+__device__ __forceinline__ int warp_run_add(const Dev& g, uint32_t x, uint32_t nbr, uint64_t s, uint32_t bl) {
+    return grp_run_add(Lanes<32>(), g, x, nbr, s, bl);
+}
 // Delete: true when the run held nbr live (now a tombstone).
-__device__ __forceinline__ bool warp_run_remove(const Dev& g, uint32_t x, uint32_t nbr, uint64_t s, uint32_t bl) {
+template <int W>
+__device__ __forceinline__ bool grp_run_remove(const Lanes<W>& L, const Dev& g, uint32_t x, uint32_t nbr, uint64_t s,
+                                               uint32_t bl) {
     uint32_t val = 0;
-    const uint64_t p = warp_bsearch_key(g.col, s, s + bl, nbr, val);
+    const uint64_t p = grp_bsearch_key(L, g.col, s, s + bl, nbr, val);
     if (p == ~0ull || val != nbr) return false;
     uint32_t old = 0;
-    if (lane_id() == 0) {
+    if (L.leader()) {
         old = atomicCAS(g.col + p, nbr, nbr | TOMB);
         if (old == nbr) {
-            atomicAdd(g.holes + x, 1u);
+            atomicSub(g.live + x, 1u);
             mark_dirty(g, x);
         }
     }
-    old = __shfl_sync(FULL, old, 0);
+    old = L.shfl(old, 0);
     return old == nbr;
 }
 
 // add_local_neighbor: claim the first INV slot unless `nbr` shows up first;
 // a full row appends to the overflow buffer (counter always advances, entry
-// stored only below capacity).
-__device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t nbr, bool exact) {
+// stored only below capacity). The row's bounds, base run and high-water
+// mark are read together up front (a mark read early is only lower: the
+// fallback scan to the row's end covers what it misses).
+template <int W>
+__device__ __forceinline__ int grp_add_slot(const Lanes<W>& L, const Dev& g, uint32_t x, uint32_t nbr, bool exact) {
     const uint64_t s = g.rp[x], e = g.rp[x + 1];
+    const uint32_t bl = (!exact && g.blen) ? ld_cg(g.blen + x) : 0u;
+    const uint32_t hw0 = ld_cg(g.hw + x);
     uint64_t from = s;
     if (!exact && g.blen) {
-        const uint32_t bl = ld_cg(g.blen + x);
         if (bl) {
-            const int r = warp_run_add(g, x, nbr, s, bl);
+            const int r = grp_run_add(L, g, x, nbr, s, bl);
             if (r >= 0) return r;
         }
         from = s + bl;  // the tail: first INV or nbr
@@ -386,7 +445,7 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
         // Sorted base entries, no holes: the scan would stop at nbr if present,
         // else at the first INV right after the base run.
         const uint64_t len = live_end(g, x, s) - s;
-        if (warp_bsearch(g.col, s, s + len, nbr) != ~0ull) return ADD_PRESENT;
+        if (grp_bsearch(L, g.col, s, s + len, nbr) != ~0ull) return ADD_PRESENT;
         // Past the sorted run: in stream order nothing else changes the row; in
         // a concurrent batch the updates of this edge are ordered, so nbr can
         // only be in the row through an earlier update of the edge, and that
@@ -397,23 +456,23 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
     // mark, so the first scan stops one slot past it (not at the end of the
     // row's slack); if a concurrent insert took those slots meanwhile, the
     // scan goes on to the end of the row.
-    uint64_t lim = s + ld_cg(g.hw + x) + 1;
+    uint64_t lim = s + hw0 + 1;
     if (lim > e) lim = e;
     for (;;) {
         uint64_t p = 0;
         uint32_t v = 0;
         const bool hit =
-            from < lim && warp_find(g.col, from, lim, [nbr](uint32_t t) { return t == INV || t == nbr; }, p, v);
+            from < lim && grp_find(L, g.col, from, lim, [nbr](uint32_t t) { return t == INV || t == nbr; }, p, v);
         if (!hit && lim < e) {
             if (lim > from) from = lim;
             lim = e;
             continue;
         }
         if (!hit) {
-            if (lane_id() == 0 && (g.abl & ABL_NO_OVERFLOW)) {  // the ablation drops the edge
+            if (L.leader() && (g.abl & ABL_NO_OVERFLOW)) {  // the ablation drops the edge
                 g.gctl[graph_of(g, x)].dropped = 1u;
                 flag_asym(g, x);
-            } else if (lane_id() == 0) {
+            } else if (L.leader()) {
                 const uint32_t pos = atomicAdd(g.ovf_count, 1u);
                 if (pos < OVF_CAP) {
                     g.ovf[pos].local_vertex_idx = x;
@@ -424,48 +483,53 @@ __device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t 
                 }
                 flag_asym(g, x);
             }
-            __syncwarp();
+            L.sync();
             return ADD_OVERFLOW;
         }
         if (v == nbr) return ADD_PRESENT;
         uint32_t old = 0;
-        if (lane_id() == 0) {
+        if (L.leader()) {
             old = atomicCAS(g.col + p, INV, nbr);
             if (old == INV) {
                 extend_row(g, x, (uint32_t)(p - s));
                 mark_dirty(g, x);
             }
         }
-        old = __shfl_sync(FULL, old, 0);
+        old = L.shfl(old, 0);
         if (old == INV) return ADD_INSERTED;
         if (old == nbr) return ADD_PRESENT;
         from = p + 1;  // lost the slot to a concurrent insert: keep scanning after it
     }
 }
+__device__ __forceinline__ int warp_add_slot(const Dev& g, uint32_t x, uint32_t nbr, bool exact) {
+    return grp_add_slot(Lanes<32>(), g, x, nbr, exact);
+}
 
 // remove_local_neighbor: first slot equal to nbr becomes INV (lazy delete).
 // Returns whether an entry was removed.
-__device__ __forceinline__ bool warp_remove_slot(const Dev& g, uint32_t x, uint32_t nbr, bool exact) {
+template <int W>
+__device__ __forceinline__ bool grp_remove_slot(const Lanes<W>& L, const Dev& g, uint32_t x, uint32_t nbr,
+                                                bool exact) {
     const uint64_t s = g.rp[x];
+    const uint32_t bl = (!exact && g.blen) ? ld_cg(g.blen + x) : 0u;
     const uint64_t e = live_end(g, x, s);
     uint64_t from = s;
     if (!exact && g.blen) {
-        const uint32_t bl = ld_cg(g.blen + x);
-        if (bl && warp_run_remove(g, x, nbr, s, bl)) return true;
+        if (bl && grp_run_remove(L, g, x, nbr, s, bl)) return true;
         from = s + bl;  // not live in the run: the tail
     } else if (pristine(g, x)) {
-        const uint64_t p = warp_bsearch(g.col, s, e, nbr);
+        const uint64_t p = grp_bsearch(L, g.col, s, e, nbr);
         if (p != ~0ull) {
             uint32_t old = 0;
-            if (lane_id() == 0) {
+            if (L.leader()) {
                 old = atomicCAS(g.col + p, nbr, INV);
                 if (old == nbr) {
                     mark_dirty(g, x);
-                    if (g.holes) atomicAdd(g.holes + x, 1u);
+                    if (g.live) atomicSub(g.live + x, 1u);
                     if (g.blen) g.blen[x] = 0;  // an INV inside the run ends it
                 }
             }
-            old = __shfl_sync(FULL, old, 0);
+            old = L.shfl(old, 0);
             if (old == nbr) return true;
         } else if (exact) {
             return false;  // absent from the sorted run and nothing after it
@@ -474,20 +538,23 @@ __device__ __forceinline__ bool warp_remove_slot(const Dev& g, uint32_t x, uint3
     for (;;) {
         uint64_t p = 0;
         uint32_t v = 0;
-        if (!warp_find(g.col, from, e, [nbr](uint32_t t) { return t == nbr; }, p, v)) return false;
+        if (!grp_find(L, g.col, from, e, [nbr](uint32_t t) { return t == nbr; }, p, v)) return false;
         uint32_t old = 0;
-        if (lane_id() == 0) {
+        if (L.leader()) {
             old = atomicCAS(g.col + p, nbr, INV);
             if (old == nbr) {
                 mark_dirty(g, x);
-                if (g.holes) atomicAdd(g.holes + x, 1u);
+                if (g.live) atomicSub(g.live + x, 1u);
                 if (g.blen && p < s + ld_cg(g.blen + x)) g.blen[x] = 0;  // an INV inside the run ends it
             }
         }
-        old = __shfl_sync(FULL, old, 0);
+        old = L.shfl(old, 0);
         if (old == nbr) return true;
         from = p + 1;
     }
+}
+__device__ __forceinline__ bool warp_remove_slot(const Dev& g, uint32_t x, uint32_t nbr, bool exact) {
+    return grp_remove_slot(Lanes<32>(), g, x, nbr, exact);
 }
 
 // ---------------- color selection (color_select.cuh:10-115) ----------------
@@ -625,8 +692,9 @@ __device__ __forceinline__ void set_bm_bit(const Dev& g, uint32_t x, uint16_t c)
 __device__ __forceinline__ void nbr_color_change(const Dev& g, uint32_t x, uint16_t oldc, uint16_t newc) {
     if (oldc == newc) return;
     if (newc != 0 && newc <= 64) set_bm_bit<true>(g, x, newc);
+    if (g.exact) return;  // no histogram rows
     const uint32_t hd = __ldg(g.hdmap + x);
-    if (hd != EMPTY && !g.exact) {
+    if (hd != EMPTY) {
         uint32_t* h = g.hist + (uint64_t)hd * g.maxc;
         if (oldc != 0 && oldc <= g.maxc) atomicSub(h + oldc - 1, 1u);
         if (newc != 0 && newc <= g.maxc) atomicAdd(h + newc - 1, 1u);
@@ -657,8 +725,9 @@ __device__ __forceinline__ uint32_t warp_load_state(const Dev& g, uint32_t x) {
 // `chosen` (nonzero) is FAC(x) already computed on the current state by the
 // caller; in stream order nothing changes in between, so it equals the call
 // the reference makes here.
-__device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x, uint16_t chosen = 0) {
-    uint32_t cur = warp_load_state(g, x);
+// warp_recolor_from: the same with x's state word `cur` as last read by the
+// caller (a stale word fails the first compare-and-swap, which re-reads it).
+__device__ __forceinline__ void warp_recolor_from(const Dev& g, uint32_t x, uint16_t chosen, uint32_t cur) {
     uint16_t newc = chosen ? chosen : warp_fac(g, x, g.st);
     if (newc == color_of(cur)) return;
     for (uint32_t tries = 0;; tries++) {
@@ -687,6 +756,9 @@ __device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x, uint16_t 
     });
     __syncwarp();
 }
+__device__ __forceinline__ void warp_recolor(const Dev& g, uint32_t x, uint16_t chosen = 0) {
+    warp_recolor_from(g, x, chosen, warp_load_state(g, x));
+}
 
 // Warp-collective: does some live neighbor of x hold color c? Stops at the
 // first round that finds one.
@@ -694,6 +766,32 @@ __device__ __forceinline__ bool warp_color_held(const Dev& g, uint32_t x, uint16
     const uint64_t s = g.rp[x], e = live_end(g, x, s);
     // rounds of 128 slots: a holder is usually among the first neighbors
     return warp_gather_each<true, 1>(g.col, s, e, g.n, g.st, [c](uint32_t, uint32_t w) { return color_of(w) == c; });
+}
+
+// Does a live neighbor among the first `lim` live slots of x hold color c?
+// `all`: those slots were the whole row.
+__device__ __forceinline__ bool warp_color_held_first(const Dev& g, uint32_t x, uint16_t c, uint32_t lim, bool& all) {
+    const uint64_t s = g.rp[x], e = live_end(g, x, s);
+    const uint64_t e1 = e - s > lim ? s + lim : e;
+    all = e1 == e;
+    return warp_gather_each<true, 4>(g.col, s, e1, g.n, g.st, [c](uint32_t, uint32_t w) { return color_of(w) == c; });
+}
+
+// Appends a row-scale operation to the pass after the batch (lane 0).
+// Warp-collective; false when nothing is deferred (no list, or it is full):
+// the caller then does the work itself.
+__device__ __forceinline__ bool warp_defer(const Dev& g, uint32_t x, uint32_t kind, uint16_t freed) {
+    if (!g.hub_ops) return false;
+    uint32_t ok = 0;
+    if (lane_id() == 0) {
+        const uint32_t pos = atomicAdd(g.hub_count, 1u);
+        if (pos < g.hub_cap) {
+            g.hub_ops[pos].x = x;
+            g.hub_ops[pos].op = (kind << 16) | freed;
+            ok = 1;
+        }
+    }
+    return __shfl_sync(FULL, ok, 0) != 0;
 }
 
 // Both endpoints' state words in one round trip (lanes 0 and 1).
@@ -802,6 +900,144 @@ __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v,
         warp_try_reduce(g, u, fu, exact, su);
         if (v == u) sv = warp_load_state(g, v);
         warp_try_reduce(g, v, fv, exact, sv);
+    }
+}
+
+// ---------------- one update of a concurrent batch ----------------
+
+// The neighbor-class bookkeeping of new_nbr / removed_nbr with x's class `hd`
+// already read (exact selection keeps no histogram rows: no load at all).
+__device__ __forceinline__ void new_nbr_cls(const Dev& g, uint32_t x, uint32_t hd, uint16_t c) {
+    if (c == 0) return;
+    if (c <= 64) set_bm_bit<false>(g, x, c);
+    if (!g.exact && hd != EMPTY && c <= g.maxc) atomicAdd(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
+}
+__device__ __forceinline__ void removed_nbr_cls(const Dev& g, uint32_t x, uint32_t hd, uint16_t c) {
+    if (!g.exact && c != 0 && hd != EMPTY && c <= g.maxc) atomicSub(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
+}
+
+// try_color_reduction in a concurrent batch, from x's state word, class and
+// bitmap as read at the start of the update (bitmap bits are only added
+// during a batch: a bit set since makes at most a conflict, which marks x for
+// the repair through its recolor). Same rule as warp_try_reduce.
+__device__ __forceinline__ void warp_try_reduce_conc(const Dev& g, uint32_t x, uint16_t freed, uint32_t state,
+                                                     uint32_t hd, unsigned long long bmv) {
+    const uint16_t cur = color_of(state);
+    if (cur == 0 || freed >= cur) return;
+    if (g.exact && hd != EMPTY) {
+        if (freed == 0) return;
+        // a holder is usually among the first neighbors; a long row without
+        // one there is finished (scan, move, walk) by the pass after the batch
+        bool all = true;
+        if (warp_color_held_first(g, x, freed, g.hub_ops ? kHubScan : 0xFFFFFFFFu, all)) return;
+        if (!all && (warp_defer(g, x, HUB_REDUCE, freed) || warp_color_held(g, x, freed))) return;
+        warp_recolor_from(g, x, freed, state);
+        return;
+    }
+    uint16_t best;
+    if (hd != EMPTY && !(g.abl & ABL_FORCE_BITMAP)) best = warp_fac_hist(g.hist + (uint64_t)hd * g.maxc, g.maxc);
+    else if (~bmv) best = (uint16_t)__ffsll((long long)~bmv);
+    else best = warp_fac_scan(g, x, g.st);
+    if (best < cur) warp_recolor_from(g, x, best, state);
+}
+
+// Row edits of one edge in both directions. For u != v the two rows are
+// different and no other warp edits those slots of theirs (the updates of an
+// edge are ordered), so the two halves of the warp make the edits at once:
+// lanes 0-15 row u, 16-31 row v. Returns the two results in (ru, rv).
+template <bool ADD>
+__device__ __forceinline__ void warp_edit_both(const Dev& g, uint32_t u, uint32_t v, int& ru, int& rv) {
+    if (u != v) {
+        const Lanes<16> H;
+        const uint32_t x = H.base ? v : u, y = H.base ? u : v;  // one call site: the halves stay converged
+        const int r = ADD ? grp_add_slot(H, g, x, y, false) : (grp_remove_slot(H, g, x, y, false) ? 1 : 0);
+        __syncwarp();
+        ru = __shfl_sync(FULL, r, 0);
+        rv = __shfl_sync(FULL, r, 16);
+    } else {
+        ru = ADD ? warp_add_slot(g, u, v, false) : (warp_remove_slot(g, u, v, false) ? 1 : 0);
+        rv = ADD ? warp_add_slot(g, v, u, false) : (warp_remove_slot(g, v, u, false) ? 1 : 0);
+    }
+}
+
+// One update of a concurrent batch: the reference's ADD / DEL sequence
+// (local_update.cu:61-147) with its loads gathered into as few dependent
+// rounds as the rules allow. The endpoints' classes (and, for a DEL, their
+// state words and bitmaps, which the reference reads before the row edits)
+// are requested first and used after the edits, so they arrive during them.
+// An ADD reads the state words after its edits and keeps them: a later change
+// by another warp is a color change (marked) or leaves this ADD's endpoints
+// equal (caught by the check after the batch).
+__device__ __forceinline__ void warp_apply_conc(const Dev& g, uint32_t u, uint32_t v, uint8_t type) {
+    const uint32_t lane = lane_id();
+    const bool del = type == SGC_UPDATE_DEL;
+    const uint32_t x = (lane & 1) ? v : u;
+    uint32_t w = 0;
+    unsigned long long bw = 0;
+    if (lane < 2) w = __ldg(g.hdmap + x);             // classes (read-only)
+    else if (lane < 4 && del) w = ld_cg(g.st + x);    // DEL: state words
+    else if (lane < 6 && del) bw = ld_cg(g.bm + x);   // DEL: bitmaps
+    if (type == SGC_UPDATE_ADD) {
+        int ru, rv;
+        warp_edit_both<true>(g, u, v, ru, rv);
+        if (ru != rv && lane == 0) flag_asym(g, u);
+        uint32_t su, sv;
+        warp_load_states2(g, u, v, su, sv);
+        const uint32_t hu = __shfl_sync(FULL, w, 0), hv = __shfl_sync(FULL, w, 1);
+        if (lane == 0 && g.touched) {  // bitmap-class endpoints: their bitmaps are rebuilt by the repair
+            if (hu == EMPTY) mark_touched(g, u);
+            if (hv == EMPTY) mark_touched(g, v);
+        }
+        if (color_of(su) == 0) {
+            su = warp_color_uncolored(g, u, su);
+            if (v == u) sv = su;
+        }
+        if (color_of(sv) == 0) {
+            if (lane == 0) new_nbr_cls(g, v, hv, color_of(su));
+            __syncwarp();
+            sv = warp_color_uncolored(g, v, sv);
+        }
+        if (lane == 0) new_nbr_cls(g, u, hu, color_of(sv));
+        else if (lane == 1) new_nbr_cls(g, v, hv, color_of(su));
+        __syncwarp();
+        const uint16_t cu = color_of(su), cv = color_of(sv);
+        if (cu == cv && cu != 0) {
+            const bool lu = prio_less(__ldg(g.deg + u), u, __ldg(g.deg + v), v);
+            const uint32_t loser = lu ? u : v;
+            // a long histogram-class row: its selection and walk go to the pass after the batch
+            const bool defer = g.hub_ops && (lu ? hu : hv) != EMPTY && row_len(g, loser) > kHubScan &&
+                               warp_defer(g, loser, HUB_RECOLOR, 0);
+            if (!defer) warp_recolor_from(g, loser, 0, lu ? su : sv);
+        }
+    } else if (del) {
+        int du, dv;
+        warp_edit_both<false>(g, u, v, du, dv);
+        const uint32_t hu = __shfl_sync(FULL, w, 0), hv = __shfl_sync(FULL, w, 1);
+        const uint32_t su = __shfl_sync(FULL, w, 2);
+        uint32_t sv = __shfl_sync(FULL, w, 3);
+        const unsigned long long bu = __shfl_sync(FULL, bw, 4), bv = __shfl_sync(FULL, bw, 5);
+        const uint16_t fu = color_of(sv), fv = color_of(su);
+        if (lane == 0) {
+            if (du != dv) flag_asym(g, u);
+            if (g.touched) {
+                if (hu == EMPTY) mark_touched(g, u);
+                if (hv == EMPTY) mark_touched(g, v);
+            }
+            removed_nbr_cls(g, u, hu, fu);
+            removed_nbr_cls(g, v, hv, fv);
+        }
+        __syncwarp();
+        warp_try_reduce_conc(g, u, fu, su, hu, bu);
+        unsigned long long bv2 = bv;
+        if (v == u) {  // the same row: its word and bitmap as the first reduction left them
+            uint32_t w2 = 0;
+            unsigned long long b2 = 0;
+            if (lane == 0) w2 = ld_cg(g.st + v);
+            else if (lane == 1) b2 = ld_cg(g.bm + v);
+            sv = __shfl_sync(FULL, w2, 0);
+            bv2 = __shfl_sync(FULL, b2, 1);
+        }
+        warp_try_reduce_conc(g, v, fv, sv, hv, bv2);
     }
 }
 

@@ -94,7 +94,10 @@ __device__ __forceinline__ uint32_t batch_n(uint32_t n, const uint32_t* dyn) { r
 __global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg, EdgeOrder eo,
                                  const uint32_t* dyn) {
     const uint32_t n = batch_n(n_arg, dyn);
-    if (blockIdx.x == 0 && threadIdx.x == 0) *eo.ticket = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *eo.ticket = 0;
+        if (g.hub_count) *g.hub_count = 0;
+    }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
         const uint32_t u = r.x, v = r.y;
@@ -144,43 +147,203 @@ __global__ void conc_prep_prev(uint32_t n_arg, EdgeOrder eo, const uint32_t* dyn
 // stream order; the later ones are skipped at their own tickets. So the
 // updates of one edge never run concurrently and no warp waits for another.
 // The batch and the ordering words were written by the copy and the prep
-// kernels before this launch: L2-coherent loads. Three blocks per SM: 80
-// registers with little spilling (the budget the one-warp-per-update version
-// ran fastest with; 64 registers spill the update path).
+// kernels before this launch: L2-coherent loads. A warp takes its next ticket
+// while it applies the current update, and reads a position's ordering words
+// and record in one round (the next update of an edge's chain with them).
+// Three blocks per SM: 80 registers (the budget the one-warp-per-update
+// version ran fastest with; 64 registers spill the update path).
 __global__ void __launch_bounds__(256, 3) conc_apply_kernel(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg,
                                                             EdgeOrder eo, const uint32_t* dyn) {
     const uint32_t n = batch_n(n_arg, dyn);
-    for (;;) {
-        uint32_t i = 0;
-        if (lane_id() == 0) i = atomicAdd(eo.ticket, 1u);
-        i = __shfl_sync(FULL, i, 0);
-        if (i >= n) break;
+    uint32_t i = 0;
+    if (lane_id() == 0) i = atomicAdd(eo.ticket, 1u);
+    i = __shfl_sync(FULL, i, 0);
+    while (i < n) {
+        uint32_t next = 0;
+        if (lane_id() == 0) next = atomicAdd(eo.ticket, 1u);  // used after this update
         const uint32_t h = ld_cg(eo.tslot + i);
+        const uint32_t prev = ld_cg(eo.tprev + i);
+        uint32_t succ = ld_cg(eo.tsucc + i);
+        uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
         if (h == NONE32) {
-            const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
             if ((r.x >= g.n || r.y >= g.n) && lane_id() == 0) atomicAdd(g.nskip, 1ull);
-            continue;
+        } else if (prev == NONE32) {  // the first update of its edge applies the whole chain
+            uint32_t steps = 1;
+            for (;;) {
+                if (r.x >= g.n || r.y >= g.n) {
+                    if (lane_id() == 0) atomicOr(g.err, ERR_CHAIN);
+                    break;
+                }
+                warp_apply_conc(g, r.x, r.y, (uint8_t)(r.z & 0xFFu));
+                const uint32_t j = succ;
+                if (j == NONE32) break;
+                if (j >= n || j < i || ++steps > n) {  // ordering words inconsistent with the batch
+                    if (lane_id() == 0) atomicOr(g.err, ERR_CHAIN);
+                    break;
+                }
+                succ = ld_cg(eo.tsucc + j);
+                r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + j));
+            }
+            if (lane_id() == 0 && h <= eo.tmask) {  // no kernel reads the table during apply: reset it for the next batch
+                eo.tkey[h] = EMPTY64;
+                eo.thead[h] = NONE32;
+            }
+            __syncwarp();
         }
-        if (ld_cg(eo.tprev + i) != NONE32) continue;  // applied with the first update of its edge
-        uint32_t steps = 0;
-        for (uint32_t j = i; j != NONE32; j = ld_cg(eo.tsucc + j)) {
-            if (j >= n || j < i || ++steps > n) {  // ordering words inconsistent with the batch
-                if (lane_id() == 0) atomicOr(g.err, ERR_CHAIN);
+        i = __shfl_sync(FULL, next, 0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The pass after a concurrent batch: row-scale operations the apply left
+// (HubOp), one block of kHubThreads per operation. Each re-reads x's state
+// word; the scans and the neighbor walk after a move take 8192 slots per
+// round over the whole block. Decisions are made on words thread 0 read and
+// shared, so every branch is block-uniform.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kHubThreads = 1024;
+
+// The ids of one round's slots: thread t loads the 16-byte chunks at
+// c + 4t and c + 4t + 4096 (INV outside [s, e) and for ids >= n).
+__device__ __forceinline__ void hub_round(const Dev& g, uint64_t c, uint64_t s, uint64_t e, uint32_t (&y)[8]) {
+    const uint64_t i0 = c + 4ull * threadIdx.x, i1 = i0 + 4ull * kHubThreads;
+    uint4 q0 = make_uint4(INV, INV, INV, INV), q1 = q0;
+    if (i0 < e) q0 = ld_cg4(g.col + i0);
+    if (i1 < e) q1 = ld_cg4(g.col + i1);
+    const uint32_t v[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+        const uint64_t p = (t < 4 ? i0 : i1) + (t & 3);
+        y[t] = (p >= s && p < e && v[t] < g.n) ? v[t] : INV;
+    }
+}
+
+// Does a live neighbor in [s, e) hold color c? Stops after the first round that finds one.
+__device__ __forceinline__ bool block_color_held(const Dev& g, uint64_t s, uint64_t e, uint16_t c) {
+    for (uint64_t r = s & ~3ull; r < e; r += 8ull * kHubThreads) {
+        uint32_t y[8];
+        hub_round(g, r, s, e, y);
+        uint32_t w[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) w[t] = y[t] != INV ? ld_cg(g.st + y[t]) : 0u;
+        bool hit = false;
+#pragma unroll
+        for (int t = 0; t < 8; t++) hit |= y[t] != INV && color_of(w[t]) == c;
+        if (__syncthreads_or(hit)) return true;
+    }
+    return false;
+}
+
+// Exact selection: the first color no live neighbor in [s, e) holds (colors
+// 1..2047, else 2048), as warp_fac_exact. `used`: 64 words of shared memory.
+__device__ __forceinline__ uint16_t block_fac_exact(const Dev& g, uint64_t s, uint64_t e, uint32_t* used,
+                                                    uint32_t* pick) {
+    if (threadIdx.x < 64) used[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t lo = 0, hi = 0;  // colors 1..64 (bits 0..63 of a 64-bit mask)
+    for (uint64_t r = s & ~3ull; r < e; r += 8ull * kHubThreads) {
+        uint32_t y[8];
+        hub_round(g, r, s, e, y);
+        uint32_t w[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) w[t] = y[t] != INV ? ld_cg(g.st + y[t]) : 0u;
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+            if (y[t] == INV) continue;
+            const uint16_t c = color_of(w[t]);
+            add_color_bit(c, lo, hi);
+            if (c > 64 && c < 2048) atomicOr(&used[c >> 5], 1u << (c & 31));
+        }
+    }
+    lo = __reduce_or_sync(FULL, lo);
+    hi = __reduce_or_sync(FULL, hi);
+    if (lane_id() == 0) {  // fold colors 1..64 into the same set (color c: word c >> 5, bit c & 31)
+        if (lo) atomicOr(&used[0], lo << 1);
+        if (lo >> 31) atomicOr(&used[1], 1u);
+        if (hi) atomicOr(&used[1], hi << 1);
+        if (hi >> 31) atomicOr(&used[2], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const uint32_t l = threadIdx.x;
+        uint32_t w0 = ~used[l], w1 = ~used[l + 32];
+        if (l == 0) w0 &= ~1u;  // color 0 is never a candidate
+        const uint32_t b0 = __ballot_sync(FULL, w0 != 0), b1 = __ballot_sync(FULL, w1 != 0);
+        if (l == 0) {
+            uint32_t c = 2048;
+            if (b0) {
+                const int src = __ffs(b0) - 1;
+                c = src * 32 + __ffs(~used[src] & (src == 0 ? ~1u : FULL)) - 1;
+            } else if (b1) {
+                const int src = __ffs(b1) - 1;
+                c = 1024 + src * 32 + __ffs(~used[src + 32]) - 1;
+            }
+            *pick = c;
+        }
+    }
+    __syncthreads();
+    const uint16_t c = (uint16_t)*pick;
+    __syncthreads();
+    return c;
+}
+
+__global__ void __launch_bounds__(kHubThreads) hub_ops_kernel(Dev g) {
+    __shared__ uint32_t used[64];
+    __shared__ uint32_t word[2];
+    const uint32_t total = ld_cg(g.hub_count);
+    const uint32_t cnt = total < g.hub_cap ? total : g.hub_cap;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && cnt) atomicAdd(g.hub_total, (unsigned long long)cnt);
+    for (uint32_t k = blockIdx.x; k < cnt; k += gridDim.x) {
+        const HubOp op = g.hub_ops[k];
+        const uint32_t x = op.x;
+        if (x >= g.n) continue;  // block-uniform: every thread read the same record
+        const uint32_t kind = op.op >> 16;
+        const uint16_t freed = (uint16_t)(op.op & 0xFFFFu);
+        const uint64_t s = g.rp[x], e = live_end(g, x, s);
+        if (threadIdx.x == 0) word[0] = ld_cg(g.st + x);
+        __syncthreads();
+        uint32_t cur = word[0];
+        __syncthreads();
+        uint16_t newc;
+        if (kind == HUB_REDUCE) {
+            if (freed == 0 || freed >= color_of(cur) || block_color_held(g, s, e, freed)) continue;
+            newc = freed;
+        } else {
+            newc = block_fac_exact(g, s, e, used, &word[1]);
+        }
+        // recolor_vertex: compare-and-swap (newc, version + 1) in; a changed word
+        // re-selects from the live neighbors, as the warp's recolor does
+        bool moved = false;
+        for (uint32_t tries = 0;; tries++) {
+            if (newc == color_of(cur)) break;
+            if (threadIdx.x == 0) word[0] = atomicCAS(g.st + x, cur, pack(newc, (uint16_t)(version_of(cur) + 1)));
+            __syncthreads();
+            const uint32_t got = word[0];
+            __syncthreads();
+            if (got == cur) {
+                moved = true;
                 break;
             }
-            const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + j));
-            const uint32_t u = r.x, v = r.y;
-            if (u >= g.n || v >= g.n) {
-                if (lane_id() == 0) atomicOr(g.err, ERR_CHAIN);
+            if (tries >= (1u << 20)) {  // the repair after the batch settles x
+                if (threadIdx.x == 0) atomicOr(g.err, ERR_RETRY);
                 break;
             }
-            warp_apply(g, u, v, (uint8_t)(r.z & 0xFFu), false);
+            cur = got;
+            newc = block_fac_exact(g, s, e, used, &word[1]);
         }
-        if (lane_id() == 0 && h <= eo.tmask) {  // no kernel reads the table during apply: reset it for the next batch
-            eo.tkey[h] = EMPTY64;
-            eo.thead[h] = NONE32;
+        if (!moved) continue;
+        if (threadIdx.x == 0) {
+            mark_touched(g, x);
+            note_color(g, x);
         }
-        __syncwarp();
+        const uint16_t oldc = color_of(cur);
+        for (uint64_t r = s & ~3ull; r < e; r += 8ull * kHubThreads) {
+            uint32_t y[8];
+            hub_round(g, r, s, e, y);
+#pragma unroll
+            for (int t = 0; t < 8; t++)
+                if (y[t] != INV) nbr_color_change(g, y[t], oldc, newc);
+        }
     }
 }
 
@@ -249,6 +412,7 @@ void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const Ed
     const uint32_t need = (n + 7) / 8;  // 8 warps per block
     if (grid > need) grid = need;
     conc_apply_kernel<<<grid, 256, 0, s>>>(g, ups, n, eo, nullptr);
+    if (g.hub_ops) hub_ops_kernel<<<num_sms, kHubThreads, 0, s>>>(g);
 }
 
 void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* dyn, const EdgeOrder& eo,
@@ -258,6 +422,7 @@ void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* 
     const int occ = conc_apply_occupancy();
     const int bps = (blocks_per_sm > 0 && blocks_per_sm < occ) ? blocks_per_sm : occ;
     conc_apply_kernel<<<num_sms * bps, 256, 0, s>>>(g, ups, 0, eo, dyn);
+    if (g.hub_ops) hub_ops_kernel<<<num_sms, kHubThreads, 0, s>>>(g);
 }
 
 // Stream order per graph, graphs side by side: warp per segment
@@ -362,8 +527,9 @@ __global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __r
         // as it is (every reader skips INV slots and tombstones); it is compacted later.
         const uint32_t run = merge ? min(g.blen[x], hwx) : 0u;
         const bool long_tail = merge && hwx - run > max(32u, hwx >> 3);
-        if (!force && g.holes && 4u * g.holes[x] <= hwx && !long_tail) {
-            if ((g.holes[x] || (merge && run < hwx)) && lane == 0)  // still a candidate (holes, or a tail to merge)
+        const uint32_t holes = g.live ? row_holes(g, x, g.hw[x]) : 0u;
+        if (!force && g.live && 4u * holes <= hwx && !long_tail) {
+            if ((holes || (merge && run < hwx)) && lane == 0)  // still a candidate (holes, or a tail to merge)
                 atomicOr(g.dirty + (x >> 5), 1u << (x & 31));
             continue;
         }
@@ -411,7 +577,7 @@ __global__ void __launch_bounds__(256) compact_kernel(Dev g, const uint32_t* __r
         }
         if (lane == 0) {
             g.hw[x] = live;
-            if (g.holes) g.holes[x] = 0;
+            if (g.live) g.live[x] = live;
             if (g.blen) g.blen[x] = (uint32_t)run_live;
         }
         __syncwarp();
@@ -628,7 +794,18 @@ __global__ void build_items_kernel(Dev g, SweepBufs b, int list_mode) {
             if (k) atomicOr(g.err, ERR_LIST_OVERFLOW);
             continue;
         }
-        for (uint32_t j = 0; j < k; j++) b.items[wbase + off + j] = (unsigned long long)x | ((unsigned long long)j << 32);
+        if (k) {
+            const uint64_t rs = g.rp[x];
+            const uint32_t len = row_len(g, x);
+            for (uint32_t j = 0; j < k; j++) {
+                const uint32_t first = j * tile;
+                SweepItem it;
+                it.x = x;
+                it.len = len - first < tile ? len - first : tile;
+                it.s = rs + first;
+                b.items[wbase + off + j] = it;
+            }
+        }
     }
 }
 void launch_build_items(const Dev& g, const SweepBufs& b, int list_mode, int num_sms, cudaStream_t s) {
@@ -649,20 +826,39 @@ __device__ __forceinline__ unsigned long long sym_term(uint32_t x, uint32_t y) {
     return pair_hash(x, y) - pair_hash(y, x);
 }
 
-// The bounds of item `it` (row x, chunk j) in slot space.
-__device__ __forceinline__ void item_bounds(const Dev& g, const SweepBufs& b, unsigned long long it, uint32_t& x,
-                                            uint64_t& s, uint64_t& e) {
-    x = (uint32_t)it;
-    const uint32_t j = (uint32_t)(it >> 32);
-    const uint64_t rs = g.rp[x];
-    s = rs + (uint64_t)j * b.tile;
-    const uint64_t re = rs + row_len(g, x);
-    e = s + b.tile < re ? s + b.tile : re;
+// Item k (one 16-byte load; the list is read-only after the builder).
+__device__ __forceinline__ SweepItem load_item(const SweepBufs& b, uint32_t k) {
+    const uint4 q = __ldg(reinterpret_cast<const uint4*>(b.items + k));
+    SweepItem it;
+    it.x = q.x;
+    it.len = q.y;
+    it.s = ((unsigned long long)q.w << 32) | q.z;
+    return it;
+}
+// The bounds of item `it` in slot space.
+__device__ __forceinline__ void item_bounds(const SweepItem& it, uint32_t& x, uint64_t& s, uint64_t& e) {
+    x = it.x;
+    s = it.s;
+    e = it.s + it.len;
+}
+
+// One round of an item's slots: lane l loads the 16-byte chunks at c + 4l and
+// c + 128 + 4l below e. The slot stream is read once per sweep: the loads are
+// marked evict-first so that L2 keeps the state words the gathers reuse.
+__device__ __forceinline__ void item_round(const Dev& g, uint64_t c, uint64_t e, uint32_t lane, uint4& q0, uint4& q1) {
+    const uint64_t i0 = c + 4ull * lane, i1 = i0 + 128;
+    q0 = make_uint4(INV, INV, INV, INV);
+    q1 = q0;
+    if (i0 < e) q0 = __ldcs(reinterpret_cast<const uint4*>(g.col + i0));
+    if (i1 < e) q1 = __ldcs(reinterpret_cast<const uint4*>(g.col + i1));
 }
 
 // Warp per item: up to b.tile live slots of one row. Nothing in the graph
 // changes during a sweep, so loads take the read-only path. Each lane keeps two
-// 16-byte slot loads and their eight state gathers in flight per round.
+// 16-byte slot loads and their eight state gathers in flight per round, and the
+// dependent chain is short: the descriptor of the warp's next item arrives
+// while this one is swept, an item's slot loads go out with its own state and
+// degree loads, and each round's gathers overlap the next round's slot loads.
 // SYM: accumulate the mirror checksum of rows whose graph wants it. PUSH
 // (independent-set rule): a same-colored neighbor that loses to x (lower
 // priority) is marked for the next sweep, which decides it from its own row.
@@ -671,10 +867,15 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
     const uint32_t cnt = *b.item_count;
-    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
+    uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    SweepItem it = k < cnt ? load_item(b, k) : SweepItem{0u, 0u, 0ull};
+    while (k < cnt) {
+        // the next item's descriptor is in flight while this item is swept
+        const uint32_t kn = k + warps;
+        const SweepItem nit = kn < cnt ? load_item(b, kn) : SweepItem{0u, 0u, 0ull};
         uint32_t x;
         uint64_t s, e;
-        item_bounds(g, b, b.items[k], x, s, e);
+        item_bounds(it, x, s, e);
         GraphCtl* gc = SYM ? &g.gctl[graph_of(g, x)] : nullptr;
         const bool symx = SYM && gc->full && ld_cg(&gc->asym);
         const uint32_t myc = color_of(__ldg(g.st + x));
@@ -682,12 +883,14 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
         uint32_t lo = 0, hi = 0;
         unsigned long long sym = 0;
         bool conf = false;
-        for (uint64_t c = s & ~3ull; c < e; c += 256) {
+        uint64_t c = s & ~3ull;
+        uint4 q0, q1;
+        item_round(g, c, e, lane, q0, q1);
+        for (; c < e; c += 256) {
             const uint64_t i0 = c + 4ull * lane, i1 = i0 + 128;
-            uint4 q0 = make_uint4(INV, INV, INV, INV), q1 = q0;
-            if (i0 < e) q0 = __ldg(reinterpret_cast<const uint4*>(g.col + i0));
-            if (i1 < e) q1 = __ldg(reinterpret_cast<const uint4*>(g.col + i1));
             uint32_t v[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+            // the next round's slots are requested before this round's gathers
+            if (c + 256 < e) item_round(g, c + 256, e, lane, q0, q1);
             uint32_t nc[8];
 #pragma unroll
             for (int t = 0; t < 8; t++) {
@@ -721,6 +924,8 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
             if (anyc) atomicOr(b.acc_fl + x, 1u);
             if (SYM && sym) atomicAdd(&gc->sym, sym);
         }
+        it = nit;
+        k = kn;
     }
 }
 
@@ -745,20 +950,23 @@ __global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b, in
 // One vertex of the finalize pass (warp-collective: every lane calls it; `valid`
 // lanes own a vertex). Short rows are swept here directly; long rows read the
 // accumulators. REBUILD writes bitmaps; TIER1 and INDEP also decide.
-// The vertex ids of a row of at most SWEEP_TINY live slots starting at slot s
-// (any alignment), INV where no vertex: the covering 16-byte chunks are loaded
-// in one round (aligned, inside the slab: chunks past the live slots are not
-// loaded), then the row's neighbor states in a second round, instead of one
-// dependent load-then-gather per slot.
-constexpr int kTinyChunks = (SWEEP_TINY + 3) / 4 + 1;
-__device__ __forceinline__ void tiny_row(const Dev& g, uint64_t s, uint32_t len, uint32_t (&y)[4 * kTinyChunks],
-                                         uint32_t (&w)[4 * kTinyChunks]) {
-    const uint64_t e = s + len, base = s & ~3ull;
+// A thread sweeps a row of at most SWEEP_TINY live slots in pieces of
+// kPiece slots: the vertex ids of slots [s, e) (any alignment; INV where no
+// vertex) come from the covering 16-byte chunks, all loaded in one round
+// (aligned, inside the slab: chunks past e are not loaded); the caller then
+// gathers what it needs for all of them in a second round. One row of up to
+// 64 entries costs a thread at most eight dependent round trips, instead of
+// two per slot, and 32 rows share a warp.
+constexpr uint32_t kPiece = 16;
+constexpr int kPieceIds = 4 * ((kPiece + 3) / 4 + 1);
+template <bool READONLY>
+__device__ __forceinline__ void piece_ids(const Dev& g, uint64_t s, uint64_t e, uint32_t (&y)[kPieceIds]) {
+    const uint64_t base = s & ~3ull;
 #pragma unroll
-    for (int c = 0; c < kTinyChunks; c++) {
+    for (int c = 0; c < kPieceIds / 4; c++) {
         const uint64_t i = base + 4ull * c;
         uint4 q = make_uint4(INV, INV, INV, INV);
-        if (i < e) q = __ldg(reinterpret_cast<const uint4*>(g.col + i));
+        if (i < e) q = READONLY ? __ldg(reinterpret_cast<const uint4*>(g.col + i)) : ld_cg4(g.col + i);
         const uint32_t v[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
         for (int t = 0; t < 4; t++) {
@@ -766,8 +974,6 @@ __device__ __forceinline__ void tiny_row(const Dev& g, uint64_t s, uint32_t len,
             y[4 * c + t] = (p >= s && p < e && v[t] < g.n) ? v[t] : INV;
         }
     }
-#pragma unroll
-    for (int t = 0; t < 4 * kTinyChunks; t++) w[t] = y[t] != INV ? __ldg(g.st + y[t]) : 0u;
 }
 
 __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, int mode, bool valid, uint32_t x,
@@ -790,18 +996,23 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
         if (len <= SWEEP_TINY) {
             const uint32_t mydeg = (g.abl & ABL_LIVE_DEG) ? len : __ldg(g.deg + x);
             uint32_t lo = 0, hi = 0;
-            uint32_t y[4 * kTinyChunks], sw[4 * kTinyChunks];
-            tiny_row(g, g.rp[x], len, y, sw);
+            const uint64_t s0 = g.rp[x], e0 = s0 + len;
+            for (uint64_t s = s0; s < e0; s += kPiece) {
+                uint32_t y[kPieceIds], sw[kPieceIds];
+                piece_ids<true>(g, s, s + kPiece < e0 ? s + kPiece : e0, y);
 #pragma unroll
-            for (int t = 0; t < 4 * kTinyChunks; t++) {
-                const uint32_t ng = y[t];
-                if (ng == INV) continue;
-                if (with_sym && ng != x) sym += sym_term(x, ng);
-                const uint32_t nc = color_of(sw[t]);
-                add_color_bit(nc, lo, hi);
-                if (nc == myc && nc != 0) {
-                    if (prio_less(mydeg, x, __ldg(g.deg + ng), ng)) conf = true;
-                    else if (push && ng != x) atomicOr(b.wmark + (ng >> 5), 1u << (ng & 31));
+                for (int t = 0; t < kPieceIds; t++) sw[t] = y[t] != INV ? __ldg(g.st + y[t]) : 0u;
+#pragma unroll
+                for (int t = 0; t < kPieceIds; t++) {
+                    const uint32_t ng = y[t];
+                    if (ng == INV) continue;
+                    if (with_sym && ng != x) sym += sym_term(x, ng);
+                    const uint32_t nc = color_of(sw[t]);
+                    add_color_bit(nc, lo, hi);
+                    if (nc == myc && nc != 0) {
+                        if (prio_less(mydeg, x, __ldg(g.deg + ng), ng)) conf = true;
+                        else if (push && ng != x) atomicOr(b.wmark + (ng >> 5), 1u << (ng & 31));
+                    }
                 }
             }
             bits = ((unsigned long long)hi << 32) | lo;
@@ -817,7 +1028,7 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
             bool decide = false;
             const bool indep = mode == SWEEP_INDEP;
             if (myc == 0) {
-                decide = len > (g.holes ? g.holes[x] : 0u);  // has_neighbors: any non-INV slot
+                decide = len > (g.live ? row_holes(g, x, g.hw[x]) : 0u);  // has_neighbors: any non-INV slot
             } else if (conf) {
                 decide = true;
                 if (myc <= 64) bits |= 1ull << (myc - 1);
@@ -918,12 +1129,12 @@ __global__ void __launch_bounds__(256) indep_items_kernel(Dev g, SweepBufs b) {
     used[lane + 32] = 0;
     __syncwarp();
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
-        const unsigned long long it = b.items[k];
-        if (!__ldg(b.needf + (uint32_t)it)) continue;
-        if (ld_cg(b.acc_fl + (uint32_t)it)) continue;  // another chunk already found it blocked
+        const SweepItem it = load_item(b, k);
+        if (!__ldg(b.needf + it.x)) continue;
+        if (ld_cg(b.acc_fl + it.x)) continue;  // another chunk already found it blocked
         uint32_t x;
         uint64_t s, e;
-        item_bounds(g, b, it, x, s, e);
+        item_bounds(it, x, s, e);
         const uint32_t hd = __ldg(g.hdmap + x);
         const bool full = hd != EMPTY && g.exact && ~b.acc_bm[x] == 0ull;
         const uint32_t base = g.gctl[graph_of(g, x)].base;  // ranks use the graph's own ids
@@ -982,12 +1193,18 @@ __global__ void __launch_bounds__(256) indep_decide_kernel(Dev g, SweepBufs b) {
         const uint32_t len = row_len(g, x);
         bool blocked = false;
         if (len <= SWEEP_TINY) {
-            const uint64_t s = g.rp[x];
             const uint32_t base = g.gctl[graph_of(g, x)].base;  // ranks use the graph's own ids
             const unsigned long long rx = sel_rank(x - base, salt);
-            for (uint32_t j = 0; j < len && !blocked; j++) {
-                const uint32_t y = __ldg(g.col + s + j);
-                if (y < g.n && y != x && __ldg(b.needf + y) && sel_rank(y - base, salt) > rx) blocked = true;
+            const uint64_t s0 = g.rp[x], e0 = s0 + len;
+            for (uint64_t s = s0; s < e0 && !blocked; s += kPiece) {
+                uint32_t y[kPieceIds];
+                uint8_t nf[kPieceIds];
+                piece_ids<true>(g, s, s + kPiece < e0 ? s + kPiece : e0, y);
+#pragma unroll
+                for (int t = 0; t < kPieceIds; t++) nf[t] = (y[t] != INV && y[t] != x) ? __ldg(b.needf + y[t]) : 0;
+#pragma unroll
+                for (int t = 0; t < kPieceIds; t++)
+                    if (nf[t] && sel_rank(y[t] - base, salt) > rx) blocked = true;
             }
         } else if (b.acc_fl[x]) {
             blocked = true;
@@ -1042,13 +1259,17 @@ __global__ void sweep_commit_kernel(Dev g, SweepBufs b, int mode) {
         if (!incr) atomicOr(b.wmark + (x >> 5), 1u << (x & 31));
         const uint32_t len = row_len(g, x);
         if (len <= SWEEP_TINY) {
-            const uint64_t s = g.rp[x];
             const uint32_t c = color_of(nw);
-            for (uint32_t j = 0; j < len; j++) {
-                const uint32_t y = g.col[s + j];
-                if (y >= g.n) continue;
-                if (!incr) atomicOr(b.wmark + (y >> 5), 1u << (y & 31));
-                else if (c != 0 && c <= 64) atomicOr((unsigned long long*)(g.bm + y), 1ull << (c - 1));
+            const uint64_t s0 = g.rp[x], e0 = s0 + len;
+            for (uint64_t s = s0; s < e0; s += kPiece) {
+                uint32_t y[kPieceIds];
+                piece_ids<false>(g, s, s + kPiece < e0 ? s + kPiece : e0, y);
+#pragma unroll
+                for (int t = 0; t < kPieceIds; t++) {
+                    if (y[t] == INV) continue;
+                    if (!incr) atomicOr(b.wmark + (y[t] >> 5), 1u << (y[t] & 31));
+                    else if (c != 0 && c <= 64) atomicOr((unsigned long long*)(g.bm + y[t]), 1ull << (c - 1));
+                }
             }
         }
     }
@@ -1063,12 +1284,12 @@ __global__ void __launch_bounds__(256) mark_items_kernel(Dev g, SweepBufs b) {
     const uint32_t cnt = *b.item_count;
     const bool incr = ld_cg(&b.rc->mode) == SWEEP_INDEP;
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
-        const unsigned long long it = b.items[k];
-        const uint32_t x0 = (uint32_t)it;
+        const SweepItem it = load_item(b, k);
+        const uint32_t x0 = it.x;
         if (!(b.rbits[x0 >> 5] & (1u << (x0 & 31)))) continue;
         uint32_t x;
         uint64_t s, e;
-        item_bounds(g, b, it, x, s, e);
+        item_bounds(it, x, s, e);
         const uint32_t c = color_of(g.st[x]);
         const unsigned long long bit = (c != 0 && c <= 64) ? 1ull << (c - 1) : 0ull;
         if (incr && !bit) continue;

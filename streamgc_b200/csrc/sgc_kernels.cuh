@@ -9,7 +9,7 @@ namespace sgc {
 
 constexpr uint32_t SWEEP_CH = 512;       // default slots per warp work item in a sweep (repair tile width)
 constexpr uint32_t SWEEP_CH_MIN = 256;   // smallest tile width (sizes the item list)
-constexpr uint32_t SWEEP_TINY = 16;      // rows this short are swept by one thread
+constexpr uint32_t SWEEP_TINY = 64;      // rows this short are swept by one thread (16-slot vector chunks)
 constexpr uint32_t NONE32 = 0xFFFFFFFFu;
 constexpr unsigned long long EMPTY64 = 0xFFFFFFFFFFFFFFFFull;
 
@@ -34,10 +34,20 @@ struct RepairCtl {
     unsigned long long live;  // first sweep's live entries
 };
 
+// One warp item of a sweep: `len` (at most the tile width) live slots of row
+// x, from slot `s` on. Written by the item builder of each sweep (rows do not
+// change during a sweep), so a warp issues the item's slot loads as soon as
+// the descriptor arrives.
+struct __align__(16) SweepItem {
+    uint32_t x;
+    uint32_t len;
+    unsigned long long s;
+};
+
 // Per-sweep work state: warp items for rows longer than SWEEP_TINY, per-vertex
 // accumulators, the Jacobi pending list and the FAC work list.
 struct SweepBufs {
-    unsigned long long* items;   // x | chunk << 32
+    SweepItem* items;
     uint32_t* item_count;
     uint32_t item_cap;
     uint32_t tile;               // slots per item (repair tile width, >= SWEEP_CH_MIN)

@@ -446,7 +446,8 @@ __global__ void check_state_kernel(Dev g, unsigned long long* out /* bad rows, f
         f = __reduce_or_sync(FULL, f);
         holes_in = __reduce_add_sync(FULL, holes_in);
         if (lane == 0) {
-            if (g.holes && g.holes[x] > he - s) f |= SGC_STATE_HOLES;  // the counter wrapped below zero
+            // the live count: exact between batches (mark minus free slots and tombstones)
+            if (g.live && hw <= cap && g.live[x] != (he - s) - holes_in) f |= SGC_STATE_HOLES;
             if (color_of(g.st[x]) > 2048) f |= SGC_STATE_COLOR;
             if (f) {
                 atomicAdd(out + 0, 1ull);
@@ -454,7 +455,6 @@ __global__ void check_state_kernel(Dev g, unsigned long long* out /* bad rows, f
                 atomicMin(out + 2, (unsigned long long)x);
             }
         }
-        (void)holes_in;
     }
 }
 

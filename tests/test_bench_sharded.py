@@ -234,7 +234,8 @@ def _rank(rank, world, port, form, q, workload="small", large_div=1):
                                  served_regrow=False, sorted_rows=False, workload=workload, cpu_batches=0,
                                  cpu_seconds=1.0, profile_window=False, graph_publish=False, ingest=False,
                                  latency_epochs=4, validate_steps=True, large_div=large_div,
-                                 full_repair_every=0, profile_full_sweep=True)
+                                 full_repair_every=0, profile_full_sweep=True,
+                                 profile_full_sweep_window=False)
     out, err = io.StringIO(), None
     old = sys.stdout
     sys.stdout = out
