@@ -470,9 +470,11 @@ def full_sweep_roofline(s0, s1, rep, peak, peak_kind):
     if ms <= 0 or n <= 0:
         return None
     ach = by / (ms / 1e3) / 1e9
+    ph = [b - a for a, b in zip(s0.get("sweep_phase_ms", [0] * 4), s1.get("sweep_phase_ms", [0] * 4))]
     return {"bound": "hbm", "kernel": "tier-1 sweep over every vertex (sweep_items + finalize + fac + commit)",
             "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
-            "algorithmic_bytes": by, "sweeps": n, "ms": ms, "proper": rep["proper"]}
+            "algorithmic_bytes": by, "sweeps": n, "ms": ms, "proper": rep["proper"],
+            "phases_ms": dict(zip(("item_build", "long_row_items", "finalize", "select_commit"), ph))}
 
 
 def cpu_baseline(g, h, bench, first_batch, nb, budget_s):

@@ -117,9 +117,8 @@ typedef struct sgc_stats {
     uint64_t kernel_launches;    /* kernels launched by this handle */
     uint64_t h2d_bytes;          /* update bytes copied host -> device by sgc_apply */
     uint64_t d2h_bytes;          /* bytes the library read back (repair counters, stats) */
-    uint64_t hub_deferred;       /* row-scale operations of concurrent batches (color reductions and
-                                    recolors of rows longer than 512 live entries) finished by the
-                                    block-wide pass after the batch (cumulative) */
+    double   sweep_phase_ms[4];  /* SGC_OPT_PROFILE: sweep_ms by phase: item build, long-row items,
+                                    per-vertex finalize, color selection and commit */
 } sgc_stats;
 
 typedef struct sgc_validation {

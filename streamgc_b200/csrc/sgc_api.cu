@@ -63,16 +63,17 @@ cudaEvent_t take_event(sgc_handle* h) {
     return e;
 }
 
-// Gathers the elapsed time of recorded sweep event pairs (stream must be idle).
+// Gathers the elapsed time of recorded sweeps, whole and per phase (stream must be idle).
 void collect_events(sgc_handle* h) {
-    for (auto& pr : h->ev_pending) {
+    for (auto& se : h->ev_pending) {
         float ms = 0;
-        if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) {
+        if (cudaEventElapsedTime(&ms, se.ev[0], se.ev[4]) == cudaSuccess) {
             h->sweep_ms += ms;
             h->sweep_count++;
+            for (int k = 0; k < 4; k++)
+                if (cudaEventElapsedTime(&ms, se.ev[k], se.ev[k + 1]) == cudaSuccess) h->sweep_phase_ms[k] += ms;
         }
-        h->ev_pool.push_back(pr.first);
-        h->ev_pool.push_back(pr.second);
+        for (int k = 0; k < 5; k++) h->ev_pool.push_back(se.ev[k]);
     }
     h->ev_pending.clear();
 }
@@ -168,16 +169,15 @@ int repair_loop(sgc_handle* h, sgc_repair_report* rep, bool force_full) {
     RepairCtl* rc = h->h_rc_out;
     for (uint32_t sweeps = 0;; sweeps++) {
         if (sweeps > hin->max_sweeps) return fail(SGC_EDEVICE, "repair loop ran past %u sweeps", hin->max_sweeps);
-        cudaEvent_t a = nullptr, b = nullptr;
+        sgc_handle::SweepEvents se{};
         if (prof) {
-            a = take_event(h);
-            b = take_event(h);
-            cudaEventRecord(a, h->stream);
+            for (int k = 0; k < 5; k++) se.ev[k] = take_event(h);
+            cudaEventRecord(se.ev[0], h->stream);
         }
-        launch_repair_sweep(h->g, h->sb, mode, h->num_sms, h->stream);
+        launch_repair_sweep(h->g, h->sb, mode, h->num_sms, h->stream, prof ? se.ev + 1 : nullptr);
         if (prof) {
-            cudaEventRecord(b, h->stream);
-            h->ev_pending.push_back({a, b});
+            cudaEventRecord(se.ev[4], h->stream);
+            h->ev_pending.push_back(se);
         }
         launch_repair_step(h->g, h->sb, h->num_sms, h->stream, nullptr);
         h->launches += 1 + (mode == SWEEP_INDEP ? 6 : 4) + 3;
@@ -435,7 +435,8 @@ int sgc_destroy(sgc_handle* h) {
     if (h->h_rc_in) cudaFreeHost(h->h_rc_in);
     if (h->h_rc_out) cudaFreeHost(h->h_rc_out);
     if (h->stage_free) cudaEventDestroy(h->stage_free);
-    for (auto& pr : h->ev_pending) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    for (auto& se : h->ev_pending)
+        for (int k = 0; k < 5; k++) cudaEventDestroy(se.ev[k]);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
     if (h->t2.rev_keys) cudaFree(h->t2.rev_keys);
     if (h->t2.rev_keys2) cudaFree(h->t2.rev_keys2);
@@ -616,12 +617,6 @@ int sgci::create_internal(const StreamGCConfig* cfg, const sgc_options* opt_in, 
     A(&eo.tsucc, mb);
     eo.ticket = &h->ctl->ticket;
     eo.tmask = tsize - 1;
-    if (g.exact) {  // row-scale operations of concurrent batches: the pass after the batch
-        A(&g.hub_ops, 2ull * mb);
-        g.hub_count = &h->ctl->hub_count;
-        g.hub_cap = 2 * mb;
-        g.hub_total = &h->ctl->hub_total;
-    }
     // sweep buffers
     SweepBufs& sb = h->sb;
     const uint64_t icap = h->total_slots / SWEEP_CH_MIN + (uint64_t)n + 1;
@@ -1179,7 +1174,7 @@ int sgc_get_stats(sgc_handle* h, sgc_stats* o) {
     o->kernel_launches = h->launches;
     o->h2d_bytes = h->h2d_bytes;
     o->d2h_bytes = h->d2h_bytes;
-    o->hub_deferred = c.hub_total;
+    for (int k = 0; k < 4; k++) o->sweep_phase_ms[k] = h->sweep_phase_ms[k];
     return c.err ? fail(SGC_EDEVICE, "device error word 0x%x", c.err) : SGC_OK;
 }
 

@@ -61,18 +61,6 @@ struct GraphCtl {
     uint32_t dropped; // an entry of this graph was dropped (a full row at drain, or the overflow buffer full)
 };
 
-// A row-scale operation of a concurrent batch left to the pass after it
-// (exact selection): HUB_REDUCE moves x to color `freed` when that is below
-// x's color and no live neighbor of x holds it; HUB_RECOLOR moves x to its
-// first free color. The pass re-reads x's state word.
-enum : uint32_t { HUB_REDUCE = 1u, HUB_RECOLOR = 2u };
-struct HubOp {
-    uint32_t x;
-    uint32_t op;  // kind << 16 | freed
-};
-// Live slots a warp scans itself before it leaves the rest of a row to the pass.
-constexpr uint32_t kHubScan = 512;
-
 // Device view of one graph's state (handle layout). Row x owns logical slots
 // [rp[x], rp[x+1]); hw[x] bounds the slots ever written since the row was last
 // compacted (every slot at or past rp[x]+hw[x] holds INV), so after compaction
@@ -109,10 +97,6 @@ struct Dev {
                                    // endpoints of an ADD whose colors are equal at the end of its batch
     uint32_t* chg;                 // single-graph handles under exact selection: bitmask of the vertices
                                    // whose color changed since the last snapshot (null otherwise)
-    HubOp* hub_ops;                // concurrent batches under exact selection: row-scale operations left
-    uint32_t* hub_count;           // to the pass after the batch (null: none are deferred); the count
-    uint32_t hub_cap;              // runs past hub_cap when the list is full (those are done in place)
-    unsigned long long* hub_total; // cumulative count of the operations the pass took
     GraphCtl* gctl;                // per graph: repair flags (one entry for a single-graph handle)
     const uint32_t* gidw;          // graph of each 32-vertex word (graphs start at multiples of 32);
                                    // null: one graph
@@ -164,7 +148,7 @@ struct Lanes {
     }
     __device__ __forceinline__ bool leader() const { return lane == 0; }
     // bit k: the group's lane k
-    __device__ __forceinline__ uint32_t ballot(bool p) const { return __ballot_sync(mask, p) >> base; }
+    __device__ __forceinline__ uint32_t ballot(bool p) const { return (__ballot_sync(mask, p) & mask) >> base; }
     template <class T>
     __device__ __forceinline__ T shfl(T v, int src) const { return __shfl_sync(mask, v, src, W); }
     __device__ __forceinline__ void sync() const { __syncwarp(mask); }
@@ -768,32 +752,6 @@ __device__ __forceinline__ bool warp_color_held(const Dev& g, uint32_t x, uint16
     return warp_gather_each<true, 1>(g.col, s, e, g.n, g.st, [c](uint32_t, uint32_t w) { return color_of(w) == c; });
 }
 
-// Does a live neighbor among the first `lim` live slots of x hold color c?
-// `all`: those slots were the whole row.
-__device__ __forceinline__ bool warp_color_held_first(const Dev& g, uint32_t x, uint16_t c, uint32_t lim, bool& all) {
-    const uint64_t s = g.rp[x], e = live_end(g, x, s);
-    const uint64_t e1 = e - s > lim ? s + lim : e;
-    all = e1 == e;
-    return warp_gather_each<true, 4>(g.col, s, e1, g.n, g.st, [c](uint32_t, uint32_t w) { return color_of(w) == c; });
-}
-
-// Appends a row-scale operation to the pass after the batch (lane 0).
-// Warp-collective; false when nothing is deferred (no list, or it is full):
-// the caller then does the work itself.
-__device__ __forceinline__ bool warp_defer(const Dev& g, uint32_t x, uint32_t kind, uint16_t freed) {
-    if (!g.hub_ops) return false;
-    uint32_t ok = 0;
-    if (lane_id() == 0) {
-        const uint32_t pos = atomicAdd(g.hub_count, 1u);
-        if (pos < g.hub_cap) {
-            g.hub_ops[pos].x = x;
-            g.hub_ops[pos].op = (kind << 16) | freed;
-            ok = 1;
-        }
-    }
-    return __shfl_sync(FULL, ok, 0) != 0;
-}
-
 // Both endpoints' state words in one round trip (lanes 0 and 1).
 __device__ __forceinline__ void warp_load_states2(const Dev& g, uint32_t u, uint32_t v, uint32_t& su, uint32_t& sv) {
     const uint32_t lane = lane_id();
@@ -861,9 +819,25 @@ __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v,
     // same values; in a concurrent batch a later change by another warp is a
     // color change (marked) or leaves this ADD's endpoints equal (caught by
     // the check after the batch).
+    // In a concurrent batch the two row edits of an edge (u != v) touch two
+    // different rows and no other warp edits those slots of theirs, so the
+    // two halves of the warp make them at once (lanes 0-15 row u, 16-31 row
+    // v). In stream order they stay in order: the overflow buffer records
+    // u's entry before v's, as the reference does.
+    const bool halves = !exact && u != v;
     if (type == SGC_UPDATE_ADD) {
-        const int ru = warp_add_slot(g, u, v, exact);
-        const int rv = warp_add_slot(g, v, u, exact);
+        int ru, rv;
+        if (halves) {
+            const Lanes<16> H;
+            const uint32_t x = H.base ? v : u, y = H.base ? u : v;  // one call site: the halves stay converged
+            const int r = grp_add_slot(H, g, x, y, false);
+            __syncwarp();
+            ru = __shfl_sync(FULL, r, 0);
+            rv = __shfl_sync(FULL, r, 16);
+        } else {
+            ru = warp_add_slot(g, u, v, exact);
+            rv = warp_add_slot(g, v, u, exact);
+        }
         if (ru != rv && lane_id() == 0) flag_asym(g, u);
         uint32_t su, sv;
         warp_load_states2(g, u, v, su, sv);
@@ -889,8 +863,18 @@ __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v,
         warp_load_states2(g, u, v, su, sv);
         const uint16_t fu = color_of(sv);
         const uint16_t fv = color_of(su);
-        const bool du = warp_remove_slot(g, u, v, exact);
-        const bool dv = warp_remove_slot(g, v, u, exact);
+        bool du, dv;
+        if (halves) {
+            const Lanes<16> H;
+            const uint32_t x = H.base ? v : u, y = H.base ? u : v;
+            const int d = grp_remove_slot(H, g, x, y, false) ? 1 : 0;
+            __syncwarp();
+            du = __shfl_sync(FULL, d, 0) != 0;
+            dv = __shfl_sync(FULL, d, 16) != 0;
+        } else {
+            du = warp_remove_slot(g, u, v, exact);
+            dv = warp_remove_slot(g, v, u, exact);
+        }
         if (lane_id() == 0) {
             if (du != dv) flag_asym(g, u);
             removed_nbr(g, u, fu);
@@ -900,144 +884,6 @@ __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v,
         warp_try_reduce(g, u, fu, exact, su);
         if (v == u) sv = warp_load_state(g, v);
         warp_try_reduce(g, v, fv, exact, sv);
-    }
-}
-
-// ---------------- one update of a concurrent batch ----------------
-
-// The neighbor-class bookkeeping of new_nbr / removed_nbr with x's class `hd`
-// already read (exact selection keeps no histogram rows: no load at all).
-__device__ __forceinline__ void new_nbr_cls(const Dev& g, uint32_t x, uint32_t hd, uint16_t c) {
-    if (c == 0) return;
-    if (c <= 64) set_bm_bit<false>(g, x, c);
-    if (!g.exact && hd != EMPTY && c <= g.maxc) atomicAdd(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
-}
-__device__ __forceinline__ void removed_nbr_cls(const Dev& g, uint32_t x, uint32_t hd, uint16_t c) {
-    if (!g.exact && c != 0 && hd != EMPTY && c <= g.maxc) atomicSub(g.hist + (uint64_t)hd * g.maxc + c - 1, 1u);
-}
-
-// try_color_reduction in a concurrent batch, from x's state word, class and
-// bitmap as read at the start of the update (bitmap bits are only added
-// during a batch: a bit set since makes at most a conflict, which marks x for
-// the repair through its recolor). Same rule as warp_try_reduce.
-__device__ __forceinline__ void warp_try_reduce_conc(const Dev& g, uint32_t x, uint16_t freed, uint32_t state,
-                                                     uint32_t hd, unsigned long long bmv) {
-    const uint16_t cur = color_of(state);
-    if (cur == 0 || freed >= cur) return;
-    if (g.exact && hd != EMPTY) {
-        if (freed == 0) return;
-        // a holder is usually among the first neighbors; a long row without
-        // one there is finished (scan, move, walk) by the pass after the batch
-        bool all = true;
-        if (warp_color_held_first(g, x, freed, g.hub_ops ? kHubScan : 0xFFFFFFFFu, all)) return;
-        if (!all && (warp_defer(g, x, HUB_REDUCE, freed) || warp_color_held(g, x, freed))) return;
-        warp_recolor_from(g, x, freed, state);
-        return;
-    }
-    uint16_t best;
-    if (hd != EMPTY && !(g.abl & ABL_FORCE_BITMAP)) best = warp_fac_hist(g.hist + (uint64_t)hd * g.maxc, g.maxc);
-    else if (~bmv) best = (uint16_t)__ffsll((long long)~bmv);
-    else best = warp_fac_scan(g, x, g.st);
-    if (best < cur) warp_recolor_from(g, x, best, state);
-}
-
-// Row edits of one edge in both directions. For u != v the two rows are
-// different and no other warp edits those slots of theirs (the updates of an
-// edge are ordered), so the two halves of the warp make the edits at once:
-// lanes 0-15 row u, 16-31 row v. Returns the two results in (ru, rv).
-template <bool ADD>
-__device__ __forceinline__ void warp_edit_both(const Dev& g, uint32_t u, uint32_t v, int& ru, int& rv) {
-    if (u != v) {
-        const Lanes<16> H;
-        const uint32_t x = H.base ? v : u, y = H.base ? u : v;  // one call site: the halves stay converged
-        const int r = ADD ? grp_add_slot(H, g, x, y, false) : (grp_remove_slot(H, g, x, y, false) ? 1 : 0);
-        __syncwarp();
-        ru = __shfl_sync(FULL, r, 0);
-        rv = __shfl_sync(FULL, r, 16);
-    } else {
-        ru = ADD ? warp_add_slot(g, u, v, false) : (warp_remove_slot(g, u, v, false) ? 1 : 0);
-        rv = ADD ? warp_add_slot(g, v, u, false) : (warp_remove_slot(g, v, u, false) ? 1 : 0);
-    }
-}
-
-// One update of a concurrent batch: the reference's ADD / DEL sequence
-// (local_update.cu:61-147) with its loads gathered into as few dependent
-// rounds as the rules allow. The endpoints' classes (and, for a DEL, their
-// state words and bitmaps, which the reference reads before the row edits)
-// are requested first and used after the edits, so they arrive during them.
-// An ADD reads the state words after its edits and keeps them: a later change
-// by another warp is a color change (marked) or leaves this ADD's endpoints
-// equal (caught by the check after the batch).
-__device__ __forceinline__ void warp_apply_conc(const Dev& g, uint32_t u, uint32_t v, uint8_t type) {
-    const uint32_t lane = lane_id();
-    const bool del = type == SGC_UPDATE_DEL;
-    const uint32_t x = (lane & 1) ? v : u;
-    uint32_t w = 0;
-    unsigned long long bw = 0;
-    if (lane < 2) w = __ldg(g.hdmap + x);             // classes (read-only)
-    else if (lane < 4 && del) w = ld_cg(g.st + x);    // DEL: state words
-    else if (lane < 6 && del) bw = ld_cg(g.bm + x);   // DEL: bitmaps
-    if (type == SGC_UPDATE_ADD) {
-        int ru, rv;
-        warp_edit_both<true>(g, u, v, ru, rv);
-        if (ru != rv && lane == 0) flag_asym(g, u);
-        uint32_t su, sv;
-        warp_load_states2(g, u, v, su, sv);
-        const uint32_t hu = __shfl_sync(FULL, w, 0), hv = __shfl_sync(FULL, w, 1);
-        if (lane == 0 && g.touched) {  // bitmap-class endpoints: their bitmaps are rebuilt by the repair
-            if (hu == EMPTY) mark_touched(g, u);
-            if (hv == EMPTY) mark_touched(g, v);
-        }
-        if (color_of(su) == 0) {
-            su = warp_color_uncolored(g, u, su);
-            if (v == u) sv = su;
-        }
-        if (color_of(sv) == 0) {
-            if (lane == 0) new_nbr_cls(g, v, hv, color_of(su));
-            __syncwarp();
-            sv = warp_color_uncolored(g, v, sv);
-        }
-        if (lane == 0) new_nbr_cls(g, u, hu, color_of(sv));
-        else if (lane == 1) new_nbr_cls(g, v, hv, color_of(su));
-        __syncwarp();
-        const uint16_t cu = color_of(su), cv = color_of(sv);
-        if (cu == cv && cu != 0) {
-            const bool lu = prio_less(__ldg(g.deg + u), u, __ldg(g.deg + v), v);
-            const uint32_t loser = lu ? u : v;
-            // a long histogram-class row: its selection and walk go to the pass after the batch
-            const bool defer = g.hub_ops && (lu ? hu : hv) != EMPTY && row_len(g, loser) > kHubScan &&
-                               warp_defer(g, loser, HUB_RECOLOR, 0);
-            if (!defer) warp_recolor_from(g, loser, 0, lu ? su : sv);
-        }
-    } else if (del) {
-        int du, dv;
-        warp_edit_both<false>(g, u, v, du, dv);
-        const uint32_t hu = __shfl_sync(FULL, w, 0), hv = __shfl_sync(FULL, w, 1);
-        const uint32_t su = __shfl_sync(FULL, w, 2);
-        uint32_t sv = __shfl_sync(FULL, w, 3);
-        const unsigned long long bu = __shfl_sync(FULL, bw, 4), bv = __shfl_sync(FULL, bw, 5);
-        const uint16_t fu = color_of(sv), fv = color_of(su);
-        if (lane == 0) {
-            if (du != dv) flag_asym(g, u);
-            if (g.touched) {
-                if (hu == EMPTY) mark_touched(g, u);
-                if (hv == EMPTY) mark_touched(g, v);
-            }
-            removed_nbr_cls(g, u, hu, fu);
-            removed_nbr_cls(g, v, hv, fv);
-        }
-        __syncwarp();
-        warp_try_reduce_conc(g, u, fu, su, hu, bu);
-        unsigned long long bv2 = bv;
-        if (v == u) {  // the same row: its word and bitmap as the first reduction left them
-            uint32_t w2 = 0;
-            unsigned long long b2 = 0;
-            if (lane == 0) w2 = ld_cg(g.st + v);
-            else if (lane == 1) b2 = ld_cg(g.bm + v);
-            sv = __shfl_sync(FULL, w2, 0);
-            bv2 = __shfl_sync(FULL, b2, 1);
-        }
-        warp_try_reduce_conc(g, v, fv, sv, hv, bv2);
     }
 }
 

@@ -36,15 +36,12 @@ struct Ctl {
     uint32_t pend_count;
     uint32_t fac_count;
     uint32_t ticket;
-    uint32_t hub_count;  // row-scale operations deferred by the last concurrent batch
-    uint32_t hub_pad;
     unsigned long long ovf_lost;
     unsigned long long nskip;
     unsigned long long drain_failed;
     unsigned long long symsum;
     unsigned long long live;
-    unsigned long long hub_total;  // cumulative: operations the pass after concurrent batches finished
-    unsigned long long pad[2];
+    unsigned long long pad[3];
 };
 
 }  // namespace sgci
@@ -86,8 +83,12 @@ struct sgc_handle {
     uint64_t updates = 0, epochs = 0, tier1_sweeps = 0, tier2_runs = 0, tier2_fixed = 0;
     // profiling
     std::vector<cudaEvent_t> ev_pool;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
+    struct SweepEvents {
+        cudaEvent_t ev[5];  // start, after the item build, the long-row items, the finalize; end
+    };
+    std::vector<SweepEvents> ev_pending;
     double sweep_ms = 0;
+    double sweep_phase_ms[4] = {0, 0, 0, 0};  // item build, long-row items, finalize, selection + commit
     uint64_t sweep_count = 0, sweep_bytes = 0, live_entries = 0;
     // stream ingest: two device slots filled on a copy stream (allocated on first use)
     cudaStream_t copy_stream = nullptr;

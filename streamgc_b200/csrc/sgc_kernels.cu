@@ -94,10 +94,7 @@ __device__ __forceinline__ uint32_t batch_n(uint32_t n, const uint32_t* dyn) { r
 __global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg, EdgeOrder eo,
                                  const uint32_t* dyn) {
     const uint32_t n = batch_n(n_arg, dyn);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        *eo.ticket = 0;
-        if (g.hub_count) *g.hub_count = 0;
-    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *eo.ticket = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
         const uint32_t u = r.x, v = r.y;
@@ -174,7 +171,7 @@ __global__ void __launch_bounds__(256, 3) conc_apply_kernel(Dev g, const EdgeUpd
                     if (lane_id() == 0) atomicOr(g.err, ERR_CHAIN);
                     break;
                 }
-                warp_apply_conc(g, r.x, r.y, (uint8_t)(r.z & 0xFFu));
+                warp_apply(g, r.x, r.y, (uint8_t)(r.z & 0xFFu), false);
                 const uint32_t j = succ;
                 if (j == NONE32) break;
                 if (j >= n || j < i || ++steps > n) {  // ordering words inconsistent with the batch
@@ -191,159 +188,6 @@ __global__ void __launch_bounds__(256, 3) conc_apply_kernel(Dev g, const EdgeUpd
             __syncwarp();
         }
         i = __shfl_sync(FULL, next, 0);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// The pass after a concurrent batch: row-scale operations the apply left
-// (HubOp), one block of kHubThreads per operation. Each re-reads x's state
-// word; the scans and the neighbor walk after a move take 8192 slots per
-// round over the whole block. Decisions are made on words thread 0 read and
-// shared, so every branch is block-uniform.
-// ---------------------------------------------------------------------------
-constexpr uint32_t kHubThreads = 1024;
-
-// The ids of one round's slots: thread t loads the 16-byte chunks at
-// c + 4t and c + 4t + 4096 (INV outside [s, e) and for ids >= n).
-__device__ __forceinline__ void hub_round(const Dev& g, uint64_t c, uint64_t s, uint64_t e, uint32_t (&y)[8]) {
-    const uint64_t i0 = c + 4ull * threadIdx.x, i1 = i0 + 4ull * kHubThreads;
-    uint4 q0 = make_uint4(INV, INV, INV, INV), q1 = q0;
-    if (i0 < e) q0 = ld_cg4(g.col + i0);
-    if (i1 < e) q1 = ld_cg4(g.col + i1);
-    const uint32_t v[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-#pragma unroll
-    for (int t = 0; t < 8; t++) {
-        const uint64_t p = (t < 4 ? i0 : i1) + (t & 3);
-        y[t] = (p >= s && p < e && v[t] < g.n) ? v[t] : INV;
-    }
-}
-
-// Does a live neighbor in [s, e) hold color c? Stops after the first round that finds one.
-__device__ __forceinline__ bool block_color_held(const Dev& g, uint64_t s, uint64_t e, uint16_t c) {
-    for (uint64_t r = s & ~3ull; r < e; r += 8ull * kHubThreads) {
-        uint32_t y[8];
-        hub_round(g, r, s, e, y);
-        uint32_t w[8];
-#pragma unroll
-        for (int t = 0; t < 8; t++) w[t] = y[t] != INV ? ld_cg(g.st + y[t]) : 0u;
-        bool hit = false;
-#pragma unroll
-        for (int t = 0; t < 8; t++) hit |= y[t] != INV && color_of(w[t]) == c;
-        if (__syncthreads_or(hit)) return true;
-    }
-    return false;
-}
-
-// Exact selection: the first color no live neighbor in [s, e) holds (colors
-// 1..2047, else 2048), as warp_fac_exact. `used`: 64 words of shared memory.
-__device__ __forceinline__ uint16_t block_fac_exact(const Dev& g, uint64_t s, uint64_t e, uint32_t* used,
-                                                    uint32_t* pick) {
-    if (threadIdx.x < 64) used[threadIdx.x] = 0;
-    __syncthreads();
-    uint32_t lo = 0, hi = 0;  // colors 1..64 (bits 0..63 of a 64-bit mask)
-    for (uint64_t r = s & ~3ull; r < e; r += 8ull * kHubThreads) {
-        uint32_t y[8];
-        hub_round(g, r, s, e, y);
-        uint32_t w[8];
-#pragma unroll
-        for (int t = 0; t < 8; t++) w[t] = y[t] != INV ? ld_cg(g.st + y[t]) : 0u;
-#pragma unroll
-        for (int t = 0; t < 8; t++) {
-            if (y[t] == INV) continue;
-            const uint16_t c = color_of(w[t]);
-            add_color_bit(c, lo, hi);
-            if (c > 64 && c < 2048) atomicOr(&used[c >> 5], 1u << (c & 31));
-        }
-    }
-    lo = __reduce_or_sync(FULL, lo);
-    hi = __reduce_or_sync(FULL, hi);
-    if (lane_id() == 0) {  // fold colors 1..64 into the same set (color c: word c >> 5, bit c & 31)
-        if (lo) atomicOr(&used[0], lo << 1);
-        if (lo >> 31) atomicOr(&used[1], 1u);
-        if (hi) atomicOr(&used[1], hi << 1);
-        if (hi >> 31) atomicOr(&used[2], 1u);
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        const uint32_t l = threadIdx.x;
-        uint32_t w0 = ~used[l], w1 = ~used[l + 32];
-        if (l == 0) w0 &= ~1u;  // color 0 is never a candidate
-        const uint32_t b0 = __ballot_sync(FULL, w0 != 0), b1 = __ballot_sync(FULL, w1 != 0);
-        if (l == 0) {
-            uint32_t c = 2048;
-            if (b0) {
-                const int src = __ffs(b0) - 1;
-                c = src * 32 + __ffs(~used[src] & (src == 0 ? ~1u : FULL)) - 1;
-            } else if (b1) {
-                const int src = __ffs(b1) - 1;
-                c = 1024 + src * 32 + __ffs(~used[src + 32]) - 1;
-            }
-            *pick = c;
-        }
-    }
-    __syncthreads();
-    const uint16_t c = (uint16_t)*pick;
-    __syncthreads();
-    return c;
-}
-
-__global__ void __launch_bounds__(kHubThreads) hub_ops_kernel(Dev g) {
-    __shared__ uint32_t used[64];
-    __shared__ uint32_t word[2];
-    const uint32_t total = ld_cg(g.hub_count);
-    const uint32_t cnt = total < g.hub_cap ? total : g.hub_cap;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && cnt) atomicAdd(g.hub_total, (unsigned long long)cnt);
-    for (uint32_t k = blockIdx.x; k < cnt; k += gridDim.x) {
-        const HubOp op = g.hub_ops[k];
-        const uint32_t x = op.x;
-        if (x >= g.n) continue;  // block-uniform: every thread read the same record
-        const uint32_t kind = op.op >> 16;
-        const uint16_t freed = (uint16_t)(op.op & 0xFFFFu);
-        const uint64_t s = g.rp[x], e = live_end(g, x, s);
-        if (threadIdx.x == 0) word[0] = ld_cg(g.st + x);
-        __syncthreads();
-        uint32_t cur = word[0];
-        __syncthreads();
-        uint16_t newc;
-        if (kind == HUB_REDUCE) {
-            if (freed == 0 || freed >= color_of(cur) || block_color_held(g, s, e, freed)) continue;
-            newc = freed;
-        } else {
-            newc = block_fac_exact(g, s, e, used, &word[1]);
-        }
-        // recolor_vertex: compare-and-swap (newc, version + 1) in; a changed word
-        // re-selects from the live neighbors, as the warp's recolor does
-        bool moved = false;
-        for (uint32_t tries = 0;; tries++) {
-            if (newc == color_of(cur)) break;
-            if (threadIdx.x == 0) word[0] = atomicCAS(g.st + x, cur, pack(newc, (uint16_t)(version_of(cur) + 1)));
-            __syncthreads();
-            const uint32_t got = word[0];
-            __syncthreads();
-            if (got == cur) {
-                moved = true;
-                break;
-            }
-            if (tries >= (1u << 20)) {  // the repair after the batch settles x
-                if (threadIdx.x == 0) atomicOr(g.err, ERR_RETRY);
-                break;
-            }
-            cur = got;
-            newc = block_fac_exact(g, s, e, used, &word[1]);
-        }
-        if (!moved) continue;
-        if (threadIdx.x == 0) {
-            mark_touched(g, x);
-            note_color(g, x);
-        }
-        const uint16_t oldc = color_of(cur);
-        for (uint64_t r = s & ~3ull; r < e; r += 8ull * kHubThreads) {
-            uint32_t y[8];
-            hub_round(g, r, s, e, y);
-#pragma unroll
-            for (int t = 0; t < 8; t++)
-                if (y[t] != INV) nbr_color_change(g, y[t], oldc, newc);
-        }
     }
 }
 
@@ -412,7 +256,6 @@ void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const Ed
     const uint32_t need = (n + 7) / 8;  // 8 warps per block
     if (grid > need) grid = need;
     conc_apply_kernel<<<grid, 256, 0, s>>>(g, ups, n, eo, nullptr);
-    if (g.hub_ops) hub_ops_kernel<<<num_sms, kHubThreads, 0, s>>>(g);
 }
 
 void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* dyn, const EdgeOrder& eo,
@@ -422,7 +265,6 @@ void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* 
     const int occ = conc_apply_occupancy();
     const int bps = (blocks_per_sm > 0 && blocks_per_sm < occ) ? blocks_per_sm : occ;
     conc_apply_kernel<<<num_sms * bps, 256, 0, s>>>(g, ups, 0, eo, dyn);
-    if (g.hub_ops) hub_ops_kernel<<<num_sms, kHubThreads, 0, s>>>(g);
 }
 
 // Stream order per graph, graphs side by side: warp per segment
@@ -794,18 +636,7 @@ __global__ void build_items_kernel(Dev g, SweepBufs b, int list_mode) {
             if (k) atomicOr(g.err, ERR_LIST_OVERFLOW);
             continue;
         }
-        if (k) {
-            const uint64_t rs = g.rp[x];
-            const uint32_t len = row_len(g, x);
-            for (uint32_t j = 0; j < k; j++) {
-                const uint32_t first = j * tile;
-                SweepItem it;
-                it.x = x;
-                it.len = len - first < tile ? len - first : tile;
-                it.s = rs + first;
-                b.items[wbase + off + j] = it;
-            }
-        }
+        for (uint32_t j = 0; j < k; j++) b.items[wbase + off + j] = (unsigned long long)x | ((unsigned long long)j << 32);
     }
 }
 void launch_build_items(const Dev& g, const SweepBufs& b, int list_mode, int num_sms, cudaStream_t s) {
@@ -826,39 +657,20 @@ __device__ __forceinline__ unsigned long long sym_term(uint32_t x, uint32_t y) {
     return pair_hash(x, y) - pair_hash(y, x);
 }
 
-// Item k (one 16-byte load; the list is read-only after the builder).
-__device__ __forceinline__ SweepItem load_item(const SweepBufs& b, uint32_t k) {
-    const uint4 q = __ldg(reinterpret_cast<const uint4*>(b.items + k));
-    SweepItem it;
-    it.x = q.x;
-    it.len = q.y;
-    it.s = ((unsigned long long)q.w << 32) | q.z;
-    return it;
-}
-// The bounds of item `it` in slot space.
-__device__ __forceinline__ void item_bounds(const SweepItem& it, uint32_t& x, uint64_t& s, uint64_t& e) {
-    x = it.x;
-    s = it.s;
-    e = it.s + it.len;
-}
-
-// One round of an item's slots: lane l loads the 16-byte chunks at c + 4l and
-// c + 128 + 4l below e. The slot stream is read once per sweep: the loads are
-// marked evict-first so that L2 keeps the state words the gathers reuse.
-__device__ __forceinline__ void item_round(const Dev& g, uint64_t c, uint64_t e, uint32_t lane, uint4& q0, uint4& q1) {
-    const uint64_t i0 = c + 4ull * lane, i1 = i0 + 128;
-    q0 = make_uint4(INV, INV, INV, INV);
-    q1 = q0;
-    if (i0 < e) q0 = __ldcs(reinterpret_cast<const uint4*>(g.col + i0));
-    if (i1 < e) q1 = __ldcs(reinterpret_cast<const uint4*>(g.col + i1));
+// The bounds of item `it` (row x, chunk j) in slot space.
+__device__ __forceinline__ void item_bounds(const Dev& g, const SweepBufs& b, unsigned long long it, uint32_t& x,
+                                            uint64_t& s, uint64_t& e) {
+    x = (uint32_t)it;
+    const uint32_t j = (uint32_t)(it >> 32);
+    const uint64_t rs = g.rp[x];
+    s = rs + (uint64_t)j * b.tile;
+    const uint64_t re = rs + row_len(g, x);
+    e = s + b.tile < re ? s + b.tile : re;
 }
 
 // Warp per item: up to b.tile live slots of one row. Nothing in the graph
 // changes during a sweep, so loads take the read-only path. Each lane keeps two
-// 16-byte slot loads and their eight state gathers in flight per round, and the
-// dependent chain is short: the descriptor of the warp's next item arrives
-// while this one is swept, an item's slot loads go out with its own state and
-// degree loads, and each round's gathers overlap the next round's slot loads.
+// 16-byte slot loads and their eight state gathers in flight per round.
 // SYM: accumulate the mirror checksum of rows whose graph wants it. PUSH
 // (independent-set rule): a same-colored neighbor that loses to x (lower
 // priority) is marked for the next sweep, which decides it from its own row.
@@ -867,15 +679,10 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
     const uint32_t cnt = *b.item_count;
-    uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    SweepItem it = k < cnt ? load_item(b, k) : SweepItem{0u, 0u, 0ull};
-    while (k < cnt) {
-        // the next item's descriptor is in flight while this item is swept
-        const uint32_t kn = k + warps;
-        const SweepItem nit = kn < cnt ? load_item(b, kn) : SweepItem{0u, 0u, 0ull};
+    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
         uint32_t x;
         uint64_t s, e;
-        item_bounds(it, x, s, e);
+        item_bounds(g, b, b.items[k], x, s, e);
         GraphCtl* gc = SYM ? &g.gctl[graph_of(g, x)] : nullptr;
         const bool symx = SYM && gc->full && ld_cg(&gc->asym);
         const uint32_t myc = color_of(__ldg(g.st + x));
@@ -883,14 +690,12 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
         uint32_t lo = 0, hi = 0;
         unsigned long long sym = 0;
         bool conf = false;
-        uint64_t c = s & ~3ull;
-        uint4 q0, q1;
-        item_round(g, c, e, lane, q0, q1);
-        for (; c < e; c += 256) {
+        for (uint64_t c = s & ~3ull; c < e; c += 256) {
             const uint64_t i0 = c + 4ull * lane, i1 = i0 + 128;
+            uint4 q0 = make_uint4(INV, INV, INV, INV), q1 = q0;
+            if (i0 < e) q0 = __ldg(reinterpret_cast<const uint4*>(g.col + i0));
+            if (i1 < e) q1 = __ldg(reinterpret_cast<const uint4*>(g.col + i1));
             uint32_t v[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-            // the next round's slots are requested before this round's gathers
-            if (c + 256 < e) item_round(g, c + 256, e, lane, q0, q1);
             uint32_t nc[8];
 #pragma unroll
             for (int t = 0; t < 8; t++) {
@@ -924,8 +729,6 @@ __device__ __forceinline__ void sweep_items_body(const Dev& g, const SweepBufs& 
             if (anyc) atomicOr(b.acc_fl + x, 1u);
             if (SYM && sym) atomicAdd(&gc->sym, sym);
         }
-        it = nit;
-        k = kn;
     }
 }
 
@@ -1129,12 +932,12 @@ __global__ void __launch_bounds__(256) indep_items_kernel(Dev g, SweepBufs b) {
     used[lane + 32] = 0;
     __syncwarp();
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
-        const SweepItem it = load_item(b, k);
-        if (!__ldg(b.needf + it.x)) continue;
-        if (ld_cg(b.acc_fl + it.x)) continue;  // another chunk already found it blocked
+        const unsigned long long it = b.items[k];
+        if (!__ldg(b.needf + (uint32_t)it)) continue;
+        if (ld_cg(b.acc_fl + (uint32_t)it)) continue;  // another chunk already found it blocked
         uint32_t x;
         uint64_t s, e;
-        item_bounds(it, x, s, e);
+        item_bounds(g, b, it, x, s, e);
         const uint32_t hd = __ldg(g.hdmap + x);
         const bool full = hd != EMPTY && g.exact && ~b.acc_bm[x] == 0ull;
         const uint32_t base = g.gctl[graph_of(g, x)].base;  // ranks use the graph's own ids
@@ -1284,12 +1087,12 @@ __global__ void __launch_bounds__(256) mark_items_kernel(Dev g, SweepBufs b) {
     const uint32_t cnt = *b.item_count;
     const bool incr = ld_cg(&b.rc->mode) == SWEEP_INDEP;
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += warps) {
-        const SweepItem it = load_item(b, k);
-        const uint32_t x0 = it.x;
+        const unsigned long long it = b.items[k];
+        const uint32_t x0 = (uint32_t)it;
         if (!(b.rbits[x0 >> 5] & (1u << (x0 & 31)))) continue;
         uint32_t x;
         uint64_t s, e;
-        item_bounds(it, x, s, e);
+        item_bounds(g, b, it, x, s, e);
         const uint32_t c = color_of(g.st[x]);
         const unsigned long long bit = (c != 0 && c <= 64) ? 1ull << (c - 1) : 0ull;
         if (incr && !bit) continue;
@@ -1337,16 +1140,18 @@ void launch_next_worklist(const Dev& g, const SweepBufs& b, int num_sms, cudaStr
 }
 
 void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int list_mode, int sym_mode, int num_sms,
-                  cudaStream_t s) {
+                  cudaStream_t s, cudaEvent_t* phase) {
     if (mode != SWEEP_REBUILD) {
         cudaMemsetAsync(b.pend_count, 0, sizeof(uint32_t), s);
         cudaMemsetAsync(b.fac_count, 0, sizeof(uint32_t), s);
         cudaMemsetAsync(b.need_count, 0, sizeof(uint32_t), s);
     }
     sweep_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b, (int)mode, sym_mode);
+    if (phase) cudaEventRecord(phase[0], s);
     uint32_t fblocks = (g.n + 255) / 256;
     if (list_mode != 0 && fblocks > (uint32_t)num_sms * 8) fblocks = num_sms * 8;
     sweep_finalize_kernel<<<fblocks ? fblocks : 1, 256, 0, s>>>(g, b, (int)mode, list_mode, sym_mode);
+    if (phase) cudaEventRecord(phase[1], s);
     if (mode == SWEEP_INDEP) {
         indep_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b);
         indep_decide_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
@@ -1505,9 +1310,11 @@ void launch_repair_begin(const Dev& g, const SweepBufs& b, SweepMode mode, int n
     (void)num_sms;
 }
 
-void launch_repair_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s) {
+void launch_repair_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s,
+                         cudaEvent_t* phase) {
     launch_build_items(g, b, 2, num_sms, s);
-    launch_sweep(g, b, mode, 2, 2, num_sms, s);
+    if (phase) cudaEventRecord(phase[0], s);
+    launch_sweep(g, b, mode, 2, 2, num_sms, s, phase ? phase + 1 : nullptr);
 }
 
 void launch_repair_step(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s,

@@ -34,20 +34,10 @@ struct RepairCtl {
     unsigned long long live;  // first sweep's live entries
 };
 
-// One warp item of a sweep: `len` (at most the tile width) live slots of row
-// x, from slot `s` on. Written by the item builder of each sweep (rows do not
-// change during a sweep), so a warp issues the item's slot loads as soon as
-// the descriptor arrives.
-struct __align__(16) SweepItem {
-    uint32_t x;
-    uint32_t len;
-    unsigned long long s;
-};
-
 // Per-sweep work state: warp items for rows longer than SWEEP_TINY, per-vertex
 // accumulators, the Jacobi pending list and the FAC work list.
 struct SweepBufs {
-    SweepItem* items;
+    unsigned long long* items;   // x | chunk << 32
     uint32_t* item_count;
     uint32_t item_cap;
     uint32_t tile;               // slots per item (repair tile width, >= SWEEP_CH_MIN)
@@ -138,8 +128,10 @@ void launch_build_items(const Dev& g, const SweepBufs& b, int list_mode, int num
 // repaired in full with asym set accumulates its checksum (sum over entries
 // x->y, y != x, y < n, of H(x,y) - H(y,x)) in its GraphCtl. The sweep index
 // (the independent-set order's salt) comes from b.rc.
+// `phase` (optional): events recorded after the long-row items and after the
+// per-vertex finalize.
 void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int list_mode, int sym_mode, int num_sms,
-                  cudaStream_t s);
+                  cudaStream_t s, cudaEvent_t* phase = nullptr);
 // After a sweep: b.wl = the next worklist (reference rule: the vertices the
 // sweep recolored and their neighbors; independent-set rule: the blocked and
 // pushed vertices). Reads the sweep's items: call before the next
@@ -149,7 +141,10 @@ void launch_next_worklist(const Dev& g, const SweepBufs& b, int num_sms, cudaStr
 // launch_repair_sweep + launch_repair_step; b.rc->cont says whether another
 // sweep runs. With `cond`, the step also sets that graph conditional.
 void launch_repair_begin(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s);
-void launch_repair_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s);
+// `phase` (optional): three events, recorded after the item build, the
+// long-row items and the per-vertex finalize.
+void launch_repair_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int num_sms, cudaStream_t s,
+                         cudaEvent_t* phase = nullptr);
 void launch_repair_step(const Dev& g, const SweepBufs& b, int num_sms, cudaStream_t s,
                         const cudaGraphConditionalHandle* cond);
 void launch_query(const uint16_t* snap, uint32_t n, const uint32_t* v, uint16_t* out, uint32_t k, cudaStream_t s);
