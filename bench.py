@@ -172,24 +172,33 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def read_traffic(profile, row):
-    """A per-launch DRAM byte count from a committed ncu summary under
-    profiles/ (its `| row | value |` line), if present."""
+def read_row(profile, row):
+    """A figure from a committed ncu summary under profiles/ (its
+    `| row | value |` line), if present."""
     p = os.path.join(ROOT, "profiles", profile)
     try:
         for line in open(p):
             if line.startswith(f"| {row} |"):
-                return int(float(line.split("|")[2]))
+                return float(line.split("|")[2])
     except (OSError, ValueError):
         pass
     return None
 
 
+def read_traffic(profile, row):
+    """A per-launch DRAM byte count from a committed ncu summary."""
+    v = read_row(profile, row)
+    return int(v) if v is not None else None
+
+
 # The ncu summaries each workload's roofline traffic comes from.
+# per workload: the apply capture, the per-epoch sweep capture, the full-sweep
+# capture (the large workload's are taken on its family at 1/16 scale with the
+# same epoch of 32,768 updates)
 PROFILES = {
-    "skewed": ("apply_skewed_rmat20.md", "sweep_items_skewed_rmat20.md"),
-    "large": ("apply_large_chunglu.md", "sweep_items_large_chunglu.md"),
-    "small": (None, None),
+    "skewed": ("apply_skewed_rmat20.md", "sweep_items_skewed_rmat20.md", None),
+    "large": ("apply_chunglu_div16.md", None, "sweep_full_chunglu_div16.md"),
+    "small": (None, None, None),
 }
 
 
@@ -386,7 +395,7 @@ def run_ours(a):
         sweep_bytes = st1["sweep_bytes"] - st0["sweep_bytes"]
         sweeps = st1["sweep_count"] - st0["sweep_count"]
         achieved = (sweep_bytes / (sweep_ms / 1e3) / 1e9) if sweep_ms > 0 else None
-        apply_prof, sweep_prof = PROFILES[a.workload] if E == 32768 else (None, None)
+        apply_prof, sweep_prof, _ = PROFILES[a.workload] if E == 32768 else (None, None, None)
         traffic = read_traffic(sweep_prof, "sweep_dram_bytes_per_launch") if sweep_prof else None
         apply_traffic = read_traffic(apply_prof, "apply_dram_bytes_per_launch") if apply_prof else None
         apply_avg = sum(apply_ms) / len(apply_ms)
@@ -441,7 +450,7 @@ def run_ours(a):
                                    "the return of the publish that makes it visible (wall clock)"},
             "roofline": roof_apply if roof_apply else roof_sweep,
             "roofline_sweep": roof_sweep,
-            "roofline_full_sweep": full_sweep_roofline(fs0, fs1, full_rep, peak, pk),
+            "roofline_full_sweep": full_sweep_roofline(fs0, fs1, full_rep, peak, pk, PROFILES[a.workload][2]),
             "apply": {"ms_per_epoch": apply_avg, "share_of_step": apply_avg / (total_ms / a.steps),
                       "algorithmic_bytes_per_update": bpu},
             "e2e": {"value": world * a.steps * E / e2e_s, "unit": "updates/s",
@@ -458,10 +467,12 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
-def full_sweep_roofline(s0, s1, rep, peak, peak_kind):
+def full_sweep_roofline(s0, s1, rep, peak, peak_kind, profile=None):
     """The sweep kernels over every vertex (the full repair run after the
     timed steps): algorithmic bytes (8 per live entry + 28 per vertex) over
-    their CUDA-event time."""
+    their CUDA-event time. `traffic`: the DRAM bytes per algorithmic byte of
+    a committed capture of the same sweep, times this sweep's algorithmic
+    bytes."""
     if rep is None:
         return None
     ms = s1["sweep_ms"] - s0["sweep_ms"]
@@ -471,9 +482,13 @@ def full_sweep_roofline(s0, s1, rep, peak, peak_kind):
         return None
     ach = by / (ms / 1e3) / 1e9
     ph = [b - a for a, b in zip(s0.get("sweep_phase_ms", [0] * 4), s1.get("sweep_phase_ms", [0] * 4))]
+    ratio = read_row(profile, "full_sweep_dram_per_algorithmic") if profile else None
     return {"bound": "hbm", "kernel": "tier-1 sweep over every vertex (sweep_items + finalize + fac + commit)",
             "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
             "algorithmic_bytes": by, "sweeps": n, "ms": ms, "proper": rep["proper"],
+            "traffic": int(ratio * by) if ratio else None,
+            "traffic_source": (f"profiles/{profile}: DRAM bytes per algorithmic byte x this sweep's bytes"
+                               if ratio else None),
             "phases_ms": dict(zip(("item_build", "long_row_items", "finalize", "select_commit"), ph))}
 
 
