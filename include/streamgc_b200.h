@@ -119,6 +119,9 @@ typedef struct sgc_stats {
     uint64_t d2h_bytes;          /* bytes the library read back (repair counters, stats) */
     double   sweep_phase_ms[4];  /* SGC_OPT_PROFILE: sweep_ms by phase: item build, long-row items,
                                     per-vertex finalize, color selection and commit */
+    uint64_t hub_deferred;       /* row-scale operations of concurrent batches (color reductions and
+                                    recolors of rows longer than 512 live entries) finished by the
+                                    block-wide pass after the batch (cumulative) */
 } sgc_stats;
 
 typedef struct sgc_validation {

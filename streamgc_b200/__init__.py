@@ -72,7 +72,8 @@ class Stats(C.Structure):
                 ("max_hist_colors", C.c_uint32), ("total_slots", C.c_uint64), ("device_bytes", C.c_uint64),
                 ("sweep_ms", C.c_double), ("sweep_count", C.c_uint64), ("sweep_bytes", C.c_uint64),
                 ("live_entries", C.c_uint64), ("kernel_launches", C.c_uint64), ("h2d_bytes", C.c_uint64),
-                ("d2h_bytes", C.c_uint64), ("sweep_phase_ms", C.c_double * 4)]
+                ("d2h_bytes", C.c_uint64), ("sweep_phase_ms", C.c_double * 4),
+                ("hub_deferred", C.c_uint64)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}

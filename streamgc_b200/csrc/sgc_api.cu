@@ -617,6 +617,12 @@ int sgci::create_internal(const StreamGCConfig* cfg, const sgc_options* opt_in, 
     A(&eo.tsucc, mb);
     eo.ticket = &h->ctl->ticket;
     eo.tmask = tsize - 1;
+    if (g.exact) {  // row-scale operations of concurrent batches: the pass after the batch
+        A(&g.hub_ops, 2ull * mb);
+        g.hub_count = &h->ctl->hub_count;
+        g.hub_cap = 2 * mb;
+        g.hub_total = &h->ctl->hub_total;
+    }
     // sweep buffers
     SweepBufs& sb = h->sb;
     const uint64_t icap = h->total_slots / SWEEP_CH_MIN + (uint64_t)n + 1;
@@ -1175,6 +1181,7 @@ int sgc_get_stats(sgc_handle* h, sgc_stats* o) {
     o->h2d_bytes = h->h2d_bytes;
     o->d2h_bytes = h->d2h_bytes;
     for (int k = 0; k < 4; k++) o->sweep_phase_ms[k] = h->sweep_phase_ms[k];
+    o->hub_deferred = c.hub_total;
     return c.err ? fail(SGC_EDEVICE, "device error word 0x%x", c.err) : SGC_OK;
 }
 

@@ -61,6 +61,21 @@ struct GraphCtl {
     uint32_t dropped; // an entry of this graph was dropped (a full row at drain, or the overflow buffer full)
 };
 
+// A row-scale operation of a concurrent batch left to the pass after it
+// (exact selection): HUB_REDUCE moves x to color `freed` when that is below
+// x's color and no live neighbor of x holds it; HUB_RECOLOR moves x to its
+// first free color. The pass re-reads x's state word.
+enum : uint32_t { HUB_REDUCE = 1u, HUB_RECOLOR = 2u };
+struct HubOp {
+    uint32_t x;
+    uint32_t op;  // kind << 16 | freed
+};
+// Live slots a warp scans itself before it leaves the rest of a row to the
+// pass, and the row length from which it does (shorter rows finish in the
+// warp within a few rounds, sooner than a pass after the batch would).
+constexpr uint32_t kHubScan = 512;
+constexpr uint32_t kHubRow = 8192;
+
 // Device view of one graph's state (handle layout). Row x owns logical slots
 // [rp[x], rp[x+1]); hw[x] bounds the slots ever written since the row was last
 // compacted (every slot at or past rp[x]+hw[x] holds INV), so after compaction
@@ -97,6 +112,10 @@ struct Dev {
                                    // endpoints of an ADD whose colors are equal at the end of its batch
     uint32_t* chg;                 // single-graph handles under exact selection: bitmask of the vertices
                                    // whose color changed since the last snapshot (null otherwise)
+    HubOp* hub_ops;                // concurrent batches under exact selection: row-scale operations left
+    uint32_t* hub_count;           // to the pass after the batch (null: none are deferred); the count
+    uint32_t hub_cap;              // runs past hub_cap when the list is full (those are done in place)
+    unsigned long long* hub_total; // cumulative count of the operations the pass took
     GraphCtl* gctl;                // per graph: repair flags (one entry for a single-graph handle)
     const uint32_t* gidw;          // graph of each 32-vertex word (graphs start at multiples of 32);
                                    // null: one graph
@@ -752,6 +771,32 @@ __device__ __forceinline__ bool warp_color_held(const Dev& g, uint32_t x, uint16
     return warp_gather_each<true, 1>(g.col, s, e, g.n, g.st, [c](uint32_t, uint32_t w) { return color_of(w) == c; });
 }
 
+// Does a live neighbor among the first `lim` live slots of x hold color c?
+// `all`: those slots were the whole row.
+__device__ __forceinline__ bool warp_color_held_first(const Dev& g, uint32_t x, uint16_t c, uint32_t lim, bool& all) {
+    const uint64_t s = g.rp[x], e = live_end(g, x, s);
+    const uint64_t e1 = e - s > lim ? s + lim : e;
+    all = e1 == e;
+    return warp_gather_each<true, 4>(g.col, s, e1, g.n, g.st, [c](uint32_t, uint32_t w) { return color_of(w) == c; });
+}
+
+// Appends a row-scale operation to the pass after the batch (lane 0).
+// Warp-collective; false when nothing is deferred (no list, or it is full):
+// the caller then does the work itself.
+__device__ __forceinline__ bool warp_defer(const Dev& g, uint32_t x, uint32_t kind, uint16_t freed) {
+    if (!g.hub_ops) return false;
+    uint32_t ok = 0;
+    if (lane_id() == 0) {
+        const uint32_t pos = atomicAdd(g.hub_count, 1u);
+        if (pos < g.hub_cap) {
+            g.hub_ops[pos].x = x;
+            g.hub_ops[pos].op = (kind << 16) | freed;
+            ok = 1;
+        }
+    }
+    return __shfl_sync(FULL, ok, 0) != 0;
+}
+
 // Both endpoints' state words in one round trip (lanes 0 and 1).
 __device__ __forceinline__ void warp_load_states2(const Dev& g, uint32_t u, uint32_t v, uint32_t& su, uint32_t& sv) {
     const uint32_t lane = lane_id();
@@ -774,7 +819,17 @@ __device__ __forceinline__ void warp_try_reduce(const Dev& g, uint32_t x, uint16
     if (cur == 0) return;
     if (freed >= cur) return;
     if (!stream_order && g.exact && __ldg(g.hdmap + x) != EMPTY) {
-        if (freed != 0 && !warp_color_held(g, x, freed)) warp_recolor(g, x, freed);
+        if (freed == 0) return;
+        if (g.hub_ops && row_len(g, x) > kHubRow) {
+            // a holder is usually among the first neighbors; a hub row without
+            // one there is finished (scan, move, walk) by the pass after the batch
+            bool all = true;
+            if (warp_color_held_first(g, x, freed, kHubScan, all)) return;
+            if (warp_defer(g, x, HUB_REDUCE, freed) || warp_color_held(g, x, freed)) return;
+        } else if (warp_color_held(g, x, freed)) {
+            return;
+        }
+        warp_recolor(g, x, freed);
         return;
     }
     const uint16_t best = warp_fac(g, x, g.st);
@@ -856,7 +911,11 @@ __device__ __forceinline__ void warp_apply(const Dev& g, uint32_t u, uint32_t v,
         const uint16_t cu = color_of(su), cv = color_of(sv);
         if (cu == cv && cu != 0) {
             const uint32_t loser = prio_less(__ldg(g.deg + u), u, __ldg(g.deg + v), v) ? u : v;
-            warp_recolor(g, loser);
+            // concurrent batches: a long histogram-class row's selection and
+            // walk go to the pass after the batch
+            const bool defer = !exact && g.hub_ops && __ldg(g.hdmap + loser) != EMPTY &&
+                               row_len(g, loser) > kHubRow && warp_defer(g, loser, HUB_RECOLOR, 0);
+            if (!defer) warp_recolor(g, loser);
         }
     } else if (type == SGC_UPDATE_DEL) {
         uint32_t su, sv;

@@ -36,12 +36,15 @@ struct Ctl {
     uint32_t pend_count;
     uint32_t fac_count;
     uint32_t ticket;
+    uint32_t hub_count;  // row-scale operations deferred by the last concurrent batch
+    uint32_t hub_pad;
     unsigned long long ovf_lost;
     unsigned long long nskip;
     unsigned long long drain_failed;
     unsigned long long symsum;
     unsigned long long live;
-    unsigned long long pad[3];
+    unsigned long long hub_total;  // cumulative: operations the pass after concurrent batches finished
+    unsigned long long pad[2];
 };
 
 }  // namespace sgci

@@ -94,7 +94,10 @@ __device__ __forceinline__ uint32_t batch_n(uint32_t n, const uint32_t* dyn) { r
 __global__ void conc_prep_insert(Dev g, const EdgeUpdate* __restrict__ ups, uint32_t n_arg, EdgeOrder eo,
                                  const uint32_t* dyn) {
     const uint32_t n = batch_n(n_arg, dyn);
-    if (blockIdx.x == 0 && threadIdx.x == 0) *eo.ticket = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *eo.ticket = 0;
+        if (g.hub_count) *g.hub_count = 0;
+    }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint4 r = ld_cg4(reinterpret_cast<const uint32_t*>(ups + i));
         const uint32_t u = r.x, v = r.y;
@@ -191,6 +194,159 @@ __global__ void __launch_bounds__(256, 3) conc_apply_kernel(Dev g, const EdgeUpd
     }
 }
 
+// ---------------------------------------------------------------------------
+// The pass after a concurrent batch: row-scale operations the apply left
+// (HubOp), one block of kHubThreads per operation. Each re-reads x's state
+// word; the scans and the neighbor walk after a move take 8192 slots per
+// round over the whole block. Decisions are made on words thread 0 read and
+// shared, so every branch is block-uniform.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kHubThreads = 1024;
+
+// The ids of one round's slots: thread t loads the 16-byte chunks at
+// c + 4t and c + 4t + 4096 (INV outside [s, e) and for ids >= n).
+__device__ __forceinline__ void hub_round(const Dev& g, uint64_t c, uint64_t s, uint64_t e, uint32_t (&y)[8]) {
+    const uint64_t i0 = c + 4ull * threadIdx.x, i1 = i0 + 4ull * kHubThreads;
+    uint4 q0 = make_uint4(INV, INV, INV, INV), q1 = q0;
+    if (i0 < e) q0 = ld_cg4(g.col + i0);
+    if (i1 < e) q1 = ld_cg4(g.col + i1);
+    const uint32_t v[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+        const uint64_t p = (t < 4 ? i0 : i1) + (t & 3);
+        y[t] = (p >= s && p < e && v[t] < g.n) ? v[t] : INV;
+    }
+}
+
+// Does a live neighbor in [s, e) hold color c? Stops after the first round that finds one.
+__device__ __forceinline__ bool block_color_held(const Dev& g, uint64_t s, uint64_t e, uint16_t c) {
+    for (uint64_t r = s & ~3ull; r < e; r += 8ull * kHubThreads) {
+        uint32_t y[8];
+        hub_round(g, r, s, e, y);
+        uint32_t w[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) w[t] = y[t] != INV ? ld_cg(g.st + y[t]) : 0u;
+        bool hit = false;
+#pragma unroll
+        for (int t = 0; t < 8; t++) hit |= y[t] != INV && color_of(w[t]) == c;
+        if (__syncthreads_or(hit)) return true;
+    }
+    return false;
+}
+
+// Exact selection: the first color no live neighbor in [s, e) holds (colors
+// 1..2047, else 2048), as warp_fac_exact. `used`: 64 words of shared memory.
+__device__ __forceinline__ uint16_t block_fac_exact(const Dev& g, uint64_t s, uint64_t e, uint32_t* used,
+                                                    uint32_t* pick) {
+    if (threadIdx.x < 64) used[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t lo = 0, hi = 0;  // colors 1..64 (bits 0..63 of a 64-bit mask)
+    for (uint64_t r = s & ~3ull; r < e; r += 8ull * kHubThreads) {
+        uint32_t y[8];
+        hub_round(g, r, s, e, y);
+        uint32_t w[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) w[t] = y[t] != INV ? ld_cg(g.st + y[t]) : 0u;
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+            if (y[t] == INV) continue;
+            const uint16_t c = color_of(w[t]);
+            add_color_bit(c, lo, hi);
+            if (c > 64 && c < 2048) atomicOr(&used[c >> 5], 1u << (c & 31));
+        }
+    }
+    lo = __reduce_or_sync(FULL, lo);
+    hi = __reduce_or_sync(FULL, hi);
+    if (lane_id() == 0) {  // fold colors 1..64 into the same set (color c: word c >> 5, bit c & 31)
+        if (lo) atomicOr(&used[0], lo << 1);
+        if (lo >> 31) atomicOr(&used[1], 1u);
+        if (hi) atomicOr(&used[1], hi << 1);
+        if (hi >> 31) atomicOr(&used[2], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const uint32_t l = threadIdx.x;
+        uint32_t w0 = ~used[l], w1 = ~used[l + 32];
+        if (l == 0) w0 &= ~1u;  // color 0 is never a candidate
+        const uint32_t b0 = __ballot_sync(FULL, w0 != 0), b1 = __ballot_sync(FULL, w1 != 0);
+        if (l == 0) {
+            uint32_t c = 2048;
+            if (b0) {
+                const int src = __ffs(b0) - 1;
+                c = src * 32 + __ffs(~used[src] & (src == 0 ? ~1u : FULL)) - 1;
+            } else if (b1) {
+                const int src = __ffs(b1) - 1;
+                c = 1024 + src * 32 + __ffs(~used[src + 32]) - 1;
+            }
+            *pick = c;
+        }
+    }
+    __syncthreads();
+    const uint16_t c = (uint16_t)*pick;
+    __syncthreads();
+    return c;
+}
+
+__global__ void __launch_bounds__(kHubThreads) hub_ops_kernel(Dev g) {
+    __shared__ uint32_t used[64];
+    __shared__ uint32_t word[2];
+    const uint32_t total = ld_cg(g.hub_count);
+    const uint32_t cnt = total < g.hub_cap ? total : g.hub_cap;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && cnt) atomicAdd(g.hub_total, (unsigned long long)cnt);
+    for (uint32_t k = blockIdx.x; k < cnt; k += gridDim.x) {
+        const HubOp op = g.hub_ops[k];
+        const uint32_t x = op.x;
+        if (x >= g.n) continue;  // block-uniform: every thread read the same record
+        const uint32_t kind = op.op >> 16;
+        const uint16_t freed = (uint16_t)(op.op & 0xFFFFu);
+        const uint64_t s = g.rp[x], e = live_end(g, x, s);
+        if (threadIdx.x == 0) word[0] = ld_cg(g.st + x);
+        __syncthreads();
+        uint32_t cur = word[0];
+        __syncthreads();
+        uint16_t newc;
+        if (kind == HUB_REDUCE) {
+            if (freed == 0 || freed >= color_of(cur) || block_color_held(g, s, e, freed)) continue;
+            newc = freed;
+        } else {
+            newc = block_fac_exact(g, s, e, used, &word[1]);
+        }
+        // recolor_vertex: compare-and-swap (newc, version + 1) in; a changed word
+        // re-selects from the live neighbors, as the warp's recolor does
+        bool moved = false;
+        for (uint32_t tries = 0;; tries++) {
+            if (newc == color_of(cur)) break;
+            if (threadIdx.x == 0) word[0] = atomicCAS(g.st + x, cur, pack(newc, (uint16_t)(version_of(cur) + 1)));
+            __syncthreads();
+            const uint32_t got = word[0];
+            __syncthreads();
+            if (got == cur) {
+                moved = true;
+                break;
+            }
+            if (tries >= 1024u) {  // the repair after the batch settles x
+                if (threadIdx.x == 0) atomicOr(g.err, ERR_RETRY);
+                break;
+            }
+            cur = got;
+            newc = block_fac_exact(g, s, e, used, &word[1]);
+        }
+        if (!moved) continue;
+        if (threadIdx.x == 0) {
+            mark_touched(g, x);
+            note_color(g, x);
+        }
+        const uint16_t oldc = color_of(cur);
+        for (uint64_t r = s & ~3ull; r < e; r += 8ull * kHubThreads) {
+            uint32_t y[8];
+            hub_round(g, r, s, e, y);
+#pragma unroll
+            for (int t = 0; t < 8; t++)
+                if (y[t] != INV) nbr_color_change(g, y[t], oldc, newc);
+        }
+    }
+}
+
 // After a batch (exact selection): both endpoints of every ADD whose colors
 // are equal are marked for the next repair. Together with the marks of every
 // color change, this makes every conflict of the rows have a marked endpoint
@@ -256,6 +412,7 @@ void launch_conc_apply(const Dev& g, const EdgeUpdate* ups, uint32_t n, const Ed
     const uint32_t need = (n + 7) / 8;  // 8 warps per block
     if (grid > need) grid = need;
     conc_apply_kernel<<<grid, 256, 0, s>>>(g, ups, n, eo, nullptr);
+    if (g.hub_ops) hub_ops_kernel<<<num_sms, kHubThreads, 0, s>>>(g);
 }
 
 void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* dyn, const EdgeOrder& eo,
@@ -265,6 +422,7 @@ void launch_conc_apply_dyn(const Dev& g, const EdgeUpdate* ups, const uint32_t* 
     const int occ = conc_apply_occupancy();
     const int bps = (blocks_per_sm > 0 && blocks_per_sm < occ) ? blocks_per_sm : occ;
     conc_apply_kernel<<<num_sms * bps, 256, 0, s>>>(g, ups, 0, eo, dyn);
+    if (g.hub_ops) hub_ops_kernel<<<num_sms, kHubThreads, 0, s>>>(g);
 }
 
 // Stream order per graph, graphs side by side: warp per segment
@@ -738,7 +896,7 @@ __device__ __forceinline__ bool want_sym(const SweepBufs& b, int sym_mode) {
     return sym_mode == 2 && ld_cg(&b.rc->it) == 0 && ld_cg(&b.rc->any_sym) != 0;
 }
 
-__global__ void __launch_bounds__(256) sweep_items_kernel(Dev g, SweepBufs b, int mode, int sym_mode) {
+__global__ void __launch_bounds__(256, 5) sweep_items_kernel(Dev g, SweepBufs b, int mode, int sym_mode) {
     const bool sym = want_sym(b, sym_mode);
     const bool push = mode == SWEEP_INDEP;
     if (push) {
@@ -884,7 +1042,7 @@ __device__ __forceinline__ void finalize_one(const Dev& g, const SweepBufs& b, i
 }
 
 // Thread per vertex (every vertex, or the worklist).
-__global__ void __launch_bounds__(256) sweep_finalize_kernel(Dev g, SweepBufs b, int mode, int list_mode,
+__global__ void __launch_bounds__(256, 3) sweep_finalize_kernel(Dev g, SweepBufs b, int mode, int list_mode,
                                                              int sym_mode) {
     const bool list = use_list(b, list_mode);
     const uint32_t lim = list ? *b.wl_count : g.n;
@@ -921,7 +1079,7 @@ __global__ void __launch_bounds__(256) sweep_fac_kernel(Dev g, SweepBufs b) {
 // chunk ranks above it; for a histogram-class row whose neighbors take every
 // color 1..64 (acc_bm, from the sweep) it also gathers the taken colors 65..2047
 // into the row's words of b.hiused. Colors are the start-of-sweep ones.
-__global__ void __launch_bounds__(256) indep_items_kernel(Dev g, SweepBufs b) {
+__global__ void __launch_bounds__(256, 5) indep_items_kernel(Dev g, SweepBufs b) {
     __shared__ uint32_t s_used[8][64];
     uint32_t* used = s_used[threadIdx.x >> 5];
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -1146,14 +1304,14 @@ void launch_sweep(const Dev& g, const SweepBufs& b, SweepMode mode, int list_mod
         cudaMemsetAsync(b.fac_count, 0, sizeof(uint32_t), s);
         cudaMemsetAsync(b.need_count, 0, sizeof(uint32_t), s);
     }
-    sweep_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b, (int)mode, sym_mode);
+    sweep_items_kernel<<<num_sms * 5, 256, 0, s>>>(g, b, (int)mode, sym_mode);  // one wave: 5 blocks per SM
     if (phase) cudaEventRecord(phase[0], s);
     uint32_t fblocks = (g.n + 255) / 256;
-    if (list_mode != 0 && fblocks > (uint32_t)num_sms * 8) fblocks = num_sms * 8;
+    if (list_mode != 0 && fblocks > (uint32_t)num_sms * 3) fblocks = num_sms * 3;  // one wave: 3 blocks per SM
     sweep_finalize_kernel<<<fblocks ? fblocks : 1, 256, 0, s>>>(g, b, (int)mode, list_mode, sym_mode);
     if (phase) cudaEventRecord(phase[1], s);
     if (mode == SWEEP_INDEP) {
-        indep_items_kernel<<<num_sms * 8, 256, 0, s>>>(g, b);
+        indep_items_kernel<<<num_sms * 5, 256, 0, s>>>(g, b);
         indep_decide_kernel<<<num_sms * 2, 256, 0, s>>>(g, b);
     }
     if (mode != SWEEP_REBUILD) {
